@@ -1,0 +1,250 @@
+/*
+ * mirorr_b200.h -- C ABI of the B200-native Mirorr block-matching registration path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, status codes.  No C++
+ * exceptions, no torch types.  Every entry point returns mirorr_status; the
+ * message of the last failure on the calling thread is mirorr_last_error().
+ *
+ * Layout conventions (those of itk::Image<float,3> / itk::Image<unsigned char,3>):
+ *   volumes are x-fastest, size = {nx, ny, nz}; voxel (x, y, z) sits at
+ *   data[(z * ny + y) * nx + x].  Images are float32, masks uint8 (0 = outside).
+ *   Physical point of index i: origin + direction * diag(spacing) * i,
+ *   direction row-major.
+ *
+ * Threading: a mirorr_ctx and the objects made from it are used from one host
+ * thread at a time (the reference's matcher is likewise driven from the
+ * single registration thread).  Work is issued on the context's CUDA stream.
+ */
+#ifndef MIRORR_B200_H
+#define MIRORR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MIRORR_ABI_VERSION 1
+
+#if defined(MIRORR_BUILD)
+#define MIRORR_API __attribute__((visibility("default")))
+#else
+#define MIRORR_API
+#endif
+
+typedef enum mirorr_status {
+  MIRORR_OK = 0,
+  MIRORR_EINVAL = 1,     /* bad argument (the reference throws std::out_of_range / runtime_error) */
+  MIRORR_ENOMEM = 2,     /* device or host allocation failed */
+  MIRORR_ENOBLOCKS = 3,  /* no block matches ("Images probably have zero overlap",
+                            itkBlockMatcher.txx:936-943, itkBlockMatcherGPU.txx:505-511) */
+  MIRORR_ECUDA = 4,      /* CUDA runtime / launch error, or no usable B200 */
+  MIRORR_ETIMEOUT = 5,   /* a bounded device-side wait gave up */
+  MIRORR_ESTATE = 6,     /* call out of order (e.g. GetOffsets before images are set) */
+  MIRORR_ERANGE = 7      /* output buffer too small; *_needed reports the size */
+} mirorr_status;
+
+typedef struct mirorr_ctx_s *mirorr_ctx;
+typedef struct mirorr_matcher_s *mirorr_matcher;
+
+/* Geometry of a volume (itk::ImageBase: size, spacing, origin, direction). */
+typedef struct mirorr_geometry {
+  int32_t size[3];
+  double spacing[3];
+  double origin[3];
+  double direction[9]; /* row-major 3x3 */
+} mirorr_geometry;
+
+/* Block-matcher parameters: itkAbstractBlockMatcher.h:231-245 (members),
+ * defaults itkAbstractBlockMatcher.txx:25-44. */
+typedef struct mirorr_bm_params {
+  uint32_t block_width;        /* m_BlockWidth: block side in voxels (default 4) */
+  uint32_t block_gap;          /* m_BlockGap: candidate stride in voxels (default 1) */
+  uint32_t nhood_gap;          /* m_NhoodGap: spacing of the block grid (default 2) */
+  uint32_t nhood_width;        /* m_NhoodWidth: candidates per axis, 2R+1 (default 5) */
+  double portion_matches_kept; /* m_PortionMatchesKept: 0 -> 0.5, outside [0,1] -> EINVAL
+                                  (itkAbstractBlockMatcher.txx:84-100) */
+  double block_keep;           /* fraction of blocks kept by base-block variance (the
+                                  reference's variance cut-off, itkBlockMatcher.txx:664-719,
+                                  which is compiled out there); >= 1 keeps every block */
+  int32_t verbosity;           /* m_Verbosity */
+} mirorr_bm_params;
+
+/* ---- context ------------------------------------------------------------ */
+MIRORR_API mirorr_status mirorr_ctx_create(int32_t device, mirorr_ctx *out);
+MIRORR_API mirorr_status mirorr_ctx_destroy(mirorr_ctx ctx);
+/* Message of the last failed call on this host thread ("" if none). */
+MIRORR_API const char *mirorr_last_error(void);
+MIRORR_API int32_t mirorr_abi_version(void);
+
+/* ---- block matcher: replaces itk::AbstractBlockMatcher<ImageType> --------
+ * (src/mirorr/itkAbstractBlockMatcher.h:41-313; GPU implementation being
+ * replaced: itkBlockMatcherGPU.h/.txx). */
+MIRORR_API mirorr_status mirorr_bm_create(mirorr_ctx ctx, mirorr_matcher *out);
+MIRORR_API mirorr_status mirorr_bm_destroy(mirorr_matcher m);
+/* AbstractBlockMatcher constructor defaults (itkAbstractBlockMatcher.txx:25-44). */
+MIRORR_API mirorr_status mirorr_bm_default_params(mirorr_bm_params *p);
+/* SetBlockWidth/SetBlockGap/SetNhoodGap/SetNhoodWidth/SetPortionMatchesKept/
+ * SetVerbosity (itkAbstractBlockMatcher.h:101-127). */
+MIRORR_API mirorr_status mirorr_bm_set_params(mirorr_matcher m, const mirorr_bm_params *p);
+/* SetBlockMetricType (itkAbstractBlockMatcher.h:159-163): only "nc" /
+ * "normalized_correlation" exists on this path; others -> EINVAL. */
+MIRORR_API mirorr_status mirorr_bm_set_metric(mirorr_matcher m, const char *name);
+/* SetBaseImage / SetSearchImage (itkAbstractBlockMatcher.txx:45-73): copies
+ * host data to device memory owned by the matcher. */
+MIRORR_API mirorr_status mirorr_bm_set_base_image(mirorr_matcher m, const mirorr_geometry *g,
+                                       const float *host);
+MIRORR_API mirorr_status mirorr_bm_set_search_image(mirorr_matcher m, const mirorr_geometry *g,
+                                         const float *host);
+/* SetBaseMask / SetSearchMask (itkAbstractBlockMatcher.h:87-95); host == NULL
+ * restores the default all-255 mask (BeforeGetOffsets, itkBlockMatcher.txx:507-529). */
+MIRORR_API mirorr_status mirorr_bm_set_base_mask(mirorr_matcher m, const uint8_t *host);
+MIRORR_API mirorr_status mirorr_bm_set_search_mask(mirorr_matcher m, const uint8_t *host);
+/* Device-resident variants: the matcher reads caller-owned device memory
+ * (no copy); the buffers must stay valid until the next set call. */
+MIRORR_API mirorr_status mirorr_bm_set_base_image_device(mirorr_matcher m, const mirorr_geometry *g,
+                                              const float *dev);
+MIRORR_API mirorr_status mirorr_bm_set_search_image_device(mirorr_matcher m, const mirorr_geometry *g,
+                                                const float *dev);
+MIRORR_API mirorr_status mirorr_bm_set_base_mask_device(mirorr_matcher m, const uint8_t *dev);
+MIRORR_API mirorr_status mirorr_bm_set_search_mask_device(mirorr_matcher m, const uint8_t *dev);
+/* SwapImageOrder (itkAbstractBlockMatcher.txx:101-112; the GPU matcher keeps
+ * its device buffers, itkBlockMatcherGPU.txx:186-202). */
+MIRORR_API mirorr_status mirorr_bm_swap_image_order(mirorr_matcher m);
+/* Number of blocks of the current grid (ComputeRegionForMatching,
+ * itkBlockMatcher.txx:531-600). */
+MIRORR_API mirorr_status mirorr_bm_grid(mirorr_matcher m, int32_t nblocks[3], int32_t start[3]);
+/* GetOffsets (itkAbstractBlockMatcher.h:139-146): fills block_positions and
+ * match_positions (n x 3 doubles each, mm, blockPositionToPoint convention of
+ * itkAbstractBlockMatcher.h:271-287) with the blocks that pass the post-filter,
+ * in block-grid raster order.  *n_out receives the count.  If capacity is
+ * too small returns ERANGE with *n_out = required count.  Zero kept blocks
+ * -> ENOBLOCKS (the GPU matcher's BlockMatcherGPUExceptionAlgo). */
+MIRORR_API mirorr_status mirorr_bm_get_offsets(mirorr_matcher m, size_t capacity, double *block_positions,
+                                    double *match_positions, size_t *n_out);
+/* Per-block results of the last GetOffsets, grid raster order, for every
+ * block of the grid: match origin voxel index (x,y,z), best and second-best
+ * squared NCC, status (0 = culled by the variance selection, 1 = searched,
+ * 3 = searched and kept by the post-filter). */
+MIRORR_API mirorr_status mirorr_bm_block_results(mirorr_matcher m, size_t capacity, int32_t *match_index,
+                                      float *best, float *second, uint8_t *status,
+                                      size_t *n_blocks);
+
+/* ---- resampler: itk::ResampleImageFilter + LinearInterpolateImageFunction
+ * as wired in itkMirorrRegistrationMethod.txx:523-570,603-604 and
+ * itkSymMirorrRegistrationMethod.txx:388-437,481-484.  The output voxel
+ * index maps to the input continuous index through c = e + C * idx
+ * (C row-major 3x3); outside -0.5 <= c < n - 0.5 the output is 0.  Either
+ * image or mask may be NULL.  Host pointers. */
+MIRORR_API mirorr_status mirorr_resample(mirorr_ctx ctx, const int32_t in_size[3], const float *in_image,
+                              const uint8_t *in_mask, const int32_t out_size[3],
+                              const double C[9], const double e[3], float *out_image,
+                              uint8_t *out_mask);
+/* Affine index map of the resampler from geometries and a transform
+ * y = M x + offset (output grid -> input continuous index). */
+MIRORR_API mirorr_status mirorr_resample_map(const mirorr_geometry *out_grid, const mirorr_geometry *in_grid,
+                                  const double M[9], const double offset[3], double C[9],
+                                  double e[3]);
+
+/* ---- transforms and the LTS fit -------------------------------------------
+ * ITK MatrixOffsetTransformBase state: y = matrix * (x - center) + center +
+ * translation = matrix * x + offset.  kind: 0 = Euler3DTransform (rigid,
+ * params: angles x,y,z (Z*X*Y) + translation), 1 = AffineTransform (params:
+ * matrix row-major + translation). */
+typedef struct mirorr_transform {
+  int32_t kind;
+  double matrix[9];
+  double offset[3];
+  double center[3];
+  double params[12];
+} mirorr_transform;
+
+/* Classic OptimizeTransform (itkMirorrRegistrationMethod.txx:758-1003):
+ * least-trimmed-squares fit of moved ~ T(initial) over n point pairs (mm),
+ * composed into *t (m_Transform->Compose(final, true)).  lts_keep replaces the
+ * hard-coded 0.5.  *inner_iterations receives the LTS iteration count. */
+MIRORR_API mirorr_status mirorr_lts_classic(mirorr_ctx ctx, mirorr_transform *t, size_t n,
+                                 const double *initial, const double *moved, double lts_keep,
+                                 int32_t *inner_iterations);
+/* Symmetric OptimizeTransform(t12F, t12B) (itkSymMirorrRegistrationMethod.txx:729-1442):
+ * updates the half-space transforms t12f, t12b and the full transform t. */
+MIRORR_API mirorr_status mirorr_lts_symmetric(mirorr_ctx ctx, mirorr_transform *t, mirorr_transform *t12f,
+                                   mirorr_transform *t12b, size_t n, const double *initial,
+                                   const double *moved, double lts_keep,
+                                   int32_t *inner_iterations);
+
+/* ---- registration: MirorrPyramidImplement::RunMirorr over the finest
+ * `levels` pyramid levels (itkMirorrPyramidImplement.txx:71-158), classic
+ * (itkMirorrRegistrationMethod.txx:422-659) or symmetric
+ * (itkSymMirorrRegistrationMethod.txx:238-720) iterations.  Reference CLI
+ * equivalents: --reg-mode, -t rigid|affine, --pyr-num L --pyr-end 0, -n,
+ * --blockwidth, --blockgap, --nhoodgap, --nhoodwidth, --pyr-min-size. */
+typedef struct mirorr_reg_params {
+  int32_t symmetric;      /* 0 classic, 1 symmetric (reference default) */
+  int32_t kind;           /* 0 rigid (Euler3D), 1 affine */
+  int32_t levels;         /* finest pyramid levels to run (0 = all) */
+  int32_t iterations;     /* block-matching iterations per level (-n; 0 -> 5) */
+  int32_t min_length;     /* --pyr-min-size (default 32) */
+  mirorr_bm_params bm;    /* CLI defaults: width 4, gap 1, nhood gap 3, nhood width 7 */
+  double lts_keep;        /* LTS keep fraction (reference: 0.5) */
+  int32_t verbosity;
+} mirorr_reg_params;
+
+typedef struct mirorr_reg_stats {
+  int32_t levels_run;
+  int32_t iterations_run[16];
+  int64_t block_ncc_evaluated; /* candidate scores computed (all levels, all calls) */
+  int64_t matcher_calls;
+  double seconds;              /* host wall time of the call */
+} mirorr_reg_stats;
+
+MIRORR_API mirorr_status mirorr_reg_default_params(mirorr_reg_params *p);
+/* Full registration from host buffers (the e2e path: uploads inside).  Masks
+ * may be NULL (all 255).  init may be NULL: centred initialisation
+ * (CenteredTransformInitializer GeometryOn, itkMirorrPyramidWrapper.txx:611-623).
+ * The result maps moving-image physical points to fixed-image points. */
+MIRORR_API mirorr_status mirorr_register(mirorr_ctx ctx, const mirorr_geometry *fixed_geom,
+                              const float *fixed, const uint8_t *fixed_mask,
+                              const mirorr_geometry *moving_geom, const float *moving,
+                              const uint8_t *moving_mask, const mirorr_reg_params *p,
+                              const mirorr_transform *init, mirorr_transform *result,
+                              mirorr_reg_stats *stats);
+/* Same with device-resident inputs (caller-owned device pointers). */
+MIRORR_API mirorr_status mirorr_register_device(mirorr_ctx ctx, const mirorr_geometry *fixed_geom,
+                                     const float *fixed, const uint8_t *fixed_mask,
+                                     const mirorr_geometry *moving_geom, const float *moving,
+                                     const uint8_t *moving_mask, const mirorr_reg_params *p,
+                                     const mirorr_transform *init, mirorr_transform *result,
+                                     mirorr_reg_stats *stats);
+
+/* Pyramid schedule (PyramidScheduleTuner::UpdateSymmetric,
+ * itkPyramidScheduleTuner.txx:291-414): per level (coarsest first) the
+ * shrink factors of the moving and fixed images. */
+MIRORR_API mirorr_status mirorr_pyramid_schedule(const mirorr_geometry *fixed_geom,
+                                      const mirorr_geometry *moving_geom, int32_t min_length,
+                                      int32_t max_levels, int32_t *n_levels,
+                                      int32_t moving_factors[16][3],
+                                      int32_t fixed_factors[16][3]);
+/* One pyramid level of a host volume: separable Gaussian (sigma = f/2 voxels,
+ * radius ceil(3 sigma), clamp-to-edge, x then y then z) followed by
+ * decimation onto the ITK pyramid grid (spacing * f, size floor(n / f),
+ * origin shifted by direction * (spacing_out - spacing_in) / 2) with the
+ * linear resampler.  out_geom receives the level geometry. */
+MIRORR_API mirorr_status mirorr_pyramid_level(mirorr_ctx ctx, const mirorr_geometry *in_geom,
+                                   const float *in_image, const int32_t factors[3],
+                                   mirorr_geometry *out_geom, float *out_image,
+                                   size_t out_capacity);
+
+/* Timing of the kernels of the last matcher call (CUDA events on the
+ * context stream), milliseconds: [0] box statistics, [1] variance selection,
+ * [2] NCC search, [3] post-filter + compaction. */
+MIRORR_API mirorr_status mirorr_bm_last_timings(mirorr_matcher m, float ms[4]);
+/* Count of kernels launched by this context since creation. */
+MIRORR_API int64_t mirorr_ctx_kernel_launches(mirorr_ctx ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MIRORR_B200_H */

@@ -1,0 +1,468 @@
+"""mirorr_b200 -- B200-native block-matching registration (Mirorr's hot path).
+
+Python binding of the C ABI in include/mirorr_b200.h (libmirorr_b200.so,
+built in tree by mirorr_b200/build.py).  The classes mirror the reference's
+interfaces:
+
+* BlockMatcher   -- itk::AbstractBlockMatcher (src/mirorr/itkAbstractBlockMatcher.h):
+  SetBaseImage / SetSearchImage / SetBaseMask / SetSearchMask / parameter
+  setters / SwapImageOrder / GetOffsets.
+* register()     -- MirorrPyramidImplement::RunMirorr with the classic or
+  symmetric method (the `mirorr` CLI's --reg-mode, -t, -n, --pyr-*, block
+  options).
+* resample(), lts_classic(), lts_symmetric() -- the resampler and
+  OptimizeTransform stages on their own.
+
+There is no CPU fallback: without the CUDA library or a B200 every call raises
+MirorrError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmirorr_b200.so")
+
+STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ENOBLOCKS", 4: "ECUDA", 5: "ETIMEOUT",
+          6: "ESTATE", 7: "ERANGE"}
+RIGID, AFFINE = 0, 1
+
+
+class MirorrError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_int32 * 3), ("spacing", ctypes.c_double * 3),
+                ("origin", ctypes.c_double * 3), ("direction", ctypes.c_double * 9)]
+
+    @staticmethod
+    def make(size_xyz, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0), direction=None):
+        g = Geometry()
+        g.size[:] = [int(v) for v in size_xyz]
+        g.spacing[:] = [float(v) for v in spacing]
+        g.origin[:] = [float(v) for v in origin]
+        d = np.eye(3) if direction is None else np.asarray(direction, np.float64)
+        g.direction[:] = [float(v) for v in d.reshape(-1)]
+        return g
+
+    @staticmethod
+    def of(data: np.ndarray, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0), direction=None):
+        nz, ny, nx = data.shape
+        return Geometry.make((nx, ny, nz), spacing, origin, direction)
+
+    def as_dict(self):
+        return dict(size=tuple(self.size), spacing=tuple(self.spacing), origin=tuple(self.origin),
+                    direction=np.array(self.direction).reshape(3, 3))
+
+
+class BMParams(ctypes.Structure):
+    _fields_ = [("block_width", ctypes.c_uint32), ("block_gap", ctypes.c_uint32),
+                ("nhood_gap", ctypes.c_uint32), ("nhood_width", ctypes.c_uint32),
+                ("portion_matches_kept", ctypes.c_double), ("block_keep", ctypes.c_double),
+                ("verbosity", ctypes.c_int32)]
+
+
+class Transform(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("matrix", ctypes.c_double * 9),
+                ("offset", ctypes.c_double * 3), ("center", ctypes.c_double * 3),
+                ("params", ctypes.c_double * 12)]
+
+    @staticmethod
+    def make(kind, params, center=(0.0, 0.0, 0.0)):
+        t = Transform()
+        t.kind = int(kind)
+        p = list(params) + [0.0] * (12 - len(params))
+        t.params[:] = [float(v) for v in p]
+        t.center[:] = [float(v) for v in center]
+        return t
+
+    @property
+    def M(self):
+        return np.array(self.matrix).reshape(3, 3)
+
+    @property
+    def off(self):
+        return np.array(self.offset)
+
+    def param_vector(self):
+        n = 6 if self.kind == RIGID else 12
+        return np.array(self.params[:n])
+
+
+class RegParams(ctypes.Structure):
+    _fields_ = [("symmetric", ctypes.c_int32), ("kind", ctypes.c_int32), ("levels", ctypes.c_int32),
+                ("iterations", ctypes.c_int32), ("min_length", ctypes.c_int32), ("bm", BMParams),
+                ("lts_keep", ctypes.c_double), ("verbosity", ctypes.c_int32)]
+
+
+class RegStats(ctypes.Structure):
+    _fields_ = [("levels_run", ctypes.c_int32), ("iterations_run", ctypes.c_int32 * 16),
+                ("block_ncc_evaluated", ctypes.c_int64), ("matcher_calls", ctypes.c_int64),
+                ("seconds", ctypes.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libmirorr_b200.so; raises MirorrError when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise MirorrError(4, f"CUDA library not built: {LIB_PATH} (run mirorr_b200/build.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    st = ctypes.c_int
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    sigs = {
+        "mirorr_ctx_create": [ctypes.c_int32, P(vp)],
+        "mirorr_ctx_destroy": [vp],
+        "mirorr_bm_create": [vp, P(vp)],
+        "mirorr_bm_destroy": [vp],
+        "mirorr_bm_default_params": [P(BMParams)],
+        "mirorr_bm_set_params": [vp, P(BMParams)],
+        "mirorr_bm_set_metric": [vp, ctypes.c_char_p],
+        "mirorr_bm_set_base_image": [vp, P(Geometry), vp],
+        "mirorr_bm_set_search_image": [vp, P(Geometry), vp],
+        "mirorr_bm_set_base_mask": [vp, vp],
+        "mirorr_bm_set_search_mask": [vp, vp],
+        "mirorr_bm_set_base_image_device": [vp, P(Geometry), vp],
+        "mirorr_bm_set_search_image_device": [vp, P(Geometry), vp],
+        "mirorr_bm_set_base_mask_device": [vp, vp],
+        "mirorr_bm_set_search_mask_device": [vp, vp],
+        "mirorr_bm_swap_image_order": [vp],
+        "mirorr_bm_grid": [vp, vp, vp],
+        "mirorr_bm_get_offsets": [vp, ctypes.c_size_t, vp, vp, P(ctypes.c_size_t)],
+        "mirorr_bm_block_results": [vp, ctypes.c_size_t, vp, vp, vp, vp, P(ctypes.c_size_t)],
+        "mirorr_bm_last_timings": [vp, vp],
+        "mirorr_resample": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
+        "mirorr_resample_map": [P(Geometry), P(Geometry), vp, vp, vp, vp],
+        "mirorr_lts_classic": [vp, P(Transform), ctypes.c_size_t, vp, vp, ctypes.c_double,
+                               P(ctypes.c_int32)],
+        "mirorr_lts_symmetric": [vp, P(Transform), P(Transform), P(Transform), ctypes.c_size_t,
+                                 vp, vp, ctypes.c_double, P(ctypes.c_int32)],
+        "mirorr_reg_default_params": [P(RegParams)],
+        "mirorr_register": [vp, P(Geometry), vp, vp, P(Geometry), vp, vp, P(RegParams),
+                            P(Transform), P(Transform), P(RegStats)],
+        "mirorr_register_device": [vp, P(Geometry), vp, vp, P(Geometry), vp, vp, P(RegParams),
+                                   P(Transform), P(Transform), P(RegStats)],
+        "mirorr_pyramid_schedule": [P(Geometry), P(Geometry), ctypes.c_int32, ctypes.c_int32,
+                                    P(ctypes.c_int32), vp, vp],
+        "mirorr_pyramid_level": [vp, P(Geometry), vp, vp, P(Geometry), vp, ctypes.c_size_t],
+    }
+    for name, args in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = st
+    L.mirorr_last_error.restype = ctypes.c_char_p
+    L.mirorr_last_error.argtypes = []
+    L.mirorr_abi_version.restype = ctypes.c_int32
+    L.mirorr_ctx_kernel_launches.restype = ctypes.c_int64
+    L.mirorr_ctx_kernel_launches.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _check(status):
+    if status != 0:
+        msg = lib().mirorr_last_error().decode(errors="replace")
+        raise MirorrError(status, msg)
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _u8(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.uint8)
+
+
+class Context:
+    """A CUDA device + stream + scratch memory (mirorr_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        _check(lib().mirorr_ctx_create(int(device), ctypes.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def kernel_launches(self) -> int:
+        return int(lib().mirorr_ctx_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            lib().mirorr_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BlockMatcher:
+    """Drop-in for itk::AbstractBlockMatcher (GPU implementation)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self._h = ctypes.c_void_p()
+        _check(lib().mirorr_bm_create(ctx.handle, ctypes.byref(self._h)))
+        self._p = BMParams()
+        _check(lib().mirorr_bm_default_params(ctypes.byref(self._p)))
+        self._keep = []  # host arrays referenced by device-pointer setters
+
+    # parameters (itkAbstractBlockMatcher.h:101-127)
+    def _apply(self):
+        _check(lib().mirorr_bm_set_params(self._h, ctypes.byref(self._p)))
+
+    def SetBlockWidth(self, v):
+        self._p.block_width = int(v); self._apply()
+
+    def SetBlockGap(self, v):
+        self._p.block_gap = int(v); self._apply()
+
+    def SetNhoodGap(self, v):
+        self._p.nhood_gap = int(v); self._apply()
+
+    def SetNhoodWidth(self, v):
+        self._p.nhood_width = int(v); self._apply()
+
+    def SetPortionMatchesKept(self, v):
+        old = self._p.portion_matches_kept
+        self._p.portion_matches_kept = float(v)
+        try:
+            self._apply()
+        except MirorrError:
+            self._p.portion_matches_kept = old
+            raise
+
+    def SetBlockKeep(self, v):
+        self._p.block_keep = float(v); self._apply()
+
+    def SetVerbosity(self, v):
+        self._p.verbosity = int(v); self._apply()
+
+    def SetBlockMetricType(self, name: str):
+        _check(lib().mirorr_bm_set_metric(self._h, name.encode()))
+
+    def GetBlockWidth(self):
+        return self._p.block_width
+
+    def GetNhoodGap(self):
+        return self._p.nhood_gap
+
+    def GetPortionMatchesKept(self):
+        return self._p.portion_matches_kept
+
+    # images
+    def SetBaseImage(self, data, spacing=(1, 1, 1), origin=(0, 0, 0), direction=None):
+        d = _f32(data)
+        _check(lib().mirorr_bm_set_base_image(self._h, ctypes.byref(Geometry.of(d, spacing, origin, direction)), _ptr(d)))
+
+    def SetSearchImage(self, data, spacing=(1, 1, 1), origin=(0, 0, 0), direction=None):
+        d = _f32(data)
+        _check(lib().mirorr_bm_set_search_image(self._h, ctypes.byref(Geometry.of(d, spacing, origin, direction)), _ptr(d)))
+
+    def SetBaseMask(self, mask):
+        _check(lib().mirorr_bm_set_base_mask(self._h, _ptr(_u8(mask))))
+
+    def SetSearchMask(self, mask):
+        _check(lib().mirorr_bm_set_search_mask(self._h, _ptr(_u8(mask))))
+
+    def SetBaseImageDevice(self, geom: Geometry, dev_ptr: int):
+        _check(lib().mirorr_bm_set_base_image_device(self._h, ctypes.byref(geom), ctypes.c_void_p(dev_ptr)))
+
+    def SetSearchImageDevice(self, geom: Geometry, dev_ptr: int):
+        _check(lib().mirorr_bm_set_search_image_device(self._h, ctypes.byref(geom), ctypes.c_void_p(dev_ptr)))
+
+    def SetBaseMaskDevice(self, dev_ptr):
+        _check(lib().mirorr_bm_set_base_mask_device(self._h, ctypes.c_void_p(dev_ptr) if dev_ptr else None))
+
+    def SetSearchMaskDevice(self, dev_ptr):
+        _check(lib().mirorr_bm_set_search_mask_device(self._h, ctypes.c_void_p(dev_ptr) if dev_ptr else None))
+
+    def SwapImageOrder(self):
+        _check(lib().mirorr_bm_swap_image_order(self._h))
+
+    def Grid(self):
+        nb = (ctypes.c_int32 * 3)()
+        st = (ctypes.c_int32 * 3)()
+        _check(lib().mirorr_bm_grid(self._h, nb, st))
+        return tuple(nb), tuple(st)
+
+    def GetOffsets(self):
+        """Returns (block_positions, match_positions): (n, 3) float64 arrays in mm."""
+        nb, _ = self.Grid()
+        cap = nb[0] * nb[1] * nb[2]
+        bp = np.zeros((cap, 3), np.float64)
+        mp = np.zeros((cap, 3), np.float64)
+        n = ctypes.c_size_t(0)
+        _check(lib().mirorr_bm_get_offsets(self._h, cap, _ptr(bp), _ptr(mp), ctypes.byref(n)))
+        return bp[:n.value], mp[:n.value]
+
+    def BlockResults(self):
+        """Per-block (match_index (N,3), best, second, status) of the last GetOffsets."""
+        nb, _ = self.Grid()
+        cap = nb[0] * nb[1] * nb[2]
+        mi = np.zeros((cap, 3), np.int32)
+        best = np.zeros(cap, np.float32)
+        second = np.zeros(cap, np.float32)
+        status = np.zeros(cap, np.uint8)
+        n = ctypes.c_size_t(0)
+        _check(lib().mirorr_bm_block_results(self._h, cap, _ptr(mi), _ptr(best), _ptr(second),
+                                             _ptr(status), ctypes.byref(n)))
+        k = n.value
+        return mi[:k], best[:k], second[:k], status[:k]
+
+    def LastTimings(self):
+        ms = np.zeros(4, np.float32)
+        _check(lib().mirorr_bm_last_timings(self._h, _ptr(ms)))
+        return ms
+
+    def close(self):
+        if self._h:
+            lib().mirorr_bm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def resample_map(out_geom: Geometry, in_geom: Geometry, M, offset):
+    C = np.zeros(9, np.float64)
+    e = np.zeros(3, np.float64)
+    Mm = np.ascontiguousarray(np.asarray(M, np.float64).reshape(-1))
+    o = np.ascontiguousarray(np.asarray(offset, np.float64))
+    _check(lib().mirorr_resample_map(ctypes.byref(out_geom), ctypes.byref(in_geom), _ptr(Mm),
+                                     _ptr(o), _ptr(C), _ptr(e)))
+    return C.reshape(3, 3), e
+
+
+def resample(ctx: Context, image, mask, out_size_xyz, C, e):
+    """Linear resampling of image (float32) and/or mask (uint8) on an index map."""
+    ref = image if image is not None else mask
+    in_size = (ctypes.c_int32 * 3)(ref.shape[2], ref.shape[1], ref.shape[0])
+    out_size = (ctypes.c_int32 * 3)(*[int(v) for v in out_size_xyz])
+    shape = (int(out_size_xyz[2]), int(out_size_xyz[1]), int(out_size_xyz[0]))
+    img = _f32(image) if image is not None else None
+    msk = _u8(mask)
+    out = np.zeros(shape, np.float32) if img is not None else None
+    outm = np.zeros(shape, np.uint8) if msk is not None else None
+    Cc = np.ascontiguousarray(np.asarray(C, np.float64).reshape(-1))
+    ec = np.ascontiguousarray(np.asarray(e, np.float64))
+    _check(lib().mirorr_resample(ctx.handle, in_size, _ptr(img), _ptr(msk), out_size, _ptr(Cc),
+                                 _ptr(ec), _ptr(out), _ptr(outm)))
+    return out, outm
+
+
+def lts_classic(ctx: Context, t: Transform, init, moved, lts_keep=0.5):
+    init = np.ascontiguousarray(init, np.float64)
+    moved = np.ascontiguousarray(moved, np.float64)
+    it = ctypes.c_int32(0)
+    _check(lib().mirorr_lts_classic(ctx.handle, ctypes.byref(t), init.shape[0], _ptr(init),
+                                    _ptr(moved), float(lts_keep), ctypes.byref(it)))
+    return it.value
+
+
+def lts_symmetric(ctx: Context, t: Transform, t12f: Transform, t12b: Transform, init, moved,
+                  lts_keep=0.5):
+    init = np.ascontiguousarray(init, np.float64)
+    moved = np.ascontiguousarray(moved, np.float64)
+    it = ctypes.c_int32(0)
+    _check(lib().mirorr_lts_symmetric(ctx.handle, ctypes.byref(t), ctypes.byref(t12f),
+                                      ctypes.byref(t12b), init.shape[0], _ptr(init), _ptr(moved),
+                                      float(lts_keep), ctypes.byref(it)))
+    return it.value
+
+
+def reg_params(symmetric=True, kind="rigid", levels=0, iterations=5, block_width=4, block_gap=1,
+               nhood_gap=3, nhood_width=7, block_keep=1.0, lts_keep=0.5, min_length=32,
+               verbosity=0) -> RegParams:
+    p = RegParams()
+    _check(lib().mirorr_reg_default_params(ctypes.byref(p)))
+    p.symmetric = 1 if symmetric else 0
+    p.kind = RIGID if kind == "rigid" else AFFINE
+    p.levels = int(levels)
+    p.iterations = int(iterations)
+    p.min_length = int(min_length)
+    p.bm.block_width = int(block_width)
+    p.bm.block_gap = int(block_gap)
+    p.bm.nhood_gap = int(nhood_gap)
+    p.bm.nhood_width = int(nhood_width)
+    p.bm.block_keep = float(block_keep)
+    p.lts_keep = float(lts_keep)
+    p.verbosity = int(verbosity)
+    return p
+
+
+def register(ctx: Context, fixed, moving, params: RegParams, fixed_geom: Geometry | None = None,
+             moving_geom: Geometry | None = None, fixed_mask=None, moving_mask=None,
+             init: Transform | None = None):
+    """Full registration from host arrays.  Returns (Transform, RegStats)."""
+    f = _f32(fixed)
+    m = _f32(moving)
+    fg = fixed_geom or Geometry.of(f)
+    mg = moving_geom or Geometry.of(m)
+    res = Transform()
+    st = RegStats()
+    _check(lib().mirorr_register(ctx.handle, ctypes.byref(fg), _ptr(f), _ptr(_u8(fixed_mask)),
+                                 ctypes.byref(mg), _ptr(m), _ptr(_u8(moving_mask)),
+                                 ctypes.byref(params), ctypes.byref(init) if init else None,
+                                 ctypes.byref(res), ctypes.byref(st)))
+    return res, st
+
+
+def register_device(ctx: Context, fixed_ptr: int, fixed_geom: Geometry, moving_ptr: int,
+                    moving_geom: Geometry, params: RegParams, fixed_mask_ptr=None,
+                    moving_mask_ptr=None, init: Transform | None = None):
+    res = Transform()
+    st = RegStats()
+    _check(lib().mirorr_register_device(
+        ctx.handle, ctypes.byref(fixed_geom), ctypes.c_void_p(fixed_ptr),
+        ctypes.c_void_p(fixed_mask_ptr) if fixed_mask_ptr else None, ctypes.byref(moving_geom),
+        ctypes.c_void_p(moving_ptr), ctypes.c_void_p(moving_mask_ptr) if moving_mask_ptr else None,
+        ctypes.byref(params), ctypes.byref(init) if init else None, ctypes.byref(res),
+        ctypes.byref(st)))
+    return res, st
+
+
+def pyramid_schedule(fixed_geom: Geometry, moving_geom: Geometry, min_length=32, max_levels=0):
+    n = ctypes.c_int32(0)
+    mf = np.zeros((16, 3), np.int32)
+    ff = np.zeros((16, 3), np.int32)
+    _check(lib().mirorr_pyramid_schedule(ctypes.byref(fixed_geom), ctypes.byref(moving_geom),
+                                         int(min_length), int(max_levels), ctypes.byref(n),
+                                         _ptr(mf), _ptr(ff)))
+    return mf[:n.value].copy(), ff[:n.value].copy()
+
+
+def pyramid_level(ctx: Context, image, factors, geom: Geometry | None = None):
+    img = _f32(image)
+    g = geom or Geometry.of(img)
+    og = Geometry()
+    cap = int(np.prod([max(1, s // f) for s, f in zip(tuple(g.size), factors)]))
+    out = np.zeros(cap, np.float32)
+    fac = (ctypes.c_int32 * 3)(*[int(v) for v in factors])
+    _check(lib().mirorr_pyramid_level(ctx.handle, ctypes.byref(g), _ptr(img), fac, ctypes.byref(og),
+                                      _ptr(out), cap))
+    nx, ny, nz = tuple(og.size)
+    return out[: nx * ny * nz].reshape(nz, ny, nx), og

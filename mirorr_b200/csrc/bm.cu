@@ -1,0 +1,649 @@
+// bm.cu -- block-matching kernels for sm_100a (plain FP32 path).
+//
+// One matcher call (AbstractBlockMatcher::GetOffsets) runs:
+//   1. box_stats:   per candidate origin p of the search image, the block mean
+//                   mu(p) (over all BW^3 voxels, unmasked, as
+//                   itkBlockMatcher.txx:57-68) and the masked sum of squares
+//                   Syy(p) = sum_{ms != 0} (y - mu)^2, both in FP64 in the
+//                   reference's raster order, stored as float2.
+//   2. selection:   (optional) dead-code variance cut-off of
+//                   itkBlockMatcher.txx:664-719, FP64 per block, exact k-th
+//                   value by a device radix select.
+//   3. ncc:         one CTA per block: base-block statistics in FP64, the
+//                   clipped +-R window staged in shared memory, every
+//                   candidate's squared NCC in FP32, best / second-best /
+//                   argmax with the reference's raster-order tie rule
+//                   (itkBlockMatcher.txx:788-834).
+//   4. postfilter:  best > 1e-7 && |best - second| > 1e-4 (itkBlockMatcher.txx:884-918),
+//                   deterministic raster-order compaction and block -> mm points
+//                   (itkAbstractBlockMatcher.h:271-287).
+#include "kernels.cuh"
+
+namespace mb2 {
+
+bool bm_geometry(const int size[3], int bw, int bgap, int ngap, int nw, BmGeom &g) {
+  if (bw <= 0 || bgap <= 0 || ngap <= 0 || nw <= 0) return false;
+  g.nblocks = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (size[d] < bw) return false;
+    g.size[d] = size[d];
+    int n = (size[d] - bw) / ngap + 1;
+    int region = ngap * (n - 1) + bw;
+    g.nb[d] = n;
+    g.st[d] = (size[d] - region) / 2;
+    g.nblocks *= n;
+  }
+  g.bw = bw;
+  g.bgap = bgap;
+  g.ngap = ngap;
+  g.nw = nw;
+  return true;
+}
+
+void point_geom(const double origin[3], const double spacing[3], const double direction[9],
+                int bw, PointGeom &pg) {
+  for (int r = 0; r < 3; ++r) {
+    pg.origin[r] = origin[r];
+    for (int c = 0; c < 3; ++c) pg.a[3 * r + c] = direction[3 * r + c] * spacing[c];
+    pg.half[r] = spacing[r] * (0.5 * (double)bw);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 1. box statistics
+// ---------------------------------------------------------------------------
+template <int BW>
+__global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict__ y,
+                                                        const uint8_t *__restrict__ ms, int nx,
+                                                        int ny, int nz, float2 *__restrict__ out) {
+  long long n = (long long)nx * ny * nz;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(p % nx);
+    int yy = (int)((p / nx) % ny);
+    int z = (int)(p / ((long long)nx * ny));
+    if (x > nx - BW || yy > ny - BW || z > nz - BW) {
+      out[p] = make_float2(0.f, 0.f);
+      continue;
+    }
+    double sum = 0.0;
+#pragma unroll
+    for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+      for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+        for (int vx = 0; vx < BW; ++vx)
+          sum = __dadd_rn(sum, (double)__ldg(&y[p + ((long long)vz * ny + vy) * nx + vx]));
+    double mean = __ddiv_rn(sum, (double)(BW * BW * BW));
+    double ss = 0.0;
+#pragma unroll
+    for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+      for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+        for (int vx = 0; vx < BW; ++vx) {
+          long long q = p + ((long long)vz * ny + vy) * nx + vx;
+          if (__ldg(&ms[q])) {
+            double d = __dsub_rn((double)__ldg(&y[q]), mean);
+            ss = __dadd_rn(ss, __dmul_rn(d, d));
+          }
+        }
+    out[p] = make_float2((float)mean, (float)ss);
+  }
+}
+
+mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8_t *smask,
+                               float2 *stats, cudaStream_t s) {
+  long long n = (long long)g.size[0] * g.size[1] * g.size[2];
+  int threads = 256;
+  long long blocks = (n + threads - 1) / threads;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  switch (g.bw) {
+#define CASE(B) \
+  case B: box_stats_kernel<B><<<(unsigned)blocks, threads, 0, s>>>(search, smask, g.size[0], g.size[1], g.size[2], stats); break;
+    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+#undef CASE
+    default:
+      set_error("block width %d not supported (1..8)", g.bw);
+      return MIRORR_EINVAL;
+  }
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// 2. variance selection
+// ---------------------------------------------------------------------------
+__device__ inline unsigned long long order_key(double v) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  return (u & 0x8000000000000000ULL) ? ~u : (u | 0x8000000000000000ULL);
+}
+
+__global__ void block_variance_kernel(const float *__restrict__ img, int nx, int ny, int nbx,
+                                      int nby, int nbz, int stx, int sty, int stz, int G, int bw,
+                                      double *__restrict__ var, unsigned long long *__restrict__ key) {
+  long long nb = (long long)nbx * nby * nbz;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
+       b += (long long)gridDim.x * blockDim.x) {
+    int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((long long)nbx * nby));
+    long long o = ((long long)(stz + bz * G) * ny + (sty + by * G)) * nx + (stx + bx * G);
+    double cnt = 0.0, sum = 0.0, ssq = 0.0;
+    for (int z = 0; z < bw; ++z)
+      for (int y = 0; y < bw; ++y)
+        for (int x = 0; x < bw; ++x) {
+          float v = __ldg(&img[o + ((long long)z * ny + y) * nx + x]);
+          cnt = __dadd_rn(cnt, 1.0);
+          sum = __dadd_rn(sum, (double)v);
+          float sq = __fmul_rn(v, v);  // float * float in the reference
+          ssq = __dadd_rn(ssq, (double)sq);
+        }
+    double mean = __ddiv_rn(sum, cnt);
+    double v = __dsub_rn(__ddiv_rn(ssq, cnt), __dmul_rn(mean, mean));
+    var[b] = v;
+    key[b] = order_key(v);
+  }
+}
+
+// Radix select control block (device memory).
+struct SelectCtl {
+  unsigned long long prefix;
+  unsigned long long mask;
+  unsigned long long k;      // rank still to find within the prefix bucket
+  unsigned long long n;
+};
+
+__global__ void select_hist_kernel(const unsigned long long *__restrict__ key, long long n,
+                                   const SelectCtl *__restrict__ ctl, int shift,
+                                   unsigned int *__restrict__ hist) {
+  __shared__ unsigned int h[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  unsigned long long prefix = ctl->prefix, mask = ctl->mask;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long k = key[i];
+    if ((k & mask) == prefix) atomicAdd(&h[(k >> shift) & 0xFF], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+__global__ void select_scan_kernel(SelectCtl *ctl, int shift, unsigned int *hist) {
+  __shared__ unsigned int h[256];
+  int t = threadIdx.x;
+  h[t] = hist[t];
+  __syncthreads();
+  if (t == 0) {
+    unsigned long long k = ctl->k, cum = 0;
+    int d = 0;
+    for (; d < 256; ++d) {
+      if (cum + h[d] > k) break;
+      cum += h[d];
+    }
+    if (d == 256) d = 255;  // cannot happen for k < count
+    ctl->k = k - cum;
+    ctl->prefix |= ((unsigned long long)d) << shift;
+    ctl->mask |= 0xFFULL << shift;
+  }
+  __syncthreads();
+  hist[t] = 0;
+}
+
+__global__ void select_flags_kernel(const double *__restrict__ var, long long n,
+                                    const SelectCtl *__restrict__ ctl,
+                                    uint8_t *__restrict__ selected) {
+  unsigned long long p = ctl->prefix;
+  unsigned long long u = (p & 0x8000000000000000ULL) ? (p & 0x7FFFFFFFFFFFFFFFULL) : ~p;
+  double cutoff = __longlong_as_double((long long)u);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    selected[i] = var[i] > cutoff ? 1 : 0;
+}
+
+mirorr_status launch_variance_selection(const BmGeom &g, const float *base, double keep,
+                                        BmWork &w, const uint8_t **selected_out,
+                                        cudaStream_t s) {
+  *selected_out = nullptr;
+  if (!(keep < 1.0)) return MIRORR_OK;
+  long long n = g.nblocks;
+  MB2_TRY(w.var.ensure(sizeof(double) * n + sizeof(unsigned long long) * n));
+  MB2_TRY(w.selected.ensure(n));
+  MB2_TRY(w.select_state.ensure(sizeof(SelectCtl)));
+  MB2_TRY(w.hist.ensure(256 * sizeof(unsigned int)));
+  double *var = w.var.as<double>();
+  unsigned long long *key = reinterpret_cast<unsigned long long *>(var + n);
+  int threads = 256;
+  long long blocks = (n + threads - 1) / threads;
+  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
+      base, g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2], g.st[0], g.st[1], g.st[2], g.ngap,
+      g.bw, var, key);
+  MB2_LAUNCH_CHECK();
+  // cut-off index (unsigned)((1 - keep) * N); index >= N -> the maximum
+  unsigned long long idx = (unsigned long long)(unsigned int)((1.0 - keep) * (double)n);
+  if (idx >= (unsigned long long)n) idx = n - 1;
+  SelectCtl c0{0ULL, 0ULL, idx, (unsigned long long)n};
+  MB2_CUDA_TRY(cudaMemcpyAsync(w.select_state.ptr, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
+  MB2_CUDA_TRY(cudaMemsetAsync(w.hist.ptr, 0, 256 * sizeof(unsigned int), s));
+  SelectCtl *ctl = w.select_state.as<SelectCtl>();
+  for (int pass = 0; pass < 8; ++pass) {
+    int shift = 56 - 8 * pass;
+    select_hist_kernel<<<(unsigned)blocks, threads, 0, s>>>(key, n, ctl, shift,
+                                                            w.hist.as<unsigned int>());
+    MB2_LAUNCH_CHECK();
+    select_scan_kernel<<<1, 256, 0, s>>>(ctl, shift, w.hist.as<unsigned int>());
+    MB2_LAUNCH_CHECK();
+  }
+  select_flags_kernel<<<(unsigned)blocks, threads, 0, s>>>(var, n, ctl, w.selected.as<uint8_t>());
+  MB2_LAUNCH_CHECK();
+  *selected_out = w.selected.as<uint8_t>();
+  return MIRORR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// 3. NCC search
+// ---------------------------------------------------------------------------
+struct NccArgs {
+  const float *base;
+  const uint8_t *bmask;
+  const float *search;
+  const uint8_t *smask;
+  const float2 *stats;
+  const uint8_t *selected;
+  int nx, ny, nz;
+  int nbx, nby, nbz;
+  int stx, sty, stz;
+  int G, g, W;
+  int emax;  // max window extent per axis
+  float *best;
+  float *second;
+  int32_t *match;
+  uint8_t *status;
+  unsigned long long *ncc_count;
+};
+
+struct Top2 {
+  float best;
+  float second;
+  int idx;
+};
+
+__device__ inline Top2 merge_top2(Top2 a, Top2 b) {
+  bool bw = (b.best > a.best) || (b.best == a.best && b.idx < a.idx);
+  Top2 w = bw ? b : a, l = bw ? a : b;
+  Top2 r;
+  r.best = w.best;
+  r.idx = w.idx;
+  float s = w.second;
+  if (l.best > s) s = l.best;
+  if (l.second > s) s = l.second;
+  r.second = s;
+  return r;
+}
+
+__device__ inline void window_axis(int o, int S, int W, int g, int bw, int &s, int &n) {
+  int st = o - (W / 2) * g;
+  int en = st + W * g;
+  int lim = S - bw + 1;
+  if (st < 0) st += ((-st + g - 1) / g) * g;
+  if (en > lim) en -= ((en - lim + g - 1) / g) * g;
+  s = st;
+  n = (en > st) ? (en - st + g - 1) / g : 0;
+}
+
+template <int BW>
+__global__ void __launch_bounds__(128) ncc_kernel(NccArgs a) {
+  constexpr int B = BW * BW * BW;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *xt = reinterpret_cast<float *>(smem);                 // B
+  float *ywin = xt + B;                                          // emax^3
+  uint8_t *mbv = reinterpret_cast<uint8_t *>(ywin + a.emax * a.emax * a.emax);  // B
+  uint8_t *mwin = mbv + B;                                       // emax^3
+  __shared__ double s_mean;
+  __shared__ float s_sxx, s_sxt;
+  __shared__ int s_mball;
+  __shared__ Top2 s_red[4];
+
+  const long long b = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int bx = (int)(b % a.nbx), by = (int)((b / a.nbx) % a.nby),
+            bz = (int)(b / ((long long)a.nbx * a.nby));
+  const int ox = a.stx + bx * a.G, oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
+  const long long obase = ((long long)oz * a.ny + oy) * a.nx + ox;
+
+  if (a.selected && !a.selected[b]) {
+    if (tid == 0) {
+      a.best[b] = -3.f;
+      a.second[b] = -3.f;
+      a.match[b] = (int32_t)obase;
+      a.status[b] = 0;
+    }
+    return;
+  }
+  int sx, sy, sz, cx_n, cy_n, cz_n;
+  window_axis(ox, a.nx, a.W, a.g, BW, sx, cx_n);
+  window_axis(oy, a.ny, a.W, a.g, BW, sy, cy_n);
+  window_axis(oz, a.nz, a.W, a.g, BW, sz, cz_n);
+  const int ex = (cx_n - 1) * a.g + BW, ey = (cy_n - 1) * a.g + BW, ez = (cz_n - 1) * a.g + BW;
+  if (cx_n <= 0 || cy_n <= 0 || cz_n <= 0) {
+    if (tid == 0) {
+      a.best[b] = -3.f;
+      a.second[b] = -3.f;
+      a.match[b] = (int32_t)obase;
+      a.status[b] = 1;
+    }
+    return;
+  }
+
+  // base block
+  for (int v = tid; v < B; v += blockDim.x) {
+    int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+    long long q = obase + ((long long)vz * a.ny + vy) * a.nx + vx;
+    xt[v] = __ldg(&a.base[q]);
+    mbv[v] = __ldg(&a.bmask[q]);
+  }
+  // search window
+  const long long wbase = ((long long)sz * a.ny + sy) * a.nx + sx;
+  const int nwin = ex * ey * ez;
+  int all_in = 1;
+  for (int i = tid; i < nwin; i += blockDim.x) {
+    int wx = i % ex, wy = (i / ex) % ey, wz = i / (ex * ey);
+    long long q = wbase + ((long long)wz * a.ny + wy) * a.nx + wx;
+    ywin[i] = __ldg(&a.search[q]);
+    uint8_t m = __ldg(&a.smask[q]);
+    mwin[i] = m;
+    if (!m) all_in = 0;
+  }
+  int ms_all = __syncthreads_and(all_in);
+  if (tid == 0) {
+    // meanBase / baseSumSqr of normalizedCorrelation, FP64 in raster order
+    double sum = 0.0;
+    int mball = 1;
+    for (int v = 0; v < B; ++v) {
+      sum = __dadd_rn(sum, (double)xt[v]);
+      if (!mbv[v]) mball = 0;
+    }
+    double mean = __ddiv_rn(sum, (double)B);
+    double sxx = 0.0, sxt = 0.0;
+    for (int v = 0; v < B; ++v) {
+      if (mbv[v]) {
+        double d = __dsub_rn((double)xt[v], mean);
+        sxx = __dadd_rn(sxx, __dmul_rn(d, d));
+        sxt = __dadd_rn(sxt, d);
+      }
+    }
+    s_mean = mean;
+    s_sxx = (float)sxx;
+    s_sxt = (float)sxt;
+    s_mball = mball;
+  }
+  __syncthreads();
+  {
+    const double mean = s_mean;
+    for (int v = tid; v < B; v += blockDim.x) xt[v] = (float)__dsub_rn((double)xt[v], mean);
+  }
+  __syncthreads();
+  const bool fast = s_mball && ms_all;
+  const float sxx_f = s_sxx, sxt_f = s_sxt;
+
+  Top2 loc{-3.f, -3.f, 0x7fffffff};
+  const int nc = cx_n * cy_n * cz_n;
+  for (int c = tid; c < nc; c += blockDim.x) {
+    int cx = c % cx_n, cy = (c / cx_n) % cy_n, cz = c / (cx_n * cy_n);
+    int px = sx + cx * a.g, py = sy + cy * a.g, pz = sz + cz * a.g;
+    float2 st = __ldg(&a.stats[((long long)pz * a.ny + py) * a.nx + px]);
+    const float mu = st.x;
+    const int woff = ((cz * a.g) * ey + cy * a.g) * ex + cx * a.g;
+    float sxy = 0.f, sxx, syy;
+    if (fast) {
+      float acc = 0.f;
+#pragma unroll
+      for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+        for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+          for (int vx = 0; vx < BW; ++vx)
+            acc = fmaf(xt[(vz * BW + vy) * BW + vx], ywin[woff + (vz * ey + vy) * ex + vx], acc);
+      sxy = acc - mu * sxt_f;
+      sxx = sxx_f;
+      syy = st.y;
+    } else {
+      float ax = 0.f, ay = 0.f;
+#pragma unroll
+      for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+        for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+          for (int vx = 0; vx < BW; ++vx) {
+            int v = (vz * BW + vy) * BW + vx;
+            int wi = woff + (vz * ey + vy) * ex + vx;
+            if (mbv[v] && mwin[wi]) {
+              float xv = xt[v];
+              float d = ywin[wi] - mu;
+              sxy = fmaf(xv, d, sxy);
+              ax = fmaf(xv, xv, ax);
+              ay = fmaf(d, d, ay);
+            }
+          }
+      sxx = ax;
+      syy = s_mball ? st.y : ay;
+      if (!s_mball) syy = ay;
+    }
+    float score = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
+    if (score > loc.best) {
+      loc.second = loc.best;
+      loc.best = score;
+      loc.idx = c;
+    } else if (score > loc.second) {
+      loc.second = score;
+    }
+  }
+  // reduce top-2 across the CTA
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    Top2 o;
+    o.best = __shfl_down_sync(0xffffffffu, loc.best, off);
+    o.second = __shfl_down_sync(0xffffffffu, loc.second, off);
+    o.idx = __shfl_down_sync(0xffffffffu, loc.idx, off);
+    loc = merge_top2(loc, o);
+  }
+  if ((tid & 31) == 0) s_red[tid >> 5] = loc;
+  __syncthreads();
+  if (tid == 0) {
+    Top2 r = s_red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = merge_top2(r, s_red[w]);
+    int c = r.idx;
+    if (c == 0x7fffffff) c = 0;
+    int cx = c % cx_n, cy = (c / cx_n) % cy_n, cz = c / (cx_n * cy_n);
+    int px = sx + cx * a.g, py = sy + cy * a.g, pz = sz + cz * a.g;
+    a.best[b] = r.best;
+    a.second[b] = r.second;
+    a.match[b] = (int32_t)(((long long)pz * a.ny + py) * a.nx + px);
+    a.status[b] = 1;
+    if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)nc);
+  }
+}
+
+mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmask,
+                         const float *search, const uint8_t *smask, const float2 *stats,
+                         const uint8_t *selected, const BmOut &out,
+                         unsigned long long *ncc_count, cudaStream_t s) {
+  NccArgs a;
+  a.base = base; a.bmask = bmask; a.search = search; a.smask = smask; a.stats = stats;
+  a.selected = selected;
+  a.nx = g.size[0]; a.ny = g.size[1]; a.nz = g.size[2];
+  a.nbx = g.nb[0]; a.nby = g.nb[1]; a.nbz = g.nb[2];
+  a.stx = g.st[0]; a.sty = g.st[1]; a.stz = g.st[2];
+  a.G = g.ngap; a.g = g.bgap; a.W = g.nw;
+  a.emax = (g.nw - 1) * g.bgap + g.bw;
+  a.best = out.best; a.second = out.second; a.match = out.match; a.status = out.status;
+  a.ncc_count = ncc_count;
+  int B = g.bw * g.bw * g.bw;
+  size_t smem = sizeof(float) * (B + (size_t)a.emax * a.emax * a.emax) + B +
+                (size_t)a.emax * a.emax * a.emax;
+  if (smem > 200 * 1024) {
+    set_error("search window too large: (nhood_width-1)*block_gap+block_width = %d", a.emax);
+    return MIRORR_EINVAL;
+  }
+  if (g.nblocks > 0x7fffffffLL) {
+    set_error("too many blocks (%lld)", g.nblocks);
+    return MIRORR_EINVAL;
+  }
+  unsigned grid = (unsigned)g.nblocks;
+  switch (g.bw) {
+#define CASE(BW)                                                                       \
+  case BW:                                                                             \
+    if (smem > 48 * 1024)                                                              \
+      MB2_CUDA_TRY(cudaFuncSetAttribute(ncc_kernel<BW>,                                \
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                        (int)smem));                                   \
+    ncc_kernel<BW><<<grid, 128, smem, s>>>(a);                                         \
+    break;
+    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
+#undef CASE
+    default:
+      set_error("block width %d not supported (1..8)", g.bw);
+      return MIRORR_EINVAL;
+  }
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// 4. post-filter + compaction
+// ---------------------------------------------------------------------------
+constexpr int kTile = 2048;  // blocks per compaction tile (256 threads x 8)
+
+__device__ inline bool keep_block(const BmOut &o, long long b) {
+  if (!(o.status[b] & 1)) return false;
+  double cb = (double)o.best[b], c2 = (double)o.second[b];
+  return cb > 1e-7 && fabs(cb - c2) > 1e-4;
+}
+
+__global__ void pf_count_kernel(BmOut o, long long n, unsigned int *tile_count) {
+  __shared__ unsigned int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  long long t0 = (long long)blockIdx.x * kTile;
+  unsigned int c = 0;
+  for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+    long long b = t0 + i;
+    if (b < n && keep_block(o, b)) ++c;
+  }
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&cnt, c);
+  __syncthreads();
+  if (threadIdx.x == 0) tile_count[blockIdx.x] = cnt;
+}
+
+__global__ void pf_scan_kernel(unsigned int *tile_count, long long ntiles, long long *total) {
+  // single CTA, 1024 threads: exclusive scan in place (tile counts -> offsets)
+  __shared__ unsigned long long carry;
+  __shared__ unsigned long long warp_sums[32];
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (long long base = 0; base < ntiles; base += blockDim.x) {
+    long long i = base + threadIdx.x;
+    unsigned long long v = (i < ntiles) ? tile_count[i] : 0;
+    unsigned long long x = v;
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      unsigned long long y = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      unsigned long long w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        unsigned long long y = __shfl_up_sync(0xffffffffu, w, off);
+        if (lane >= off) w += y;
+      }
+      warp_sums[lane] = w;
+    }
+    __syncthreads();
+    unsigned long long excl = x - v + (wid > 0 ? warp_sums[wid - 1] : 0) + carry;
+    if (i < ntiles) tile_count[i] = (unsigned int)excl;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = (long long)carry;
+}
+
+__device__ inline void block_point(const PointGeom &pg, int ix, int iy, int iz, double *out) {
+  const double idx[3] = {(double)ix, (double)iy, (double)iz};
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    double v = pg.origin[r];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v = __dadd_rn(v, __dmul_rn(pg.a[3 * r + c], idx[c]));
+    out[r] = __dadd_rn(v, pg.half[r]);
+  }
+}
+
+__global__ void pf_write_kernel(BmOut o, long long n, const unsigned int *tile_off, BmGeom g,
+                                PointGeom pg, double *pts_base, double *pts_match,
+                                const long long *offset_dev) {
+  __shared__ unsigned int wsum[8];
+  const int per = kTile / 256;  // 8 consecutive blocks per thread
+  long long t0 = (long long)blockIdx.x * kTile + (long long)threadIdx.x * per;
+  unsigned int flags = 0, c = 0;
+  for (int k = 0; k < per; ++k) {
+    long long b = t0 + k;
+    if (b < n && keep_block(o, b)) {
+      flags |= 1u << k;
+      ++c;
+      o.status[b] |= 2;
+    }
+  }
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned int x = c;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    unsigned int y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  unsigned int before = 0;
+  for (int w = 0; w < wid; ++w) before += wsum[w];
+  unsigned long long pos = (unsigned long long)tile_off[blockIdx.x] + before + x - c;
+  if (!pts_base) return;
+  if (offset_dev) pos += (unsigned long long)*offset_dev;
+  for (int k = 0; k < per; ++k) {
+    if (!(flags & (1u << k))) continue;
+    long long b = t0 + k;
+    int bx = (int)(b % g.nb[0]), by = (int)((b / g.nb[0]) % g.nb[1]),
+        bz = (int)(b / ((long long)g.nb[0] * g.nb[1]));
+    int ox = g.st[0] + bx * g.ngap, oy = g.st[1] + by * g.ngap, oz = g.st[2] + bz * g.ngap;
+    int m = o.match[b];
+    int mx = m % g.size[0], my = (m / g.size[0]) % g.size[1], mz = m / (g.size[0] * g.size[1]);
+    block_point(pg, ox, oy, oz, pts_base + 3 * pos);
+    block_point(pg, mx, my, mz, pts_match + 3 * pos);
+    ++pos;
+  }
+}
+
+mirorr_status launch_postfilter(const BmGeom &g, const BmOut &out, BmWork &w,
+                                const PointGeom &pg, double *pts_base, double *pts_match,
+                                long long *count_dev, const long long *offset_dev,
+                                cudaStream_t s) {
+  long long n = g.nblocks;
+  long long ntiles = (n + kTile - 1) / kTile;
+  MB2_TRY(w.tiles.ensure(sizeof(unsigned int) * (ntiles + 1)));
+  unsigned int *tiles = w.tiles.as<unsigned int>();
+  pf_count_kernel<<<(unsigned)ntiles, 256, 0, s>>>(out, n, tiles);
+  MB2_LAUNCH_CHECK();
+  pf_scan_kernel<<<1, 1024, 0, s>>>(tiles, ntiles, count_dev);
+  MB2_LAUNCH_CHECK();
+  pf_write_kernel<<<(unsigned)ntiles, 256, 0, s>>>(out, n, tiles, g, pg, pts_base, pts_match,
+                                                    offset_dev);
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
+}
+
+}  // namespace mb2

@@ -1,0 +1,1239 @@
+// capi.cu -- C ABI of mirorr_b200 (declared in include/mirorr_b200.h):
+// context, block matcher (the AbstractBlockMatcher replacement), resampler,
+// LTS fit, pyramid, and the device-resident registration driver
+// (MirorrPyramidImplement::RunMirorr + the classic / symmetric iteration loops).
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace mb2 {
+
+static thread_local char t_err[512] = "";
+int64_t g_launches = 0;
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(t_err, sizeof(t_err), fmt, ap);
+  va_end(ap);
+}
+void clear_error() { t_err[0] = 0; }
+const char *get_error() { return t_err; }
+
+}  // namespace mb2
+
+using namespace mb2;
+
+// Per-stage timing of matcher calls, accumulated from CUDA events.
+struct StageTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  double ms[4] = {0, 0, 0, 0};
+  long long calls = 0;
+  cudaEvent_t *take(size_t k) {
+    while (pool.size() < used + k) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      pool.push_back(e);
+    }
+    cudaEvent_t *p = &pool[used];
+    used += k;
+    return p;
+  }
+  // call after a stream synchronize
+  void harvest() {
+    for (size_t i = 0; i + 5 <= used; i += 5) {
+      for (int s = 0; s < 4; ++s) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, pool[i + s], pool[i + s + 1]) == cudaSuccess) ms[s] += t;
+      }
+      ++calls;
+    }
+    used = 0;
+    cudaGetLastError();
+  }
+  void release() {
+    for (auto e : pool) cudaEventDestroy(e);
+    pool.clear();
+    used = 0;
+  }
+};
+
+struct mirorr_ctx_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches0 = 0;
+  BmWork bmw;
+  LtsWork ltsw;
+  DevBuf counts;      // long long[4]
+  DevBuf ncc_count;   // unsigned long long
+  DevBuf ones;        // default all-255 mask
+  long long ones_n = 0;
+  StageTimer timer;
+  // registration scratch
+  DevBuf lvl_f, lvl_m, tmp_a, tmp_b, weights;
+  DevBuf img_b, img_s, msk_b, msk_s;
+  DevBuf best, second, match, status;
+  DevBuf pts_i, pts_m;
+  DevBuf up_f, up_m, up_fm, up_mm;
+};
+
+struct Vol {
+  const float *img = nullptr;
+  const uint8_t *mask = nullptr;
+  DevBuf own_img, own_mask;
+  bool has = false;
+  bool has_mask = false;
+  mirorr_geometry geom{};
+};
+
+struct mirorr_matcher_s {
+  mirorr_ctx ctx = nullptr;
+  mirorr_bm_params p{};
+  Vol base, search;
+  DevBuf best, second, match, status, pts_b, pts_m;
+  BmGeom last{};
+  bool has_results = false;
+  long long kept = 0;
+  cudaEvent_t ev[5] = {};
+  float timings[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+mirorr_status check_device(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device available (%s)",
+              e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+    return MIRORR_ECUDA;
+  }
+  if (device < 0 || device >= n) {
+    set_error("device %d out of range (%d devices)", device, n);
+    return MIRORR_EINVAL;
+  }
+  cudaDeviceProp prop;
+  MB2_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) {
+    set_error("device %d is sm_%d%d; this library is built for sm_100a (B200)", device,
+              prop.major, prop.minor);
+    return MIRORR_ECUDA;
+  }
+  return MIRORR_OK;
+}
+
+bool valid_geom(const mirorr_geometry *g) {
+  if (!g) return false;
+  for (int d = 0; d < 3; ++d)
+    if (g->size[d] <= 0 || !(g->spacing[d] > 0.0)) return false;
+  double A[9], Ai[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) A[3 * r + c] = g->direction[3 * r + c] * g->spacing[c];
+  return mn_inverse<3>(A, Ai);
+}
+
+mirorr_status ensure_ones(mirorr_ctx c, long long n) {
+  if (c->ones_n >= n) return MIRORR_OK;
+  MB2_TRY(c->ones.ensure(n));
+  MB2_TRY(launch_fill_u8(c->ones.as<uint8_t>(), n, 255, c->stream));
+  c->ones_n = n;
+  return MIRORR_OK;
+}
+
+void index_to_physical(const mirorr_geometry &g, double *A) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) A[3 * r + c] = g.direction[3 * r + c] * g.spacing[c];
+}
+
+// out index -> in continuous index: C = Ain^-1 M Aout, e = Ain^-1 (M Oout + off - Oin)
+bool make_map(const mirorr_geometry &out, const mirorr_geometry &in, const double *M,
+              const double *off, ResampleMap &m) {
+  double Aout[9], Ain[9], Ainv[9], MA[9], v[3], w[3];
+  index_to_physical(out, Aout);
+  index_to_physical(in, Ain);
+  if (!mn_inverse<3>(Ain, Ainv)) return false;
+  m3_mul(M, Aout, MA);
+  m3_mul(Ainv, MA, m.C);
+  m3_vec(M, out.origin, v);
+  for (int i = 0; i < 3; ++i) w[i] = v[i] + off[i] - in.origin[i];
+  m3_vec(Ainv, w, m.e);
+  return true;
+}
+
+void center_of(const mirorr_geometry &g, double *c) {
+  double A[9], ci[3];
+  index_to_physical(g, A);
+  for (int d = 0; d < 3; ++d) ci[d] = ((double)g.size[d] - 1.0) / 2.0;
+  m3_vec(A, ci, c);
+  for (int d = 0; d < 3; ++d) c[d] += g.origin[d];
+}
+
+void to_public(const Tfm &t, mirorr_transform &o) {
+  o.kind = t.kind;
+  for (int i = 0; i < 9; ++i) o.matrix[i] = t.M[i];
+  for (int i = 0; i < 3; ++i) { o.offset[i] = t.off[i]; o.center[i] = t.c[i]; }
+  for (int i = 0; i < 12; ++i) o.params[i] = 0.0;
+  tfm_params(t, o.params);
+}
+
+bool from_public(const mirorr_transform &o, Tfm &t) {
+  if (o.kind != KIND_RIGID && o.kind != KIND_AFFINE) return false;
+  tfm_identity(t, o.kind);
+  tfm_set_center(t, o.center);
+  tfm_set_params(t, o.params);
+  return true;
+}
+
+mirorr_status check_bm_params(const mirorr_bm_params &p) {
+  if (p.block_width < 1 || p.block_width > 8) {
+    set_error("block_width %u not supported (1..8)", p.block_width);
+    return MIRORR_EINVAL;
+  }
+  if (p.block_gap < 1 || p.nhood_gap < 1 || p.nhood_width < 1) {
+    set_error("block_gap, nhood_gap and nhood_width must be >= 1");
+    return MIRORR_EINVAL;
+  }
+  double pk = p.portion_matches_kept;
+  if (pk < 0.0 || pk > 1.0 || pk != pk) {
+    set_error("PortionMatchesKept is %g. It should be between 0 and 1.0.", pk);
+    return MIRORR_EINVAL;
+  }
+  if (!(p.block_keep > 0.0)) {
+    set_error("block_keep must be > 0 (>= 1 keeps every block)");
+    return MIRORR_EINVAL;
+  }
+  int e = ((int)p.nhood_width - 1) * (int)p.block_gap + (int)p.block_width;
+  size_t smem = (size_t)e * e * e * 5 + 1024;
+  if (e > 40 || smem > 200 * 1024) {
+    set_error("search window too large: (nhood_width-1)*block_gap+block_width = %d", e);
+    return MIRORR_EINVAL;
+  }
+  return MIRORR_OK;
+}
+
+// ---- one matcher call on device data ---------------------------------------
+struct MatchCall {
+  const float *base, *search;
+  const uint8_t *bmask, *smask;
+  int size[3];
+  mirorr_geometry point_geom;  // base image geometry (blockPositionToPoint)
+};
+
+mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall &mc,
+                        BmGeom &g, DevBuf &best, DevBuf &second, DevBuf &match,
+                        DevBuf &status, double *pts_b, double *pts_m, long long *count_dev,
+                        const long long *offset_dev, cudaEvent_t *ev) {
+  if (!bm_geometry(mc.size, (int)p.block_width, (int)p.block_gap, (int)p.nhood_gap,
+                   (int)p.nhood_width, g)) {
+    set_error("image smaller than one block or invalid block parameters");
+    return MIRORR_EINVAL;
+  }
+  long long nvox = (long long)mc.size[0] * mc.size[1] * mc.size[2];
+  MB2_TRY(c->bmw.stats.ensure(sizeof(float2) * nvox));
+  MB2_TRY(best.ensure(sizeof(float) * g.nblocks));
+  MB2_TRY(second.ensure(sizeof(float) * g.nblocks));
+  MB2_TRY(match.ensure(sizeof(int32_t) * g.nblocks));
+  MB2_TRY(status.ensure(g.nblocks));
+  cudaStream_t s = c->stream;
+  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], s));
+  MB2_TRY(launch_box_stats(g, mc.search, mc.smask, c->bmw.stats.as<float2>(), s));
+  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], s));
+  const uint8_t *sel = nullptr;
+  MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s));
+  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
+  BmOut out{best.as<float>(), second.as<float>(), match.as<int32_t>(), status.as<uint8_t>()};
+  MB2_TRY(launch_ncc(g, mc.base, mc.bmask, mc.search, mc.smask, c->bmw.stats.as<float2>(), sel,
+                     out, c->ncc_count.as<unsigned long long>(), s));
+  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[3], s));
+  PointGeom pg;
+  point_geom(mc.point_geom.origin, mc.point_geom.spacing, mc.point_geom.direction,
+             (int)p.block_width, pg);
+  MB2_TRY(launch_postfilter(g, out, c->bmw, pg, pts_b, pts_m, count_dev, offset_dev, s));
+  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[4], s));
+  return MIRORR_OK;
+}
+
+// ---- pyramid schedule: PyramidScheduleTuner::UpdateSymmetric -----------------
+double num_octaves(double dim, double base) { return std::floor(std::log(dim / base) / std::log(2.0)); }
+unsigned num_levels(double dim, double base) {
+  return 1u + (unsigned)std::max(0.0, num_octaves(dim, base));
+}
+unsigned best_rate(double big, double small) {
+  unsigned e = (unsigned)std::max(0.0, num_octaves(big * (4.0 / 3.0), small));
+  return 1u << e;
+}
+
+int pyramid_schedule(const mirorr_geometry &fg, const mirorr_geometry &mg, int min_length,
+                     int max_levels, int sm_out[16][3], int sf_out[16][3]) {
+  double ml = std::max({mg.size[0], mg.size[1], mg.size[2]});
+  double fl = std::max({fg.size[0], fg.size[1], fg.size[2]});
+  int mpl = 1 + (int)std::max(num_levels(ml, min_length), num_levels(fl, min_length));
+  std::vector<std::array<long long, 3>> sm(mpl), sf(mpl);
+  for (auto &r : sm) r = {-1, -1, -1};
+  for (auto &r : sf) r = {-1, -1, -1};
+  for (int d = 0; d < 3; ++d) {
+    int r = 1;
+    sm[mpl - r][d] = 1;
+    sf[mpl - r][d] = 1;
+    double mb = mg.spacing[d], fb = fg.spacing[d];
+    long long me = 1LL << (num_levels(mg.size[d], min_length) - 1);
+    long long fe = 1LL << (num_levels(fg.size[d], min_length) - 1);
+    r = 2;
+    if (mb < fb) {
+      long long rate = std::min<long long>(best_rate(fb, mb), me);
+      for (long long s = rate >= 2 ? 2 : 1; s <= rate; s *= 2) {
+        sm[mpl - r][d] = s; sf[mpl - r][d] = 1; ++r;
+      }
+    } else if (mb > fb) {
+      long long rate = std::min<long long>(best_rate(mb, fb), fe);
+      for (long long s = rate >= 2 ? 2 : 1; s <= rate; s *= 2) {
+        sm[mpl - r][d] = 1; sf[mpl - r][d] = s; ++r;
+      }
+    } else {
+      sm[mpl - r][d] = 1; sf[mpl - r][d] = 1; ++r;
+    }
+    for (int lev = mpl - r; lev >= 0; --lev) {
+      if (2 * sm[lev + 1][d] > me || 2 * sf[lev + 1][d] > fe) {
+        sm[lev][d] = sm[lev + 1][d]; sf[lev][d] = sf[lev + 1][d];
+      } else {
+        sm[lev][d] = 2 * sm[lev + 1][d]; sf[lev][d] = 2 * sf[lev + 1][d];
+      }
+    }
+  }
+  int first = 0;
+  {
+    int nd = 0;
+    for (int d = 0; d < 3; ++d) {
+      if (sm[mpl - 1][d] != sm[mpl - 2][d]) ++nd;
+      if (sf[mpl - 1][d] != sf[mpl - 2][d]) ++nd;
+    }
+    if (nd == 0) first = 1;
+  }
+  int last = mpl;
+  for (int lev = 2; lev < mpl; ++lev) {
+    int nd = 0;
+    for (int d = 0; d < 3; ++d) {
+      if (sm[mpl - lev - 1][d] != sm[mpl - lev][d]) ++nd;
+      if (sf[mpl - lev - 1][d] != sf[mpl - lev][d]) ++nd;
+    }
+    if (nd < 3) { last = lev; break; }
+  }
+  int n = last - first;
+  if (max_levels > 0 && n > max_levels) n = max_levels;
+  if (n > 16) n = 16;
+  for (int lev = 0; lev < n; ++lev)
+    for (int d = 0; d < 3; ++d) {
+      sm_out[n - lev - 1][d] = (int)sm[mpl - first - lev - 1][d];
+      sf_out[n - lev - 1][d] = (int)sf[mpl - first - lev - 1][d];
+    }
+  return n;
+}
+
+// Gaussian of sigma = f/2 voxels, radius ceil(3 sigma), normalised by the
+// sequential sum.
+int gaussian_weights(int f, double *w) {
+  if (f <= 1) { w[0] = 1.0; return 0; }
+  double sigma = f / 2.0;
+  int r = (int)std::ceil(3.0 * sigma);
+  double s = 0.0;
+  for (int k = -r; k <= r; ++k) {
+    w[k + r] = std::exp(-((double)k * (double)k) / (2.0 * sigma * sigma));
+  }
+  for (int k = 0; k <= 2 * r; ++k) s += w[k];
+  for (int k = 0; k <= 2 * r; ++k) w[k] = w[k] / s;
+  return r;
+}
+
+void level_geometry(const mirorr_geometry &in, const int f[3], mirorr_geometry &out) {
+  out = in;
+  double ds[3];
+  for (int d = 0; d < 3; ++d) {
+    out.size[d] = std::max(1, (int)std::floor((double)in.size[d] / (double)f[d]));
+    out.spacing[d] = in.spacing[d] * (double)f[d];
+    ds[d] = (out.spacing[d] - in.spacing[d]) * 0.5;
+  }
+  double v[3];
+  m3_vec(in.direction, ds, v);
+  for (int d = 0; d < 3; ++d) out.origin[d] = in.origin[d] + v[d];
+}
+
+// Builds one pyramid level on the device.  When every factor is 1 the input
+// itself is the level (*out_ptr = in, no copy).
+mirorr_status make_level(mirorr_ctx c, const mirorr_geometry &ig, const float *in,
+                         const int f[3], mirorr_geometry &og, DevBuf &out, const float **out_ptr) {
+  level_geometry(ig, f, og);
+  if (f[0] == 1 && f[1] == 1 && f[2] == 1) {
+    *out_ptr = in;
+    return MIRORR_OK;
+  }
+  cudaStream_t s = c->stream;
+  long long n = vox(ig.size);
+  MB2_TRY(c->tmp_a.ensure(sizeof(float) * n));
+  MB2_TRY(c->tmp_b.ensure(sizeof(float) * n));
+  MB2_TRY(c->weights.ensure(sizeof(double) * 3 * 64));
+  double w[3][64];
+  int rad[3];
+  for (int d = 0; d < 3; ++d) {
+    if (f[d] > 20) {
+      set_error("pyramid factor %d too large", f[d]);
+      return MIRORR_EINVAL;
+    }
+    rad[d] = gaussian_weights(f[d], w[d]);
+  }
+  MB2_CUDA_TRY(cudaMemcpyAsync(c->weights.ptr, w, sizeof(w), cudaMemcpyHostToDevice, s));
+  const float *cur = in;
+  float *bufs[2] = {c->tmp_a.as<float>(), c->tmp_b.as<float>()};
+  int bi = 0;
+  for (int d = 0; d < 3; ++d) {
+    if (f[d] <= 1) continue;
+    MB2_TRY(launch_smooth_axis(ig.size, cur, bufs[bi], d, c->weights.as<double>() + 64 * d,
+                               rad[d], s));
+    cur = bufs[bi];
+    bi ^= 1;
+  }
+  MB2_TRY(out.ensure(sizeof(float) * vox(og.size)));
+  ResampleMap m;
+  for (int i = 0; i < 9; ++i) m.C[i] = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    m.C[4 * d] = (double)f[d];
+    m.e[d] = ((double)f[d] - 1.0) / 2.0;
+  }
+  MB2_TRY(launch_resample(ig.size, cur, nullptr, og.size, m, out.as<float>(), nullptr, s));
+  *out_ptr = out.as<float>();
+  return MIRORR_OK;
+}
+
+// ---- registration ----------------------------------------------------------
+struct RegImage {
+  const float *img;
+  mirorr_geometry g;
+};
+
+struct RegRun {
+  mirorr_ctx c;
+  const mirorr_reg_params *p;
+  const uint8_t *fmask;   // full resolution
+  const uint8_t *mmask;
+  mirorr_geometry fmask_g, mmask_g;
+  mirorr_reg_stats *stats;
+  int level;
+};
+
+mirorr_status resample_into(mirorr_ctx c, const RegImage &src, const uint8_t *mask,
+                            const mirorr_geometry &mask_g, const mirorr_geometry &grid,
+                            const Tfm &t, DevBuf &img, DevBuf &msk) {
+  ResampleMap mi, mm;
+  if (!make_map(grid, src.g, t.M, t.off, mi) || !make_map(grid, mask_g, t.M, t.off, mm)) {
+    set_error("singular image geometry");
+    return MIRORR_EINVAL;
+  }
+  long long n = vox(grid.size);
+  MB2_TRY(img.ensure(sizeof(float) * n));
+  MB2_TRY(msk.ensure(n));
+  MB2_TRY(launch_resample(src.g.size, src.img, nullptr, grid.size, mi, img.as<float>(), nullptr,
+                          c->stream));
+  MB2_TRY(launch_resample(mask_g.size, nullptr, mask, grid.size, mm, nullptr, msk.as<uint8_t>(),
+                          c->stream));
+  return MIRORR_OK;
+}
+
+mirorr_status run_lts(RegRun &r, LtsState &hs, long long nmax, long long *n_used) {
+  int inner = 0;
+  mirorr_ctx c = r.c;
+  MB2_TRY(lts_run(c->ltsw, hs, c->pts_i.as<double>(), c->pts_m.as<double>(),
+                  c->counts.as<long long>(), nmax, c->stream, &inner, n_used));
+  if (c->timer.on) c->timer.harvest();
+  if (*n_used == 0) {
+    set_error("No block matches occurred. Images probably have zero overlap. "
+              "Try supplying a better initial transform.");
+    return MIRORR_ENOBLOCKS;
+  }
+  return MIRORR_OK;
+}
+
+mirorr_status ensure_pts(mirorr_ctx c, long long n) {
+  MB2_TRY(c->pts_i.ensure(sizeof(double) * 3 * std::max(1LL, n)));
+  MB2_TRY(c->pts_m.ensure(sizeof(double) * 3 * std::max(1LL, n)));
+  return MIRORR_OK;
+}
+
+double param_delta(const double *a, const double *b, int n) {
+  double d = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double e = a[i] - b[i];
+    d += e * e;
+  }
+  return d;
+}
+
+void grid_geom(const double *origin, const double *spacing, const int *size,
+               const double *direction, mirorr_geometry &g) {
+  for (int d = 0; d < 3; ++d) {
+    g.origin[d] = origin[d];
+    g.spacing[d] = spacing[d];
+    g.size[d] = size[d];
+  }
+  for (int i = 0; i < 9; ++i) g.direction[i] = direction[i];
+}
+
+mirorr_status match_into(RegRun &r, const float *base, const uint8_t *bmask, const float *search,
+                         const uint8_t *smask, const mirorr_geometry &base_g, double *pts_b,
+                         double *pts_m, int count_slot, const long long *offset_dev) {
+  mirorr_ctx c = r.c;
+  MatchCall mc{base, search, bmask, smask, {base_g.size[0], base_g.size[1], base_g.size[2]},
+               base_g};
+  BmGeom g;
+  cudaEvent_t *ev = c->timer.on ? c->timer.take(5) : nullptr;
+  MB2_TRY(run_match(c, r.p->bm, mc, g, c->best, c->second, c->match, c->status, pts_b, pts_m,
+                    c->counts.as<long long>() + count_slot, offset_dev, ev));
+  if (r.stats) r.stats->matcher_calls += 1;
+  return MIRORR_OK;
+}
+
+mirorr_status classic_level(RegRun &r, const RegImage &fl, const RegImage &ml, Tfm &tfm) {
+  mirorr_ctx c = r.c;
+  const mirorr_reg_params &p = *r.p;
+  double cf[3], cm[3], origin[3], spacing[3];
+  int size[3];
+  center_of(fl.g, cf);
+  center_of(ml.g, cm);
+  for (int d = 0; d < 3; ++d) {
+    origin[d] = cm[d] + ((fl.g.origin[d] - cf[d]) + (ml.g.origin[d] - cm[d])) / 2.0;
+    spacing[d] = (fl.g.spacing[d] + ml.g.spacing[d]) / 2.0;
+    size[d] = (int)(((double)fl.g.size[d] + (double)ml.g.size[d] + 0.5) / 2.0);
+  }
+  mirorr_geometry grid_f, grid_m;
+  grid_geom(origin, spacing, size, fl.g.direction, grid_f);
+  grid_geom(origin, spacing, size, ml.g.direction, grid_m);
+  Tfm ident;
+  tfm_identity(ident, KIND_AFFINE);
+  MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, ident, c->img_b, c->msk_b));
+  BmGeom g;
+  if (!bm_geometry(size, (int)p.bm.block_width, (int)p.bm.block_gap, (int)p.bm.nhood_gap,
+                   (int)p.bm.nhood_width, g)) {
+    set_error("middle-space image smaller than one block");
+    return MIRORR_EINVAL;
+  }
+  MB2_TRY(ensure_pts(c, g.nblocks));
+  double last[12], cur[12];
+  tfm_params(tfm, last);
+  int np = tfm_nparams(tfm);
+  int it = 0;
+  for (; it < std::abs(p.iterations); ++it) {
+    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, tfm, c->img_s, c->msk_s));
+    MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
+    MB2_TRY(match_into(r, c->img_b.as<float>(), c->msk_b.as<uint8_t>(), c->img_s.as<float>(),
+                       c->msk_s.as<uint8_t>(), grid_m, c->pts_i.as<double>(),
+                       c->pts_m.as<double>(), 0, nullptr));
+    LtsState hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.kind = tfm.kind;
+    hs.symmetric = 0;
+    hs.lts_keep = p.lts_keep;
+    hs.tfm = tfm;
+    long long used = 0;
+    MB2_TRY(run_lts(r, hs, g.nblocks, &used));
+    tfm = hs.tfm;
+    tfm_params(tfm, cur);
+    double d = param_delta(last, cur, np);
+    for (int i = 0; i < 12; ++i) last[i] = cur[i];
+    if (p.verbosity >= 1)
+      printf("level %d iteration %d: blocks %lld, delta %.6g\n", r.level, it + 1, used, d);
+    if (d < 1e-3) { ++it; break; }
+  }
+  if (r.stats && r.level < 16) r.stats->iterations_run[r.level] = it;
+  return MIRORR_OK;
+}
+
+mirorr_status symmetric_level(RegRun &r, const RegImage &fl, const RegImage &ml, Tfm &tfm) {
+  mirorr_ctx c = r.c;
+  const mirorr_reg_params &p = *r.p;
+  double cf[3], cm[3], origin[3], spacing[3];
+  int size[3];
+  center_of(fl.g, cf);
+  center_of(ml.g, cm);
+  for (int d = 0; d < 3; ++d) {
+    origin[d] = ((fl.g.origin[d] - cf[d]) + (ml.g.origin[d] - cm[d])) / 2.0;
+    spacing[d] = (fl.g.spacing[d] + ml.g.spacing[d]) / 2.0;
+    size[d] = (int)(((double)fl.g.size[d] + (double)ml.g.size[d] + 0.5) / 2.0);
+  }
+  mirorr_geometry grid_f, grid_m;
+  grid_geom(origin, spacing, size, fl.g.direction, grid_f);
+  grid_geom(origin, spacing, size, ml.g.direction, grid_m);
+  double initial_center[3] = {tfm.c[0], tfm.c[1], tfm.c[2]};
+  tfm_center_to_origin(tfm);
+  Tfm fixed_tr, moving_tr, ifixed;
+  tfm_identity(fixed_tr, KIND_RIGID);
+  tfm_identity(moving_tr, KIND_RIGID);
+  double pf[6] = {0, 0, 0, cf[0], cf[1], cf[2]}, pm[6] = {0, 0, 0, cm[0], cm[1], cm[2]};
+  tfm_set_params(fixed_tr, pf);
+  tfm_set_params(moving_tr, pm);
+  tfm_inverse(fixed_tr, ifixed);
+  tfm_compose(tfm, ifixed, false);
+  tfm_compose(tfm, moving_tr, true);
+  Tfm t12f, t12b;
+  half_space(tfm, t12f, t12b);
+  BmGeom g;
+  if (!bm_geometry(size, (int)p.bm.block_width, (int)p.bm.block_gap, (int)p.bm.nhood_gap,
+                   (int)p.bm.nhood_width, g)) {
+    set_error("middle-space image smaller than one block");
+    return MIRORR_EINVAL;
+  }
+  MB2_TRY(ensure_pts(c, 2 * g.nblocks));
+  double last[12], cur[12], prm[12];
+  tfm_params(tfm, last);
+  int np = tfm_nparams(tfm);
+  auto centered = [&](Tfm &cF, Tfm &cB) {
+    tfm_identity(cF, tfm.kind);
+    tfm_identity(cB, tfm.kind);
+    tfm_params(t12f, prm);
+    tfm_set_params(cF, prm);
+    tfm_compose(cF, fixed_tr, false);
+    tfm_params(t12b, prm);
+    tfm_set_params(cB, prm);
+    tfm_compose(cB, moving_tr, false);
+  };
+  int it = 0;
+  for (; it < std::abs(p.iterations); ++it) {
+    Tfm cF, cB;
+    centered(cF, cB);
+    MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, cB, c->img_b, c->msk_b));
+    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, cF, c->img_s, c->msk_s));
+    MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
+    double *pi = c->pts_i.as<double>(), *pmv = c->pts_m.as<double>();
+    // forward: base = moving, search = fixed
+    MB2_TRY(match_into(r, c->img_b.as<float>(), c->msk_b.as<uint8_t>(), c->img_s.as<float>(),
+                       c->msk_s.as<uint8_t>(), grid_m, pi, pmv, 0, nullptr));
+    // swapped: base = fixed, search = moving; its lists are appended with
+    // roles reversed (itkSymMirorrRegistrationMethod.txx:595-602)
+    MB2_TRY(match_into(r, c->img_s.as<float>(), c->msk_s.as<uint8_t>(), c->img_b.as<float>(),
+                       c->msk_b.as<uint8_t>(), grid_f, pmv, pi, 1, c->counts.as<long long>()));
+    LtsState hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.kind = tfm.kind;
+    hs.symmetric = 1;
+    hs.lts_keep = p.lts_keep;
+    hs.tfm = tfm;
+    hs.t12f = t12f;
+    hs.t12b = t12b;
+    long long used = 0;
+    MB2_TRY(run_lts(r, hs, 2 * g.nblocks, &used));
+    tfm = hs.tfm;
+    t12f = hs.t12f;
+    t12b = hs.t12b;
+    tfm_params(tfm, cur);
+    double d = param_delta(last, cur, np);
+    for (int i = 0; i < 12; ++i) last[i] = cur[i];
+    if (p.verbosity >= 1)
+      printf("level %d iteration %d: blocks %lld, delta %.6g\n", r.level, it + 1, used, d);
+    if (d < 1e-3) { ++it; break; }
+  }
+  if (r.stats && r.level < 16) r.stats->iterations_run[r.level] = it;
+  Tfm cF, cB, ib;
+  centered(cF, cB);
+  tfm_inverse(cB, ib);
+  tfm_identity(tfm, tfm.kind);
+  tfm_compose(tfm, ib, true);
+  tfm_compose(tfm, cF, false);
+  tfm_update_center(tfm, initial_center);
+  return MIRORR_OK;
+}
+
+mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float *fixed,
+                            const uint8_t *fmask, const mirorr_geometry *mg, const float *moving,
+                            const uint8_t *mmask, const mirorr_reg_params *p,
+                            const mirorr_transform *init, mirorr_transform *result,
+                            mirorr_reg_stats *stats) {
+  if (!c || !fg || !mg || !fixed || !moving || !p || !result) {
+    set_error("null argument");
+    return MIRORR_EINVAL;
+  }
+  if (!valid_geom(fg) || !valid_geom(mg)) {
+    set_error("invalid image geometry");
+    return MIRORR_EINVAL;
+  }
+  if (p->kind != KIND_RIGID && p->kind != KIND_AFFINE) {
+    set_error("transform kind must be 0 (rigid) or 1 (affine)");
+    return MIRORR_EINVAL;
+  }
+  MB2_TRY(check_bm_params(p->bm));
+  if (!(p->lts_keep > 0.0 && p->lts_keep <= 1.0)) {
+    set_error("lts_keep must lie in (0, 1]");
+    return MIRORR_EINVAL;
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  mirorr_reg_params pp = *p;
+  if (pp.iterations == 0) pp.iterations = 5;
+  if (pp.min_length <= 0) pp.min_length = 32;
+  MB2_TRY(c->counts.ensure(4 * sizeof(long long)));
+  MB2_TRY(c->ncc_count.ensure(sizeof(unsigned long long)));
+  MB2_CUDA_TRY(cudaMemsetAsync(c->ncc_count.ptr, 0, sizeof(unsigned long long), c->stream));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  long long nmax = std::max(vox(fg->size), vox(mg->size));
+  if (!fmask || !mmask) MB2_TRY(ensure_ones(c, nmax));
+  RegRun r{c, &pp, fmask ? fmask : c->ones.as<uint8_t>(), mmask ? mmask : c->ones.as<uint8_t>(),
+           *fg, *mg, stats, 0};
+  int sm[16][3], sf[16][3];
+  int nl = pyramid_schedule(*fg, *mg, pp.min_length, pp.levels, sm, sf);
+  Tfm tfm;
+  if (init) {
+    if (!from_public(*init, tfm) || init->kind != pp.kind) {
+      set_error("initial transform kind does not match the requested kind");
+      return MIRORR_EINVAL;
+    }
+  } else {
+    double cfix[3], cmov[3], tr[3];
+    center_of(*fg, cfix);
+    center_of(*mg, cmov);
+    tfm_identity(tfm, pp.kind);
+    tfm_set_center(tfm, cmov);
+    for (int d = 0; d < 3; ++d) tr[d] = cfix[d] - cmov[d];
+    tfm_set_translation(tfm, tr);
+  }
+  double params[12];
+  tfm_params(tfm, params);
+  for (int lev = 0; lev < nl; ++lev) {
+    RegImage fl, ml;
+    MB2_TRY(make_level(c, *fg, fixed, sf[lev], fl.g, c->lvl_f, &fl.img));
+    MB2_TRY(make_level(c, *mg, moving, sm[lev], ml.g, c->lvl_m, &ml.img));
+    tfm_set_params(tfm, params);
+    r.level = lev;
+    if (pp.symmetric) MB2_TRY(symmetric_level(r, fl, ml, tfm));
+    else MB2_TRY(classic_level(r, fl, ml, tfm));
+    tfm_params(tfm, params);
+  }
+  tfm_set_params(tfm, params);
+  to_public(tfm, *result);
+  if (stats) {
+    stats->levels_run = nl;
+    unsigned long long cnt = 0;
+    MB2_CUDA_TRY(cudaMemcpyAsync(&cnt, c->ncc_count.ptr, sizeof(cnt), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    stats->block_ncc_evaluated = (int64_t)cnt;
+    stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return MIRORR_OK;
+}
+
+mirorr_status upload(mirorr_ctx c, DevBuf &b, const void *host, size_t bytes) {
+  MB2_TRY(b.ensure(bytes));
+  MB2_CUDA_TRY(cudaMemcpyAsync(b.ptr, host, bytes, cudaMemcpyHostToDevice, c->stream));
+  return MIRORR_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+const char *mirorr_last_error(void) { return mb2::get_error(); }
+int32_t mirorr_abi_version(void) { return MIRORR_ABI_VERSION; }
+
+mirorr_status mirorr_ctx_create(int32_t device, mirorr_ctx *out) {
+  if (!out) { set_error("null argument"); return MIRORR_EINVAL; }
+  *out = nullptr;
+  MB2_TRY(check_device(device));
+  MB2_CUDA_TRY(cudaSetDevice(device));
+  mirorr_ctx c = new (std::nothrow) mirorr_ctx_s;
+  if (!c) { set_error("out of host memory"); return MIRORR_ENOMEM; }
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    set_error("cudaStreamCreate failed: %s", cudaGetErrorString(e));
+    return MIRORR_ECUDA;
+  }
+  c->launches0 = g_launches;
+  mirorr_status s = c->counts.ensure(4 * sizeof(long long));
+  if (s == MIRORR_OK) s = c->ncc_count.ensure(sizeof(unsigned long long));
+  if (s != MIRORR_OK) { mirorr_ctx_destroy(c); return s; }
+  *out = c;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
+  if (!c) return MIRORR_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
+                    &c->bmw.hist, &c->bmw.tiles, &c->ltsw.state, &c->ltsw.resid,
+                    &c->ltsw.partial, &c->ltsw.hist, &c->ltsw.ctrl, &c->ltsw.cand, &c->counts,
+                    &c->ncc_count, &c->ones, &c->lvl_f, &c->lvl_m, &c->tmp_a, &c->tmp_b,
+                    &c->weights, &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best,
+                    &c->second, &c->match, &c->status, &c->pts_i, &c->pts_m, &c->up_f,
+                    &c->up_m, &c->up_fm, &c->up_mm};
+  for (DevBuf *b : bufs) b->release();
+  c->timer.release();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return MIRORR_OK;
+}
+
+int64_t mirorr_ctx_kernel_launches(mirorr_ctx c) { return c ? g_launches - c->launches0 : g_launches; }
+
+// ---- block matcher -----------------------------------------------------------
+mirorr_status mirorr_bm_default_params(mirorr_bm_params *p) {
+  if (!p) { set_error("null argument"); return MIRORR_EINVAL; }
+  p->block_width = 4;
+  p->block_gap = 1;
+  p->nhood_gap = 2;
+  p->nhood_width = 5;
+  p->portion_matches_kept = 0.5;
+  p->block_keep = 1.0;
+  p->verbosity = 0;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_create(mirorr_ctx c, mirorr_matcher *out) {
+  if (!c || !out) { set_error("null argument"); return MIRORR_EINVAL; }
+  mirorr_matcher m = new (std::nothrow) mirorr_matcher_s;
+  if (!m) { set_error("out of host memory"); return MIRORR_ENOMEM; }
+  m->ctx = c;
+  mirorr_bm_default_params(&m->p);
+  for (auto &e : m->ev) {
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      set_error("cudaEventCreate failed");
+      mirorr_bm_destroy(m);
+      return MIRORR_ECUDA;
+    }
+  }
+  *out = m;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_destroy(mirorr_matcher m) {
+  if (!m) return MIRORR_OK;
+  if (m->ctx && m->ctx->stream) cudaStreamSynchronize(m->ctx->stream);
+  for (auto &e : m->ev)
+    if (e) cudaEventDestroy(e);
+  DevBuf *bufs[] = {&m->base.own_img, &m->base.own_mask, &m->search.own_img,
+                    &m->search.own_mask, &m->best, &m->second, &m->match, &m->status,
+                    &m->pts_b, &m->pts_m};
+  for (DevBuf *b : bufs) b->release();
+  delete m;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_set_params(mirorr_matcher m, const mirorr_bm_params *p) {
+  if (!m || !p) { set_error("null argument"); return MIRORR_EINVAL; }
+  mirorr_bm_params q = *p;
+  if (q.portion_matches_kept == 0.0) q.portion_matches_kept = 0.5;
+  MB2_TRY(check_bm_params(q));
+  m->p = q;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_set_metric(mirorr_matcher m, const char *name) {
+  if (!m || !name) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!strcmp(name, "nc") || !strcmp(name, "normalized_correlation")) return MIRORR_OK;
+  set_error("block metric '%s' is not available on this path (only normalized_correlation)", name);
+  return MIRORR_EINVAL;
+}
+
+static mirorr_status set_image(mirorr_matcher m, Vol &v, const mirorr_geometry *g,
+                               const float *p, bool host) {
+  if (!m || !g || !p) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!valid_geom(g)) { set_error("invalid geometry"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(m->ctx->device));
+  if (host) {
+    MB2_TRY(upload(m->ctx, v.own_img, p, sizeof(float) * vox(g->size)));
+    v.img = v.own_img.as<float>();
+  } else {
+    v.img = p;
+  }
+  if (v.has && vox(v.geom.size) != vox(g->size) && v.has_mask) {
+    v.has_mask = false;  // a mask of the old size no longer applies
+    v.mask = nullptr;
+  }
+  v.geom = *g;
+  v.has = true;
+  m->has_results = false;
+  return MIRORR_OK;
+}
+
+static mirorr_status set_mask(mirorr_matcher m, Vol &v, const uint8_t *p, bool host) {
+  if (!m) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!p) {
+    v.has_mask = false;
+    v.mask = nullptr;
+    return MIRORR_OK;
+  }
+  if (!v.has) { set_error("set the image before its mask"); return MIRORR_ESTATE; }
+  MB2_CUDA_TRY(cudaSetDevice(m->ctx->device));
+  if (host) {
+    MB2_TRY(upload(m->ctx, v.own_mask, p, vox(v.geom.size)));
+    v.mask = v.own_mask.as<uint8_t>();
+  } else {
+    v.mask = p;
+  }
+  v.has_mask = true;
+  m->has_results = false;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_set_base_image(mirorr_matcher m, const mirorr_geometry *g, const float *h) {
+  return set_image(m, m->base, g, h, true);
+}
+mirorr_status mirorr_bm_set_search_image(mirorr_matcher m, const mirorr_geometry *g, const float *h) {
+  return set_image(m, m->search, g, h, true);
+}
+mirorr_status mirorr_bm_set_base_image_device(mirorr_matcher m, const mirorr_geometry *g,
+                                              const float *d) {
+  return set_image(m, m->base, g, d, false);
+}
+mirorr_status mirorr_bm_set_search_image_device(mirorr_matcher m, const mirorr_geometry *g,
+                                                const float *d) {
+  return set_image(m, m->search, g, d, false);
+}
+mirorr_status mirorr_bm_set_base_mask(mirorr_matcher m, const uint8_t *h) {
+  return m ? set_mask(m, m->base, h, true) : MIRORR_EINVAL;
+}
+mirorr_status mirorr_bm_set_search_mask(mirorr_matcher m, const uint8_t *h) {
+  return m ? set_mask(m, m->search, h, true) : MIRORR_EINVAL;
+}
+mirorr_status mirorr_bm_set_base_mask_device(mirorr_matcher m, const uint8_t *d) {
+  return m ? set_mask(m, m->base, d, false) : MIRORR_EINVAL;
+}
+mirorr_status mirorr_bm_set_search_mask_device(mirorr_matcher m, const uint8_t *d) {
+  return m ? set_mask(m, m->search, d, false) : MIRORR_EINVAL;
+}
+
+mirorr_status mirorr_bm_swap_image_order(mirorr_matcher m) {
+  if (!m) { set_error("null argument"); return MIRORR_EINVAL; }
+  std::swap(m->base.img, m->search.img);
+  std::swap(m->base.mask, m->search.mask);
+  std::swap(m->base.has, m->search.has);
+  std::swap(m->base.has_mask, m->search.has_mask);
+  std::swap(m->base.geom, m->search.geom);
+  std::swap(m->base.own_img, m->search.own_img);
+  std::swap(m->base.own_mask, m->search.own_mask);
+  m->has_results = false;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_grid(mirorr_matcher m, int32_t nblocks[3], int32_t start[3]) {
+  if (!m || !nblocks || !start) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!m->base.has) { set_error("base image not set"); return MIRORR_ESTATE; }
+  BmGeom g;
+  if (!bm_geometry(m->base.geom.size, (int)m->p.block_width, (int)m->p.block_gap,
+                   (int)m->p.nhood_gap, (int)m->p.nhood_width, g)) {
+    set_error("image smaller than one block");
+    return MIRORR_EINVAL;
+  }
+  for (int d = 0; d < 3; ++d) { nblocks[d] = g.nb[d]; start[d] = g.st[d]; }
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_get_offsets(mirorr_matcher m, size_t capacity, double *bp, double *mp,
+                                    size_t *n_out) {
+  if (!m || !n_out) { set_error("null argument"); return MIRORR_EINVAL; }
+  *n_out = 0;
+  if (!m->base.has || !m->search.has) {
+    set_error("base and search images must be set before GetOffsets");
+    return MIRORR_ESTATE;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (m->base.geom.size[d] != m->search.geom.size[d]) {
+      set_error("base and search images must share one grid size");
+      return MIRORR_EINVAL;
+    }
+  mirorr_ctx c = m->ctx;
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  long long nv = vox(m->base.geom.size);
+  if (!m->base.has_mask || !m->search.has_mask) MB2_TRY(ensure_ones(c, nv));
+  const uint8_t *bmask = m->base.has_mask ? m->base.mask : c->ones.as<uint8_t>();
+  const uint8_t *smask = m->search.has_mask ? m->search.mask : c->ones.as<uint8_t>();
+  BmGeom g;
+  if (!bm_geometry(m->base.geom.size, (int)m->p.block_width, (int)m->p.block_gap,
+                   (int)m->p.nhood_gap, (int)m->p.nhood_width, g)) {
+    set_error("image smaller than one block");
+    return MIRORR_EINVAL;
+  }
+  MB2_TRY(m->pts_b.ensure(sizeof(double) * 3 * g.nblocks));
+  MB2_TRY(m->pts_m.ensure(sizeof(double) * 3 * g.nblocks));
+  MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
+  MatchCall mc{m->base.img, m->search.img, bmask, smask,
+               {m->base.geom.size[0], m->base.geom.size[1], m->base.geom.size[2]},
+               m->base.geom};
+  MB2_TRY(run_match(c, m->p, mc, g, m->best, m->second, m->match, m->status,
+                    m->pts_b.as<double>(), m->pts_m.as<double>(), c->counts.as<long long>(),
+                    nullptr, m->ev));
+  long long kept = 0;
+  MB2_CUDA_TRY(cudaMemcpyAsync(&kept, c->counts.ptr, sizeof(kept), cudaMemcpyDeviceToHost,
+                               c->stream));
+  MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < 4; ++s) cudaEventElapsedTime(&m->timings[s], m->ev[s], m->ev[s + 1]);
+  m->last = g;
+  m->kept = kept;
+  m->has_results = true;
+  *n_out = (size_t)kept;
+  if (kept == 0) {
+    set_error("No block matches occurred. Images probably have zero overlap. "
+              "Try supplying a better initial transform.");
+    return MIRORR_ENOBLOCKS;
+  }
+  if ((size_t)kept > capacity) {
+    set_error("output capacity %zu < %lld kept blocks", capacity, kept);
+    return MIRORR_ERANGE;
+  }
+  if (bp)
+    MB2_CUDA_TRY(cudaMemcpy(bp, m->pts_b.ptr, sizeof(double) * 3 * kept, cudaMemcpyDeviceToHost));
+  if (mp)
+    MB2_CUDA_TRY(cudaMemcpy(mp, m->pts_m.ptr, sizeof(double) * 3 * kept, cudaMemcpyDeviceToHost));
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_block_results(mirorr_matcher m, size_t capacity, int32_t *match_index,
+                                      float *best, float *second, uint8_t *status,
+                                      size_t *n_blocks) {
+  if (!m || !n_blocks) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!m->has_results) { set_error("no results: call GetOffsets first"); return MIRORR_ESTATE; }
+  long long n = m->last.nblocks;
+  *n_blocks = (size_t)n;
+  if ((size_t)n > capacity) { set_error("capacity too small"); return MIRORR_ERANGE; }
+  MB2_CUDA_TRY(cudaSetDevice(m->ctx->device));
+  if (match_index) {
+    std::vector<int32_t> lin(n);
+    MB2_CUDA_TRY(cudaMemcpy(lin.data(), m->match.ptr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    const int nx = m->last.size[0], ny = m->last.size[1];
+    for (long long b = 0; b < n; ++b) {
+      int v = lin[b];
+      match_index[3 * b] = v % nx;
+      match_index[3 * b + 1] = (v / nx) % ny;
+      match_index[3 * b + 2] = v / (nx * ny);
+    }
+  }
+  if (best) MB2_CUDA_TRY(cudaMemcpy(best, m->best.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  if (second) MB2_CUDA_TRY(cudaMemcpy(second, m->second.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  if (status) MB2_CUDA_TRY(cudaMemcpy(status, m->status.ptr, n, cudaMemcpyDeviceToHost));
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_bm_last_timings(mirorr_matcher m, float ms[4]) {
+  if (!m || !ms) { set_error("null argument"); return MIRORR_EINVAL; }
+  for (int i = 0; i < 4; ++i) ms[i] = m->timings[i];
+  return MIRORR_OK;
+}
+
+// ---- resampler -----------------------------------------------------------------
+mirorr_status mirorr_resample_map(const mirorr_geometry *out_grid, const mirorr_geometry *in_grid,
+                                  const double M[9], const double offset[3], double C[9],
+                                  double e[3]) {
+  if (!out_grid || !in_grid || !M || !offset || !C || !e) {
+    set_error("null argument");
+    return MIRORR_EINVAL;
+  }
+  ResampleMap m;
+  if (!make_map(*out_grid, *in_grid, M, offset, m)) {
+    set_error("singular input geometry");
+    return MIRORR_EINVAL;
+  }
+  memcpy(C, m.C, sizeof(m.C));
+  memcpy(e, m.e, sizeof(m.e));
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_resample(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
+                              const uint8_t *in_mask, const int32_t out_size[3], const double C[9],
+                              const double e[3], float *out_image, uint8_t *out_mask) {
+  if (!c || !in_size || !out_size || !C || !e) { set_error("null argument"); return MIRORR_EINVAL; }
+  if ((in_image && !out_image) || (in_mask && !out_mask)) {
+    set_error("output buffer missing");
+    return MIRORR_EINVAL;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (in_size[d] <= 0 || out_size[d] <= 0) { set_error("empty volume"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  long long ni = vox(in_size), no = vox(out_size);
+  DevBuf di, dm, oi, om;
+  mirorr_status st = MIRORR_OK;
+  const float *pi = nullptr;
+  const uint8_t *pm = nullptr;
+  if (in_image) {
+    if ((st = upload(c, di, in_image, sizeof(float) * ni)) != MIRORR_OK) goto done;
+    pi = di.as<float>();
+    if ((st = oi.ensure(sizeof(float) * no)) != MIRORR_OK) goto done;
+  }
+  if (in_mask) {
+    if ((st = upload(c, dm, in_mask, ni)) != MIRORR_OK) goto done;
+    pm = dm.as<uint8_t>();
+    if ((st = om.ensure(no)) != MIRORR_OK) goto done;
+  }
+  {
+    ResampleMap m;
+    memcpy(m.C, C, sizeof(m.C));
+    memcpy(m.e, e, sizeof(m.e));
+    if (pi && (st = launch_resample(in_size, pi, nullptr, out_size, m, oi.as<float>(), nullptr,
+                                    c->stream)) != MIRORR_OK)
+      goto done;
+    if (pm && (st = launch_resample(in_size, nullptr, pm, out_size, m, nullptr, om.as<uint8_t>(),
+                                    c->stream)) != MIRORR_OK)
+      goto done;
+    if (pi && cudaMemcpyAsync(out_image, oi.ptr, sizeof(float) * no, cudaMemcpyDeviceToHost,
+                              c->stream) != cudaSuccess) { st = MIRORR_ECUDA; goto done; }
+    if (pm && cudaMemcpyAsync(out_mask, om.ptr, no, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) {
+      st = MIRORR_ECUDA;
+      goto done;
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+      set_error("resample failed: %s", cudaGetErrorString(cudaGetLastError()));
+      st = MIRORR_ECUDA;
+    }
+  }
+done:
+  cudaStreamSynchronize(c->stream);
+  di.release(); dm.release(); oi.release(); om.release();
+  return st;
+}
+
+// ---- LTS ---------------------------------------------------------------------------
+static mirorr_status lts_common(mirorr_ctx c, mirorr_transform *t, mirorr_transform *t12f,
+                                mirorr_transform *t12b, size_t n, const double *init,
+                                const double *moved, double lts_keep, int32_t *inner, bool sym) {
+  if (!c || !t || (n && (!init || !moved)) || (sym && (!t12f || !t12b))) {
+    set_error("null argument");
+    return MIRORR_EINVAL;
+  }
+  if (!(lts_keep > 0.0 && lts_keep <= 1.0)) { set_error("lts_keep must lie in (0, 1]"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  LtsState hs;
+  memset(&hs, 0, sizeof(hs));
+  if (!from_public(*t, hs.tfm)) { set_error("bad transform kind"); return MIRORR_EINVAL; }
+  hs.kind = t->kind;
+  hs.symmetric = sym ? 1 : 0;
+  hs.lts_keep = lts_keep;
+  if (sym) {
+    if (!from_public(*t12f, hs.t12f) || !from_public(*t12b, hs.t12b)) {
+      set_error("bad transform kind");
+      return MIRORR_EINVAL;
+    }
+  }
+  MB2_TRY(ensure_pts(c, (long long)n));
+  if (n) {
+    MB2_CUDA_TRY(cudaMemcpyAsync(c->pts_i.ptr, init, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    MB2_CUDA_TRY(cudaMemcpyAsync(c->pts_m.ptr, moved, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+  }
+  long long cnt[4] = {(long long)n, 0, 0, 0};
+  MB2_CUDA_TRY(cudaMemcpyAsync(c->counts.ptr, cnt, sizeof(cnt), cudaMemcpyHostToDevice, c->stream));
+  int it = 0;
+  long long used = 0;
+  MB2_TRY(lts_run(c->ltsw, hs, c->pts_i.as<double>(), c->pts_m.as<double>(),
+                  c->counts.as<long long>(), (long long)n, c->stream, &it, &used));
+  if (inner) *inner = it;
+  to_public(hs.tfm, *t);
+  if (sym) {
+    to_public(hs.t12f, *t12f);
+    to_public(hs.t12b, *t12b);
+  }
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_lts_classic(mirorr_ctx c, mirorr_transform *t, size_t n, const double *init,
+                                 const double *moved, double lts_keep, int32_t *inner) {
+  return lts_common(c, t, nullptr, nullptr, n, init, moved, lts_keep, inner, false);
+}
+
+mirorr_status mirorr_lts_symmetric(mirorr_ctx c, mirorr_transform *t, mirorr_transform *t12f,
+                                   mirorr_transform *t12b, size_t n, const double *init,
+                                   const double *moved, double lts_keep, int32_t *inner) {
+  return lts_common(c, t, t12f, t12b, n, init, moved, lts_keep, inner, true);
+}
+
+// ---- registration ----------------------------------------------------------------
+mirorr_status mirorr_reg_default_params(mirorr_reg_params *p) {
+  if (!p) { set_error("null argument"); return MIRORR_EINVAL; }
+  memset(p, 0, sizeof(*p));
+  p->symmetric = 1;
+  p->kind = KIND_RIGID;
+  p->levels = 0;
+  p->iterations = 5;
+  p->min_length = 32;
+  mirorr_bm_default_params(&p->bm);
+  p->bm.nhood_gap = 3;
+  p->bm.nhood_width = 7;
+  p->lts_keep = 0.5;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_register_device(mirorr_ctx c, const mirorr_geometry *fg, const float *fixed,
+                                     const uint8_t *fmask, const mirorr_geometry *mg,
+                                     const float *moving, const uint8_t *mmask,
+                                     const mirorr_reg_params *p, const mirorr_transform *init,
+                                     mirorr_transform *result, mirorr_reg_stats *stats) {
+  if (!c) { set_error("null argument"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  return register_impl(c, fg, fixed, fmask, mg, moving, mmask, p, init, result, stats);
+}
+
+mirorr_status mirorr_register(mirorr_ctx c, const mirorr_geometry *fg, const float *fixed,
+                              const uint8_t *fmask, const mirorr_geometry *mg, const float *moving,
+                              const uint8_t *mmask, const mirorr_reg_params *p,
+                              const mirorr_transform *init, mirorr_transform *result,
+                              mirorr_reg_stats *stats) {
+  if (!c || !fg || !mg || !fixed || !moving) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!valid_geom(fg) || !valid_geom(mg)) { set_error("invalid image geometry"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  auto t0 = std::chrono::steady_clock::now();
+  MB2_TRY(upload(c, c->up_f, fixed, sizeof(float) * vox(fg->size)));
+  MB2_TRY(upload(c, c->up_m, moving, sizeof(float) * vox(mg->size)));
+  const uint8_t *dfm = nullptr, *dmm = nullptr;
+  if (fmask) { MB2_TRY(upload(c, c->up_fm, fmask, vox(fg->size))); dfm = c->up_fm.as<uint8_t>(); }
+  if (mmask) { MB2_TRY(upload(c, c->up_mm, mmask, vox(mg->size))); dmm = c->up_mm.as<uint8_t>(); }
+  mirorr_status s = register_impl(c, fg, c->up_f.as<float>(), dfm, mg, c->up_m.as<float>(), dmm, p,
+                                  init, result, stats);
+  if (s == MIRORR_OK && stats)
+    stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return s;
+}
+
+mirorr_status mirorr_pyramid_schedule(const mirorr_geometry *fg, const mirorr_geometry *mg,
+                                      int32_t min_length, int32_t max_levels, int32_t *n_levels,
+                                      int32_t moving_factors[16][3], int32_t fixed_factors[16][3]) {
+  if (!fg || !mg || !n_levels || !moving_factors || !fixed_factors) {
+    set_error("null argument");
+    return MIRORR_EINVAL;
+  }
+  if (!valid_geom(fg) || !valid_geom(mg)) { set_error("invalid geometry"); return MIRORR_EINVAL; }
+  int sm[16][3], sf[16][3];
+  int n = pyramid_schedule(*fg, *mg, min_length > 0 ? min_length : 32, max_levels, sm, sf);
+  *n_levels = n;
+  for (int l = 0; l < n; ++l)
+    for (int d = 0; d < 3; ++d) { moving_factors[l][d] = sm[l][d]; fixed_factors[l][d] = sf[l][d]; }
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_pyramid_level(mirorr_ctx c, const mirorr_geometry *ig, const float *in,
+                                   const int32_t factors[3], mirorr_geometry *og, float *out,
+                                   size_t out_capacity) {
+  if (!c || !ig || !in || !factors || !og || !out) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!valid_geom(ig)) { set_error("invalid geometry"); return MIRORR_EINVAL; }
+  for (int d = 0; d < 3; ++d)
+    if (factors[d] < 1) { set_error("factors must be >= 1"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  mirorr_geometry g;
+  level_geometry(*ig, factors, g);
+  if ((size_t)vox(g.size) > out_capacity) {
+    *og = g;
+    set_error("output capacity too small");
+    return MIRORR_ERANGE;
+  }
+  MB2_TRY(upload(c, c->up_f, in, sizeof(float) * vox(ig->size)));
+  const float *lp = nullptr;
+  MB2_TRY(make_level(c, *ig, c->up_f.as<float>(), factors, g, c->lvl_f, &lp));
+  MB2_CUDA_TRY(cudaMemcpyAsync(out, lp, sizeof(float) * vox(g.size), cudaMemcpyDeviceToHost, c->stream));
+  MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *og = g;
+  return MIRORR_OK;
+}
+
+}  // extern "C"

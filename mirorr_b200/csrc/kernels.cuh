@@ -1,0 +1,99 @@
+// kernels.cuh -- host-side launchers of the mirorr_b200 CUDA kernels.
+#pragma once
+
+#include "common.cuh"
+#include "tfm.cuh"
+
+namespace mb2 {
+
+// Geometry of one block-matching call (both images share the grid of the
+// base image, as in itkBlockMatcher.txx:734-737).
+struct BmGeom {
+  int size[3];     // nx, ny, nz
+  int nb[3];       // blocks per axis
+  int st[3];       // origin of the block grid
+  int bw, bgap, ngap, nw;
+  long long nblocks;
+};
+
+bool bm_geometry(const int size[3], int bw, int bgap, int ngap, int nw, BmGeom &g);
+
+// Scratch needed by one matcher call.
+struct BmWork {
+  DevBuf stats;     // float2 per voxel of the search image: (mean, masked SS)
+  DevBuf var;       // double per block (variance selection)
+  DevBuf selected;  // uint8 per block
+  DevBuf select_state;
+  DevBuf hist;
+  DevBuf tiles;     // compaction tile counts/offsets
+};
+
+struct BmOut {
+  float *best;
+  float *second;
+  int32_t *match;   // linear voxel index of the match origin
+  uint8_t *status;  // 0 culled, 1 searched, 3 searched + kept
+};
+
+// Per-block points in mm (double3) for base and match blocks.
+struct PointGeom {
+  double origin[3];
+  double a[9];      // direction * diag(spacing), row-major
+  double half[3];   // spacing * block_width / 2
+};
+void point_geom(const double origin[3], const double spacing[3], const double direction[9],
+                int bw, PointGeom &pg);
+
+mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8_t *smask,
+                               float2 *stats, cudaStream_t s);
+mirorr_status launch_variance_selection(const BmGeom &g, const float *base, double keep,
+                                        BmWork &w, const uint8_t **selected_out,
+                                        cudaStream_t s);
+// ncc_count (optional): device counter incremented by the number of candidate
+// scores evaluated.
+mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmask,
+                         const float *search, const uint8_t *smask, const float2 *stats,
+                         const uint8_t *selected, const BmOut &out,
+                         unsigned long long *ncc_count, cudaStream_t s);
+// Post-filter (itkBlockMatcher.txx:884-918).  Marks kept blocks (status |= 2),
+// counts them into *count_dev and, when pts != nullptr, writes the kept
+// blocks' base / match points (mm) in raster order into pts_base / pts_match
+// starting at element `pts_offset`.
+// offset_dev (optional): device counter added to the output position, so a
+// second call can append after a first one without a host round trip.
+mirorr_status launch_postfilter(const BmGeom &g, const BmOut &out, BmWork &w,
+                                const PointGeom &pg, double *pts_base, double *pts_match,
+                                long long *count_dev, const long long *offset_dev,
+                                cudaStream_t s);
+
+// Linear resampling with an explicit affine index map (see mirorr_b200.h).
+struct ResampleMap {
+  double C[9];
+  double e[3];
+};
+mirorr_status launch_resample(const int in_size[3], const float *in, const uint8_t *in_mask,
+                              const int out_size[3], const ResampleMap &map, float *out,
+                              uint8_t *out_mask, cudaStream_t s);
+// Separable Gaussian smoothing along one axis (axis 0 = x).
+mirorr_status launch_smooth_axis(const int size[3], const float *in, float *out, int axis,
+                                 const double *w, int radius, cudaStream_t s);
+mirorr_status launch_fill_u8(uint8_t *p, long long n, uint8_t v, cudaStream_t s);
+
+// LTS fit on device (one cooperative launch for the whole inner loop).
+struct LtsWork {
+  DevBuf state;     // LtsState
+  DevBuf resid;     // double per point
+  DevBuf partial;   // per-CTA partial sums
+  DevBuf hist;      // radix histograms
+  DevBuf ctrl;      // barrier + select control
+  DevBuf cand;      // candidate keys
+  int max_ctas = 0;
+};
+// n_dev: two device counters whose sum is the number of point pairs; n_max is
+// an upper bound used for sizing.  Runs lts_begin / the inner loop /
+// lts_finish on host_state.
+mirorr_status lts_run(LtsWork &w, LtsState &host_state, const double *init_dev,
+                      const double *moved_dev, const long long *n_dev, long long n_max,
+                      cudaStream_t s, int *inner_iters, long long *n_used);
+
+}  // namespace mb2

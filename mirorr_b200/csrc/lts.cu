@@ -1,0 +1,402 @@
+// lts.cu -- the least-trimmed-squares fit on the device.
+//
+// One cooperative launch runs the whole inner loop of OptimizeTransform
+// (classic: itkMirorrRegistrationMethod.txx:785-999; symmetric:
+// itkSymMirorrRegistrationMethod.txx:771-1442).  Per inner iteration:
+//   residuals r_i (FP64) under the current final transform(s);
+//   the threshold r_nth: the maximum on the first iteration, otherwise the
+//     exact value of rank min(floor(f N), N-1) by an MSD radix select on the
+//     residual bit patterns (grid-wide histograms, then the few keys left in
+//     the chosen bucket are sorted in shared memory);
+//   subset {r_i <= r_nth}: barycentres, then the 6x6 second moments of the
+//     centred (initial, moved) pairs, reduced per CTA and summed in a fixed
+//     order (deterministic);
+//   the FP64 solve (affine normal equations / Horn quaternion, symmetric
+//     half-space algebra) in one thread, and the loop test.
+// CTAs meet at a software grid barrier whose wait is bounded (about one
+// second); a timeout raises an error flag and every CTA returns.
+#include <cooperative_groups.h>
+
+#include "kernels.cuh"
+
+namespace mb2 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kBins = 4096;
+constexpr int kCandMax = 2048;
+constexpr int kPartial = 32;  // doubles per CTA partial
+
+struct LtsCtl {
+  unsigned int bar_count;
+  unsigned int bar_gen;
+  int err;
+  int pad;
+  unsigned long long maxkey;
+  unsigned long long ncand;
+};
+
+struct LtsArgs {
+  LtsState *state;
+  const double *init;
+  const double *moved;
+  const long long *n_dev;
+  double *resid;
+  double *partial;        // gridDim.x * kPartial
+  unsigned int *hist;     // 3 * kBins
+  unsigned long long *cand;
+  LtsCtl *ctl;
+};
+
+__device__ bool grid_sync(LtsCtl *ctl) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *genp = &ctl->bar_gen;
+    volatile int *errp = &ctl->err;
+    unsigned int gen = *genp;
+    __threadfence();
+    unsigned int arrived = atomicAdd(&ctl->bar_count, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(&ctl->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&ctl->bar_gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*genp == gen && *errp == 0) {
+        __nanosleep(100);
+        if (++spins > (1LL << 23)) {
+          atomicExch(&ctl->err, 1);
+          break;
+        }
+      }
+    }
+    __threadfence();
+    s_ok = (*errp == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__device__ inline void load_cg(void *dst, const void *src, int bytes) {
+  const unsigned long long *s = static_cast<const unsigned long long *>(src);
+  unsigned long long *d = static_cast<unsigned long long *>(dst);
+  for (int i = threadIdx.x; i < bytes / 8; i += blockDim.x) d[i] = __ldcg(s + i);
+}
+
+__device__ inline double block_sum(double v, double *red) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += red[w];
+  return r;  // valid in thread 0
+}
+
+__device__ inline double residual(const LtsState &s, const double *x, const double *y) {
+  double p[3], q[3];
+  tfm_apply(s.fin, x, p);
+  if (s.symmetric) {
+    tfm_apply(s.finb, y, q);
+  } else {
+    q[0] = y[0]; q[1] = y[1]; q[2] = y[2];
+  }
+  double r = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    double d = p[i] - q[i];
+    r += d * d;
+  }
+  return r;
+}
+
+__global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
+  __shared__ __align__(16) LtsState s;
+  __shared__ unsigned int h[kBins];
+  __shared__ unsigned long long ck[kCandMax];
+  __shared__ double red[32];
+  __shared__ double s_nth;
+  __shared__ unsigned long long s_key;
+  const long long n = __ldcg(&a.n_dev[0]) + __ldcg(&a.n_dev[1]);
+  const long long gstride = (long long)gridDim.x * blockDim.x;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+
+  for (int guard = 0; guard < 200; ++guard) {
+    load_cg(&s, a.state, sizeof(LtsState));
+    __syncthreads();
+    if (!s.running || n <= 0) break;
+    const bool first = s.fraction > 0.99999;
+    // ---- residuals (+ max or first histogram) ----------------------------
+    for (int i = threadIdx.x; i < kBins; i += blockDim.x) h[i] = 0;
+    if (blockIdx.x == 0)
+      for (int i = threadIdx.x; i < kBins; i += blockDim.x) {
+        a.hist[kBins + i] = 0;  // next two passes' buffers
+      }
+    __syncthreads();
+    unsigned long long kmax = 0;
+    for (long long i = gtid; i < n; i += gstride) {
+      double r = residual(s, a.init + 3 * i, a.moved + 3 * i);
+      a.resid[i] = r;
+      unsigned long long key = (unsigned long long)__double_as_longlong(r);
+      if (first) {
+        if (key > kmax) kmax = key;
+      } else {
+        atomicAdd(&h[(unsigned)(key >> 52) & (kBins - 1)], 1u);
+      }
+    }
+    if (first) {
+      for (int off = 16; off > 0; off >>= 1) {
+        unsigned long long o = __shfl_down_sync(0xffffffffu, kmax, off);
+        if (o > kmax) kmax = o;
+      }
+      if ((threadIdx.x & 31) == 0 && kmax) atomicMax(&a.ctl->maxkey, kmax);
+    } else {
+      __syncthreads();
+      for (int i = threadIdx.x; i < kBins; i += blockDim.x)
+        if (h[i]) atomicAdd(&a.hist[i], h[i]);
+    }
+    if (!grid_sync(a.ctl)) return;
+    double nth;
+    if (first) {
+      if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->maxkey);
+      __syncthreads();
+      nth = __longlong_as_double((long long)s_key);
+    } else {
+      // ---- radix select of rank k -----------------------------------------
+      unsigned long long k = (unsigned long long)(unsigned int)(s.fraction * (double)n);
+      if (k > (unsigned long long)(n - 1)) k = n - 1;
+      unsigned long long prefix = 0, mask = 0;
+      int shift = 52, bits = 12, pass = 0;
+      unsigned long long bucket = 0;
+      while (true) {
+        // every CTA scans the global histogram of this pass identically
+        const unsigned int *gh = a.hist + (pass % 3) * kBins;
+        __syncthreads();
+        for (int i = threadIdx.x; i < kBins; i += blockDim.x) h[i] = __ldcg(&gh[i]);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          unsigned long long cum = 0;
+          int d = 0;
+          int nb = 1 << bits;
+          for (; d < nb; ++d) {
+            if (cum + h[d] > k) break;
+            cum += h[d];
+          }
+          if (d >= nb) d = nb - 1;
+          s_key = ((unsigned long long)d << 32) | (unsigned long long)h[d];
+          red[0] = (double)cum;
+        }
+        __syncthreads();
+        int d = (int)(s_key >> 32);
+        bucket = s_key & 0xffffffffULL;
+        k -= (unsigned long long)red[0];
+        prefix |= (unsigned long long)d << shift;
+        mask |= ((1ULL << bits) - 1ULL) << shift;
+        __syncthreads();
+        if (bucket <= (unsigned long long)kCandMax || shift == 0) break;
+        // next pass
+        ++pass;
+        bits = shift >= 12 ? 12 : shift;
+        shift -= bits;
+        if (blockIdx.x == 0) {
+          unsigned int *zb = a.hist + ((pass + 1) % 3) * kBins;
+          for (int i = threadIdx.x; i < kBins; i += blockDim.x) zb[i] = 0;
+        }
+        for (int i = threadIdx.x; i < kBins; i += blockDim.x) h[i] = 0;
+        __syncthreads();
+        for (long long i = gtid; i < n; i += gstride) {
+          unsigned long long key = (unsigned long long)__double_as_longlong(a.resid[i]);
+          if ((key & mask) == prefix)
+            atomicAdd(&h[(unsigned)(key >> shift) & ((1u << bits) - 1u)], 1u);
+        }
+        __syncthreads();
+        unsigned int *gh2 = a.hist + (pass % 3) * kBins;
+        for (int i = threadIdx.x; i < kBins; i += blockDim.x)
+          if (h[i]) atomicAdd(&gh2[i], h[i]);
+        if (!grid_sync(a.ctl)) return;
+      }
+      // ---- gather the bucket's keys and pick rank k -----------------------
+      for (long long i = gtid; i < n; i += gstride) {
+        unsigned long long key = (unsigned long long)__double_as_longlong(a.resid[i]);
+        if ((key & mask) == prefix) {
+          unsigned long long pos = atomicAdd(&a.ctl->ncand, 1ULL);
+          if (pos < (unsigned long long)kCandMax) a.cand[pos] = key;
+        }
+      }
+      if (!grid_sync(a.ctl)) return;
+      if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->ncand);
+      __syncthreads();
+      int nc = (int)(s_key < (unsigned long long)kCandMax ? s_key : kCandMax);
+      for (int i = threadIdx.x; i < kCandMax; i += blockDim.x)
+        ck[i] = (i < nc) ? __ldcg(&a.cand[i]) : ~0ULL;
+      __syncthreads();
+      // bitonic sort of kCandMax keys
+      for (int size = 2; size <= kCandMax; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          for (int i = threadIdx.x; i < kCandMax; i += blockDim.x) {
+            int j = i ^ stride;
+            if (j > i) {
+              bool up = (i & size) == 0;
+              unsigned long long x = ck[i], y = ck[j];
+              if ((x > y) == up) { ck[i] = y; ck[j] = x; }
+            }
+          }
+          __syncthreads();
+        }
+      if (threadIdx.x == 0) s_nth = __longlong_as_double((long long)ck[k < (unsigned long long)nc ? k : (nc > 0 ? nc - 1 : 0)]);
+      __syncthreads();
+      nth = s_nth;
+    }
+    // ---- subset barycentres ---------------------------------------------
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (long long i = gtid; i < n; i += gstride) {
+      if (a.resid[i] <= nth) {
+        acc[0] += 1.0;
+        for (int c = 0; c < 3; ++c) {
+          acc[1 + c] += a.init[3 * i + c];
+          acc[4 + c] += a.moved[3 * i + c];
+        }
+      }
+    }
+    for (int c = 0; c < 7; ++c) {
+      double v = block_sum(acc[c], red);
+      if (threadIdx.x == 0) a.partial[(long long)blockIdx.x * kPartial + c] = v;
+    }
+    if (!grid_sync(a.ctl)) return;
+    __shared__ double s_mean[7];
+    if (threadIdx.x < 7) {
+      double t = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(&a.partial[(long long)b * kPartial + threadIdx.x]);
+      s_mean[threadIdx.x] = t;
+    }
+    __syncthreads();
+    const double cnt = s_mean[0];
+    double mi[3], mm[3];
+    for (int c = 0; c < 3; ++c) { mi[c] = s_mean[1 + c] / cnt; mm[c] = s_mean[4 + c] / cnt; }
+    // ---- centred second moments (21 unique of the 6x6) -------------------
+    double z2[21];
+    for (int q = 0; q < 21; ++q) z2[q] = 0.0;
+    for (long long i = gtid; i < n; i += gstride) {
+      if (a.resid[i] <= nth) {
+        double z[6];
+        for (int c = 0; c < 3; ++c) {
+          z[c] = a.init[3 * i + c] - mi[c];
+          z[3 + c] = a.moved[3 * i + c] - mm[c];
+        }
+        int q = 0;
+        for (int r = 0; r < 6; ++r)
+          for (int c = r; c < 6; ++c) z2[q++] += z[r] * z[c];
+      }
+    }
+    __syncthreads();
+    for (int q = 0; q < 21; ++q) {
+      double v = block_sum(z2[q], red);
+      if (threadIdx.x == 0) a.partial[(long long)blockIdx.x * kPartial + 8 + q] = v;
+    }
+    if (!grid_sync(a.ctl)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      LtsMoments mo;
+      mo.n = cnt;
+      for (int c = 0; c < 3; ++c) { mo.mean_i[c] = mi[c]; mo.mean_m[c] = mm[c]; }
+      double zz[21];
+      for (int q = 0; q < 21; ++q) {
+        double t = 0.0;
+        for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(&a.partial[(long long)b * kPartial + 8 + q]);
+        zz[q] = t;
+      }
+      int q = 0;
+      for (int r = 0; r < 6; ++r)
+        for (int c = r; c < 6; ++c) { mo.Z[6 * r + c] = zz[q]; mo.Z[6 * c + r] = zz[q]; ++q; }
+      if (s.symmetric) lts_symmetric_step(s, mo);
+      else lts_classic_step(s, mo);
+      s.fraction = s.lts_keep;
+      s.iter += 1;
+      s.running = lts_continue(s) ? 1 : 0;
+      if (s.iter > 101) s.running = 0;
+      // reset select scratch for the next iteration
+      a.ctl->maxkey = 0;
+      a.ctl->ncand = 0;
+      *a.state = s;
+      __threadfence();
+    }
+    if (blockIdx.x == 0) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < kBins; i += blockDim.x) a.hist[i] = 0;
+    }
+    if (!grid_sync(a.ctl)) return;
+  }
+}
+
+}  // namespace
+
+mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const double *moved_dev,
+                      const long long *n_dev, long long n, cudaStream_t st, int *inner_iters,
+                      long long *n_used) {
+  lts_begin(hs);
+  if (n <= 0) {
+    lts_finish(hs);
+    if (inner_iters) *inner_iters = 0;
+    if (n_used) *n_used = 0;
+    return MIRORR_OK;
+  }
+  int dev = 0;
+  MB2_CUDA_TRY(cudaGetDevice(&dev));
+  if (w.max_ctas == 0) {
+    int sms = 0, per = 0, coop = 0;
+    MB2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MB2_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) {
+      set_error("device does not support cooperative launches");
+      return MIRORR_ECUDA;
+    }
+    MB2_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lts_kernel, kThreads, 0));
+    if (per < 1) {
+      set_error("LTS kernel cannot be resident");
+      return MIRORR_ECUDA;
+    }
+    w.max_ctas = sms * (per > 1 ? 1 : per);
+  }
+  long long want = (n + 4 * kThreads - 1) / (4 * kThreads);
+  int grid = (int)(want < 1 ? 1 : (want > w.max_ctas ? w.max_ctas : want));
+  MB2_TRY(w.state.ensure(sizeof(LtsState)));
+  MB2_TRY(w.resid.ensure(sizeof(double) * n));
+  MB2_TRY(w.partial.ensure(sizeof(double) * kPartial * (size_t)grid));
+  MB2_TRY(w.hist.ensure(sizeof(unsigned int) * 3 * kBins));
+  MB2_TRY(w.ctrl.ensure(sizeof(LtsCtl)));
+  MB2_TRY(w.cand.ensure(sizeof(unsigned long long) * kCandMax));
+  MB2_CUDA_TRY(cudaMemcpyAsync(w.state.ptr, &hs, sizeof(LtsState), cudaMemcpyHostToDevice, st));
+  MB2_CUDA_TRY(cudaMemsetAsync(w.hist.ptr, 0, sizeof(unsigned int) * 3 * kBins, st));
+  MB2_CUDA_TRY(cudaMemsetAsync(w.ctrl.ptr, 0, sizeof(LtsCtl), st));
+  LtsArgs a;
+  a.state = w.state.as<LtsState>();
+  a.init = init_dev;
+  a.moved = moved_dev;
+  a.n_dev = n_dev;
+  a.resid = w.resid.as<double>();
+  a.partial = w.partial.as<double>();
+  a.hist = w.hist.as<unsigned int>();
+  a.cand = w.cand.as<unsigned long long>();
+  a.ctl = w.ctrl.as<LtsCtl>();
+  void *args[] = {&a};
+  MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)lts_kernel, dim3(grid), dim3(kThreads), args, 0, st));
+  ++g_launches;
+  LtsCtl ctl;
+  long long nn[2] = {0, 0};
+  MB2_CUDA_TRY(cudaMemcpyAsync(&hs, w.state.ptr, sizeof(LtsState), cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(&ctl, w.ctrl.ptr, sizeof(LtsCtl), cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(nn, n_dev, sizeof(nn), cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaStreamSynchronize(st));
+  if (n_used) *n_used = nn[0] + nn[1];
+  if (ctl.err) {
+    set_error("LTS grid barrier timed out");
+    return MIRORR_ETIMEOUT;
+  }
+  if (inner_iters) *inner_iters = hs.iter;
+  lts_finish(hs);
+  return MIRORR_OK;
+}
+
+}  // namespace mb2

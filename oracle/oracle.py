@@ -888,14 +888,16 @@ def pyramid_schedule(fixed_size, moving_size, fixed_spacing, moving_spacing, min
 
 def gaussian_weights(factor):
     """Discrete Gaussian of sigma = factor / 2 voxels, radius ceil(3 sigma),
-    normalised to unit sum (FP64)."""
+    normalised by the sequential sum of its taps (FP64, libm exp)."""
     if factor <= 1:
         return np.array([1.0])
     sigma = factor / 2.0
     r = int(math.ceil(3.0 * sigma))
-    k = np.arange(-r, r + 1, dtype=np.float64)
-    w = np.exp(-(k * k) / (2.0 * sigma * sigma))
-    return w / w.sum()
+    w = [math.exp(-(float(k) * float(k)) / (2.0 * sigma * sigma)) for k in range(-r, r + 1)]
+    s = 0.0
+    for v in w:
+        s += v
+    return np.array([v / s for v in w], dtype=np.float64)
 
 
 def smooth_axis(vol: np.ndarray, w: np.ndarray, axis: int) -> np.ndarray:
