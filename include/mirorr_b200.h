@@ -197,6 +197,8 @@ typedef struct mirorr_reg_stats {
   int64_t block_ncc_evaluated; /* candidate scores computed (all levels, all calls) */
   int64_t matcher_calls;
   double seconds;              /* host wall time of the call */
+  int64_t h2d_bytes;           /* host -> device bytes copied by the call */
+  int64_t d2h_bytes;           /* device -> host bytes copied by the call */
 } mirorr_reg_stats;
 
 MIRORR_API mirorr_status mirorr_reg_default_params(mirorr_reg_params *p);
@@ -240,8 +242,21 @@ MIRORR_API mirorr_status mirorr_pyramid_level(mirorr_ctx ctx, const mirorr_geome
  * context stream), milliseconds: [0] box statistics, [1] variance selection,
  * [2] NCC search, [3] post-filter + compaction. */
 MIRORR_API mirorr_status mirorr_bm_last_timings(mirorr_matcher m, float ms[4]);
+/* Diagnostics of the last GetOffsets: [0] candidates re-scored in FP64 by the
+ * exact refinement, [1] blocks re-scored entirely in FP64 (refinement list
+ * overflow), [2] kept blocks, [3] blocks of the grid. */
+MIRORR_API mirorr_status mirorr_bm_last_diagnostics(mirorr_matcher m, int64_t out[4]);
 /* Count of kernels launched by this context since creation. */
 MIRORR_API int64_t mirorr_ctx_kernel_launches(mirorr_ctx ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events against the library's. */
+MIRORR_API void *mirorr_ctx_stream(mirorr_ctx ctx);
+/* Per-stage timing of the matcher calls made by registrations: when enabled,
+ * CUDA events bracket each stage; mirorr_ctx_stage_times returns the
+ * accumulated milliseconds of [box statistics, variance selection, NCC
+ * search, post-filter] and the number of matcher calls, and resets them. */
+MIRORR_API mirorr_status mirorr_ctx_set_profiling(mirorr_ctx ctx, int32_t on);
+MIRORR_API mirorr_status mirorr_ctx_stage_times(mirorr_ctx ctx, double ms[4], int64_t *calls);
 
 #ifdef __cplusplus
 }

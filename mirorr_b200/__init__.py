@@ -18,9 +18,11 @@ MirorrError.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes
 import os
-from dataclasses import dataclass, field
+import sys
+import weakref
 
 import numpy as np
 
@@ -106,10 +108,21 @@ class RegParams(ctypes.Structure):
 class RegStats(ctypes.Structure):
     _fields_ = [("levels_run", ctypes.c_int32), ("iterations_run", ctypes.c_int32 * 16),
                 ("block_ncc_evaluated", ctypes.c_int64), ("matcher_calls", ctypes.c_int64),
-                ("seconds", ctypes.c_double)]
+                ("seconds", ctypes.c_double), ("h2d_bytes", ctypes.c_int64),
+                ("d2h_bytes", ctypes.c_int64)]
 
 
 _lib = None
+_live_matchers = weakref.WeakSet()
+_live_contexts = weakref.WeakSet()
+
+
+@atexit.register
+def _close_all():
+    for m in list(_live_matchers):
+        m.close()
+    for c in list(_live_contexts):
+        c.close()
 
 
 def lib():
@@ -144,6 +157,7 @@ def lib():
         "mirorr_bm_get_offsets": [vp, ctypes.c_size_t, vp, vp, P(ctypes.c_size_t)],
         "mirorr_bm_block_results": [vp, ctypes.c_size_t, vp, vp, vp, vp, P(ctypes.c_size_t)],
         "mirorr_bm_last_timings": [vp, vp],
+        "mirorr_bm_last_diagnostics": [vp, vp],
         "mirorr_resample": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
         "mirorr_resample_map": [P(Geometry), P(Geometry), vp, vp, vp, vp],
         "mirorr_lts_classic": [vp, P(Transform), ctypes.c_size_t, vp, vp, ctypes.c_double,
@@ -168,6 +182,12 @@ def lib():
     L.mirorr_abi_version.restype = ctypes.c_int32
     L.mirorr_ctx_kernel_launches.restype = ctypes.c_int64
     L.mirorr_ctx_kernel_launches.argtypes = [vp]
+    L.mirorr_ctx_stream.restype = vp
+    L.mirorr_ctx_stream.argtypes = [vp]
+    L.mirorr_ctx_set_profiling.restype = st
+    L.mirorr_ctx_set_profiling.argtypes = [vp, ctypes.c_int32]
+    L.mirorr_ctx_stage_times.restype = st
+    L.mirorr_ctx_stage_times.argtypes = [vp, vp, P(ctypes.c_int64)]
     _lib = L
     return L
 
@@ -196,6 +216,7 @@ class Context:
     def __init__(self, device: int = 0):
         self._h = ctypes.c_void_p()
         _check(lib().mirorr_ctx_create(int(device), ctypes.byref(self._h)))
+        _live_contexts.add(self)
 
     @property
     def handle(self):
@@ -204,12 +225,31 @@ class Context:
     def kernel_launches(self) -> int:
         return int(lib().mirorr_ctx_kernel_launches(self._h))
 
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer."""
+        return int(lib().mirorr_ctx_stream(self._h) or 0)
+
+    def set_profiling(self, on: bool):
+        _check(lib().mirorr_ctx_set_profiling(self._h, 1 if on else 0))
+
+    def stage_times(self):
+        """(ms[box_stats, selection, ncc, postfilter], matcher calls) since the last read."""
+        ms = np.zeros(4, np.float64)
+        calls = ctypes.c_int64(0)
+        _check(lib().mirorr_ctx_stage_times(self._h, _ptr(ms), ctypes.byref(calls)))
+        return ms, calls.value
+
     def close(self):
         if self._h:
+            for m in list(_live_matchers):
+                if m.ctx is self:
+                    m.close()
             lib().mirorr_ctx_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:
@@ -225,7 +265,7 @@ class BlockMatcher:
         _check(lib().mirorr_bm_create(ctx.handle, ctypes.byref(self._h)))
         self._p = BMParams()
         _check(lib().mirorr_bm_default_params(ctypes.byref(self._p)))
-        self._keep = []  # host arrays referenced by device-pointer setters
+        _live_matchers.add(self)
 
     # parameters (itkAbstractBlockMatcher.h:101-127)
     def _apply(self):
@@ -335,12 +375,20 @@ class BlockMatcher:
         _check(lib().mirorr_bm_last_timings(self._h, _ptr(ms)))
         return ms
 
+    def LastDiagnostics(self):
+        """(FP64-refined candidates, fully re-scored blocks, kept blocks, grid blocks)."""
+        d = np.zeros(4, np.int64)
+        _check(lib().mirorr_bm_last_diagnostics(self._h, _ptr(d)))
+        return tuple(int(v) for v in d)
+
     def close(self):
         if self._h:
             lib().mirorr_bm_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:

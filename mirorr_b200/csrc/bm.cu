@@ -9,11 +9,7 @@
 //   2. selection:   (optional) dead-code variance cut-off of
 //                   itkBlockMatcher.txx:664-719, FP64 per block, exact k-th
 //                   value by a device radix select.
-//   3. ncc:         one CTA per block: base-block statistics in FP64, the
-//                   clipped +-R window staged in shared memory, every
-//                   candidate's squared NCC in FP32, best / second-best /
-//                   argmax with the reference's raster-order tie rule
-//                   (itkBlockMatcher.txx:788-834).
+//   3. ncc:         the search itself (ncc.cu).
 //   4. postfilter:  best > 1e-7 && |best - second| > 1e-4 (itkBlockMatcher.txx:884-918),
 //                   deterministic raster-order compaction and block -> mm points
 //                   (itkAbstractBlockMatcher.h:271-287).
@@ -238,275 +234,6 @@ mirorr_status launch_variance_selection(const BmGeom &g, const float *base, doub
   select_flags_kernel<<<(unsigned)blocks, threads, 0, s>>>(var, n, ctl, w.selected.as<uint8_t>());
   MB2_LAUNCH_CHECK();
   *selected_out = w.selected.as<uint8_t>();
-  return MIRORR_OK;
-}
-
-// ---------------------------------------------------------------------------
-// 3. NCC search
-// ---------------------------------------------------------------------------
-struct NccArgs {
-  const float *base;
-  const uint8_t *bmask;
-  const float *search;
-  const uint8_t *smask;
-  const float2 *stats;
-  const uint8_t *selected;
-  int nx, ny, nz;
-  int nbx, nby, nbz;
-  int stx, sty, stz;
-  int G, g, W;
-  int emax;  // max window extent per axis
-  float *best;
-  float *second;
-  int32_t *match;
-  uint8_t *status;
-  unsigned long long *ncc_count;
-};
-
-struct Top2 {
-  float best;
-  float second;
-  int idx;
-};
-
-__device__ inline Top2 merge_top2(Top2 a, Top2 b) {
-  bool bw = (b.best > a.best) || (b.best == a.best && b.idx < a.idx);
-  Top2 w = bw ? b : a, l = bw ? a : b;
-  Top2 r;
-  r.best = w.best;
-  r.idx = w.idx;
-  float s = w.second;
-  if (l.best > s) s = l.best;
-  if (l.second > s) s = l.second;
-  r.second = s;
-  return r;
-}
-
-__device__ inline void window_axis(int o, int S, int W, int g, int bw, int &s, int &n) {
-  int st = o - (W / 2) * g;
-  int en = st + W * g;
-  int lim = S - bw + 1;
-  if (st < 0) st += ((-st + g - 1) / g) * g;
-  if (en > lim) en -= ((en - lim + g - 1) / g) * g;
-  s = st;
-  n = (en > st) ? (en - st + g - 1) / g : 0;
-}
-
-template <int BW>
-__global__ void __launch_bounds__(128) ncc_kernel(NccArgs a) {
-  constexpr int B = BW * BW * BW;
-  extern __shared__ __align__(16) unsigned char smem[];
-  float *xt = reinterpret_cast<float *>(smem);                 // B
-  float *ywin = xt + B;                                          // emax^3
-  uint8_t *mbv = reinterpret_cast<uint8_t *>(ywin + a.emax * a.emax * a.emax);  // B
-  uint8_t *mwin = mbv + B;                                       // emax^3
-  __shared__ double s_mean;
-  __shared__ float s_sxx, s_sxt;
-  __shared__ int s_mball;
-  __shared__ Top2 s_red[4];
-
-  const long long b = blockIdx.x;
-  const int tid = threadIdx.x;
-  const int bx = (int)(b % a.nbx), by = (int)((b / a.nbx) % a.nby),
-            bz = (int)(b / ((long long)a.nbx * a.nby));
-  const int ox = a.stx + bx * a.G, oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
-  const long long obase = ((long long)oz * a.ny + oy) * a.nx + ox;
-
-  if (a.selected && !a.selected[b]) {
-    if (tid == 0) {
-      a.best[b] = -3.f;
-      a.second[b] = -3.f;
-      a.match[b] = (int32_t)obase;
-      a.status[b] = 0;
-    }
-    return;
-  }
-  int sx, sy, sz, cx_n, cy_n, cz_n;
-  window_axis(ox, a.nx, a.W, a.g, BW, sx, cx_n);
-  window_axis(oy, a.ny, a.W, a.g, BW, sy, cy_n);
-  window_axis(oz, a.nz, a.W, a.g, BW, sz, cz_n);
-  const int ex = (cx_n - 1) * a.g + BW, ey = (cy_n - 1) * a.g + BW, ez = (cz_n - 1) * a.g + BW;
-  if (cx_n <= 0 || cy_n <= 0 || cz_n <= 0) {
-    if (tid == 0) {
-      a.best[b] = -3.f;
-      a.second[b] = -3.f;
-      a.match[b] = (int32_t)obase;
-      a.status[b] = 1;
-    }
-    return;
-  }
-
-  // base block
-  for (int v = tid; v < B; v += blockDim.x) {
-    int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
-    long long q = obase + ((long long)vz * a.ny + vy) * a.nx + vx;
-    xt[v] = __ldg(&a.base[q]);
-    mbv[v] = __ldg(&a.bmask[q]);
-  }
-  // search window
-  const long long wbase = ((long long)sz * a.ny + sy) * a.nx + sx;
-  const int nwin = ex * ey * ez;
-  int all_in = 1;
-  for (int i = tid; i < nwin; i += blockDim.x) {
-    int wx = i % ex, wy = (i / ex) % ey, wz = i / (ex * ey);
-    long long q = wbase + ((long long)wz * a.ny + wy) * a.nx + wx;
-    ywin[i] = __ldg(&a.search[q]);
-    uint8_t m = __ldg(&a.smask[q]);
-    mwin[i] = m;
-    if (!m) all_in = 0;
-  }
-  int ms_all = __syncthreads_and(all_in);
-  if (tid == 0) {
-    // meanBase / baseSumSqr of normalizedCorrelation, FP64 in raster order
-    double sum = 0.0;
-    int mball = 1;
-    for (int v = 0; v < B; ++v) {
-      sum = __dadd_rn(sum, (double)xt[v]);
-      if (!mbv[v]) mball = 0;
-    }
-    double mean = __ddiv_rn(sum, (double)B);
-    double sxx = 0.0, sxt = 0.0;
-    for (int v = 0; v < B; ++v) {
-      if (mbv[v]) {
-        double d = __dsub_rn((double)xt[v], mean);
-        sxx = __dadd_rn(sxx, __dmul_rn(d, d));
-        sxt = __dadd_rn(sxt, d);
-      }
-    }
-    s_mean = mean;
-    s_sxx = (float)sxx;
-    s_sxt = (float)sxt;
-    s_mball = mball;
-  }
-  __syncthreads();
-  {
-    const double mean = s_mean;
-    for (int v = tid; v < B; v += blockDim.x) xt[v] = (float)__dsub_rn((double)xt[v], mean);
-  }
-  __syncthreads();
-  const bool fast = s_mball && ms_all;
-  const float sxx_f = s_sxx, sxt_f = s_sxt;
-
-  Top2 loc{-3.f, -3.f, 0x7fffffff};
-  const int nc = cx_n * cy_n * cz_n;
-  for (int c = tid; c < nc; c += blockDim.x) {
-    int cx = c % cx_n, cy = (c / cx_n) % cy_n, cz = c / (cx_n * cy_n);
-    int px = sx + cx * a.g, py = sy + cy * a.g, pz = sz + cz * a.g;
-    float2 st = __ldg(&a.stats[((long long)pz * a.ny + py) * a.nx + px]);
-    const float mu = st.x;
-    const int woff = ((cz * a.g) * ey + cy * a.g) * ex + cx * a.g;
-    float sxy = 0.f, sxx, syy;
-    if (fast) {
-      float acc = 0.f;
-#pragma unroll
-      for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-        for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-          for (int vx = 0; vx < BW; ++vx)
-            acc = fmaf(xt[(vz * BW + vy) * BW + vx], ywin[woff + (vz * ey + vy) * ex + vx], acc);
-      sxy = acc - mu * sxt_f;
-      sxx = sxx_f;
-      syy = st.y;
-    } else {
-      float ax = 0.f, ay = 0.f;
-#pragma unroll
-      for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-        for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-          for (int vx = 0; vx < BW; ++vx) {
-            int v = (vz * BW + vy) * BW + vx;
-            int wi = woff + (vz * ey + vy) * ex + vx;
-            if (mbv[v] && mwin[wi]) {
-              float xv = xt[v];
-              float d = ywin[wi] - mu;
-              sxy = fmaf(xv, d, sxy);
-              ax = fmaf(xv, xv, ax);
-              ay = fmaf(d, d, ay);
-            }
-          }
-      sxx = ax;
-      syy = s_mball ? st.y : ay;
-      if (!s_mball) syy = ay;
-    }
-    float score = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
-    if (score > loc.best) {
-      loc.second = loc.best;
-      loc.best = score;
-      loc.idx = c;
-    } else if (score > loc.second) {
-      loc.second = score;
-    }
-  }
-  // reduce top-2 across the CTA
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    Top2 o;
-    o.best = __shfl_down_sync(0xffffffffu, loc.best, off);
-    o.second = __shfl_down_sync(0xffffffffu, loc.second, off);
-    o.idx = __shfl_down_sync(0xffffffffu, loc.idx, off);
-    loc = merge_top2(loc, o);
-  }
-  if ((tid & 31) == 0) s_red[tid >> 5] = loc;
-  __syncthreads();
-  if (tid == 0) {
-    Top2 r = s_red[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = merge_top2(r, s_red[w]);
-    int c = r.idx;
-    if (c == 0x7fffffff) c = 0;
-    int cx = c % cx_n, cy = (c / cx_n) % cy_n, cz = c / (cx_n * cy_n);
-    int px = sx + cx * a.g, py = sy + cy * a.g, pz = sz + cz * a.g;
-    a.best[b] = r.best;
-    a.second[b] = r.second;
-    a.match[b] = (int32_t)(((long long)pz * a.ny + py) * a.nx + px);
-    a.status[b] = 1;
-    if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)nc);
-  }
-}
-
-mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmask,
-                         const float *search, const uint8_t *smask, const float2 *stats,
-                         const uint8_t *selected, const BmOut &out,
-                         unsigned long long *ncc_count, cudaStream_t s) {
-  NccArgs a;
-  a.base = base; a.bmask = bmask; a.search = search; a.smask = smask; a.stats = stats;
-  a.selected = selected;
-  a.nx = g.size[0]; a.ny = g.size[1]; a.nz = g.size[2];
-  a.nbx = g.nb[0]; a.nby = g.nb[1]; a.nbz = g.nb[2];
-  a.stx = g.st[0]; a.sty = g.st[1]; a.stz = g.st[2];
-  a.G = g.ngap; a.g = g.bgap; a.W = g.nw;
-  a.emax = (g.nw - 1) * g.bgap + g.bw;
-  a.best = out.best; a.second = out.second; a.match = out.match; a.status = out.status;
-  a.ncc_count = ncc_count;
-  int B = g.bw * g.bw * g.bw;
-  size_t smem = sizeof(float) * (B + (size_t)a.emax * a.emax * a.emax) + B +
-                (size_t)a.emax * a.emax * a.emax;
-  if (smem > 200 * 1024) {
-    set_error("search window too large: (nhood_width-1)*block_gap+block_width = %d", a.emax);
-    return MIRORR_EINVAL;
-  }
-  if (g.nblocks > 0x7fffffffLL) {
-    set_error("too many blocks (%lld)", g.nblocks);
-    return MIRORR_EINVAL;
-  }
-  unsigned grid = (unsigned)g.nblocks;
-  switch (g.bw) {
-#define CASE(BW)                                                                       \
-  case BW:                                                                             \
-    if (smem > 48 * 1024)                                                              \
-      MB2_CUDA_TRY(cudaFuncSetAttribute(ncc_kernel<BW>,                                \
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                        (int)smem));                                   \
-    ncc_kernel<BW><<<grid, 128, smem, s>>>(a);                                         \
-    break;
-    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8)
-#undef CASE
-    default:
-      set_error("block width %d not supported (1..8)", g.bw);
-      return MIRORR_EINVAL;
-  }
-  MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
 

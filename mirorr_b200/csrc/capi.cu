@@ -252,7 +252,7 @@ mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall
   if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
   BmOut out{best.as<float>(), second.as<float>(), match.as<int32_t>(), status.as<uint8_t>()};
   MB2_TRY(launch_ncc(g, mc.base, mc.bmask, mc.search, mc.smask, c->bmw.stats.as<float2>(), sel,
-                     out, c->ncc_count.as<unsigned long long>(), s));
+                     out, c->bmw, c->ncc_count.as<unsigned long long>(), s));
   if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[3], s));
   PointGeom pg;
   point_geom(mc.point_geom.origin, mc.point_geom.spacing, mc.point_geom.direction,
@@ -451,6 +451,10 @@ mirorr_status run_lts(RegRun &r, LtsState &hs, long long nmax, long long *n_used
   mirorr_ctx c = r.c;
   MB2_TRY(lts_run(c->ltsw, hs, c->pts_i.as<double>(), c->pts_m.as<double>(),
                   c->counts.as<long long>(), nmax, c->stream, &inner, n_used));
+  if (r.stats) {
+    r.stats->h2d_bytes += (int64_t)sizeof(LtsState);
+    r.stats->d2h_bytes += (int64_t)(sizeof(LtsState) + 2 * sizeof(long long) + 32);
+  }
   if (c->timer.on) c->timer.harvest();
   if (*n_used == 0) {
     set_error("No block matches occurred. Images probably have zero overlap. "
@@ -720,6 +724,7 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float
                                  c->stream));
     MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
     stats->block_ncc_evaluated = (int64_t)cnt;
+    stats->d2h_bytes += (int64_t)sizeof(cnt);
     stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
   return MIRORR_OK;
@@ -766,7 +771,7 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
-                    &c->bmw.hist, &c->bmw.tiles, &c->ltsw.state, &c->ltsw.resid,
+                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->ltsw.state, &c->ltsw.resid,
                     &c->ltsw.partial, &c->ltsw.hist, &c->ltsw.ctrl, &c->ltsw.cand, &c->counts,
                     &c->ncc_count, &c->ones, &c->lvl_f, &c->lvl_m, &c->tmp_a, &c->tmp_b,
                     &c->weights, &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best,
@@ -780,6 +785,24 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
 }
 
 int64_t mirorr_ctx_kernel_launches(mirorr_ctx c) { return c ? g_launches - c->launches0 : g_launches; }
+
+void *mirorr_ctx_stream(mirorr_ctx c) { return c ? (void *)c->stream : nullptr; }
+
+mirorr_status mirorr_ctx_set_profiling(mirorr_ctx c, int32_t on) {
+  if (!c) { set_error("null argument"); return MIRORR_EINVAL; }
+  c->timer.on = on != 0;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_ctx_stage_times(mirorr_ctx c, double ms[4], int64_t *calls) {
+  if (!c || !ms) { set_error("null argument"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->timer.harvest();
+  for (int i = 0; i < 4; ++i) { ms[i] = c->timer.ms[i]; c->timer.ms[i] = 0.0; }
+  if (calls) *calls = c->timer.calls;
+  c->timer.calls = 0;
+  return MIRORR_OK;
+}
 
 // ---- block matcher -----------------------------------------------------------
 mirorr_status mirorr_bm_default_params(mirorr_bm_params *p) {
@@ -813,7 +836,6 @@ mirorr_status mirorr_bm_create(mirorr_ctx c, mirorr_matcher *out) {
 
 mirorr_status mirorr_bm_destroy(mirorr_matcher m) {
   if (!m) return MIRORR_OK;
-  if (m->ctx && m->ctx->stream) cudaStreamSynchronize(m->ctx->stream);
   for (auto &e : m->ev)
     if (e) cudaEventDestroy(e);
   DevBuf *bufs[] = {&m->base.own_img, &m->base.own_mask, &m->search.own_img,
@@ -1019,6 +1041,19 @@ mirorr_status mirorr_bm_block_results(mirorr_matcher m, size_t capacity, int32_t
   return MIRORR_OK;
 }
 
+mirorr_status mirorr_bm_last_diagnostics(mirorr_matcher m, int64_t out[4]) {
+  if (!m || !out) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!m->has_results) { set_error("no results: call GetOffsets first"); return MIRORR_ESTATE; }
+  unsigned int ctl[8] = {0};
+  MB2_CUDA_TRY(cudaSetDevice(m->ctx->device));
+  MB2_CUDA_TRY(cudaMemcpy(ctl, m->ctx->bmw.ncc_ctl.ptr, sizeof(ctl), cudaMemcpyDeviceToHost));
+  out[0] = ctl[1];
+  out[1] = ctl[2];
+  out[2] = m->kept;
+  out[3] = m->last.nblocks;
+  return MIRORR_OK;
+}
+
 mirorr_status mirorr_bm_last_timings(mirorr_matcher m, float ms[4]) {
   if (!m || !ms) { set_error("null argument"); return MIRORR_EINVAL; }
   for (int i = 0; i < 4; ++i) ms[i] = m->timings[i];
@@ -1191,8 +1226,11 @@ mirorr_status mirorr_register(mirorr_ctx c, const mirorr_geometry *fg, const flo
   if (mmask) { MB2_TRY(upload(c, c->up_mm, mmask, vox(mg->size))); dmm = c->up_mm.as<uint8_t>(); }
   mirorr_status s = register_impl(c, fg, c->up_f.as<float>(), dfm, mg, c->up_m.as<float>(), dmm, p,
                                   init, result, stats);
-  if (s == MIRORR_OK && stats)
+  if (s == MIRORR_OK && stats) {
     stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    stats->h2d_bytes += (int64_t)(sizeof(float) * (vox(fg->size) + vox(mg->size)) +
+                                  (fmask ? vox(fg->size) : 0) + (mmask ? vox(mg->size) : 0));
+  }
   return s;
 }
 

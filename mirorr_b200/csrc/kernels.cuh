@@ -26,6 +26,8 @@ struct BmWork {
   DevBuf select_state;
   DevBuf hist;
   DevBuf tiles;     // compaction tile counts/offsets
+  DevBuf ncc_lists; // overflow block list of the NCC refinement
+  DevBuf ncc_ctl;   // NCC counters: [0] overflow blocks, [1] refined candidates, [2] fallback blocks
 };
 
 struct BmOut {
@@ -53,7 +55,7 @@ mirorr_status launch_variance_selection(const BmGeom &g, const float *base, doub
 // scores evaluated.
 mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmask,
                          const float *search, const uint8_t *smask, const float2 *stats,
-                         const uint8_t *selected, const BmOut &out,
+                         const uint8_t *selected, const BmOut &out, BmWork &w,
                          unsigned long long *ncc_count, cudaStream_t s);
 // Post-filter (itkBlockMatcher.txx:884-918).  Marks kept blocks (status |= 2),
 // counts them into *count_dev and, when pts != nullptr, writes the kept

@@ -1,13 +1,14 @@
 """Block matcher (mirorr_bm_* through the C ABI) against the oracle.
 
-Tolerances (FP32 search vs the FP64 oracle):
-* variance selection: bit-exact (same blocks searched);
-* argmax: identical wherever the oracle's best-vs-second gap exceeds 2e-4,
-  and on >= 99.5 % of all searched blocks;
-* best / second scores: |diff| <= 2e-5; -2 (degenerate) exactly where the oracle has -2;
-* post-filter keep set: identical except blocks whose oracle gap lies within
-  2e-5 of the 1e-4 threshold;
-* block / match points (mm): bit-exact for blocks kept by both with the same match.
+The CUDA search scores candidates in FP32 and re-scores every candidate that
+can still be the best or second-best in FP64 with the reference's arithmetic,
+so its per-block results must equal the FP64 oracle's exactly:
+* variance selection: same blocks searched;
+* best and second-best scores (float storage): bit-identical;
+* argmax (match origin): identical for every searched block;
+* post-filter keep set and the emitted block / match points (mm): identical.
+The reference's own criterion (argmax equal wherever its best-vs-second gap
+exceeds 1e-4, >= 99.5 % overall) is implied.
 """
 import numpy as np
 import pytest
@@ -69,44 +70,30 @@ def check_parity(res, gp, c, geom):
     bp, mp, mi, best, second, status = gp
     p = O.BMParams(c["bw"], c["g"], c["G"], c["nw"], c["keep"])
     ob, om, okept = O.emit_points(res, geom, p, order=0)
-    # selection: bit-exact
     np.testing.assert_array_equal((status & 1).astype(np.uint8), res.status)
     s = res.status == 1
-    ogap = res.best.astype(np.float64) - res.second.astype(np.float64)
-    same = np.all(mi == res.match, axis=1)
-    clear = s & (ogap > 2e-4)
-    assert np.all(same[clear]), f"argmax differs on {np.sum(~same[clear])} clear blocks"
-    assert same[s].mean() >= 0.995
-    both = s & (res.best > -2.5)
-    np.testing.assert_array_equal(best[both] == -2.0, res.best[both] == -2.0)
-    np.testing.assert_allclose(best[s], res.best[s], atol=2e-5, rtol=0)
-    np.testing.assert_allclose(second[s], res.second[s], atol=2e-5, rtol=0)
-    # keep set
-    gkept = (status & 2) != 0
-    okeep = np.zeros_like(gkept)
-    okeep[okept] = True
-    border = s & (np.abs(ogap - 1e-4) < 2e-5)
-    np.testing.assert_array_equal(gkept[~border], okeep[~border])
-    # points of blocks kept by both with the same match: bit-exact
-    gidx = np.flatnonzero(gkept)
-    opos = {int(b): i for i, b in enumerate(okept)}
-    common = [(i, opos[int(b)]) for i, b in enumerate(gidx) if int(b) in opos and same[b]]
-    assert len(common) > 0.5 * len(okept)
-    gi = np.array([a for a, _ in common])
-    oi = np.array([b for _, b in common])
-    np.testing.assert_array_equal(bp[gi], ob[oi])
-    np.testing.assert_array_equal(mp[gi], om[oi])
-    assert bp.shape[0] == int(gkept.sum())
+    np.testing.assert_array_equal(best[s], res.best[s])
+    np.testing.assert_array_equal(second[s], res.second[s])
+    np.testing.assert_array_equal(mi[s], res.match[s])
+    gkept = np.flatnonzero((status & 2) != 0)
+    np.testing.assert_array_equal(gkept, okept)
+    np.testing.assert_array_equal(bp, ob)
+    np.testing.assert_array_equal(mp, om)
 
 
 @pytest.mark.parametrize("c", CASES, ids=[c["id"] for c in CASES])
 def test_matcher_matches_oracle(ctx, c):
     base, search, bm, sm = make_inputs(c)
     spacing, origin = (1.0, 1.2, 0.9), (-3.0, 4.0, 10.0)
-    gp = run_gpu(ctx, c, base, search, bm, sm, spacing, origin)[1:]
+    m, *gp = run_gpu(ctx, c, base, search, bm, sm, spacing, origin)
     res = O.match_blocks(base, search, bm, sm, O.BMParams(c["bw"], c["g"], c["G"], c["nw"], c["keep"]))
     geom = O.Image(base, np.array(spacing), np.array(origin))
     check_parity(res, gp, c, geom)
+    refined, full, kept, nblocks = m.LastDiagnostics()
+    assert kept == gp[0].shape[0] and nblocks == res.best.size
+    assert refined >= int(res.status.sum())
+    print(f"{c['id']}: {refined} candidates refined in FP64 over {nblocks} blocks, "
+          f"{full} blocks fully re-scored")
 
 
 def test_swap_image_order(ctx):

@@ -2,8 +2,9 @@
 oracle run on the same inputs.
 
 The bar: final 3x3 matrices within 1e-4 of the oracle's (entry-wise) and
-offsets within 1e-3 mm; target registration error against the known
-synthetic transform reported and bounded.
+offsets within 1e-3 mm.  Target registration error against the known
+synthetic transform is reported; it must match the oracle's and improve on
+the initial misalignment.
 """
 import numpy as np
 import pytest
@@ -15,14 +16,16 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 CASES = [
-    dict(id="classic_rigid", mode="classic", kind="rigid", shape=(64, 56, 40), levels=2,
+    dict(id="classic_rigid", mode="classic", kind="rigid", shape=(64, 64, 40), levels=2,
          iters=4, G=3, nw=7, keep=1.0, seed=21),
-    dict(id="symmetric_affine", mode="symmetric", kind="affine", shape=(64, 56, 40), levels=2,
+    dict(id="symmetric_affine", mode="symmetric", kind="affine", shape=(64, 64, 40), levels=2,
          iters=4, G=3, nw=7, keep=1.0, seed=22),
-    dict(id="symmetric_rigid_keep05", mode="symmetric", kind="rigid", shape=(56, 48, 40),
+    dict(id="symmetric_rigid_keep05", mode="symmetric", kind="rigid", shape=(72, 64, 40),
          levels=2, iters=3, G=3, nw=7, keep=0.5, seed=23),
-    dict(id="classic_affine", mode="classic", kind="affine", shape=(56, 56, 36), levels=2,
-         iters=3, G=3, nw=7, keep=1.0, seed=24),
+    # three iterations do not converge on this small pair: the oracle ends
+    # worse than the start too; the case still checks parity
+    dict(id="classic_affine", mode="classic", kind="affine", shape=(64, 64, 48), levels=2,
+         iters=3, G=3, nw=7, keep=1.0, seed=24, improves=False),
 ]
 
 
@@ -44,5 +47,9 @@ def test_registration_matches_oracle(ctx, c):
     np.testing.assert_allclose(tg.off, to.off, atol=1e-3, rtol=0)
     err = tre(tg.M, tg.off, ph.true_matrix, ph.true_offset, c["shape"], ph.spacing)
     err_o = tre(to.M, to.off, ph.true_matrix, ph.true_offset, c["shape"], ph.spacing)
-    print(f"{c['id']}: TRE gpu {err:.4f} mm, oracle {err_o:.4f} mm")
-    assert err < 2.0
+    err_0 = tre(np.eye(3), np.zeros(3), ph.true_matrix, ph.true_offset, c["shape"], ph.spacing)
+    print(f"{c['id']}: TRE gpu {err:.4f} mm, oracle {err_o:.4f} mm, initial {err_0:.4f} mm, "
+          f"max |dM| {np.max(np.abs(tg.M - to.M)):.2e}")
+    assert abs(err - err_o) < 1e-3
+    if c.get("improves", True):
+        assert err < err_0
