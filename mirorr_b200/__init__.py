@@ -376,8 +376,9 @@ class BlockMatcher:
         return ms
 
     def LastDiagnostics(self):
-        """(FP64-refined candidates, fully re-scored blocks, kept blocks, grid blocks)."""
-        d = np.zeros(4, np.int64)
+        """(FP64-refined candidates, fully re-scored blocks, kept blocks, grid blocks,
+        fast-path blocks, general-path blocks)."""
+        d = np.zeros(6, np.int64)
         _check(lib().mirorr_bm_last_diagnostics(self._h, _ptr(d)))
         return tuple(int(v) for v in d)
 

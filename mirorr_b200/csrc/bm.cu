@@ -5,7 +5,8 @@
 //                   mu(p) (over all BW^3 voxels, unmasked, as
 //                   itkBlockMatcher.txx:57-68) and the masked sum of squares
 //                   Syy(p) = sum_{ms != 0} (y - mu)^2, both in FP64 in the
-//                   reference's raster order, stored as float2.
+//                   reference's raster order, stored as float2; the sign bit
+//                   of Syy is set when a search-mask voxel of the footprint is 0.
 //   2. selection:   (optional) dead-code variance cut-off of
 //                   itkBlockMatcher.txx:664-719, FP64 per block, exact k-th
 //                   value by a device radix select.
@@ -72,6 +73,7 @@ __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict_
           sum = __dadd_rn(sum, (double)__ldg(&y[p + ((long long)vz * ny + vy) * nx + vx]));
     double mean = __ddiv_rn(sum, (double)(BW * BW * BW));
     double ss = 0.0;
+    bool all_in = true;
 #pragma unroll
     for (int vz = 0; vz < BW; ++vz)
 #pragma unroll
@@ -82,9 +84,12 @@ __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict_
           if (__ldg(&ms[q])) {
             double d = __dsub_rn((double)__ldg(&y[q]), mean);
             ss = __dadd_rn(ss, __dmul_rn(d, d));
+          } else {
+            all_in = false;
           }
         }
-    out[p] = make_float2((float)mean, (float)ss);
+    float fs = (float)ss;
+    out[p] = make_float2((float)mean, all_in ? fs : -fs);
   }
 }
 

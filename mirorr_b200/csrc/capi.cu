@@ -771,7 +771,7 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
-                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->ltsw.state, &c->ltsw.resid,
+                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->ltsw.state, &c->ltsw.resid,
                     &c->ltsw.partial, &c->ltsw.hist, &c->ltsw.ctrl, &c->ltsw.cand, &c->counts,
                     &c->ncc_count, &c->ones, &c->lvl_f, &c->lvl_m, &c->tmp_a, &c->tmp_b,
                     &c->weights, &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best,
@@ -1041,16 +1041,18 @@ mirorr_status mirorr_bm_block_results(mirorr_matcher m, size_t capacity, int32_t
   return MIRORR_OK;
 }
 
-mirorr_status mirorr_bm_last_diagnostics(mirorr_matcher m, int64_t out[4]) {
+mirorr_status mirorr_bm_last_diagnostics(mirorr_matcher m, int64_t out[6]) {
   if (!m || !out) { set_error("null argument"); return MIRORR_EINVAL; }
   if (!m->has_results) { set_error("no results: call GetOffsets first"); return MIRORR_ESTATE; }
   unsigned int ctl[8] = {0};
   MB2_CUDA_TRY(cudaSetDevice(m->ctx->device));
   MB2_CUDA_TRY(cudaMemcpy(ctl, m->ctx->bmw.ncc_ctl.ptr, sizeof(ctl), cudaMemcpyDeviceToHost));
-  out[0] = ctl[1];
-  out[1] = ctl[2];
+  out[0] = ctl[2];
+  out[1] = ctl[1];
   out[2] = m->kept;
   out[3] = m->last.nblocks;
+  out[4] = ctl[3];
+  out[5] = ctl[0];
   return MIRORR_OK;
 }
 

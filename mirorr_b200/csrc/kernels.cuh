@@ -26,8 +26,11 @@ struct BmWork {
   DevBuf select_state;
   DevBuf hist;
   DevBuf tiles;     // compaction tile counts/offsets
-  DevBuf ncc_lists; // overflow block list of the NCC refinement
-  DevBuf ncc_ctl;   // NCC counters: [0] overflow blocks, [1] refined candidates, [2] fallback blocks
+  DevBuf ncc_lists; // block lists of the NCC stages (general path, fallback)
+  DevBuf ncc_ctl;   // NCC counters: [0] general-path blocks, [1] fallback blocks,
+                    // [2] FP64-refined candidates, [3] fast-path blocks
+  DevBuf ncc_rec;   // per-block FP32 stage results
+  DevBuf ncc_bstat; // per-block base statistics
 };
 
 struct BmOut {

@@ -11,25 +11,52 @@
 //     if (best < s) { second = best; best = s; arg = p } else if (second < s) second = s
 // starting from -3.
 //
-// Implementation: a two-stage search.
-//   1. FP32 scores of all candidates (the throughput stage).  The window
-//      mean and masked sum of squares of each candidate come from box_stats.
-//   2. Exact refinement.  Every candidate whose FP32 score lies within 2*delta
-//      of the FP32 second-best (delta bounds the FP32 error) is re-scored in
-//      FP64 with the reference's arithmetic and summation order, and the
-//      reference's sequential best/second update is replayed over them in
-//      raster order.  No other candidate can be the best or the second-best,
-//      so best, second and argmax equal those of the FP64 reference.
-//   Blocks whose candidate list overflows go to a fallback kernel that
-//   re-scores their whole window in FP64.
+// Two stages:
+//   1. FP32 search.  Every candidate is scored in FP32 (the window mean and
+//      masked sum of squares come from box_stats, the base block's from
+//      block_stats).  Per block the stage records the FP32 best and second
+//      and the list of candidates whose FP32 score lies within 2*delta of the
+//      FP32 second-best (delta bounds |FP32 - FP64|), plus the first two
+//      degenerate candidates when fewer than two are non-degenerate.
+//        * ncc_fast_kernel: blocks whose base block and search window are
+//          wholly inside both masks, block gap 1.  Several blocks per CTA;
+//          each thread keeps a TY x W tile of candidates in registers and
+//          streams window rows from shared memory (cross term only: one FMA
+//          per voxel and candidate).
+//        * ncc_general_kernel: every other block (any mask pattern, any gap),
+//          one CTA per block.
+//   2. ncc_refine_kernel, one thread per block: the listed candidates are
+//      re-scored in FP64 with the reference's arithmetic and summation order
+//      and the sequential best/second update is replayed over them in
+//      raster order.  No unlisted candidate can be the best or the second,
+//      so the block's best, second and argmax equal the FP64 reference's.
+//      Blocks whose list overflowed are re-scored entirely by
+//      ncc_fallback_kernel.
 #include "kernels.cuh"
 
 namespace mb2 {
 
 namespace {
 
-constexpr int kLMax = 64;          // refinement list per block
+constexpr int kK = 8;              // refinement list capacity per block
 constexpr float kDelta = 1e-4f;    // bound on |FP32 score - FP64 score|
+
+// Per-block result of the FP32 stage.
+struct NccRec {
+  float f1, f2;
+  int cnt;        // listed candidates; -1: final result already written; > kK: overflow
+  int pad;
+  int32_t p[kK + 2];  // candidate origins (linear voxel index)
+};
+
+// Base-block statistics for the FP32 stage.
+struct BlockStat {
+  double mean;
+  float sxx;   // sum over masked voxels of (x - mean)^2
+  float sxt;   // sum over masked voxels of (x - mean)
+  int mball;   // every base-mask voxel non-zero
+  float c;     // window shift: mean of the block's own candidate footprint
+};
 
 struct NccArgs {
   const float *base;
@@ -38,10 +65,11 @@ struct NccArgs {
   const uint8_t *smask;
   const float2 *stats;
   const uint8_t *selected;
+  const BlockStat *bstat;
   int nx, ny, nz;
   int nbx, nby, nbz;
   int stx, sty, stz;
-  int G, g, W;
+  int G, g, W, bw;
   int emax;
   long long nblocks;
   float *best;
@@ -49,8 +77,11 @@ struct NccArgs {
   int32_t *match;
   uint8_t *status;
   unsigned long long *ncc_count;
-  int *ovf_list;
-  unsigned int *ctl;  // [0] overflow count, [1] refined candidates, [2] fallback blocks
+  NccRec *rec;
+  int *gen_list;    // blocks for the general kernel
+  int *ovf_list;    // blocks for the fallback kernel
+  unsigned int *ctl;  // [0] general blocks, [1] overflow blocks, [2] refined candidates,
+                      // [3] register-blocked blocks, [4] masked-window blocks
 };
 
 __device__ inline void window_axis(int o, int S, int W, int g, int bw, int &s, int &n) {
@@ -63,28 +94,25 @@ __device__ inline void window_axis(int o, int S, int W, int g, int bw, int &s, i
   n = (en > st) ? (en - st + g - 1) / g : 0;
 }
 
-// Geometry of one block's search, shared by the kernels.
 struct BlockWin {
-  long long b;
   int ox, oy, oz;
   int sx, sy, sz;
   int nx, ny, nz;   // candidates per axis
-  int ex, ey, ez;   // staged window extent
+  int ex, ey, ez;   // clipped window extent
   int nc;
 };
 
-__device__ inline bool block_window(const NccArgs &a, long long b, int bw, BlockWin &w) {
-  w.b = b;
+__device__ inline bool block_window(const NccArgs &a, long long b, BlockWin &w) {
   int bx = (int)(b % a.nbx), by = (int)((b / a.nbx) % a.nby), bz = (int)(b / ((long long)a.nbx * a.nby));
   w.ox = a.stx + bx * a.G;
   w.oy = a.sty + by * a.G;
   w.oz = a.stz + bz * a.G;
-  window_axis(w.ox, a.nx, a.W, a.g, bw, w.sx, w.nx);
-  window_axis(w.oy, a.ny, a.W, a.g, bw, w.sy, w.ny);
-  window_axis(w.oz, a.nz, a.W, a.g, bw, w.sz, w.nz);
-  w.ex = (w.nx - 1) * a.g + bw;
-  w.ey = (w.ny - 1) * a.g + bw;
-  w.ez = (w.nz - 1) * a.g + bw;
+  window_axis(w.ox, a.nx, a.W, a.g, a.bw, w.sx, w.nx);
+  window_axis(w.oy, a.ny, a.W, a.g, a.bw, w.sy, w.ny);
+  window_axis(w.oz, a.nz, a.W, a.g, a.bw, w.sz, w.nz);
+  w.ex = (w.nx - 1) * a.g + a.bw;
+  w.ey = (w.ny - 1) * a.g + a.bw;
+  w.ez = (w.nz - 1) * a.g + a.bw;
   w.nc = w.nx * w.ny * w.nz;
   return w.nx > 0 && w.ny > 0 && w.nz > 0;
 }
@@ -93,7 +121,7 @@ __device__ inline long long lin(const NccArgs &a, int x, int y, int z) {
   return ((long long)z * a.ny + y) * a.nx + x;
 }
 
-__device__ inline void write_block(const NccArgs &a, long long b, float best, float second,
+__device__ inline void write_final(const NccArgs &a, long long b, float best, float second,
                                    long long match, uint8_t status) {
   a.best[b] = best;
   a.second[b] = second;
@@ -101,53 +129,831 @@ __device__ inline void write_block(const NccArgs &a, long long b, float best, fl
   a.status[b] = status;
 }
 
-// Shared-memory view of one staged block (raw values, as the reference reads them).
-struct Staged {
-  const float *x;      // base block, B floats
-  const uint8_t *mb;   // base mask, B
-  const float *y;      // search window, ex*ey*ez
-  const uint8_t *ms;   // search mask window
-  double mean_b;       // meanBase of normalizedCorrelation
-};
-
-// FP64 score of candidate (cx, cy, cz) with the reference's arithmetic:
-// two sequential passes in raster order, no contraction.
-template <int BW>
-__device__ double exact_score(const Staged &s, const BlockWin &w, int g, int c) {
-  constexpr int B = BW * BW * BW;
-  int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
-  const int woff = ((cz * g) * w.ey + cy * g) * w.ex + cx * g;
-  double ms = 0.0;
-#pragma unroll
-  for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-    for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-      for (int vx = 0; vx < BW; ++vx)
-        ms = __dadd_rn(ms, (double)s.y[woff + (vz * w.ey + vy) * w.ex + vx]);
-  ms = __ddiv_rn(ms, (double)B);
-  double prod = 0.0, bss = 0.0, sss = 0.0;
-#pragma unroll
-  for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-    for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-      for (int vx = 0; vx < BW; ++vx) {
-        int v = (vz * BW + vy) * BW + vx;
-        int wi = woff + (vz * w.ey + vy) * w.ex + vx;
-        if (s.mb[v] && s.ms[wi]) {
-          double bb = __dsub_rn((double)s.x[v], s.mean_b);
-          double sb = __dsub_rn((double)s.y[wi], ms);
-          prod = __dadd_rn(prod, __dmul_rn(bb, sb));
-          bss = __dadd_rn(bss, __dmul_rn(bb, bb));
-          sss = __dadd_rn(sss, __dmul_rn(sb, sb));
-        }
-      }
-  if (bss <= 0.0 || sss <= 0.0) return -2.0;
-  return __ddiv_rn(__ddiv_rn(__dmul_rn(prod, prod), bss), sss);
+__device__ inline void top2_merge(float &a1, float &a2, float b1, float b2) {
+  float m1 = fmaxf(a1, b1);
+  float m2 = fmaxf(fminf(a1, b1), fmaxf(a2, b2));
+  a1 = m1;
+  a2 = m2;
 }
 
-// The reference's running best / second-best update, float storage.
+__device__ inline void min2_merge(int &a1, int &a2, int b1, int b2) {
+  // two smallest non-negative values of {a1, a2, b1, b2} (negative = none)
+  int v[4] = {a1, a2, b1, b2};
+  int m1 = -1, m2 = -1;
+  for (int i = 0; i < 4; ++i) {
+    int x = v[i];
+    if (x < 0 || x == m1 || x == m2) continue;
+    if (m1 < 0 || x < m1) { m2 = m1; m1 = x; }
+    else if (m2 < 0 || x < m2) { m2 = x; }
+  }
+  a1 = m1;
+  a2 = m2;
+}
+
+__device__ inline void cp_async4(float *dst, const float *src) {
+  unsigned int d = (unsigned int)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ inline void cp_async8(void *dst, const void *src) {
+  unsigned int d = (unsigned int)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ inline void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// box_stats stores Syy with its sign bit set when some search-mask voxel of
+// the candidate's footprint is zero.
+__device__ inline bool footprint_in_mask(float syy_field) { return !signbit(syy_field); }
+__device__ inline float syy_of(float syy_field) { return fabsf(syy_field); }
+
+__device__ inline void push_deg(int &d1, int &d2, int p) {
+  if (d1 < 0) d1 = p;
+  else if (d2 < 0) d2 = p;
+}
+
+// ---------------------------------------------------------------------------
+// base-block statistics (one thread per block)
+// ---------------------------------------------------------------------------
+__global__ void block_stat_kernel(NccArgs a) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
+       b += (long long)gridDim.x * blockDim.x) {
+    int bx = (int)(b % a.nbx), by = (int)((b / a.nbx) % a.nby), bz = (int)(b / ((long long)a.nbx * a.nby));
+    long long o = lin(a, a.stx + bx * a.G, a.sty + by * a.G, a.stz + bz * a.G);
+    const int bw = a.bw;
+    double sum = 0.0;
+    int mball = 1;
+    for (int z = 0; z < bw; ++z)
+      for (int y = 0; y < bw; ++y)
+        for (int x = 0; x < bw; ++x) {
+          long long q = o + ((long long)z * a.ny + y) * a.nx + x;
+          sum = __dadd_rn(sum, (double)__ldg(&a.base[q]));
+          if (!__ldg(&a.bmask[q])) mball = 0;
+        }
+    double mean = __ddiv_rn(sum, (double)(bw * bw * bw));
+    double sxx = 0.0, sxt = 0.0;
+    for (int z = 0; z < bw; ++z)
+      for (int y = 0; y < bw; ++y)
+        for (int x = 0; x < bw; ++x) {
+          long long q = o + ((long long)z * a.ny + y) * a.nx + x;
+          if (__ldg(&a.bmask[q])) {
+            double d = __dsub_rn((double)__ldg(&a.base[q]), mean);
+            sxx = __dadd_rn(sxx, __dmul_rn(d, d));
+            sxt = __dadd_rn(sxt, d);
+          }
+        }
+    BlockStat s;
+    s.mean = mean;
+    s.sxx = (float)sxx;
+    s.sxt = (float)sxt;
+    s.mball = mball;
+    s.c = __ldg(&a.stats[o]).x;
+    const_cast<BlockStat *>(a.bstat)[b] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Register-blocked FP32 search, block gap 1.  Several blocks per CTA; each
+// thread owns a TY x W tile of candidates (one z plane) and streams window
+// rows from shared memory.  The window is staged as y - c with c the mean of
+// the block's own candidate (a per-block constant that keeps the FP32 cross
+// term free of cancellation): Sxy = sum x~ (y - c) - (mu - c) sum x~.
+//   MASKED = false: base block and whole window inside both masks,
+//                   Sxy from one correlation, Syy from box_stats.
+//   MASKED = true : base block inside its mask, window partly masked (m = ms):
+//                   C1 = sum x~ ms (y - c), C2 = sum x~ ms, C3 = sum x~^2 ms,
+//                   Sxy = C1 - (mu - c) C2, Sxx = C3, Syy from box_stats.
+// The unmasked kernel runs over every block and routes the others: blocks
+// with a partly masked window to the masked kernel, blocks with a partly
+// masked base block to the general kernel.
+// ---------------------------------------------------------------------------
+template <int BW_, int W_, int TY_, int BPC_>
+struct FastCfg {
+  static constexpr int BW = BW_, W = W_, TY = TY_, BPC = BPC_;
+  static constexpr int B = BW * BW * BW;
+  static constexpr int R = W / 2;
+  static constexpr int E = W + BW - 1;                 // window extent (x, z)
+  static constexpr int NYG = (W + TY - 1) / TY;        // y-groups per block
+  static constexpr int EY = NYG * TY + BW - 1;         // rows per plane (zero padded)
+  static constexpr int EXP = (E + 3) & ~3;             // row stride (float4 aligned)
+  static constexpr int Q = EY * EXP / 4;               // plane in float4 units
+  static constexpr int PS = (Q + ((3 - (Q % 8)) + 8) % 8) * 4;  // plane stride, conflict-free
+  static constexpr int WIN = E * PS;                   // floats per block window
+  static constexpr int TPB = W * NYG;                  // threads per block
+  static constexpr int NT = ((BPC * TPB + 31) / 32) * 32;
+  static_assert(WIN % 4 == 0 && EXP % 4 == 0 && PS % 4 == 0 && B > 0, "alignment");
+};
+
+template <class C, bool MASKED>
+__global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
+  constexpr int BW = C::BW, W = C::W, TY = C::TY, BPC = C::BPC, B = C::B, R = C::R, E = C::E;
+  constexpr int EY = C::EY, EXP = C::EXP, PS = C::PS, WIN = C::WIN, TPB = C::TPB, NYG = C::NYG;
+  constexpr int NWIN = E * EY * E;
+  extern __shared__ __align__(16) float sm[];
+  float *win = sm;                                  // BPC * WIN: y - c
+  float *mwin = win + BPC * WIN;                    // BPC * WIN: ms != 0 (MASKED only)
+  float *xt = win + (MASKED ? 2 : 1) * BPC * WIN;   // BPC * B
+  __shared__ float s_red[BPC][TPB][2];
+  __shared__ int s_deg[BPC][TPB][2];
+  __shared__ float s_f[BPC][2];
+  __shared__ int s_d[BPC][2];
+  __shared__ int s_cnt[BPC];
+  __shared__ int s_list[BPC][kK];
+  __shared__ int s_state[BPC];           // 1 compute, 0 skip
+  __shared__ int s_inmask[BPC];
+  __shared__ int s_b[BPC];
+  __shared__ int s_o[BPC][3];            // window origin (block origin - R)
+  __shared__ float s_c[BPC];
+  __shared__ float s_sxt[BPC];
+  __shared__ float s_sxx[BPC];
+  __shared__ double s_mean[BPC];
+  const int tid = threadIdx.x;
+  const int slot = tid / TPB;
+  const int lt = tid - slot * TPB;
+  const bool worker = slot < BPC;
+  const int cz = lt / NYG;
+  const int cy0 = (lt - cz * NYG) * TY;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long long nlist = MASKED ? (long long)*(volatile unsigned int *)&a.ctl[4] : a.nblocks;
+
+  for (long long base = (long long)blockIdx.x * BPC; base < nlist; base += (long long)gridDim.x * BPC) {
+    __syncthreads();
+    if (tid < BPC) {
+      long long i = base + tid;
+      int state = 0;
+      s_inmask[tid] = 1;
+      s_cnt[tid] = 0;
+      if (i < nlist) {
+        const int b = MASKED ? a.gen_list[a.nblocks + 1 + i] : (int)i;
+        s_b[tid] = b;
+        const int bx = b % a.nbx, by = (b / a.nbx) % a.nby, bz = b / (a.nbx * a.nby);
+        const int ox = a.stx + bx * a.G, oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
+        s_o[tid][0] = ox - R;
+        s_o[tid][1] = oy - R;
+        s_o[tid][2] = oz - R;
+        const long long o = ((long long)oz * ny + oy) * nx + ox;
+        bool ok = true;
+        if (!MASKED) {
+          BlockWin w;
+          ok = block_window(a, b, w);
+          if (a.selected && !a.selected[b]) {
+            write_final(a, b, -3.f, -3.f, o, 0);
+            a.rec[b].cnt = -1;
+            ok = false;
+          } else if (!ok) {
+            write_final(a, b, -3.f, -3.f, o, 1);
+            a.rec[b].cnt = -1;
+          }
+        }
+        if (ok) {
+          BlockStat st = a.bstat[b];
+          if (st.mball) {
+            state = 1;
+            s_sxt[tid] = st.sxt;
+            s_sxx[tid] = st.sxx;
+            s_mean[tid] = st.mean;
+            s_c[tid] = __ldg(&a.stats[o]).x;  // the block's own position is a candidate
+          } else {
+            unsigned int p = atomicAdd(&a.ctl[0], 1u);
+            a.gen_list[p] = b;
+          }
+        }
+      }
+      s_state[tid] = state;
+    }
+    __syncthreads();
+    // stage windows (zero outside the image), masks and the raw base blocks
+    // with asynchronous copies; test the candidates' mask flags
+    for (int i = tid; i < BPC * NWIN; i += blockDim.x) {
+      const int s = i / NWIN;
+      if (!s_state[s]) continue;
+      const int r = i - s * NWIN;
+      const int x = r % E, y = (r / E) % EY, z = r / (E * EY);
+      const int gx = s_o[s][0] + x, gy = s_o[s][1] + y, gz = s_o[s][2] + z;
+      const int off = s * WIN + z * PS + y * EXP + x;
+      if (y < E && gx >= 0 && gy >= 0 && gz >= 0 && gx < nx && gy < ny && gz < nz) {
+        const long long q = ((long long)gz * ny + gy) * nx + gx;
+        cp_async4(&win[off], &a.search[q]);
+        if (MASKED) mwin[off] = __ldg(&a.smask[q]) ? 1.f : 0.f;
+      } else {
+        win[off] = 0.f;
+        if (MASKED) mwin[off] = 0.f;
+      }
+    }
+    for (int i = tid; i < BPC * B; i += blockDim.x) {
+      const int s = i / B;
+      if (!s_state[s]) continue;
+      const int v = i - s * B;
+      const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+      const long long q = ((long long)(s_o[s][2] + R + vz) * ny + (s_o[s][1] + R + vy)) * nx +
+                          (s_o[s][0] + R + vx);
+      cp_async4(&xt[i], &a.base[q]);
+    }
+    if (!MASKED && worker && s_state[slot]) {
+      const int px0 = s_o[slot][0], py0 = s_o[slot][1] + cy0, pz = s_o[slot][2] + cz;
+      bool ok = true;
+      if (pz >= 0 && pz <= nz - BW) {
+#pragma unroll
+        for (int j = 0; j < TY; ++j) {
+          const int py = py0 + j;
+          if (cy0 + j >= W || py < 0 || py > ny - BW) continue;
+#pragma unroll
+          for (int x = 0; x < W; ++x) {
+            const int px = px0 + x;
+            if (px < 0 || px > nx - BW) continue;
+            if (!footprint_in_mask(__ldg(&a.stats[((long long)pz * ny + py) * nx + px]).y)) ok = false;
+          }
+        }
+      }
+      if (!ok) s_inmask[slot] = 0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i = tid; i < BPC * NWIN; i += blockDim.x) {
+      const int s = i / NWIN;
+      if (!s_state[s]) continue;
+      const int r = i - s * NWIN;
+      const int x = r % E, y = (r / E) % EY, z = r / (E * EY);
+      const int off = s * WIN + z * PS + y * EXP + x;
+      if (MASKED) {
+        if (mwin[off] != 0.f) win[off] = win[off] - s_c[s];
+        else win[off] = 0.f;
+      } else {
+        win[off] = win[off] - s_c[s];
+      }
+    }
+    for (int i = tid; i < BPC * B; i += blockDim.x) {
+      const int s = i / B;
+      if (!s_state[s]) continue;
+      xt[i] = (float)__dsub_rn((double)xt[i], s_mean[s]);
+    }
+    if (!MASKED && tid < BPC && s_state[tid] && !s_inmask[tid]) {
+      // partly masked window: the masked kernel takes it
+      unsigned int p = atomicAdd(&a.ctl[4], 1u);
+      a.gen_list[a.nblocks + 1 + p] = s_b[tid];
+      s_state[tid] = 0;
+    }
+    __syncthreads();
+    const bool active = worker && s_state[slot];
+    float sc[TY][W];
+    float c2[MASKED ? TY : 1][MASKED ? W : 1];
+    float c3[MASKED ? TY : 1][MASKED ? W : 1];
+    float l1 = -3.f, l2 = -3.f;
+    int d1 = -1, d2 = -1;
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < TY; ++j)
+#pragma unroll
+        for (int x = 0; x < W; ++x) {
+          sc[j][x] = 0.f;
+          if (MASKED) { c2[j][x] = 0.f; c3[j][x] = 0.f; }
+        }
+      const int wo = slot * WIN + cz * PS + cy0 * EXP;
+      const float *tp = xt + slot * B;
+#pragma unroll 1
+      for (int vz = 0; vz < BW; ++vz) {
+        float t[BW][BW];
+#pragma unroll
+        for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+          for (int vx = 0; vx < BW; ++vx) t[vy][vx] = tp[(vz * BW + vy) * BW + vx];
+#pragma unroll
+        for (int j = 0; j < TY + BW - 1; ++j) {
+          float r[EXP], m[MASKED ? EXP : 1];
+          const float4 *rp = reinterpret_cast<const float4 *>(win + wo + vz * PS + j * EXP);
+#pragma unroll
+          for (int k = 0; k < EXP / 4; ++k) {
+            float4 q = rp[k];
+            r[4 * k] = q.x; r[4 * k + 1] = q.y; r[4 * k + 2] = q.z; r[4 * k + 3] = q.w;
+          }
+          if (MASKED) {
+            const float4 *mp = reinterpret_cast<const float4 *>(mwin + wo + vz * PS + j * EXP);
+#pragma unroll
+            for (int k = 0; k < EXP / 4; ++k) {
+              float4 q = mp[k];
+              m[4 * k] = q.x; m[4 * k + 1] = q.y; m[4 * k + 2] = q.z; m[4 * k + 3] = q.w;
+            }
+          }
+#pragma unroll
+          for (int vy = 0; vy < BW; ++vy) {
+            const int jj = j - vy;
+            if (jj < 0 || jj >= TY) continue;
+#pragma unroll
+            for (int x = 0; x < W; ++x) {
+              float acc = sc[jj][x];
+#pragma unroll
+              for (int vx = 0; vx < BW; ++vx) acc = fmaf(t[vy][vx], r[x + vx], acc);
+              sc[jj][x] = acc;
+              if (MASKED) {
+                float a2 = c2[jj][x], a3 = c3[jj][x];
+#pragma unroll
+                for (int vx = 0; vx < BW; ++vx) {
+                  const float tm = t[vy][vx] * m[x + vx];
+                  a2 += tm;
+                  a3 = fmaf(tm, t[vy][vx], a3);
+                }
+                c2[jj][x] = a2;
+                c3[jj][x] = a3;
+              }
+            }
+          }
+        }
+      }
+      // scores
+      const float sxt = s_sxt[slot], sxx_b = s_sxx[slot], cc = s_c[slot];
+      const int pz = s_o[slot][2] + cz;
+#pragma unroll
+      for (int j = 0; j < TY; ++j) {
+        const int cy = cy0 + j;
+        const int py = s_o[slot][1] + cy;
+        const bool rowok = cy < W && py >= 0 && py <= ny - BW && pz >= 0 && pz <= nz - BW;
+#pragma unroll
+        for (int x = 0; x < W; ++x) {
+          const int px = s_o[slot][0] + x;
+          float s = -4.f;  // not a candidate
+          if (rowok && px >= 0 && px <= nx - BW) {
+            const long long p = ((long long)pz * ny + py) * nx + px;
+            const float2 st = __ldg(&a.stats[p]);
+            const float syy = syy_of(st.y);
+            const float dm = st.x - cc;
+            float sxy, sxx;
+            if (MASKED) {
+              sxy = sc[j][x] - dm * c2[j][x];
+              sxx = c3[j][x];
+            } else {
+              sxy = sc[j][x] - dm * sxt;
+              sxx = sxx_b;
+            }
+            s = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
+            if (s == -2.f) push_deg(d1, d2, (int)p);
+            top2_merge(l1, l2, s, -3.f);
+          }
+          sc[j][x] = s;
+        }
+      }
+    }
+    if (worker) {
+      s_red[slot][lt][0] = l1;
+      s_red[slot][lt][1] = l2;
+      s_deg[slot][lt][0] = d1;
+      s_deg[slot][lt][1] = d2;
+    }
+    __syncthreads();
+    if (active && lt == 0) {
+      float f1 = -3.f, f2 = -3.f;
+      int e1 = -1, e2 = -1;
+      for (int k = 0; k < TPB; ++k) {
+        top2_merge(f1, f2, s_red[slot][k][0], s_red[slot][k][1]);
+        min2_merge(e1, e2, s_deg[slot][k][0], s_deg[slot][k][1]);
+      }
+      s_f[slot][0] = f1;
+      s_f[slot][1] = f2;
+      s_d[slot][0] = e1;
+      s_d[slot][1] = e2;
+    }
+    __syncthreads();
+    if (active) {
+      const float T = s_f[slot][1] - 2.f * kDelta;
+      const int pz = s_o[slot][2] + cz;
+#pragma unroll
+      for (int j = 0; j < TY; ++j)
+#pragma unroll
+        for (int x = 0; x < W; ++x) {
+          float s = sc[j][x];
+          if (s > -2.f && s >= T) {
+            int pos = atomicAdd(&s_cnt[slot], 1);
+            if (pos < kK)
+              s_list[slot][pos] = (int)(((long long)pz * ny + s_o[slot][1] + cy0 + j) * nx + s_o[slot][0] + x);
+          }
+        }
+    }
+    __syncthreads();
+    if (active && lt == 0) {
+      NccRec &rc = a.rec[s_b[slot]];
+      int cnt = s_cnt[slot];
+      rc.f1 = s_f[slot][0];
+      rc.f2 = s_f[slot][1];
+      if (cnt <= kK) {
+        for (int k = 0; k < cnt; ++k) rc.p[k] = s_list[slot][k];
+        if (s_f[slot][1] <= -2.f) {
+          if (s_d[slot][0] >= 0) rc.p[cnt++] = s_d[slot][0];
+          if (s_d[slot][1] >= 0) rc.p[cnt++] = s_d[slot][1];
+        }
+      }
+      rc.cnt = cnt;
+      atomicAdd(&a.ctl[3], 1u);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-level register-blocked FP32 search for blocks whose base block and
+// window are wholly inside both masks (block gap 1).  Each warp holds SPW
+// blocks (one per LPS = 32/SPW lanes) and runs independently of the other
+// warps of its CTA (no CTA barrier): stage the window rows and the base
+// block with asynchronous copies, score a TY x W tile of candidates per lane
+// (one z plane, cross term only) streaming window rows from shared memory,
+// reduce with shuffles, emit the block's refinement list.  The window is
+// staged as y - c (c: mean of the block's own candidate), so
+// Sxy = sum x~ (y - c) - (mu - c) sum x~ has no FP32 cancellation.  Blocks
+// with a partly masked window go to the masked kernel, blocks with a partly
+// masked base block to the general kernel.
+// ---------------------------------------------------------------------------
+template <int BW_, int W_, int TY_, int SPW_, int WPC_, int MINB_>
+struct WarpCfg {
+  static constexpr int BW = BW_, W = W_, TY = TY_, SPW = SPW_;
+  static constexpr int MINB = MINB_;                   // resident CTAs per SM aimed for
+  static constexpr int LPS = 32 / SPW;                 // lanes per block
+  static constexpr int B = BW * BW * BW;
+  static constexpr int R = W / 2;
+  static constexpr int E = W + BW - 1;
+  static constexpr int NYG = (W + TY - 1) / TY;
+  static constexpr int TPB = W * NYG;                  // working lanes per block
+  static constexpr int EY = NYG * TY + BW - 1;
+  static constexpr int EXP = (E + 3) & ~3;
+  static constexpr int Q = EY * EXP / 4;
+  static constexpr int PS = (Q + ((3 - (Q % 8)) + 8) % 8) * 4;
+  static constexpr int WIN = E * PS;
+  static constexpr int NSTAT = W * W * W;             // candidate statistics (float2)
+  // floats per block slot; a multiple of 4 keeps every slot's window rows
+  // 16-byte aligned for the float4 row loads
+  static constexpr int SLOT = (WIN + ((B + 3) & ~3) + 2 * NSTAT + 3) & ~3;
+  static_assert(SLOT % 4 == 0 && WIN % 4 == 0 && EXP % 4 == 0 && PS % 4 == 0, "alignment");
+  static constexpr int WPC = WPC_;                     // warps per CTA
+  static_assert(TPB <= LPS, "tile does not fit the lanes of a block");
+};
+
+template <class C>
+__global__ void __launch_bounds__(C::WPC * 32, C::MINB) ncc_warp_kernel(NccArgs a) {
+  constexpr int BW = C::BW, W = C::W, TY = C::TY, SPW = C::SPW, LPS = C::LPS, B = C::B;
+  constexpr int R = C::R, E = C::E, NYG = C::NYG, TPB = C::TPB, EY = C::EY, EXP = C::EXP;
+  constexpr int PS = C::PS, WIN = C::WIN, SLOT = C::SLOT, WPC = C::WPC;
+  extern __shared__ __align__(16) float sm[];
+  __shared__ int s_cnt[WPC * SPW];
+  __shared__ int s_list[WPC * SPW][kK];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sl = lane / LPS, sln = lane - sl * LPS;
+  const int slot = warp * SPW + sl;
+  float *win = sm + slot * SLOT;
+  float *xt = win + WIN;
+  float2 *sst = reinterpret_cast<float2 *>(xt + ((B + 3) & ~3));  // W^3 candidate statistics
+  const bool worker = sln < TPB;
+  const int cz = sln / NYG;
+  const int cy0 = (sln - cz * NYG) * TY;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const unsigned full = 0xffffffffu;
+  const int src = sl * LPS;
+  const unsigned seg = (LPS == 32) ? full : (((1u << LPS) - 1u) << src);
+  const long long stride = (long long)gridDim.x * WPC * SPW;
+
+  for (long long base = ((long long)blockIdx.x * WPC + warp) * SPW; base < a.nblocks; base += stride) {
+    const long long bl = base + sl;
+    const bool valid = bl < a.nblocks;
+    const int b = valid ? (int)bl : 0;
+    // ---- set-up: every lane of the block reads the same statistics --------
+    const BlockStat st = a.bstat[b];
+    const int bx = b % a.nbx, by = (b / a.nbx) % a.nby, bz = b / (a.nbx * a.nby);
+    const int bx0 = a.stx + bx * a.G, by0 = a.sty + by * a.G, bz0 = a.stz + bz * a.G;
+    const int ox = bx0 - R, oy = by0 - R, oz = bz0 - R;
+    int state = 0;
+    if (valid) {
+      // with block gap 1 every window holds at least the block's own origin
+      const bool sel = !a.selected || a.selected[b];
+      if (!sel) {
+        if (sln == 0) {
+          write_final(a, b, -3.f, -3.f, ((long long)bz0 * ny + by0) * nx + bx0, 0);
+          a.rec[b].cnt = -1;
+        }
+      } else if (st.mball) {
+        state = 1;
+      } else if (sln == 0) {
+        unsigned int p = atomicAdd(&a.ctl[0], 1u);
+        a.gen_list[p] = b;
+      }
+    }
+    if (sln == 0) s_cnt[slot] = 0;
+    const float cc = st.c;
+    // ---- staging: coalesced asynchronous copies (x fastest across lanes) ---
+    if (state) {
+      for (int e = sln; e < E * EY * E; e += LPS) {
+        const int row = e / E, x = e - row * E;
+        const int z = row / EY, y = row - z * EY;
+        const int gx = ox + x, gy = oy + y, gz = oz + z;
+        float *dst = win + z * PS + y * EXP + x;
+        if (y < E && gx >= 0 && gy >= 0 && gz >= 0 && gx < nx && gy < ny && gz < nz)
+          cp_async4(dst, a.search + ((long long)gz * ny + gy) * nx + gx);
+        else
+          *dst = 0.f;
+      }
+      for (int v = sln; v < B; v += LPS) {
+        const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+        cp_async4(xt + v, a.base + ((long long)(bz0 + vz) * ny + (by0 + vy)) * nx + (bx0 + vx));
+      }
+      for (int e = sln; e < W * W * W; e += LPS) {
+        const int row = e / W, x = e - row * W;
+        const int z = row / W, y = row - z * W;
+        const int gx = ox + x, gy = oy + y, gz = oz + z;
+        if (gx >= 0 && gy >= 0 && gz >= 0 && gx <= nx - BW && gy <= ny - BW && gz <= nz - BW)
+          cp_async8(sst + e, a.stats + ((long long)gz * ny + gy) * nx + gx);
+        else
+          sst[e] = make_float2(__int_as_float(0x7fc00000), 0.f);  // not a candidate (NaN)
+      }
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    // partly masked window -> masked kernel
+    bool inmask = true;
+    if (state) {
+      for (int e = sln; e < W * W * W; e += LPS) {
+        const float2 q = sst[e];
+        if (q.x == q.x && !footprint_in_mask(q.y)) inmask = false;
+      }
+    }
+    const unsigned bad = __ballot_sync(full, !inmask);
+    if (state && (bad & seg)) {
+      if (sln == 0) {
+        unsigned int p = atomicAdd(&a.ctl[4], 1u);
+        a.gen_list[a.nblocks + 1 + p] = b;
+      }
+      state = 0;
+    }
+    if (state) {
+      for (int r = sln; r < E * EY; r += LPS) {
+        const int z = r / EY, y = r - z * EY;
+        float4 *p4 = reinterpret_cast<float4 *>(win + z * PS + y * EXP);
+#pragma unroll
+        for (int k = 0; k < EXP / 4; ++k) {
+          float4 q = p4[k];
+          q.x -= cc; q.y -= cc; q.z -= cc; q.w -= cc;
+          p4[k] = q;
+        }
+      }
+      for (int v = sln; v < B; v += LPS) xt[v] = (float)__dsub_rn((double)xt[v], st.mean);
+    }
+    __syncwarp();
+    // ---- FP32 scores of the lane's tile -----------------------------------
+    float sc[TY][W];
+    float l1 = -3.f, l2 = -3.f;
+    int d1 = -1, d2 = -1;
+    const bool active = state && worker;
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < TY; ++j)
+#pragma unroll
+        for (int x = 0; x < W; ++x) sc[j][x] = 0.f;
+      const float *wp = win + cz * PS + cy0 * EXP;
+#pragma unroll 1
+      for (int vz = 0; vz < BW; ++vz) {
+        float t[BW][BW];
+#pragma unroll
+        for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+          for (int vx = 0; vx < BW; ++vx) t[vy][vx] = xt[(vz * BW + vy) * BW + vx];
+#pragma unroll
+        for (int j = 0; j < TY + BW - 1; ++j) {
+          float r[EXP];
+          const float4 *rp = reinterpret_cast<const float4 *>(wp + vz * PS + j * EXP);
+#pragma unroll
+          for (int k = 0; k < EXP / 4; ++k) {
+            float4 q = rp[k];
+            r[4 * k] = q.x; r[4 * k + 1] = q.y; r[4 * k + 2] = q.z; r[4 * k + 3] = q.w;
+          }
+#pragma unroll
+          for (int vy = 0; vy < BW; ++vy) {
+            const int jj = j - vy;
+            if (jj < 0 || jj >= TY) continue;
+#pragma unroll
+            for (int x = 0; x < W; ++x) {
+              float acc = sc[jj][x];
+#pragma unroll
+              for (int vx = 0; vx < BW; ++vx) acc = fmaf(t[vy][vx], r[x + vx], acc);
+              sc[jj][x] = acc;
+            }
+          }
+        }
+      }
+      const float sxt = st.sxt, sxx_b = st.sxx;
+#pragma unroll
+      for (int j = 0; j < TY; ++j) {
+        const int cy = cy0 + j;
+#pragma unroll
+        for (int x = 0; x < W; ++x) {
+          float s = -4.f;  // not a candidate
+          if (cy < W) {
+            const float2 q = sst[(cz * W + cy) * W + x];
+            if (q.x == q.x) {
+              const float syy = syy_of(q.y);
+              const float sxy = sc[j][x] - (q.x - cc) * sxt;
+              s = (sxx_b <= 0.f || syy <= 0.f) ? -2.f : __fdividef(__fdividef(sxy * sxy, sxx_b), syy);
+              if (s == -2.f) push_deg(d1, d2, (int)(((long long)(oz + cz) * ny + oy + cy) * nx + ox + x));
+              top2_merge(l1, l2, s, -3.f);
+            }
+          }
+          sc[j][x] = s;
+        }
+      }
+    }
+    // ---- block-level reduction (within the block's lanes) -----------------
+#pragma unroll
+    for (int off = LPS / 2; off > 0; off >>= 1) {
+      float o1 = __shfl_down_sync(full, l1, off, LPS);
+      float o2 = __shfl_down_sync(full, l2, off, LPS);
+      int e1 = __shfl_down_sync(full, d1, off, LPS);
+      int e2 = __shfl_down_sync(full, d2, off, LPS);
+      top2_merge(l1, l2, o1, o2);
+      min2_merge(d1, d2, e1, e2);
+    }
+    const float f1 = __shfl_sync(full, l1, src), f2 = __shfl_sync(full, l2, src);
+    d1 = __shfl_sync(full, d1, src);
+    d2 = __shfl_sync(full, d2, src);
+    if (active) {
+      const float T = f2 - 2.f * kDelta;
+#pragma unroll
+      for (int j = 0; j < TY; ++j)
+#pragma unroll
+        for (int x = 0; x < W; ++x) {
+          const float s = sc[j][x];
+          if (s > -2.f && s >= T) {
+            const int pos = atomicAdd(&s_cnt[slot], 1);
+            if (pos < kK)
+              s_list[slot][pos] = (int)(((long long)(oz + cz) * ny + oy + cy0 + j) * nx + ox + x);
+          }
+        }
+    }
+    __syncwarp();
+    if (state && sln == 0) {
+      NccRec &rc = a.rec[b];
+      int cnt = s_cnt[slot];
+      rc.f1 = f1;
+      rc.f2 = f2;
+      if (cnt <= kK) {
+        for (int k = 0; k < cnt; ++k) rc.p[k] = s_list[slot][k];
+        if (f2 <= -2.f) {
+          if (d1 >= 0) rc.p[cnt++] = d1;
+          if (d2 >= 0) rc.p[cnt++] = d2;
+        }
+      }
+      rc.cnt = cnt;
+      atomicAdd(&a.ctl[3], 1u);
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// General FP32 search: one CTA (128 threads) per block, any mask pattern.
+// ---------------------------------------------------------------------------
+template <int BW>
+__global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_list) {
+  constexpr int B = BW * BW * BW;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int e3 = a.emax * a.emax * a.emax;
+  float *xt = reinterpret_cast<float *>(smem);  // B centred (float)
+  float *yw = xt + B;                            // e3
+  uint8_t *mb = reinterpret_cast<uint8_t *>(yw + e3);
+  uint8_t *mw = mb + B;
+  __shared__ int s_cnt, s_list[kK];
+  __shared__ float s_red[4][2];
+  __shared__ int s_deg[4][2];
+  const int tid = threadIdx.x;
+  const long long n = use_list ? (long long)*(volatile unsigned int *)&a.ctl[0] : a.nblocks;
+
+  for (long long i = blockIdx.x; i < n; i += gridDim.x) {
+    __syncthreads();
+    const long long b = use_list ? (long long)a.gen_list[i] : i;
+    BlockWin w;
+    bool ok = block_window(a, b, w);
+    const long long obase = lin(a, w.ox, w.oy, w.oz);
+    if (!use_list) {
+      if (a.selected && !a.selected[b]) {
+        if (tid == 0) { write_final(a, b, -3.f, -3.f, obase, 0); a.rec[b].cnt = -1; }
+        continue;
+      }
+      if (!ok) {
+        if (tid == 0) { write_final(a, b, -3.f, -3.f, obase, 1); a.rec[b].cnt = -1; }
+        continue;
+      }
+    }
+    const BlockStat bst = a.bstat[b];
+    for (int v = tid; v < B; v += blockDim.x) {
+      int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+      long long q = obase + ((long long)vz * a.ny + vy) * a.nx + vx;
+      xt[v] = (float)__dsub_rn((double)__ldg(&a.base[q]), bst.mean);
+      mb[v] = __ldg(&a.bmask[q]);
+    }
+    const long long wbase = lin(a, w.sx, w.sy, w.sz);
+    const int nwin = w.ex * w.ey * w.ez;
+    int all_in = 1;
+    for (int k = tid; k < nwin; k += blockDim.x) {
+      int wx = k % w.ex, wy = (k / w.ex) % w.ey, wz = k / (w.ex * w.ey);
+      long long q = wbase + ((long long)wz * a.ny + wy) * a.nx + wx;
+      yw[k] = __ldg(&a.search[q]);
+      uint8_t m = __ldg(&a.smask[q]);
+      mw[k] = m;
+      if (!m) all_in = 0;
+    }
+    if (tid == 0) s_cnt = 0;
+    const int ms_all = __syncthreads_and(all_in);
+    const bool fast = bst.mball && ms_all;
+    float l1 = -3.f, l2 = -3.f;
+    int d1 = -1, d2 = -1;
+    // pass 1: FP32 top-2 and the first degenerate candidates
+    for (int pass = 0; pass < 2; ++pass) {
+      float T = 0.f;
+      if (pass == 1) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          float o1 = __shfl_down_sync(0xffffffffu, l1, off);
+          float o2 = __shfl_down_sync(0xffffffffu, l2, off);
+          int e1 = __shfl_down_sync(0xffffffffu, d1, off);
+          int e2 = __shfl_down_sync(0xffffffffu, d2, off);
+          top2_merge(l1, l2, o1, o2);
+          min2_merge(d1, d2, e1, e2);
+        }
+        if ((tid & 31) == 0) {
+          s_red[tid >> 5][0] = l1; s_red[tid >> 5][1] = l2;
+          s_deg[tid >> 5][0] = d1; s_deg[tid >> 5][1] = d2;
+        }
+        __syncthreads();
+        l1 = s_red[0][0]; l2 = s_red[0][1]; d1 = s_deg[0][0]; d2 = s_deg[0][1];
+        for (int k = 1; k < 4; ++k) {
+          top2_merge(l1, l2, s_red[k][0], s_red[k][1]);
+          min2_merge(d1, d2, s_deg[k][0], s_deg[k][1]);
+        }
+        T = l2 - 2.f * kDelta;
+      }
+      for (int c = tid; c < w.nc; c += blockDim.x) {
+        int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
+        int px = w.sx + cx * a.g, py = w.sy + cy * a.g, pz = w.sz + cz * a.g;
+        long long p = lin(a, px, py, pz);
+        float2 st = __ldg(&a.stats[p]);
+        const float mu = st.x;
+        const int woff = ((cz * a.g) * w.ey + cy * a.g) * w.ex + cx * a.g;
+        float sxy = 0.f, sxx, syy;
+        if (fast) {
+          float acc = 0.f;
+#pragma unroll
+          for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+            for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+              for (int vx = 0; vx < BW; ++vx)
+                acc = fmaf(xt[(vz * BW + vy) * BW + vx], yw[woff + (vz * w.ey + vy) * w.ex + vx], acc);
+          sxy = acc - mu * bst.sxt;
+          sxx = bst.sxx;
+          syy = syy_of(st.y);
+        } else {
+          float ax = 0.f, ay = 0.f;
+#pragma unroll
+          for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+            for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+              for (int vx = 0; vx < BW; ++vx) {
+                int v = (vz * BW + vy) * BW + vx;
+                int wi = woff + (vz * w.ey + vy) * w.ex + vx;
+                if (mb[v] && mw[wi]) {
+                  float xv = xt[v];
+                  float d = yw[wi] - mu;
+                  sxy = fmaf(xv, d, sxy);
+                  ax = fmaf(xv, xv, ax);
+                  ay = fmaf(d, d, ay);
+                }
+              }
+          sxx = ax;
+          syy = bst.mball ? syy_of(st.y) : ay;
+        }
+        float s = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
+        if (pass == 0) {
+          top2_merge(l1, l2, s, -3.f);
+          if (s == -2.f) push_deg(d1, d2, (int)p);
+        } else if (s > -2.f && s >= T) {
+          int pos = atomicAdd(&s_cnt, 1);
+          if (pos < kK) s_list[pos] = (int)p;
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      NccRec &rc = a.rec[b];
+      int cnt = s_cnt;
+      rc.f1 = l1;
+      rc.f2 = l2;
+      if (cnt <= kK) {
+        for (int k = 0; k < cnt; ++k) rc.p[k] = s_list[k];
+        if (l2 <= -2.f) {
+          if (d1 >= 0) rc.p[cnt++] = d1;
+          if (d2 >= 0) rc.p[cnt++] = d2;
+        }
+      }
+      rc.cnt = cnt;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 refinement: one thread per block.
+// ---------------------------------------------------------------------------
 struct SeqTop2 {
   float best = -3.f, second = -3.f;
   int arg = -1;
@@ -162,217 +968,78 @@ struct SeqTop2 {
   }
 };
 
-__device__ inline void top2_merge(float &a1, float &a2, float b1, float b2) {
-  float m1 = fmaxf(a1, b1);
-  float m2 = fmaxf(fminf(a1, b1), fmaxf(a2, b2));
-  a1 = m1;
-  a2 = m2;
-}
-
-__device__ inline void stage_block(const NccArgs &a, const BlockWin &w, int B, int bw, float *x,
-                                   uint8_t *mb, float *y, uint8_t *ms, int &all_in_out) {
-  const int tid = threadIdx.x;
-  const long long obase = lin(a, w.ox, w.oy, w.oz);
-  for (int v = tid; v < B; v += blockDim.x) {
-    int vx = v % bw, vy = (v / bw) % bw, vz = v / (bw * bw);
-    long long q = obase + ((long long)vz * a.ny + vy) * a.nx + vx;
-    x[v] = __ldg(&a.base[q]);
-    mb[v] = __ldg(&a.bmask[q]);
-  }
-  const long long wbase = lin(a, w.sx, w.sy, w.sz);
-  const int nwin = w.ex * w.ey * w.ez;
-  int all_in = 1;
-  for (int i = tid; i < nwin; i += blockDim.x) {
-    int wx = i % w.ex, wy = (i / w.ex) % w.ey, wz = i / (w.ex * w.ey);
-    long long q = wbase + ((long long)wz * a.ny + wy) * a.nx + wx;
-    y[i] = __ldg(&a.search[q]);
-    uint8_t m = __ldg(&a.smask[q]);
-    ms[i] = m;
-    if (!m) all_in = 0;
-  }
-  all_in_out = all_in;
-}
-
-// ---------------------------------------------------------------------------
-// General kernel: one CTA (128 threads) per block, any mask pattern.
-// ---------------------------------------------------------------------------
+// normalizedCorrelation in FP64 with the reference's summation order.
 template <int BW>
-__global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a) {
+__device__ double exact_score(const NccArgs &a, const float *x, const uint8_t *mb, double mean_b,
+                              long long p) {
   constexpr int B = BW * BW * BW;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int e3 = a.emax * a.emax * a.emax;
-  const int cmax = a.W * a.W * a.W;
-  float *xr = reinterpret_cast<float *>(smem);  // B raw
-  float *xt = xr + B;                            // B centred (float)
-  float *yw = xt + B;                            // e3
-  float *sc = yw + e3;                           // cmax FP32 scores
-  uint8_t *mb = reinterpret_cast<uint8_t *>(sc + cmax);
-  uint8_t *mw = mb + B;
-  __shared__ double s_mean;
-  __shared__ float s_sxx, s_sxt;
-  __shared__ int s_mball, s_cnt, s_deg[2];
-  __shared__ float s_red[8];
-  __shared__ int s_list[kLMax];
-  __shared__ double s_ex[kLMax];
-  const int tid = threadIdx.x;
+  double ms = 0.0;
+  for (int vz = 0; vz < BW; ++vz)
+    for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+      for (int vx = 0; vx < BW; ++vx)
+        ms = __dadd_rn(ms, (double)__ldg(&a.search[p + ((long long)vz * a.ny + vy) * a.nx + vx]));
+  ms = __ddiv_rn(ms, (double)B);
+  double prod = 0.0, bss = 0.0, sss = 0.0;
+  for (int vz = 0; vz < BW; ++vz)
+    for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+      for (int vx = 0; vx < BW; ++vx) {
+        const int v = (vz * BW + vy) * BW + vx;
+        const long long q = p + ((long long)vz * a.ny + vy) * a.nx + vx;
+        if (mb[v] && __ldg(&a.smask[q])) {
+          double bb = __dsub_rn((double)x[v], mean_b);
+          double sb = __dsub_rn((double)__ldg(&a.search[q]), ms);
+          prod = __dadd_rn(prod, __dmul_rn(bb, sb));
+          bss = __dadd_rn(bss, __dmul_rn(bb, bb));
+          sss = __dadd_rn(sss, __dmul_rn(sb, sb));
+        }
+      }
+  if (bss <= 0.0 || sss <= 0.0) return -2.0;
+  return __ddiv_rn(__ddiv_rn(__dmul_rn(prod, prod), bss), sss);
+}
 
-  for (long long b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
-    __syncthreads();
+template <int BW>
+__global__ void __launch_bounds__(128) ncc_refine_kernel(NccArgs a) {
+  constexpr int B = BW * BW * BW;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
+       b += (long long)gridDim.x * blockDim.x) {
+    NccRec rc = a.rec[b];
+    if (rc.cnt < 0) continue;
+    if (rc.cnt > kK) {
+      unsigned int pos = atomicAdd(&a.ctl[1], 1u);
+      a.ovf_list[pos] = (int)b;
+      continue;
+    }
     BlockWin w;
-    bool ok = block_window(a, b, BW, w);
-    const long long obase = lin(a, w.ox, w.oy, w.oz);
-    if (a.selected && !a.selected[b]) {
-      if (tid == 0) write_block(a, b, -3.f, -3.f, obase, 0);
-      continue;
-    }
-    if (!ok) {
-      if (tid == 0) write_block(a, b, -3.f, -3.f, obase, 1);
-      continue;
-    }
-    int all_in;
-    stage_block(a, w, B, BW, xr, mb, yw, mw, all_in);
-    const int ms_all = __syncthreads_and(all_in);
-    if (tid == 0) {
-      double sum = 0.0;
-      int mball = 1;
-      for (int v = 0; v < B; ++v) {
-        sum = __dadd_rn(sum, (double)xr[v]);
-        if (!mb[v]) mball = 0;
-      }
-      double mean = __ddiv_rn(sum, (double)B);
-      double sxx = 0.0, sxt = 0.0;
-      for (int v = 0; v < B; ++v)
-        if (mb[v]) {
-          double d = __dsub_rn((double)xr[v], mean);
-          sxx = __dadd_rn(sxx, __dmul_rn(d, d));
-          sxt = __dadd_rn(sxt, d);
+    block_window(a, b, w);
+    const long long o = lin(a, w.ox, w.oy, w.oz);
+    float x[B];
+    uint8_t mb[B];
+    double sum = 0.0;
+    for (int vz = 0; vz < BW; ++vz)
+      for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+        for (int vx = 0; vx < BW; ++vx) {
+          const int v = (vz * BW + vy) * BW + vx;
+          const long long q = o + ((long long)vz * a.ny + vy) * a.nx + vx;
+          x[v] = __ldg(&a.base[q]);
+          mb[v] = __ldg(&a.bmask[q]);
+          sum = __dadd_rn(sum, (double)x[v]);
         }
-      s_mean = mean;
-      s_sxx = (float)sxx;
-      s_sxt = (float)sxt;
-      s_mball = mball;
-      s_cnt = 0;
-      s_deg[0] = s_deg[1] = -1;
+    const double mean_b = __ddiv_rn(sum, (double)B);
+    // raster order = increasing linear index
+    int n = rc.cnt;
+    for (int i = 1; i < n; ++i) {
+      int v = rc.p[i], j = i - 1;
+      while (j >= 0 && rc.p[j] > v) { rc.p[j + 1] = rc.p[j]; --j; }
+      rc.p[j + 1] = v;
     }
-    __syncthreads();
-    for (int v = tid; v < B; v += blockDim.x) xt[v] = (float)__dsub_rn((double)xr[v], s_mean);
-    __syncthreads();
-    const bool fast = s_mball && ms_all;
-    const float sxx_f = s_sxx, sxt_f = s_sxt;
-    // ---- stage 1: FP32 scores -------------------------------------------
-    float l1 = -3.f, l2 = -3.f;
-    for (int c = tid; c < w.nc; c += blockDim.x) {
-      int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
-      int px = w.sx + cx * a.g, py = w.sy + cy * a.g, pz = w.sz + cz * a.g;
-      float2 st = __ldg(&a.stats[lin(a, px, py, pz)]);
-      const float mu = st.x;
-      const int woff = ((cz * a.g) * w.ey + cy * a.g) * w.ex + cx * a.g;
-      float sxy = 0.f, sxx, syy;
-      if (fast) {
-        float acc = 0.f;
-#pragma unroll
-        for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-          for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-            for (int vx = 0; vx < BW; ++vx)
-              acc = fmaf(xt[(vz * BW + vy) * BW + vx], yw[woff + (vz * w.ey + vy) * w.ex + vx], acc);
-        sxy = acc - mu * sxt_f;
-        sxx = sxx_f;
-        syy = st.y;
-      } else {
-        float ax = 0.f, ay = 0.f;
-#pragma unroll
-        for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-          for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-            for (int vx = 0; vx < BW; ++vx) {
-              int v = (vz * BW + vy) * BW + vx;
-              int wi = woff + (vz * w.ey + vy) * w.ex + vx;
-              if (mb[v] && mw[wi]) {
-                float xv = xt[v];
-                float d = yw[wi] - mu;
-                sxy = fmaf(xv, d, sxy);
-                ax = fmaf(xv, xv, ax);
-                ay = fmaf(d, d, ay);
-              }
-            }
-        sxx = ax;
-        syy = s_mball ? st.y : ay;
-      }
-      float score = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
-      sc[c] = score;
-      top2_merge(l1, l2, score, -3.f);
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      float o1 = __shfl_down_sync(0xffffffffu, l1, off);
-      float o2 = __shfl_down_sync(0xffffffffu, l2, off);
-      top2_merge(l1, l2, o1, o2);
-    }
-    if ((tid & 31) == 0) { s_red[2 * (tid >> 5)] = l1; s_red[2 * (tid >> 5) + 1] = l2; }
-    __syncthreads();
-    float f1 = s_red[0], f2 = s_red[1];
-    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) top2_merge(f1, f2, s_red[2 * k], s_red[2 * k + 1]);
-    // ---- stage 2: exact refinement --------------------------------------
-    const float T = f2 - 2.f * kDelta;
-    for (int c = tid; c < w.nc; c += blockDim.x) {
-      float s = sc[c];
-      if (s > -2.f && s >= T) {
-        int p = atomicAdd(&s_cnt, 1);
-        if (p < kLMax) s_list[p] = c;
-      }
-    }
-    if (f2 <= -2.f && tid == 0) {
-      // fewer than two non-degenerate candidates: the first two degenerate
-      // ones (in raster order) decide the second-best / the argmax
-      int k = 0;
-      for (int c = 0; c < w.nc && k < 2; ++c)
-        if (sc[c] == -2.f) s_deg[k++] = c;
-    }
-    __syncthreads();
-    int cnt = s_cnt;
-    if (cnt > kLMax) {
-      if (tid == 0) {
-        unsigned int p = atomicAdd(&a.ctl[0], 1u);
-        a.ovf_list[p] = (int)b;
-      }
-      continue;
-    }
-    if (tid == 0) {
-      for (int k = 0; k < 2; ++k)
-        if (s_deg[k] >= 0) s_list[cnt++] = s_deg[k];
-      s_cnt = cnt;
-    }
-    __syncthreads();
-    cnt = s_cnt;
-    Staged sg{xr, mb, yw, mw, s_mean};
-    for (int t = tid; t < cnt; t += blockDim.x) s_ex[t] = exact_score<BW>(sg, w, a.g, s_list[t]);
-    __syncthreads();
-    if (tid == 0) {
-      // replay the sequential update in raster order
-      for (int i = 1; i < cnt; ++i) {
-        int ci = s_list[i];
-        double ei = s_ex[i];
-        int j = i - 1;
-        while (j >= 0 && s_list[j] > ci) {
-          s_list[j + 1] = s_list[j];
-          s_ex[j + 1] = s_ex[j];
-          --j;
-        }
-        s_list[j + 1] = ci;
-        s_ex[j + 1] = ei;
-      }
-      SeqTop2 r;
-      for (int i = 0; i < cnt; ++i) r.push(s_ex[i], s_list[i]);
-      int c = r.arg < 0 ? 0 : r.arg;
-      int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
-      write_block(a, b, r.best, r.second,
-                  lin(a, w.sx + cx * a.g, w.sy + cy * a.g, w.sz + cz * a.g), 1);
-      if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)w.nc);
-      atomicAdd(&a.ctl[1], (unsigned int)cnt);
-    }
+    SeqTop2 r;
+    for (int i = 0; i < n; ++i) r.push(exact_score<BW>(a, x, mb, mean_b, rc.p[i]), rc.p[i]);
+    write_final(a, b, r.best, r.second, r.arg < 0 ? lin(a, w.sx, w.sy, w.sz) : r.arg, 1);
+    if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)w.nc);
+    atomicAdd(&a.ctl[2], (unsigned int)n);
   }
 }
 
@@ -383,65 +1050,89 @@ template <int BW>
 __global__ void __launch_bounds__(128) ncc_fallback_kernel(NccArgs a) {
   constexpr int B = BW * BW * BW;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int e3 = a.emax * a.emax * a.emax;
-  const int cmax = a.W * a.W * a.W;
-  double *ex = reinterpret_cast<double *>(smem);  // cmax
-  float *xr = reinterpret_cast<float *>(ex + cmax);
-  float *yw = xr + B;
-  uint8_t *mb = reinterpret_cast<uint8_t *>(yw + e3);
-  uint8_t *mw = mb + B;
+  double *ex = reinterpret_cast<double *>(smem);  // W^3
+  __shared__ float xs[B];
+  __shared__ uint8_t mbs[B];
   __shared__ double s_mean;
   const int tid = threadIdx.x;
-  const unsigned int n = *(volatile unsigned int *)&a.ctl[0];
+  const unsigned int n = *(volatile unsigned int *)&a.ctl[1];
   for (unsigned int i = blockIdx.x; i < n; i += gridDim.x) {
     __syncthreads();
-    long long b = a.ovf_list[i];
+    const long long b = a.ovf_list[i];
     BlockWin w;
-    block_window(a, b, BW, w);
-    int all_in;
-    stage_block(a, w, B, BW, xr, mb, yw, mw, all_in);
+    block_window(a, b, w);
+    const long long o = lin(a, w.ox, w.oy, w.oz);
+    for (int v = tid; v < B; v += blockDim.x) {
+      int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+      long long q = o + ((long long)vz * a.ny + vy) * a.nx + vx;
+      xs[v] = __ldg(&a.base[q]);
+      mbs[v] = __ldg(&a.bmask[q]);
+    }
     __syncthreads();
     if (tid == 0) {
       double sum = 0.0;
-      for (int v = 0; v < B; ++v) sum = __dadd_rn(sum, (double)xr[v]);
+      for (int v = 0; v < B; ++v) sum = __dadd_rn(sum, (double)xs[v]);
       s_mean = __ddiv_rn(sum, (double)B);
     }
     __syncthreads();
-    Staged sg{xr, mb, yw, mw, s_mean};
-    for (int c = tid; c < w.nc; c += blockDim.x) ex[c] = exact_score<BW>(sg, w, a.g, c);
+    for (int c = tid; c < w.nc; c += blockDim.x) {
+      int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
+      ex[c] = exact_score<BW>(a, xs, mbs, s_mean,
+                              lin(a, w.sx + cx * a.g, w.sy + cy * a.g, w.sz + cz * a.g));
+    }
     __syncthreads();
-    if (tid < 32) {
+    if (tid == 0) {
       SeqTop2 r;
-      for (int base = 0; base < w.nc; base += 32) {
-        // all lanes replay the same sequence; lane 0 writes
-        int lim = min(32, w.nc - base);
-        for (int j = 0; j < lim; ++j) r.push(ex[base + j], base + j);
-      }
-      if (tid == 0) {
-        int c = r.arg < 0 ? 0 : r.arg;
-        int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
-        write_block(a, b, r.best, r.second,
-                    lin(a, w.sx + cx * a.g, w.sy + cy * a.g, w.sz + cz * a.g), 1);
-        if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)w.nc);
-        atomicAdd(&a.ctl[2], 1u);
-      }
+      for (int c = 0; c < w.nc; ++c) r.push(ex[c], c);
+      int c = r.arg < 0 ? 0 : r.arg;
+      int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
+      write_final(a, b, r.best, r.second, lin(a, w.sx + cx * a.g, w.sy + cy * a.g, w.sz + cz * a.g), 1);
+      if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)w.nc);
     }
   }
 }
 
 template <class K>
 mirorr_status set_smem(K kernel, size_t smem) {
-  if (smem > 48 * 1024)
-    MB2_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  MB2_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return MIRORR_OK;
+}
+
+template <class C, bool MASKED>
+mirorr_status launch_fast1(const NccArgs &a, cudaStream_t s) {
+  size_t smem = sizeof(float) * (size_t)C::BPC * ((MASKED ? 2 : 1) * C::WIN + C::B);
+  MB2_TRY(set_smem(ncc_fast_kernel<C, MASKED>, smem));
+  long long need = (a.nblocks + C::BPC - 1) / C::BPC;
+  long long grid = need < 148LL * 8 ? need : 148LL * 8;
+  ncc_fast_kernel<C, MASKED><<<(unsigned)grid, C::NT, smem, s>>>(a);
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
+}
+
+template <class CW>
+mirorr_status launch_warp(const NccArgs &a, cudaStream_t s) {
+  size_t smem = sizeof(float) * (size_t)CW::WPC * CW::SPW * CW::SLOT;
+  MB2_TRY(set_smem(ncc_warp_kernel<CW>, smem));
+  long long need = (a.nblocks + CW::WPC * CW::SPW - 1) / (CW::WPC * CW::SPW);
+  long long grid = need < 148LL * CW::MINB * 4 ? need : 148LL * CW::MINB * 4;
+  ncc_warp_kernel<CW><<<(unsigned)grid, CW::WPC * 32, smem, s>>>(a);
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
+}
+
+template <class CW, class CM>
+mirorr_status launch_fast(const NccArgs &a, cudaStream_t s) {
+  MB2_TRY((launch_warp<CW>(a, s)));
+  MB2_TRY((launch_fast1<CM, true>(a, s)));
   return MIRORR_OK;
 }
 
 template <int BW>
-mirorr_status launch_bw(const NccArgs &a, cudaStream_t s) {
+mirorr_status launch_rest(const NccArgs &a, bool all_general, cudaStream_t s) {
   constexpr int B = BW * BW * BW;
   const size_t e3 = (size_t)a.emax * a.emax * a.emax, cmax = (size_t)a.W * a.W * a.W;
-  size_t smem_g = sizeof(float) * (2 * B + e3 + cmax) + B + e3 + 16;
-  size_t smem_f = sizeof(double) * cmax + sizeof(float) * (B + e3) + B + e3 + 16;
+  size_t smem_g = sizeof(float) * (B + e3) + B + e3 + 16;
+  size_t smem_f = sizeof(double) * cmax + 16;
   if (smem_g > 200 * 1024 || smem_f > 200 * 1024) {
     set_error("search window too large for shared memory (window %d^3, %d candidates)",
               a.emax, (int)cmax);
@@ -450,11 +1141,33 @@ mirorr_status launch_bw(const NccArgs &a, cudaStream_t s) {
   MB2_TRY(set_smem(ncc_general_kernel<BW>, smem_g));
   MB2_TRY(set_smem(ncc_fallback_kernel<BW>, smem_f));
   long long grid = a.nblocks < 148LL * 16 ? a.nblocks : 148LL * 16;
-  ncc_general_kernel<BW><<<(unsigned)grid, 128, smem_g, s>>>(a);
+  ncc_general_kernel<BW><<<(unsigned)grid, 128, smem_g, s>>>(a, all_general ? 0 : 1);
+  MB2_LAUNCH_CHECK();
+  long long rgrid = (a.nblocks + 127) / 128;
+  ncc_refine_kernel<BW><<<(unsigned)rgrid, 128, 0, s>>>(a);
   MB2_LAUNCH_CHECK();
   ncc_fallback_kernel<BW><<<148, 128, smem_f, s>>>(a);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
+}
+
+// Block width / window combinations with a register-blocked fast kernel.
+bool run_fast(const NccArgs &a, cudaStream_t s, mirorr_status &st) {
+  if (a.g != 1) return false;
+  if ((long long)a.nx * a.ny * a.nz >= (1LL << 31)) return false;
+  if (a.bw == 4 && a.W == 9) {
+    st = launch_fast<WarpCfg<4, 9, 3, 1, 5, 3>, FastCfg<4, 9, 1, 3>>(a, s);
+    return true;
+  }
+  if (a.bw == 4 && a.W == 7) {
+    st = launch_fast<WarpCfg<4, 7, 4, 2, 4, 3>, FastCfg<4, 7, 1, 5>>(a, s);
+    return true;
+  }
+  if (a.bw == 5 && a.W == 11) {
+    st = launch_fast<WarpCfg<5, 11, 6, 1, 4, 2>, FastCfg<5, 11, 1, 2>>(a, s);
+    return true;
+  }
+  return false;
 }
 
 }  // namespace
@@ -467,31 +1180,45 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
     set_error("too many blocks (%lld)", g.nblocks);
     return MIRORR_EINVAL;
   }
-  MB2_TRY(w.ncc_lists.ensure(sizeof(int) * (g.nblocks + 1)));
+  MB2_TRY(w.ncc_lists.ensure(sizeof(int) * 3 * (g.nblocks + 1)));
   MB2_TRY(w.ncc_ctl.ensure(sizeof(unsigned int) * 8));
+  MB2_TRY(w.ncc_rec.ensure(sizeof(NccRec) * g.nblocks));
+  MB2_TRY(w.ncc_bstat.ensure(sizeof(BlockStat) * g.nblocks));
   MB2_CUDA_TRY(cudaMemsetAsync(w.ncc_ctl.ptr, 0, sizeof(unsigned int) * 8, s));
   NccArgs a;
   a.base = base; a.bmask = bmask; a.search = search; a.smask = smask; a.stats = stats;
   a.selected = selected;
+  a.bstat = w.ncc_bstat.as<BlockStat>();
   a.nx = g.size[0]; a.ny = g.size[1]; a.nz = g.size[2];
   a.nbx = g.nb[0]; a.nby = g.nb[1]; a.nbz = g.nb[2];
   a.stx = g.st[0]; a.sty = g.st[1]; a.stz = g.st[2];
-  a.G = g.ngap; a.g = g.bgap; a.W = g.nw;
+  a.G = g.ngap; a.g = g.bgap; a.W = g.nw; a.bw = g.bw;
   a.emax = (g.nw - 1) * g.bgap + g.bw;
   a.nblocks = g.nblocks;
   a.best = out.best; a.second = out.second; a.match = out.match; a.status = out.status;
   a.ncc_count = ncc_count;
-  a.ovf_list = w.ncc_lists.as<int>();
+  a.rec = w.ncc_rec.as<NccRec>();
+  a.gen_list = w.ncc_lists.as<int>();
+  a.ovf_list = a.gen_list + 2 * (g.nblocks + 1);
   a.ctl = w.ncc_ctl.as<unsigned int>();
+  {
+    long long grid = (g.nblocks + 127) / 128;
+    if (grid > 148LL * 16) grid = 148LL * 16;
+    block_stat_kernel<<<(unsigned)grid, 128, 0, s>>>(a);
+    MB2_LAUNCH_CHECK();
+  }
+  mirorr_status st = MIRORR_OK;
+  bool fast = run_fast(a, s, st);
+  MB2_TRY(st);
   switch (g.bw) {
-    case 1: return launch_bw<1>(a, s);
-    case 2: return launch_bw<2>(a, s);
-    case 3: return launch_bw<3>(a, s);
-    case 4: return launch_bw<4>(a, s);
-    case 5: return launch_bw<5>(a, s);
-    case 6: return launch_bw<6>(a, s);
-    case 7: return launch_bw<7>(a, s);
-    case 8: return launch_bw<8>(a, s);
+    case 1: return launch_rest<1>(a, !fast, s);
+    case 2: return launch_rest<2>(a, !fast, s);
+    case 3: return launch_rest<3>(a, !fast, s);
+    case 4: return launch_rest<4>(a, !fast, s);
+    case 5: return launch_rest<5>(a, !fast, s);
+    case 6: return launch_rest<6>(a, !fast, s);
+    case 7: return launch_rest<7>(a, !fast, s);
+    case 8: return launch_rest<8>(a, !fast, s);
     default:
       set_error("block width %d not supported (1..8)", g.bw);
       return MIRORR_EINVAL;
