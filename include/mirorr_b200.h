@@ -174,6 +174,32 @@ MIRORR_API mirorr_status mirorr_lts_symmetric(mirorr_ctx ctx, mirorr_transform *
                                    const double *moved, double lts_keep,
                                    int32_t *inner_iterations);
 
+/* No reference counterpart.  The LTS fit of mirorr_lts_classic (t12f and t12b
+ * both NULL) or mirorr_lts_symmetric (both non-NULL) on point pairs that are
+ * already in device memory on the context's device (initial_dev, moved_dev:
+ * n x 3 doubles each, 8-byte aligned), allocating no device memory: its
+ * scratch (residuals, radix histograms, per-CTA partial sums, fit state) is
+ * one static device array of about 4.2 MB per device, sized for
+ * MIRORR_LTS_NOALLOC_MAX_POINTS pairs.  For callers that must not allocate
+ * once set up: cudaFree synchronises the whole device, and cudaMalloc fails
+ * when another allocator (the caching allocator of a serving process, say)
+ * already holds the free memory.  Results equal mirorr_lts_classic /
+ * mirorr_lts_symmetric on the same pairs.
+ *   - The first call on a device does the set-up (it looks up the array's
+ *     address and the cooperative-launch size); make it before any stream
+ *     capture.
+ *   - n > MIRORR_LTS_NOALLOC_MAX_POINTS returns MIRORR_ERANGE; host pointers
+ *     or pointers on another device return MIRORR_EINVAL.
+ *   - All calls on one device share the array: calls that overlap in time
+ *     (several threads, contexts or streams) race and give wrong results.
+ *   - Like the other LTS entry points it copies the fit state in and out and
+ *     synchronises the context's stream before returning. */
+#define MIRORR_LTS_NOALLOC_MAX_POINTS 524288
+MIRORR_API mirorr_status mirorr_lts_noalloc(mirorr_ctx ctx, mirorr_transform *t, mirorr_transform *t12f,
+                                 mirorr_transform *t12b, size_t n, const double *initial_dev,
+                                 const double *moved_dev, double lts_keep,
+                                 int32_t *inner_iterations);
+
 /* ---- registration: MirorrPyramidImplement::RunMirorr over the finest
  * `levels` pyramid levels (itkMirorrPyramidImplement.txx:71-158), classic
  * (itkMirorrRegistrationMethod.txx:422-659) or symmetric

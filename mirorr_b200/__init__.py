@@ -164,6 +164,8 @@ def lib():
                                P(ctypes.c_int32)],
         "mirorr_lts_symmetric": [vp, P(Transform), P(Transform), P(Transform), ctypes.c_size_t,
                                  vp, vp, ctypes.c_double, P(ctypes.c_int32)],
+        "mirorr_lts_noalloc": [vp, P(Transform), vp, vp, ctypes.c_size_t, vp, vp,
+                               ctypes.c_double, P(ctypes.c_int32)],
         "mirorr_reg_default_params": [P(RegParams)],
         "mirorr_register": [vp, P(Geometry), vp, vp, P(Geometry), vp, vp, P(RegParams),
                             P(Transform), P(Transform), P(RegStats)],
@@ -440,6 +442,33 @@ def lts_symmetric(ctx: Context, t: Transform, t12f: Transform, t12b: Transform, 
     _check(lib().mirorr_lts_symmetric(ctx.handle, ctypes.byref(t), ctypes.byref(t12f),
                                       ctypes.byref(t12b), init.shape[0], _ptr(init), _ptr(moved),
                                       float(lts_keep), ctypes.byref(it)))
+    return it.value
+
+
+LTS_NOALLOC_MAX_POINTS = 524288
+
+
+def lts_noalloc(ctx: Context, t: Transform, n: int, init_dev: int, moved_dev: int,
+                lts_keep=0.5, t12f: Transform | None = None, t12b: Transform | None = None):
+    """LTS fit on point pairs already in device memory, allocating no device memory.
+
+    No reference counterpart.  For callers that must not allocate after
+    set-up (cudaFree synchronises the device; cudaMalloc fails when another
+    allocator holds the memory).  init_dev / moved_dev are device addresses
+    of n x 3 float64 arrays on the context's device (e.g. a CUDA tensor's
+    data_ptr()).  Classic fit when t12f and t12b are None, symmetric when
+    both are given; the results equal lts_classic / lts_symmetric.  The
+    scratch is a static device array sized for LTS_NOALLOC_MAX_POINTS pairs
+    (larger n raises MirorrError with MIRORR_ERANGE).  The first call on a
+    device does the set-up; make it before any stream capture.  Calls on one
+    device share the scratch, so calls that overlap in time race.
+    Returns the number of LTS inner iterations."""
+    it = ctypes.c_int32(0)
+    pf = None if t12f is None else ctypes.byref(t12f)
+    pb = None if t12b is None else ctypes.byref(t12b)
+    _check(lib().mirorr_lts_noalloc(ctx.handle, ctypes.byref(t), pf, pb, int(n),
+                                    ctypes.c_void_p(init_dev), ctypes.c_void_p(moved_dev),
+                                    float(lts_keep), ctypes.byref(it)))
     return it.value
 
 

@@ -1186,6 +1186,65 @@ mirorr_status mirorr_lts_symmetric(mirorr_ctx c, mirorr_transform *t, mirorr_tra
   return lts_common(c, t, t12f, t12b, n, init, moved, lts_keep, inner, true);
 }
 
+// True when p is device memory (or managed memory) usable on device dev.
+static bool device_pointer_on(const void *p, int dev) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (at.type == cudaMemoryTypeManaged) return true;
+  return at.type == cudaMemoryTypeDevice && at.device == dev;
+}
+
+mirorr_status mirorr_lts_noalloc(mirorr_ctx c, mirorr_transform *t, mirorr_transform *t12f,
+                                 mirorr_transform *t12b, size_t n, const double *init,
+                                 const double *moved, double lts_keep, int32_t *inner) {
+  if (!c || !t || (n && (!init || !moved)) || ((t12f == nullptr) != (t12b == nullptr))) {
+    set_error("null argument (t12f and t12b must both be given or both be NULL)");
+    return MIRORR_EINVAL;
+  }
+  const bool sym = t12f != nullptr;
+  if (!(lts_keep > 0.0 && lts_keep <= 1.0)) { set_error("lts_keep must lie in (0, 1]"); return MIRORR_EINVAL; }
+  if (n > (size_t)MIRORR_LTS_NOALLOC_MAX_POINTS) {
+    set_error("%zu point pairs exceed the no-allocation LTS limit of %d", n,
+              (int)MIRORR_LTS_NOALLOC_MAX_POINTS);
+    return MIRORR_ERANGE;
+  }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  if (n) {
+    if (((uintptr_t)init | (uintptr_t)moved) & 7u) {
+      set_error("point arrays must be 8-byte aligned");
+      return MIRORR_EINVAL;
+    }
+    if (!device_pointer_on(init, c->device) || !device_pointer_on(moved, c->device)) {
+      set_error("point arrays must be device memory on the context's device %d", c->device);
+      return MIRORR_EINVAL;
+    }
+  }
+  LtsState hs;
+  memset(&hs, 0, sizeof(hs));
+  if (!from_public(*t, hs.tfm)) { set_error("bad transform kind"); return MIRORR_EINVAL; }
+  hs.kind = t->kind;
+  hs.symmetric = sym ? 1 : 0;
+  hs.lts_keep = lts_keep;
+  if (sym) {
+    if (!from_public(*t12f, hs.t12f) || !from_public(*t12b, hs.t12b)) {
+      set_error("bad transform kind");
+      return MIRORR_EINVAL;
+    }
+  }
+  int it = 0;
+  MB2_TRY(lts_run_noalloc(hs, init, moved, (long long)n, c->stream, &it));
+  if (inner) *inner = it;
+  to_public(hs.tfm, *t);
+  if (sym) {
+    to_public(hs.t12f, *t12f);
+    to_public(hs.t12b, *t12b);
+  }
+  return MIRORR_OK;
+}
+
 // ---- registration ----------------------------------------------------------------
 mirorr_status mirorr_reg_default_params(mirorr_reg_params *p) {
   if (!p) { set_error("null argument"); return MIRORR_EINVAL; }

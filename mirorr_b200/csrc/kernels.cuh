@@ -100,5 +100,11 @@ struct LtsWork {
 mirorr_status lts_run(LtsWork &w, LtsState &host_state, const double *init_dev,
                       const double *moved_dev, const long long *n_dev, long long n_max,
                       cudaStream_t s, int *inner_iters, long long *n_used);
+// lts_run with every scratch buffer in a static device array sized for
+// MIRORR_LTS_NOALLOC_MAX_POINTS pairs: allocates no device memory.  n is the
+// number of pairs (no device counters).  Calls on one device must not overlap.
+mirorr_status lts_run_noalloc(LtsState &host_state, const double *init_dev,
+                              const double *moved_dev, long long n, cudaStream_t s,
+                              int *inner_iters);
 
 }  // namespace mb2

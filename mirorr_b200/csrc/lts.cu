@@ -17,6 +17,8 @@
 // second); a timeout raises an error flag and every CTA returns.
 #include <cooperative_groups.h>
 
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace mb2 {
@@ -390,6 +392,134 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
   MB2_CUDA_TRY(cudaMemcpyAsync(nn, n_dev, sizeof(nn), cudaMemcpyDeviceToHost, st));
   MB2_CUDA_TRY(cudaStreamSynchronize(st));
   if (n_used) *n_used = nn[0] + nn[1];
+  if (ctl.err) {
+    set_error("LTS grid barrier timed out");
+    return MIRORR_ETIMEOUT;
+  }
+  if (inner_iters) *inner_iters = hs.iter;
+  lts_finish(hs);
+  return MIRORR_OK;
+}
+
+// ---- allocation-free variant ----------------------------------------------------
+//
+// lts_run_noalloc runs the same kernel with the same grid as lts_run, but every
+// scratch buffer lives in one static device array, so the call allocates no
+// device memory.  Its address is looked up once per device (the first call on
+// that device) with cudaGetSymbolAddress.  Layout, in bytes:
+//   [0, 4096)        LtsState (uploaded each call)
+//   [4096, 4352)     LtsCtl (zeroed each call)
+//   [4352, 4608)     point-pair counters {n, 0} (uploaded each call)
+//   [4608, +48 KB)   3 radix histograms of 4096 bins (zeroed each call)
+//   then             2048 candidate keys, kNaMaxCtas * 32 partial sums,
+//                    MIRORR_LTS_NOALLOC_MAX_POINTS residuals.
+// Two calls in flight on one device share the array and race.
+
+namespace {
+
+constexpr int kNaMaxCtas = 256;
+constexpr int kNaMaxDevices = 64;
+constexpr size_t kNaState = 0;
+constexpr size_t kNaCtl = 4096;
+constexpr size_t kNaCount = kNaCtl + 256;
+constexpr size_t kNaHist = kNaCount + 256;
+constexpr size_t kNaCand = kNaHist + sizeof(unsigned int) * 3 * kBins;
+constexpr size_t kNaPartial = kNaCand + sizeof(unsigned long long) * kCandMax;
+constexpr size_t kNaResid = kNaPartial + sizeof(double) * kPartial * kNaMaxCtas;
+constexpr size_t kNaBytes = kNaResid + sizeof(double) * (size_t)MIRORR_LTS_NOALLOC_MAX_POINTS;
+static_assert(sizeof(LtsState) <= kNaCtl - kNaState, "LtsState slot");
+static_assert(sizeof(LtsCtl) <= kNaCount - kNaCtl, "LtsCtl slot");
+static_assert(kNaHist % 256 == 0 && kNaCand % 256 == 0 && kNaPartial % 256 == 0 &&
+                  kNaResid % 256 == 0, "slot alignment");
+
+static __device__ __align__(256) unsigned char g_lts_scratch[kNaBytes];
+
+std::mutex g_na_mu;
+unsigned char *g_na_ptr[kNaMaxDevices];
+int g_na_ctas[kNaMaxDevices];
+
+// One-time set-up per device (the calling thread's current device): the
+// scratch address and the co-resident CTA count of the cooperative launch.
+mirorr_status na_setup(int dev, unsigned char **ptr, int *ctas) {
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (dev < 0 || dev >= kNaMaxDevices) {
+    set_error("device ordinal %d is beyond the %d devices the no-allocation LTS supports", dev,
+              kNaMaxDevices);
+    return MIRORR_ERANGE;
+  }
+  if (!g_na_ptr[dev]) {
+    int sms = 0, per = 0, coop = 0;
+    MB2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MB2_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) {
+      set_error("device does not support cooperative launches");
+      return MIRORR_ECUDA;
+    }
+    MB2_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lts_kernel, kThreads, 0));
+    if (per < 1) {
+      set_error("LTS kernel cannot be resident");
+      return MIRORR_ECUDA;
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_lts_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error("cudaGetSymbolAddress of the LTS scratch array failed on device %d: %s", dev,
+                cudaGetErrorString(e));
+      return MIRORR_ECUDA;
+    }
+    g_na_ctas[dev] = sms * (per > 1 ? 1 : per);
+    g_na_ptr[dev] = static_cast<unsigned char *>(p);
+  }
+  *ptr = g_na_ptr[dev];
+  *ctas = g_na_ctas[dev];
+  return MIRORR_OK;
+}
+
+}  // namespace
+
+mirorr_status lts_run_noalloc(LtsState &hs, const double *init_dev, const double *moved_dev,
+                              long long n, cudaStream_t st, int *inner_iters) {
+  if (n > (long long)MIRORR_LTS_NOALLOC_MAX_POINTS) {
+    set_error("%lld point pairs exceed the no-allocation LTS limit of %d", n,
+              (int)MIRORR_LTS_NOALLOC_MAX_POINTS);
+    return MIRORR_ERANGE;
+  }
+  lts_begin(hs);
+  if (n <= 0) {
+    lts_finish(hs);
+    if (inner_iters) *inner_iters = 0;
+    return MIRORR_OK;
+  }
+  int dev = 0;
+  MB2_CUDA_TRY(cudaGetDevice(&dev));
+  unsigned char *base = nullptr;
+  int max_ctas = 0;
+  MB2_TRY(na_setup(dev, &base, &max_ctas));
+  if (max_ctas > kNaMaxCtas) max_ctas = kNaMaxCtas;
+  long long want = (n + 4 * kThreads - 1) / (4 * kThreads);
+  int grid = (int)(want < 1 ? 1 : (want > max_ctas ? max_ctas : want));
+  long long counts[2] = {n, 0};
+  MB2_CUDA_TRY(cudaMemcpyAsync(base + kNaState, &hs, sizeof(LtsState), cudaMemcpyHostToDevice, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(base + kNaCount, counts, sizeof(counts), cudaMemcpyHostToDevice, st));
+  MB2_CUDA_TRY(cudaMemsetAsync(base + kNaHist, 0, sizeof(unsigned int) * 3 * kBins, st));
+  MB2_CUDA_TRY(cudaMemsetAsync(base + kNaCtl, 0, sizeof(LtsCtl), st));
+  LtsArgs a;
+  a.state = reinterpret_cast<LtsState *>(base + kNaState);
+  a.init = init_dev;
+  a.moved = moved_dev;
+  a.n_dev = reinterpret_cast<const long long *>(base + kNaCount);
+  a.resid = reinterpret_cast<double *>(base + kNaResid);
+  a.partial = reinterpret_cast<double *>(base + kNaPartial);
+  a.hist = reinterpret_cast<unsigned int *>(base + kNaHist);
+  a.cand = reinterpret_cast<unsigned long long *>(base + kNaCand);
+  a.ctl = reinterpret_cast<LtsCtl *>(base + kNaCtl);
+  void *args[] = {&a};
+  MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)lts_kernel, dim3(grid), dim3(kThreads), args, 0, st));
+  ++g_launches;
+  LtsCtl ctl;
+  MB2_CUDA_TRY(cudaMemcpyAsync(&hs, base + kNaState, sizeof(LtsState), cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(&ctl, base + kNaCtl, sizeof(LtsCtl), cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaStreamSynchronize(st));
   if (ctl.err) {
     set_error("LTS grid barrier timed out");
     return MIRORR_ETIMEOUT;
