@@ -67,7 +67,7 @@ __device__ bool grid_sync(LtsCtl *ctl) {
     } else {
       long long spins = 0;
       while (*genp == gen && *errp == 0) {
-        __nanosleep(100);
+        if (spins > 256) __nanosleep(100);
         if (++spins > (1LL << 23)) {
           atomicExch(&ctl->err, 1);
           break;
@@ -87,16 +87,95 @@ __device__ inline void load_cg(void *dst, const void *src, int bytes) {
   for (int i = threadIdx.x; i < bytes / 8; i += blockDim.x) d[i] = __ldcg(s + i);
 }
 
-__device__ inline double block_sum(double v, double *red) {
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+// Adds 1 to bin of a shared histogram, one atomic per group of lanes of the
+// warp that hit the same bin.
+__device__ inline void hist_add(unsigned int *h, unsigned int bin) {
+  const unsigned active = __activemask();
+  const unsigned same = __match_any_sync(active, bin);
+  if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicAdd(&h[bin], (unsigned)__popc(same));
+}
+
+// Bucket of rank k in the shared histogram h[0, kBins): the bin d with
+// cum(d) <= k < cum(d) + h[d] (cum = sum of the bins below d), found with a
+// block-wide scan.  Returns d in *d_out and cum(d) in *cum_out (every thread).
+__device__ inline void find_bucket(const unsigned int *h, unsigned long long k, int nb,
+                                   unsigned long long *s_pair, int *d_out,
+                                   unsigned long long *cum_out) {
+  constexpr int kPer = kBins / kThreads;  // bins per thread
+  __shared__ unsigned long long s_wsum[kThreads / 32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  unsigned long long local = 0;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) local += h[t * kPer + i];
+  unsigned long long inc = local;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    unsigned long long o = __shfl_up_sync(0xffffffffu, inc, off);
+    if (lane >= off) inc += o;
+  }
+  if (lane == 31) s_wsum[wid] = inc;
+  if (t == 0) { s_pair[0] = ~0ULL; s_pair[1] = 0; }
   __syncthreads();
-  if (lane == 0) red[wid] = v;
+  unsigned long long wbase = 0;
+  for (int w = 0; w < wid; ++w) wbase += s_wsum[w];
+  const unsigned long long base = wbase + inc - local;
+  if (local > 0 && base <= k && k < base + local) {
+    unsigned long long cum = base;
+    int d = t * kPer;
+    for (int i = 0; i < kPer; ++i, ++d) {
+      if (cum + h[d] > k) break;
+      cum += h[d];
+    }
+    s_pair[0] = (unsigned long long)d;
+    s_pair[1] = cum;
+  }
   __syncthreads();
-  double r = 0.0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += red[w];
-  return r;  // valid in thread 0
+  if (s_pair[0] == ~0ULL) {
+    // k beyond the histogram's count: the last bin, cum = total
+    unsigned long long total = 0;
+    for (int w = 0; w < kThreads / 32; ++w) total += s_wsum[w];
+    *d_out = nb - 1;
+    *cum_out = total;
+  } else {
+    *d_out = (int)s_pair[0];
+    *cum_out = s_pair[1];
+  }
+  __syncthreads();
+}
+
+// Sums each of v[0, N) over the CTA (per value: shuffle tree within each
+// warp, then the warps in order); out[q] in shared memory, valid for every
+// thread on return.
+template <int N>
+__device__ inline void block_sums(const double (&v)[N], double *red /* N * 32 */, double *out) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    double x = v[q];
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if (lane == 0) red[q * 32 + wid] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < N) {
+    double r = 0.0;
+    for (int w = 0; w < nw; ++w) r += red[threadIdx.x * 32 + w];
+    out[threadIdx.x] = r;
+  }
+  __syncthreads();
+}
+
+// out[q] = sum over the grid's CTAs b of part[b * kPartial + q0 + q], q < nq:
+// warp q % nwarps takes value q, its lanes stride over b, then a shuffle tree
+// (a fixed order).  out in shared memory, valid for every thread on return.
+__device__ inline void grid_partial_sums(const double *part, int q0, int nq, double *out) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int q = wid; q < nq; q += nw) {
+    double x = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(&part[(long long)b * kPartial + q0 + q]);
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if (lane == 0) out[q] = x;
+  }
+  __syncthreads();
 }
 
 __device__ inline double residual(const LtsState &s, const double *x, const double *y) {
@@ -119,9 +198,10 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
   __shared__ __align__(16) LtsState s;
   __shared__ unsigned int h[kBins];
   __shared__ unsigned long long ck[kCandMax];
-  __shared__ double red[32];
+  __shared__ double red_n[21 * 32];
   __shared__ double s_nth;
   __shared__ unsigned long long s_key;
+  __shared__ unsigned long long s_pair[2];
   const long long n = __ldcg(&a.n_dev[0]) + __ldcg(&a.n_dev[1]);
   const long long gstride = (long long)gridDim.x * blockDim.x;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
       if (first) {
         if (key > kmax) kmax = key;
       } else {
-        atomicAdd(&h[(unsigned)(key >> 52) & (kBins - 1)], 1u);
+        hist_add(h, (unsigned)(key >> 52) & (kBins - 1));
       }
     }
     if (first) {
@@ -179,22 +259,11 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         __syncthreads();
         for (int i = threadIdx.x; i < kBins; i += blockDim.x) h[i] = __ldcg(&gh[i]);
         __syncthreads();
-        if (threadIdx.x == 0) {
-          unsigned long long cum = 0;
-          int d = 0;
-          int nb = 1 << bits;
-          for (; d < nb; ++d) {
-            if (cum + h[d] > k) break;
-            cum += h[d];
-          }
-          if (d >= nb) d = nb - 1;
-          s_key = ((unsigned long long)d << 32) | (unsigned long long)h[d];
-          red[0] = (double)cum;
-        }
-        __syncthreads();
-        int d = (int)(s_key >> 32);
-        bucket = s_key & 0xffffffffULL;
-        k -= (unsigned long long)red[0];
+        int d = 0;
+        unsigned long long cum = 0;
+        find_bucket(h, k, 1 << bits, s_pair, &d, &cum);
+        bucket = h[d];
+        k -= cum;
         prefix |= (unsigned long long)d << shift;
         mask |= ((1ULL << bits) - 1ULL) << shift;
         __syncthreads();
@@ -211,8 +280,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         __syncthreads();
         for (long long i = gtid; i < n; i += gstride) {
           unsigned long long key = (unsigned long long)__double_as_longlong(a.resid[i]);
-          if ((key & mask) == prefix)
-            atomicAdd(&h[(unsigned)(key >> shift) & ((1u << bits) - 1u)], 1u);
+          if ((key & mask) == prefix) hist_add(h, (unsigned)(key >> shift) & ((1u << bits) - 1u));
         }
         __syncthreads();
         unsigned int *gh2 = a.hist + (pass % 3) * kBins;
@@ -232,6 +300,25 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
       if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->ncand);
       __syncthreads();
       int nc = (int)(s_key < (unsigned long long)kCandMax ? s_key : kCandMax);
+      const unsigned long long kk = k < (unsigned long long)nc ? k : (nc > 0 ? nc - 1 : 0);
+      if (nc <= kThreads) {
+        // rank by counting: key i has rank k iff lo_i <= k < lo_i + eq_i
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) ck[i] = __ldcg(&a.cand[i]);
+        __syncthreads();
+        if (threadIdx.x < nc) {
+          const unsigned long long v = ck[threadIdx.x];
+          int lo = 0, eq = 0;
+          for (int j = 0; j < nc; ++j) {
+            const unsigned long long u = ck[j];
+            lo += u < v;
+            eq += u == v;
+          }
+          if ((unsigned long long)lo <= kk && kk < (unsigned long long)(lo + eq))
+            s_nth = __longlong_as_double((long long)v);
+        }
+        __syncthreads();
+        nth = s_nth;
+      } else {
       for (int i = threadIdx.x; i < kCandMax; i += blockDim.x)
         ck[i] = (i < nc) ? __ldcg(&a.cand[i]) : ~0ULL;
       __syncthreads();
@@ -248,9 +335,10 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
           }
           __syncthreads();
         }
-      if (threadIdx.x == 0) s_nth = __longlong_as_double((long long)ck[k < (unsigned long long)nc ? k : (nc > 0 ? nc - 1 : 0)]);
+      if (threadIdx.x == 0) s_nth = __longlong_as_double((long long)ck[kk]);
       __syncthreads();
       nth = s_nth;
+      }
     }
     // ---- subset barycentres ---------------------------------------------
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -263,18 +351,12 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         }
       }
     }
-    for (int c = 0; c < 7; ++c) {
-      double v = block_sum(acc[c], red);
-      if (threadIdx.x == 0) a.partial[(long long)blockIdx.x * kPartial + c] = v;
-    }
+    __shared__ double s_out[21];
+    block_sums<7>(acc, red_n, s_out);
+    if (threadIdx.x < 7) a.partial[(long long)blockIdx.x * kPartial + threadIdx.x] = s_out[threadIdx.x];
     if (!grid_sync(a.ctl)) return;
     __shared__ double s_mean[7];
-    if (threadIdx.x < 7) {
-      double t = 0.0;
-      for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(&a.partial[(long long)b * kPartial + threadIdx.x]);
-      s_mean[threadIdx.x] = t;
-    }
-    __syncthreads();
+    grid_partial_sums(a.partial, 0, 7, s_mean);
     const double cnt = s_mean[0];
     double mi[3], mm[3];
     for (int c = 0; c < 3; ++c) { mi[c] = s_mean[1 + c] / cnt; mm[c] = s_mean[4 + c] / cnt; }
@@ -294,21 +376,16 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
       }
     }
     __syncthreads();
-    for (int q = 0; q < 21; ++q) {
-      double v = block_sum(z2[q], red);
-      if (threadIdx.x == 0) a.partial[(long long)blockIdx.x * kPartial + 8 + q] = v;
-    }
+    block_sums<21>(z2, red_n, s_out);
+    if (threadIdx.x < 21) a.partial[(long long)blockIdx.x * kPartial + 8 + threadIdx.x] = s_out[threadIdx.x];
     if (!grid_sync(a.ctl)) return;
+    if (blockIdx.x == 0) grid_partial_sums(a.partial, 8, 21, s_out);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       LtsMoments mo;
       mo.n = cnt;
       for (int c = 0; c < 3; ++c) { mo.mean_i[c] = mi[c]; mo.mean_m[c] = mm[c]; }
       double zz[21];
-      for (int q = 0; q < 21; ++q) {
-        double t = 0.0;
-        for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(&a.partial[(long long)b * kPartial + 8 + q]);
-        zz[q] = t;
-      }
+      for (int q = 0; q < 21; ++q) zz[q] = s_out[q];
       int q = 0;
       for (int r = 0; r < 6; ++r)
         for (int c = r; c < 6; ++c) { mo.Z[6 * r + c] = zz[q]; mo.Z[6 * c + r] = zz[q]; ++q; }
