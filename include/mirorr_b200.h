@@ -214,7 +214,7 @@ typedef struct mirorr_reg_params {
   int32_t min_length;     /* --pyr-min-size (default 32) */
   mirorr_bm_params bm;    /* CLI defaults: width 4, gap 1, nhood gap 3, nhood width 7 */
   double lts_keep;        /* LTS keep fraction (reference: 0.5) */
-  int32_t verbosity;
+  int32_t verbosity;      /* 1: per-iteration lines; 2: also per-call block routing */
 } mirorr_reg_params;
 
 typedef struct mirorr_reg_stats {

@@ -250,9 +250,9 @@ class Context:
             self._h = ctypes.c_void_p()
 
     def __del__(self):
-        if sys.is_finalizing():
-            return
         try:
+            if sys.is_finalizing():
+                return
             self.close()
         except Exception:
             pass
@@ -390,9 +390,9 @@ class BlockMatcher:
             self._h = ctypes.c_void_p()
 
     def __del__(self):
-        if sys.is_finalizing():
-            return
         try:
+            if sys.is_finalizing():
+                return
             self.close()
         except Exception:
             pass

@@ -500,6 +500,15 @@ mirorr_status match_into(RegRun &r, const float *base, const uint8_t *bmask, con
   MB2_TRY(run_match(c, r.p->bm, mc, g, c->best, c->second, c->match, c->status, pts_b, pts_m,
                     c->counts.as<long long>() + count_slot, offset_dev, ev));
   if (r.stats) r.stats->matcher_calls += 1;
+  if (r.p->verbosity >= 2) {
+    // per-call routing of the blocks through the search kernels
+    unsigned int ctl[8] = {0};
+    MB2_CUDA_TRY(cudaMemcpyAsync(ctl, c->bmw.ncc_ctl.ptr, sizeof(ctl), cudaMemcpyDeviceToHost, c->stream));
+    MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    printf("  matcher: %lld blocks, register-blocked %u, masked-window %u, general %u, "
+           "refined candidates %u, overflowed %u\n",
+           g.nblocks, ctl[3], ctl[4], ctl[0], ctl[2], ctl[1]);
+  }
   return MIRORR_OK;
 }
 
@@ -771,7 +780,7 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
-                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->ltsw.state, &c->ltsw.resid,
+                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->bmw.ncc_pad, &c->bmw.ncc_wand, &c->ltsw.state, &c->ltsw.resid,
                     &c->ltsw.partial, &c->ltsw.hist, &c->ltsw.ctrl, &c->ltsw.cand, &c->counts,
                     &c->ncc_count, &c->ones, &c->lvl_f, &c->lvl_m, &c->tmp_a, &c->tmp_b,
                     &c->weights, &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best,

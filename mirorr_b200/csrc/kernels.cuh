@@ -28,9 +28,12 @@ struct BmWork {
   DevBuf tiles;     // compaction tile counts/offsets
   DevBuf ncc_lists; // block lists of the NCC stages (general path, fallback)
   DevBuf ncc_ctl;   // NCC counters: [0] general-path blocks, [1] fallback blocks,
-                    // [2] FP64-refined candidates, [3] fast-path blocks
+                    // [2] FP64-refined candidates, [3] fast-path blocks,
+                    // [4] masked-window blocks
   DevBuf ncc_rec;   // per-block FP32 stage results
   DevBuf ncc_bstat; // per-block base statistics
+  DevBuf ncc_pad;   // search image with 16-byte aligned rows (when its own are not)
+  DevBuf ncc_wand;  // window-AND of the footprint flags (two passes' buffers)
 };
 
 struct BmOut {

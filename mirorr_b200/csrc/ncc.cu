@@ -54,7 +54,7 @@ struct BlockStat {
   double mean;
   float sxx;   // sum over masked voxels of (x - mean)^2
   float sxt;   // sum over masked voxels of (x - mean)
-  int mball;   // every base-mask voxel non-zero
+  int mmode;   // base mask over the block: 1 every voxel non-zero, 2 every voxel zero, 0 mixed
   float c;     // window shift: mean of the block's own candidate footprint
 };
 
@@ -82,6 +82,8 @@ struct NccArgs {
   int *ovf_list;    // blocks for the fallback kernel
   unsigned int *ctl;  // [0] general blocks, [1] overflow blocks, [2] refined candidates,
                       // [3] register-blocked blocks, [4] masked-window blocks
+  const float *search_al;  // the search image with rows of spitch floats, 16-byte aligned
+  int spitch;
 };
 
 __device__ inline void window_axis(int o, int S, int W, int g, int bw, int &s, int &n) {
@@ -158,6 +160,10 @@ __device__ inline void cp_async8(void *dst, const void *src) {
   unsigned int d = (unsigned int)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ inline void cp_async16(float *dst, const float *src) {
+  unsigned int d = (unsigned int)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ inline void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
@@ -172,6 +178,21 @@ __device__ inline void push_deg(int &d1, int &d2, int p) {
   else if (d2 < 0) d2 = p;
 }
 
+// A block whose base mask is zero everywhere has Sxx = 0 for every candidate,
+// so every score is -2 (normalizedCorrelation's degenerate case): the
+// sequential update leaves best = -2, second = -2 (-3 with one candidate) and
+// the match at the first candidate in raster order, the clipped window's start.
+__device__ inline void finish_unmasked_block(const NccArgs &a, long long b) {
+  BlockWin w;
+  if (block_window(a, b, w)) {
+    write_final(a, b, -2.f, w.nc >= 2 ? -2.f : -3.f, lin(a, w.sx, w.sy, w.sz), 1);
+    if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)w.nc);
+  } else {
+    write_final(a, b, -3.f, -3.f, lin(a, w.ox, w.oy, w.oz), 1);
+  }
+  a.rec[b].cnt = -1;
+}
+
 // ---------------------------------------------------------------------------
 // base-block statistics (one thread per block)
 // ---------------------------------------------------------------------------
@@ -182,13 +203,13 @@ __global__ void block_stat_kernel(NccArgs a) {
     long long o = lin(a, a.stx + bx * a.G, a.sty + by * a.G, a.stz + bz * a.G);
     const int bw = a.bw;
     double sum = 0.0;
-    int mball = 1;
+    int nin = 0;
     for (int z = 0; z < bw; ++z)
       for (int y = 0; y < bw; ++y)
         for (int x = 0; x < bw; ++x) {
           long long q = o + ((long long)z * a.ny + y) * a.nx + x;
           sum = __dadd_rn(sum, (double)__ldg(&a.base[q]));
-          if (!__ldg(&a.bmask[q])) mball = 0;
+          if (__ldg(&a.bmask[q])) ++nin;
         }
     double mean = __ddiv_rn(sum, (double)(bw * bw * bw));
     double sxx = 0.0, sxt = 0.0;
@@ -206,7 +227,7 @@ __global__ void block_stat_kernel(NccArgs a) {
     s.mean = mean;
     s.sxx = (float)sxx;
     s.sxt = (float)sxt;
-    s.mball = mball;
+    s.mmode = nin == bw * bw * bw ? 1 : (nin == 0 ? 2 : 0);
     s.c = __ldg(&a.stats[o]).x;
     const_cast<BlockStat *>(a.bstat)[b] = s;
   }
@@ -307,7 +328,7 @@ __global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
         }
         if (ok) {
           BlockStat st = a.bstat[b];
-          if (st.mball) {
+          if (st.mmode == 1) {
             state = 1;
             s_sxt[tid] = st.sxt;
             s_sxx[tid] = st.sxx;
@@ -624,11 +645,15 @@ __global__ void __launch_bounds__(C::WPC * 32, C::MINB) ncc_warp_kernel(NccArgs 
           write_final(a, b, -3.f, -3.f, ((long long)bz0 * ny + by0) * nx + bx0, 0);
           a.rec[b].cnt = -1;
         }
-      } else if (st.mball) {
+      } else if (st.mmode == 1) {
         state = 1;
       } else if (sln == 0) {
-        unsigned int p = atomicAdd(&a.ctl[0], 1u);
-        a.gen_list[p] = b;
+        if (st.mmode == 2) {
+          finish_unmasked_block(a, b);
+        } else {
+          unsigned int p = atomicAdd(&a.ctl[0], 1u);
+          a.gen_list[p] = b;
+        }
       }
     }
     if (sln == 0) s_cnt[slot] = 0;
@@ -801,6 +826,328 @@ __global__ void __launch_bounds__(C::WPC * 32, C::MINB) ncc_warp_kernel(NccArgs 
 }
 
 // ---------------------------------------------------------------------------
+// Window-AND of the footprint flags.  wand[s] (s = window start, each axis
+// from -R, stored at s + R) is 1 when every candidate of the W^3 window
+// starting at s whose footprint lies inside the volume has its footprint
+// wholly inside the search mask (box_stats: Syy sign bit clear).  Separable:
+// one pass per axis, out-of-range positions count as 1.
+// ---------------------------------------------------------------------------
+__global__ void wand_x_kernel(const float2 *stats, uint8_t *out, int nx, int ny, int nz, int W,
+                              int bw) {
+  const int R = W / 2, nxo = nx + R;
+  const long long n = (long long)nxo * ny * nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int sx = (int)(i % nxo) - R;
+    const long long yz = i / nxo;
+    const int y = (int)(yz % ny), z = (int)(yz / ny);
+    unsigned v = 1;
+    if (y <= ny - bw && z <= nz - bw) {
+      const float *fy = reinterpret_cast<const float *>(stats + yz * nx) + 1;
+      for (int q = sx < 0 ? 0 : sx; q < sx + W && q <= nx - bw; ++q)
+        v &= footprint_in_mask(__ldg(fy + 2 * q)) ? 1u : 0u;
+    }
+    out[i] = (uint8_t)v;
+  }
+}
+
+// AND over a window of W along the middle axis of [outer][n][inner] -> [outer][n + R][inner].
+__global__ void wand_axis_kernel(const uint8_t *in, uint8_t *out, long long inner, int n,
+                                 long long outer, int W) {
+  const int R = W / 2, no = n + R;
+  const long long total = outer * no * inner;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long ii = i % inner;
+    const long long r = i / inner;
+    const int sa = (int)(r % no) - R;
+    const long long o = r / no;
+    unsigned v = 1;
+    for (int q = sa < 0 ? 0 : sa; q < sa + W && q < n; ++q) v &= in[(o * n + q) * inner + ii];
+    out[i] = (uint8_t)v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Lane-per-x-offset FP32 search, block width 4, block gap 1, for blocks whose
+// base block and window lie wholly inside both masks.
+//
+// A warp takes BPW = 32 / W consecutive blocks of one row of the block grid
+// (same by, bz).  Lane (k, x) scores the W x W candidates of block k whose x
+// offset in the window is x, i.e. every (cy, cz).  The blocks' windows
+// overlap along x, so the warp stages their union once, with rows starting at
+// a 16-byte aligned x (16-byte asynchronous copies); at every load the lanes
+// read consecutive floats of one row (no bank conflicts).  The lane's base
+// block (x~ = x - mean, 64 values) sits in registers and each window row is
+// read once, shifted by the block's constant c as it is read
+// (Sxy = sum x~ (y - c) - (mu - c) sum x~ keeps the FP32 cross term free of
+// cancellation).  A window plane wz feeds the candidate planes wz - 3 .. wz;
+// their accumulators rotate through four register sets and a plane is scored
+// once its last window plane has been read.  The scores go to the shared
+// memory of a window plane already consumed; after the block-level top-2
+// reduction one pass over them lists the candidates within 2 delta of the
+// block's FP32 second-best.  Blocks whose window is partly masked (window-AND
+// of the footprint flags) go to the masked kernel, blocks with a partly
+// masked base block to the general kernel.
+// ---------------------------------------------------------------------------
+constexpr int kXMinBlocks = 12;
+
+struct XArgs {
+  const uint8_t *wand;  // window-AND of the footprint flags, (nz+R) x (ny+R) x (nx+R)
+  int rpu;              // union row pitch in floats (multiple of 4)
+  int nch;              // 16-byte chunks per union row
+  int tpr;              // warp tiles per row of the block grid
+  long long ntiles;
+};
+
+template <int W>
+__global__ void __launch_bounds__(32, kXMinBlocks) ncc_xlane_kernel(NccArgs a, XArgs xa) {
+  constexpr int R = W / 2, E = W + 3, BPW = 32 / W;
+  extern __shared__ __align__(16) float sm[];
+  float *win = sm;                      // E * E * rpu
+  float *xt = sm + E * E * xa.rpu;      // BPW * 64
+  float2 *qbuf = reinterpret_cast<float2 *>(xt + BPW * 64);  // 32 * W
+  __shared__ float s_red[BPW][W][2];
+  __shared__ int s_deg[BPW][W][2];
+  __shared__ float s_f[BPW][2];
+  __shared__ int s_cnt[BPW];
+  __shared__ int s_list[BPW][kK];
+  const int lane = threadIdx.x;
+  const int k = lane / W, x = lane - k * W;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const unsigned full = 0xffffffffu;
+  const unsigned seg = ((1u << W) - 1u) << (k < BPW ? k * W : 0);
+
+  for (long long tile = blockIdx.x; tile < xa.ntiles; tile += gridDim.x) {
+    const long long grow = tile / xa.tpr;
+    const int bx0 = (int)(tile - grow * xa.tpr) * BPW;
+    const int by = (int)(grow % a.nby), bz = (int)(grow / a.nby);
+    const int nbt = min(BPW, a.nbx - bx0);
+    const bool mine = k < nbt;
+    const long long brow = ((long long)bz * a.nby + by) * a.nbx;
+    const long long b = brow + bx0 + (mine ? k : 0);
+    const int oy = a.sty + by * a.G - R, oz = a.stz + bz * a.G - R;
+    const int ox0 = a.stx + bx0 * a.G - R;
+    const int ox = ox0 + k * a.G;
+    const int xu = ox0 & ~3;             // union origin, rounded down to 16 bytes
+    // ---- routing ----------------------------------------------------------
+    int state = 0;
+    BlockStat st;
+    st.mean = 0.0; st.sxx = 0.f; st.sxt = 0.f; st.mmode = 0; st.c = 0.f;
+    if (mine) {
+      st = a.bstat[b];
+      const bool sel = !a.selected || a.selected[b];
+      if (!sel) {
+        if (x == 0) {
+          write_final(a, b, -3.f, -3.f, lin(a, ox + R, oy + R, oz + R), 0);
+          a.rec[b].cnt = -1;
+        }
+      } else if (st.mmode == 1) {
+        state = 1;
+      } else if (x == 0) {
+        if (st.mmode == 2) {
+          finish_unmasked_block(a, b);
+        } else {
+          unsigned int p = atomicAdd(&a.ctl[0], 1u);
+          a.gen_list[p] = (int)b;
+        }
+      }
+    }
+    if (lane < BPW) s_cnt[lane] = 0;
+    // ---- window inside the search mask? -----------------------------------
+    const int px = ox + x;
+    const bool xok = px >= 0 && px <= nx - 4;
+    unsigned yok = 0;
+#pragma unroll
+    for (int cy = 0; cy < W; ++cy)
+      if (oy + cy >= 0 && oy + cy <= ny - 4) yok |= 1u << cy;
+    const bool inmask =
+        !state || xa.wand[((long long)(oz + R) * (ny + R) + (oy + R)) * (nx + R) + (ox + R)];
+    const unsigned bad = __ballot_sync(full, state && !inmask);
+    if (state && (bad & seg)) {
+      if (x == 0) {
+        unsigned int p = atomicAdd(&a.ctl[4], 1u);
+        a.gen_list[a.nblocks + 1 + p] = (int)b;
+      }
+      state = 0;
+    }
+    const unsigned act = __ballot_sync(full, state);
+    if (act == 0) continue;
+    // ---- staging: union window rows and the base blocks (x~) ---------------
+    const int nch = xa.nch, rpu = xa.rpu;
+    for (int r = lane; r < E * E; r += 32) {
+      const int z = r / E, y = r - z * E;
+      const int gz = oz + z, gy = oy + y;
+      float4 *dst = reinterpret_cast<float4 *>(win + r * rpu);
+      if (gz < 0 || gz >= nz || gy < 0 || gy >= ny) {
+        for (int ch = 0; ch < nch; ++ch) dst[ch] = make_float4(0.f, 0.f, 0.f, 0.f);
+        continue;
+      }
+      const float *src = a.search_al + ((long long)gz * ny + gy) * a.spitch;
+      for (int ch = 0; ch < nch; ++ch) {
+        const int gx = xu + 4 * ch;
+        if (gx >= 0 && gx + 4 <= nx) {
+          cp_async16(reinterpret_cast<float *>(dst + ch), src + gx);
+        } else {
+          float4 v;
+          v.x = (gx >= 0 && gx < nx) ? src[gx] : 0.f;
+          v.y = (gx + 1 >= 0 && gx + 1 < nx) ? src[gx + 1] : 0.f;
+          v.z = (gx + 2 >= 0 && gx + 2 < nx) ? src[gx + 2] : 0.f;
+          v.w = (gx + 3 >= 0 && gx + 3 < nx) ? src[gx + 3] : 0.f;
+          dst[ch] = v;
+        }
+      }
+    }
+    for (int i = lane; i < nbt * 64; i += 32) {
+      const int kk = i >> 6, v = i & 63;
+      const int vx = v & 3, vy = (v >> 2) & 3, vz = v >> 4;
+      const long long q = ((long long)(oz + R + vz) * ny + (oy + R + vy)) * nx +
+                          (ox0 + kk * a.G + R + vx);
+      const double mk = a.bstat[brow + bx0 + kk].mean;
+      xt[i] = (float)__dsub_rn((double)__ldg(&a.base[q]), mk);
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    // ---- FP32 scores ---------------------------------------------------------
+    float l1 = -3.f, l2 = -3.f;
+    int d1 = -1, d2 = -1;
+    const int E_rpu = E * rpu;
+    if (state) {
+      float t[64];
+      const float4 *tp = reinterpret_cast<const float4 *>(xt + k * 64);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float4 q = tp[i];
+        t[4 * i] = q.x; t[4 * i + 1] = q.y; t[4 * i + 2] = q.z; t[4 * i + 3] = q.w;
+      }
+      const float c = st.c, sxt = st.sxt, sxx = st.sxx;
+      float2 *qb = qbuf + lane * W;
+      const float2 *st0 = a.stats + (((long long)oz * ny + oy) * nx + px);
+      const float *rp = win + (ox - xu) + x;
+      // acc[j]: candidate plane cz = wz - 3 + j.  Window plane wz feeds the
+      // planes wz - 3 .. wz (j = 3 - vz); planes outside 0 .. W-1, fed at the
+      // first and last three window planes, are never scored.
+      float acc[4][W];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int cy = 0; cy < W; ++cy) acc[j][cy] = 0.f;
+#pragma unroll 1
+      for (int wz = 0; wz < E; ++wz) {
+        const int cz = wz - 3;
+        const bool zok = cz >= 0 && xok && oz + cz >= 0 && oz + cz <= nz - 4;
+        if (zok) {
+          // statistics of the plane completed below, fetched meanwhile
+#pragma unroll
+          for (int cy = 0; cy < W; ++cy)
+            if ((yok >> cy) & 1u) cp_async8(qb + cy, st0 + ((long long)cz * ny + cy) * nx);
+          asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
+#pragma unroll
+        for (int wy = 0; wy < E; ++wy) {
+          float r[4];
+#pragma unroll
+          for (int vx = 0; vx < 4; ++vx) r[vx] = rp[vx] - c;
+          rp += rpu;
+#pragma unroll
+          for (int vx = 0; vx < 4; ++vx)
+#pragma unroll
+            for (int vz = 0; vz < 4; ++vz)
+#pragma unroll
+              for (int vy = 0; vy < 4; ++vy) {
+                const int cy = wy - vy;
+                if (cy < 0 || cy >= W) continue;
+                acc[3 - vz][cy] = fmaf(t[(vz * 4 + vy) * 4 + vx], r[vx], acc[3 - vz][cy]);
+              }
+        }
+        if (cz >= 0) {
+          // window plane cz was read three planes ago: its rows now hold the
+          // scores of candidate plane cz (lane-major, W per lane)
+          __syncwarp(act);
+          if (zok) {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            float *sc = win + cz * E_rpu + lane * W;
+            const long long prow = ((long long)(oz + cz) * ny + oy) * nx + px;
+#pragma unroll
+            for (int cy = 0; cy < W; ++cy) {
+              if (!((yok >> cy) & 1u)) continue;
+              const float2 q = qb[cy];
+              const float sxy = acc[0][cy] - (q.x - c) * sxt;
+              const float s = (sxx <= 0.f || q.y <= 0.f)
+                                  ? -2.f : __fdividef(__fdividef(sxy * sxy, sxx), q.y);
+              top2_merge(l1, l2, s, -3.f);
+              if (s == -2.f) push_deg(d1, d2, (int)(prow + (long long)cy * nx));
+              sc[cy] = s;
+            }
+          }
+        }
+        // rotate: plane wz - 3 is done, plane wz + 1 starts
+#pragma unroll
+        for (int cy = 0; cy < W; ++cy) {
+          acc[0][cy] = acc[1][cy];
+          acc[1][cy] = acc[2][cy];
+          acc[2][cy] = acc[3][cy];
+          acc[3][cy] = 0.f;
+        }
+      }
+    }
+    // ---- block-level reduction and refinement list --------------------------
+    if (state) {
+      s_red[k][x][0] = l1; s_red[k][x][1] = l2;
+      s_deg[k][x][0] = d1; s_deg[k][x][1] = d2;
+    }
+    __syncwarp();
+    if (state && x == 0) {
+      float f1 = -3.f, f2 = -3.f;
+      int e1 = -1, e2 = -1;
+      for (int j = 0; j < W; ++j) {
+        top2_merge(f1, f2, s_red[k][j][0], s_red[k][j][1]);
+        min2_merge(e1, e2, s_deg[k][j][0], s_deg[k][j][1]);
+      }
+      s_f[k][0] = f1; s_f[k][1] = f2;
+      s_deg[k][0][0] = e1; s_deg[k][0][1] = e2;
+    }
+    __syncwarp();
+    if (state && xok) {
+      // candidates within 2 delta of the block's FP32 second-best
+      const float T2 = s_f[k][1] - 2.f * kDelta;
+      for (int cz = 0; cz < W; ++cz) {
+        if (oz + cz < 0 || oz + cz > nz - 4) continue;
+        const float *sc = win + cz * E_rpu + lane * W;
+        const long long prow = ((long long)(oz + cz) * ny + oy) * nx + px;
+#pragma unroll
+        for (int cy = 0; cy < W; ++cy) {
+          if (!((yok >> cy) & 1u)) continue;
+          const float sv = sc[cy];
+          if (sv > -2.f && sv >= T2) {
+            const int pos = atomicAdd(&s_cnt[k], 1);
+            if (pos < kK) s_list[k][pos] = (int)(prow + (long long)cy * nx);
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (state && x == 0) {
+      NccRec &rc = a.rec[b];
+      const float f1 = s_f[k][0], f2 = s_f[k][1];
+      int cnt = s_cnt[k];
+      rc.f1 = f1;
+      rc.f2 = f2;
+      if (cnt <= kK) {
+        for (int j = 0; j < cnt; ++j) rc.p[j] = s_list[k][j];
+        if (f2 <= -2.f) {
+          if (s_deg[k][0][0] >= 0) rc.p[cnt++] = s_deg[k][0][0];
+          if (s_deg[k][0][1] >= 0) rc.p[cnt++] = s_deg[k][0][1];
+        }
+      }
+      rc.cnt = cnt;
+      atomicAdd(&a.ctl[3], 1u);
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // General FP32 search: one CTA (128 threads) per block, any mask pattern.
 // ---------------------------------------------------------------------------
 template <int BW>
@@ -835,6 +1182,10 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
       }
     }
     const BlockStat bst = a.bstat[b];
+    if (bst.mmode == 2) {
+      if (tid == 0) finish_unmasked_block(a, b);
+      continue;
+    }
     for (int v = tid; v < B; v += blockDim.x) {
       int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
       long long q = obase + ((long long)vz * a.ny + vy) * a.nx + vx;
@@ -854,7 +1205,7 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
     }
     if (tid == 0) s_cnt = 0;
     const int ms_all = __syncthreads_and(all_in);
-    const bool fast = bst.mball && ms_all;
+    const bool fast = bst.mmode == 1 && ms_all;
     float l1 = -3.f, l2 = -3.f;
     int d1 = -1, d2 = -1;
     // pass 1: FP32 top-2 and the first degenerate candidates
@@ -921,7 +1272,7 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
                 }
               }
           sxx = ax;
-          syy = bst.mball ? syy_of(st.y) : ay;
+          syy = bst.mmode == 1 ? syy_of(st.y) : ay;
         }
         float s = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
         if (pass == 0) {
@@ -1151,15 +1502,77 @@ mirorr_status launch_rest(const NccArgs &a, bool all_general, cudaStream_t s) {
   return MIRORR_OK;
 }
 
+// Per-x-lane search (block width 4) and the masked-window kernel; done is
+// false when the union window would not fit (very wide block spacing).
+template <int W, class CM>
+mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done) {
+  constexpr int E = W + 3, BPW = 32 / W;
+  done = false;
+  const long long u = (long long)(BPW - 1) * a.G + E;   // union row length
+  XArgs xa;
+  xa.nch = (int)((u + 6) / 4);
+  xa.rpu = 4 * xa.nch;
+  // each window plane must hold one plane of scores (W per lane) once read
+  const int min_rpu = ((BPW * W + E - 1) / E + 3) & ~3;
+  if (xa.rpu < min_rpu) {
+    xa.rpu = min_rpu;
+    xa.nch = min_rpu / 4;
+  }
+  xa.tpr = (a.nbx + BPW - 1) / BPW;
+  xa.ntiles = (long long)xa.tpr * a.nby * a.nbz;
+  const size_t smem = sizeof(float) * ((size_t)E * E * xa.rpu + BPW * 64 + 64 * W);
+  if (xa.nch > 32 || smem > 64 * 1024) return MIRORR_OK;
+  // rows of the search image must start on 16 bytes for the 16-byte copies
+  a.search_al = a.search;
+  a.spitch = a.nx;
+  if ((a.nx & 3) || (reinterpret_cast<uintptr_t>(a.search) & 15)) {
+    a.spitch = (a.nx + 3) & ~3;
+    MB2_TRY(w.ncc_pad.ensure(sizeof(float) * (size_t)a.spitch * a.ny * a.nz));
+    MB2_CUDA_TRY(cudaMemcpy2DAsync(w.ncc_pad.ptr, sizeof(float) * a.spitch, a.search,
+                                   sizeof(float) * a.nx, sizeof(float) * a.nx,
+                                   (size_t)a.ny * a.nz, cudaMemcpyDeviceToDevice, s));
+    a.search_al = w.ncc_pad.as<float>();
+  }
+  // window-AND of the footprint flags, one pass per axis
+  {
+    constexpr int R = W / 2;
+    const long long nxo = a.nx + R, nyo = a.ny + R, nzo = a.nz + R;
+    const size_t bytes = (size_t)(nxo * nyo * nzo);
+    MB2_TRY(w.ncc_wand.ensure(2 * bytes));
+    uint8_t *b0 = w.ncc_wand.as<uint8_t>(), *b1 = b0 + bytes;
+    const unsigned g = 148 * 8;
+    wand_x_kernel<<<g, 256, 0, s>>>(a.stats, b0, a.nx, a.ny, a.nz, W, 4);
+    MB2_LAUNCH_CHECK();
+    wand_axis_kernel<<<g, 256, 0, s>>>(b0, b1, nxo, a.ny, a.nz, W);
+    MB2_LAUNCH_CHECK();
+    wand_axis_kernel<<<g, 256, 0, s>>>(b1, b0, nxo * nyo, a.nz, 1, W);
+    MB2_LAUNCH_CHECK();
+    xa.wand = b0;
+  }
+  MB2_TRY(set_smem(ncc_xlane_kernel<W>, smem));
+  const long long grid = xa.ntiles < 148LL * kXMinBlocks ? xa.ntiles : 148LL * kXMinBlocks;
+  ncc_xlane_kernel<W><<<(unsigned)grid, 32, smem, s>>>(a, xa);
+  MB2_LAUNCH_CHECK();
+  MB2_TRY((launch_fast1<CM, true>(a, s)));
+  done = true;
+  return MIRORR_OK;
+}
+
 // Block width / window combinations with a register-blocked fast kernel.
-bool run_fast(const NccArgs &a, cudaStream_t s, mirorr_status &st) {
+bool run_fast(NccArgs &a, BmWork &w, cudaStream_t s, mirorr_status &st) {
   if (a.g != 1) return false;
   if ((long long)a.nx * a.ny * a.nz >= (1LL << 31)) return false;
   if (a.bw == 4 && a.W == 9) {
+    bool done = false;
+    st = launch_xlane<9, FastCfg<4, 9, 1, 3>>(a, w, s, done);
+    if (st != MIRORR_OK || done) return true;
     st = launch_fast<WarpCfg<4, 9, 3, 1, 5, 3>, FastCfg<4, 9, 1, 3>>(a, s);
     return true;
   }
   if (a.bw == 4 && a.W == 7) {
+    bool done = false;
+    st = launch_xlane<7, FastCfg<4, 7, 1, 5>>(a, w, s, done);
+    if (st != MIRORR_OK || done) return true;
     st = launch_fast<WarpCfg<4, 7, 4, 2, 4, 3>, FastCfg<4, 7, 1, 5>>(a, s);
     return true;
   }
@@ -1201,6 +1614,8 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
   a.gen_list = w.ncc_lists.as<int>();
   a.ovf_list = a.gen_list + 2 * (g.nblocks + 1);
   a.ctl = w.ncc_ctl.as<unsigned int>();
+  a.search_al = search;
+  a.spitch = g.size[0];
   {
     long long grid = (g.nblocks + 127) / 128;
     if (grid > 148LL * 16) grid = 148LL * 16;
@@ -1208,7 +1623,7 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
     MB2_LAUNCH_CHECK();
   }
   mirorr_status st = MIRORR_OK;
-  bool fast = run_fast(a, s, st);
+  bool fast = run_fast(a, w, s, st);
   MB2_TRY(st);
   switch (g.bw) {
     case 1: return launch_rest<1>(a, !fast, s);
