@@ -53,6 +53,19 @@ WORKLOAD = ("symmetric affine registration, 256x256x128 float32 phantom pair (80
             "LTS keep 0.5, 10 iterations/level")
 
 
+def traffic_bytes_per_candidate():
+    """DRAM bytes per scored candidate of the search kernel, from the committed
+    ncu summary (line 'bytes_per_candidate: X'); None when absent."""
+    p = os.path.join(ROOT, "profiles", "ncc_xlane_kernel_256x256x128.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.strip().startswith("bytes_per_candidate:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -180,6 +193,8 @@ def run_cuda(args):
         times, stats, res = [], [], None
         ctx.set_profiling(profile)
         ctx.stage_times()
+        if profile:
+            ctx.search_kernel_times()
         l0 = ctx.kernel_launches()
         for _ in range(args.steps):
             flush.fill_(1.0)  # L2 flush between steps, outside the events
@@ -194,14 +209,15 @@ def run_cuda(args):
             stats.append(st)
         launches = ctx.kernel_launches() - l0
         stage_ms, calls = ctx.stage_times()
+        kern = ctx.search_kernel_times() if profile else (0.0, 0, 0)
         ctx.set_profiling(False)
-        return times, stats, res, launches, stage_ms, calls
+        return times, stats, res, launches, (stage_ms, kern), calls
 
     sampler = ClockSampler(dev)
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    t_dev, st_dev, res_dev, launches, stage_ms, calls = timed(step_device, True)
+    t_dev, st_dev, res_dev, launches, (stage_ms, kern), calls = timed(step_device, True)
     t_e2e, st_e2e, res_e2e, _, _, _ = timed(step_e2e, False)
     clocks = sampler.stop()
     torch.cuda.synchronize()
@@ -218,14 +234,22 @@ def run_cuda(args):
     e2e_value = regs / (total_e2e / 1e3)
     ncc = st_dev[-1].block_ncc_evaluated
     peaks, peak_src = load_peaks()
-    # NCC search kernel roofline: FP32 FMA bound, 2*B algorithmic flops per
-    # block-NCC (the cross term; mean and sum of squares come from box_stats)
+    # Roofline of the dominant kernel, the per-x-lane FP32 NCC search: FP32 FMA
+    # bound, 2*B algorithmic flops per block-NCC (the cross term; mean and sum
+    # of squares come from box_stats).  Its launches are bracketed by CUDA
+    # events on the context's stream and a device counter adds up the
+    # candidates it scores.
     flops_per_ncc = 2 * BW ** 3
+    k_ms, k_launches, k_cands = kern
+    k_avg_ms = k_ms / max(k_launches, 1)
+    k_cands_per_launch = k_cands / max(k_launches, 1)
+    achieved = flops_per_ncc * k_cands / (k_ms / 1e3) / 1e12 if k_ms > 0 else 0.0
+    fma_peak = 148 * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    bpc = traffic_bytes_per_candidate()
+    traffic = round(bpc * k_cands_per_launch) if bpc else None
     ncc_ms_per_call = stage_ms[2] / max(calls, 1)
     ncc_per_call = sum(s.block_ncc_evaluated for s in st_dev) / max(
         sum(s.matcher_calls for s in st_dev), 1)
-    achieved = flops_per_ncc * ncc_per_call / (ncc_ms_per_call / 1e3) / 1e12
-    fma_peak = 148 * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
     err = tre(res_dev.M, res_dev.off, ph.true_matrix, ph.true_offset, SHAPE, ph.spacing)
     d_e2e = np.max(np.abs(res_e2e.M - res_dev.M))
     out = {
@@ -249,14 +273,21 @@ def run_cuda(args):
                 "d2h_bytes_per_step": int(st_e2e[-1].d2h_bytes),
                 "latency_ms": {"p50": round(float(np.percentile(t_e2e, 50)), 3),
                                "p99": round(float(np.percentile(t_e2e, 99)), 3)}},
-        "roofline": {"kernel": "ncc_kernel (NCC search)", "bound": "fma",
+        "roofline": {"kernel": f"ncc_xlane_kernel<{NW}> (FP32 NCC search)", "bound": "fma",
                      "achieved": round(achieved, 3), "peak": round(fma_peak, 2),
-                     "unit": "TFLOP/s", "frac": round(achieved / fma_peak, 4), "traffic": None,
+                     "unit": "TFLOP/s", "frac": round(achieved / fma_peak, 4), "traffic": traffic,
                      "peak_source": "nominal FP32 FMA: 148 SMs x 128 lanes x 2 x sm_max_mhz "
                                     f"from MEASURED_PEAKS.json ({peak_src}); that file has no "
                                     "FP32 figure",
                      "flops_per_block_ncc": flops_per_ncc,
-                     "avg_launch_ms": round(ncc_ms_per_call, 4)},
+                     "launches": int(k_launches),
+                     "avg_launch_ms": round(k_avg_ms, 4),
+                     "candidates_per_launch": round(k_cands_per_launch),
+                     "traffic_source": "dram bytes read+written per candidate from the ncu "
+                                       "capture in profiles/ncc_xlane_kernel_256x256x128.md, "
+                                       "times this run's candidates per launch",
+                     "ncc_stage_ms_per_call": round(ncc_ms_per_call, 4),
+                     "ncc_stage_block_ncc_per_call": round(ncc_per_call)},
         "stage_ms_per_registration": {k: round(v / args.steps, 3) for k, v in
                                       zip(["box_stats", "selection", "ncc", "postfilter"], stage_ms)},
         "gpu_launches": int(launches),

@@ -285,6 +285,13 @@ MIRORR_API void *mirorr_ctx_stream(mirorr_ctx ctx);
  * search, post-filter] and the number of matcher calls, and resets them. */
 MIRORR_API mirorr_status mirorr_ctx_set_profiling(mirorr_ctx ctx, int32_t on);
 MIRORR_API mirorr_status mirorr_ctx_stage_times(mirorr_ctx ctx, double ms[4], int64_t *calls);
+/* With profiling on, CUDA events also bracket each launch of the FP32 search
+ * kernel for block width 4 (the per-x-lane kernel, the NCC stage's dominant
+ * kernel) and a device counter adds up the candidates it scores.  Returns the
+ * accumulated milliseconds, launches and candidates, and resets them.  A
+ * profiling aid with no counterpart in the reference. */
+MIRORR_API mirorr_status mirorr_ctx_search_kernel_times(mirorr_ctx ctx, double *ms, int64_t *launches,
+                                             int64_t *candidates);
 
 #ifdef __cplusplus
 }

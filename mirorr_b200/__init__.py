@@ -190,6 +190,9 @@ def lib():
     L.mirorr_ctx_set_profiling.argtypes = [vp, ctypes.c_int32]
     L.mirorr_ctx_stage_times.restype = st
     L.mirorr_ctx_stage_times.argtypes = [vp, vp, P(ctypes.c_int64)]
+    L.mirorr_ctx_search_kernel_times.restype = st
+    L.mirorr_ctx_search_kernel_times.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_int64),
+                                                 P(ctypes.c_int64)]
     _lib = L
     return L
 
@@ -240,6 +243,16 @@ class Context:
         calls = ctypes.c_int64(0)
         _check(lib().mirorr_ctx_stage_times(self._h, _ptr(ms), ctypes.byref(calls)))
         return ms, calls.value
+
+    def search_kernel_times(self):
+        """(ms, launches, candidates) of the per-x-lane FP32 search kernel since
+        the last read (profiling on)."""
+        ms = ctypes.c_double(0.0)
+        launches = ctypes.c_int64(0)
+        cands = ctypes.c_int64(0)
+        _check(lib().mirorr_ctx_search_kernel_times(self._h, ctypes.byref(ms), ctypes.byref(launches),
+                                                    ctypes.byref(cands)))
+        return ms.value, launches.value, cands.value
 
     def close(self):
         if self._h:

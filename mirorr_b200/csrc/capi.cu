@@ -32,11 +32,15 @@ using namespace mb2;
 
 // Per-stage timing of matcher calls, accumulated from CUDA events.
 struct StageTimer {
+  static constexpr size_t kPerCall = 7;  // 5 stage boundaries + the search kernel's 2
   bool on = false;
   std::vector<cudaEvent_t> pool;
   size_t used = 0;
   double ms[4] = {0, 0, 0, 0};
   long long calls = 0;
+  double search_ms = 0.0;     // the FP32 search kernel (events 5, 6 of a call)
+  long long search_calls = 0;
+  std::vector<char> ran;      // per call: the search kernel ran (events 5, 6 recorded)
   cudaEvent_t *take(size_t k) {
     while (pool.size() < used + k) {
       cudaEvent_t e;
@@ -49,19 +53,28 @@ struct StageTimer {
   }
   // call after a stream synchronize
   void harvest() {
-    for (size_t i = 0; i + 5 <= used; i += 5) {
+    for (size_t i = 0; i + kPerCall <= used; i += kPerCall) {
       for (int s = 0; s < 4; ++s) {
         float t = 0.f;
         if (cudaEventElapsedTime(&t, pool[i + s], pool[i + s + 1]) == cudaSuccess) ms[s] += t;
       }
+      const size_t j = i / kPerCall;
+      float t = 0.f;
+      if (j < ran.size() && ran[j] &&
+          cudaEventElapsedTime(&t, pool[i + 5], pool[i + 6]) == cudaSuccess) {
+        search_ms += t;
+        ++search_calls;
+      }
       ++calls;
     }
+    ran.clear();
     used = 0;
     cudaGetLastError();
   }
   void release() {
     for (auto e : pool) cudaEventDestroy(e);
     pool.clear();
+    ran.clear();
     used = 0;
   }
 };
@@ -77,6 +90,7 @@ struct mirorr_ctx_s {
   DevBuf ones;        // default all-255 mask
   long long ones_n = 0;
   StageTimer timer;
+  DevBuf xl_count;    // unsigned long long: candidates scored by the search kernel
   // registration scratch
   DevBuf lvl_f, lvl_m, tmp_a, tmp_b, weights;
   DevBuf img_b, img_s, msk_b, msk_s;
@@ -231,7 +245,9 @@ struct MatchCall {
 mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall &mc,
                         BmGeom &g, DevBuf &best, DevBuf &second, DevBuf &match,
                         DevBuf &status, double *pts_b, double *pts_m, long long *count_dev,
-                        const long long *offset_dev, cudaEvent_t *ev) {
+                        const long long *offset_dev, cudaEvent_t *ev,
+                        cudaEvent_t *kev = nullptr, unsigned long long *xl_count = nullptr,
+                        bool *xl_ran = nullptr) {
   if (!bm_geometry(mc.size, (int)p.block_width, (int)p.block_gap, (int)p.nhood_gap,
                    (int)p.nhood_width, g)) {
     set_error("image smaller than one block or invalid block parameters");
@@ -252,7 +268,8 @@ mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall
   if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
   BmOut out{best.as<float>(), second.as<float>(), match.as<int32_t>(), status.as<uint8_t>()};
   MB2_TRY(launch_ncc(g, mc.base, mc.bmask, mc.search, mc.smask, c->bmw.stats.as<float2>(), sel,
-                     out, c->bmw, c->ncc_count.as<unsigned long long>(), s));
+                     out, c->bmw, c->ncc_count.as<unsigned long long>(), s, kev, xl_count,
+                     xl_ran));
   if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[3], s));
   PointGeom pg;
   point_geom(mc.point_geom.origin, mc.point_geom.spacing, mc.point_geom.direction,
@@ -496,9 +513,12 @@ mirorr_status match_into(RegRun &r, const float *base, const uint8_t *bmask, con
   MatchCall mc{base, search, bmask, smask, {base_g.size[0], base_g.size[1], base_g.size[2]},
                base_g};
   BmGeom g;
-  cudaEvent_t *ev = c->timer.on ? c->timer.take(5) : nullptr;
+  cudaEvent_t *ev = c->timer.on ? c->timer.take(StageTimer::kPerCall) : nullptr;
+  bool xl_ran = false;
   MB2_TRY(run_match(c, r.p->bm, mc, g, c->best, c->second, c->match, c->status, pts_b, pts_m,
-                    c->counts.as<long long>() + count_slot, offset_dev, ev));
+                    c->counts.as<long long>() + count_slot, offset_dev, ev, ev ? ev + 5 : nullptr,
+                    ev ? c->xl_count.as<unsigned long long>() : nullptr, &xl_ran));
+  if (ev) c->timer.ran.push_back(xl_ran ? 1 : 0);
   if (r.stats) r.stats->matcher_calls += 1;
   if (r.p->verbosity >= 2) {
     // per-call routing of the blocks through the search kernels
@@ -780,7 +800,7 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
-                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->bmw.ncc_pad, &c->bmw.ncc_wand, &c->ltsw.state, &c->ltsw.resid,
+                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->bmw.ncc_pad, &c->bmw.ncc_wand, &c->ltsw.state, &c->ltsw.resid, &c->xl_count,
                     &c->ltsw.partial, &c->ltsw.hist, &c->ltsw.ctrl, &c->ltsw.cand, &c->counts,
                     &c->ncc_count, &c->ones, &c->lvl_f, &c->lvl_m, &c->tmp_a, &c->tmp_b,
                     &c->weights, &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best,
@@ -799,7 +819,31 @@ void *mirorr_ctx_stream(mirorr_ctx c) { return c ? (void *)c->stream : nullptr; 
 
 mirorr_status mirorr_ctx_set_profiling(mirorr_ctx c, int32_t on) {
   if (!c) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (on && !c->xl_count.ptr) {
+    MB2_CUDA_TRY(cudaSetDevice(c->device));
+    MB2_TRY(c->xl_count.ensure(sizeof(unsigned long long)));
+    MB2_CUDA_TRY(cudaMemsetAsync(c->xl_count.ptr, 0, sizeof(unsigned long long), c->stream));
+  }
   c->timer.on = on != 0;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_ctx_search_kernel_times(mirorr_ctx c, double *ms, int64_t *launches,
+                                             int64_t *candidates) {
+  if (!c || !ms) { set_error("null argument"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->timer.harvest();
+  unsigned long long n = 0;
+  if (c->xl_count.ptr) {
+    MB2_CUDA_TRY(cudaMemcpy(&n, c->xl_count.ptr, sizeof(n), cudaMemcpyDeviceToHost));
+    MB2_CUDA_TRY(cudaMemset(c->xl_count.ptr, 0, sizeof(n)));
+  }
+  *ms = c->timer.search_ms;
+  if (launches) *launches = c->timer.search_calls;
+  if (candidates) *candidates = (int64_t)n;
+  c->timer.search_ms = 0.0;
+  c->timer.search_calls = 0;
   return MIRORR_OK;
 }
 

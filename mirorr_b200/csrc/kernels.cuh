@@ -58,11 +58,15 @@ mirorr_status launch_variance_selection(const BmGeom &g, const float *base, doub
                                         BmWork &w, const uint8_t **selected_out,
                                         cudaStream_t s);
 // ncc_count (optional): device counter incremented by the number of candidate
-// scores evaluated.
+// scores evaluated.  Profiling (optional): kev[0], kev[1] are recorded around
+// the per-x-lane search kernel's launch and xl_count adds up the candidates it
+// scores; *xl_ran tells whether that kernel ran.
 mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmask,
                          const float *search, const uint8_t *smask, const float2 *stats,
                          const uint8_t *selected, const BmOut &out, BmWork &w,
-                         unsigned long long *ncc_count, cudaStream_t s);
+                         unsigned long long *ncc_count, cudaStream_t s,
+                         cudaEvent_t *kev = nullptr, unsigned long long *xl_count = nullptr,
+                         bool *xl_ran = nullptr);
 // Post-filter (itkBlockMatcher.txx:884-918).  Marks kept blocks (status |= 2),
 // counts them into *count_dev and, when pts != nullptr, writes the kept
 // blocks' base / match points (mm) in raster order into pts_base / pts_match

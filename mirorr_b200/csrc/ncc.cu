@@ -84,6 +84,7 @@ struct NccArgs {
                       // [3] register-blocked blocks, [4] masked-window blocks
   const float *search_al;  // the search image with rows of spitch floats, 16-byte aligned
   int spitch;
+  unsigned long long *xl_count;  // optional: candidates scored by the per-x-lane kernel
 };
 
 __device__ inline void window_axis(int o, int S, int W, int g, int bw, int &s, int &n) {
@@ -1142,6 +1143,14 @@ __global__ void __launch_bounds__(32, kXMinBlocks) ncc_xlane_kernel(NccArgs a, X
       }
       rc.cnt = cnt;
       atomicAdd(&a.ctl[3], 1u);
+      if (a.xl_count) {
+        // candidates of the clipped window: valid offsets per axis
+        auto nval = [](int o, int n) {
+          const int lo = o < 0 ? -o : 0, hi = min(W - 1, n - 4 - o);
+          return hi >= lo ? hi - lo + 1 : 0;
+        };
+        atomicAdd(a.xl_count, (unsigned long long)nval(ox, nx) * nval(oy, ny) * nval(oz, nz));
+      }
     }
     __syncwarp();
   }
@@ -1505,7 +1514,8 @@ mirorr_status launch_rest(const NccArgs &a, bool all_general, cudaStream_t s) {
 // Per-x-lane search (block width 4) and the masked-window kernel; done is
 // false when the union window would not fit (very wide block spacing).
 template <int W, class CM>
-mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done) {
+mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
+                           cudaEvent_t *kev) {
   constexpr int E = W + 3, BPW = 32 / W;
   done = false;
   const long long u = (long long)(BPW - 1) * a.G + E;   // union row length
@@ -1551,27 +1561,33 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done) {
   }
   MB2_TRY(set_smem(ncc_xlane_kernel<W>, smem));
   const long long grid = xa.ntiles < 148LL * kXMinBlocks ? xa.ntiles : 148LL * kXMinBlocks;
+  if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[0], s));
   ncc_xlane_kernel<W><<<(unsigned)grid, 32, smem, s>>>(a, xa);
   MB2_LAUNCH_CHECK();
+  if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[1], s));
   MB2_TRY((launch_fast1<CM, true>(a, s)));
   done = true;
   return MIRORR_OK;
 }
 
 // Block width / window combinations with a register-blocked fast kernel.
-bool run_fast(NccArgs &a, BmWork &w, cudaStream_t s, mirorr_status &st) {
+bool run_fast(NccArgs &a, BmWork &w, cudaStream_t s, mirorr_status &st, cudaEvent_t *kev,
+              bool &xl_ran) {
+  xl_ran = false;
   if (a.g != 1) return false;
   if ((long long)a.nx * a.ny * a.nz >= (1LL << 31)) return false;
   if (a.bw == 4 && a.W == 9) {
     bool done = false;
-    st = launch_xlane<9, FastCfg<4, 9, 1, 3>>(a, w, s, done);
+    st = launch_xlane<9, FastCfg<4, 9, 1, 3>>(a, w, s, done, kev);
+    xl_ran = done;
     if (st != MIRORR_OK || done) return true;
     st = launch_fast<WarpCfg<4, 9, 3, 1, 5, 3>, FastCfg<4, 9, 1, 3>>(a, s);
     return true;
   }
   if (a.bw == 4 && a.W == 7) {
     bool done = false;
-    st = launch_xlane<7, FastCfg<4, 7, 1, 5>>(a, w, s, done);
+    st = launch_xlane<7, FastCfg<4, 7, 1, 5>>(a, w, s, done, kev);
+    xl_ran = done;
     if (st != MIRORR_OK || done) return true;
     st = launch_fast<WarpCfg<4, 7, 4, 2, 4, 3>, FastCfg<4, 7, 1, 5>>(a, s);
     return true;
@@ -1588,7 +1604,8 @@ bool run_fast(NccArgs &a, BmWork &w, cudaStream_t s, mirorr_status &st) {
 mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmask,
                          const float *search, const uint8_t *smask, const float2 *stats,
                          const uint8_t *selected, const BmOut &out, BmWork &w,
-                         unsigned long long *ncc_count, cudaStream_t s) {
+                         unsigned long long *ncc_count, cudaStream_t s, cudaEvent_t *kev,
+                         unsigned long long *xl_count, bool *xl_ran) {
   if (g.nblocks > 0x7fffffffLL) {
     set_error("too many blocks (%lld)", g.nblocks);
     return MIRORR_EINVAL;
@@ -1616,6 +1633,7 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
   a.ctl = w.ncc_ctl.as<unsigned int>();
   a.search_al = search;
   a.spitch = g.size[0];
+  a.xl_count = xl_count;
   {
     long long grid = (g.nblocks + 127) / 128;
     if (grid > 148LL * 16) grid = 148LL * 16;
@@ -1623,7 +1641,9 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
     MB2_LAUNCH_CHECK();
   }
   mirorr_status st = MIRORR_OK;
-  bool fast = run_fast(a, w, s, st);
+  bool ran = false;
+  bool fast = run_fast(a, w, s, st, kev, ran);
+  if (xl_ran) *xl_ran = ran;
   MB2_TRY(st);
   switch (g.bw) {
     case 1: return launch_rest<1>(a, !fast, s);
