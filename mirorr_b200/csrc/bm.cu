@@ -49,53 +49,94 @@ void point_geom(const double origin[3], const double spacing[3], const double di
 // ---------------------------------------------------------------------------
 // 1. box statistics
 // ---------------------------------------------------------------------------
+// Each thread computes PX consecutive x positions of one row: every footprint
+// row of PX + BW - 1 floats is loaded once and serves all PX positions.  Per
+// position the FP64 arithmetic and its order are the two-pass loop of
+// normalizedCorrelation (mean over all voxels, then the masked sum of squares
+// in raster order, itkBlockMatcher.txx:57-95).
+constexpr int kBoxPX = 4;
+
 template <int BW>
 __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict__ y,
                                                         const uint8_t *__restrict__ ms, int nx,
                                                         int ny, int nz, float2 *__restrict__ out) {
-  long long n = (long long)nx * ny * nz;
+  constexpr int PX = kBoxPX, RL = PX + BW - 1;
+  const int ngx = (nx + PX - 1) / PX;
+  const long long n = (long long)ngx * ny * nz;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
        p += (long long)gridDim.x * blockDim.x) {
-    int x = (int)(p % nx);
-    int yy = (int)((p / nx) % ny);
-    int z = (int)(p / ((long long)nx * ny));
-    if (x > nx - BW || yy > ny - BW || z > nz - BW) {
-      out[p] = make_float2(0.f, 0.f);
-      continue;
+    const int x0 = (int)(p % ngx) * PX;
+    const int yy = (int)((p / ngx) % ny);
+    const int z = (int)(p / ((long long)ngx * ny));
+    const long long o = ((long long)z * ny + yy) * nx + x0;
+    const bool rowok = yy <= ny - BW && z <= nz - BW;
+    double sum[PX], mean[PX], ss[PX];
+    bool all_in[PX], ok[PX];
+#pragma unroll
+    for (int j = 0; j < PX; ++j) {
+      sum[j] = 0.0;
+      ss[j] = 0.0;
+      all_in[j] = true;
+      ok[j] = rowok && x0 + j <= nx - BW;
     }
-    double sum = 0.0;
+    if (rowok && x0 <= nx - BW) {
 #pragma unroll
-    for (int vz = 0; vz < BW; ++vz)
+      for (int vz = 0; vz < BW; ++vz)
 #pragma unroll
-      for (int vy = 0; vy < BW; ++vy)
+        for (int vy = 0; vy < BW; ++vy) {
+          const float *r = y + o + ((long long)vz * ny + vy) * nx;
+          float v[RL];
 #pragma unroll
-        for (int vx = 0; vx < BW; ++vx)
-          sum = __dadd_rn(sum, (double)__ldg(&y[p + ((long long)vz * ny + vy) * nx + vx]));
-    double mean = __ddiv_rn(sum, (double)(BW * BW * BW));
-    double ss = 0.0;
-    bool all_in = true;
+          for (int i = 0; i < RL; ++i) v[i] = (x0 + i < nx) ? __ldg(r + i) : 0.f;
 #pragma unroll
-    for (int vz = 0; vz < BW; ++vz)
+          for (int vx = 0; vx < BW; ++vx)
 #pragma unroll
-      for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-        for (int vx = 0; vx < BW; ++vx) {
-          long long q = p + ((long long)vz * ny + vy) * nx + vx;
-          if (__ldg(&ms[q])) {
-            double d = __dsub_rn((double)__ldg(&y[q]), mean);
-            ss = __dadd_rn(ss, __dmul_rn(d, d));
-          } else {
-            all_in = false;
-          }
+            for (int j = 0; j < PX; ++j) sum[j] = __dadd_rn(sum[j], (double)v[j + vx]);
         }
-    float fs = (float)ss;
-    out[p] = make_float2((float)mean, all_in ? fs : -fs);
+#pragma unroll
+      for (int j = 0; j < PX; ++j) mean[j] = __ddiv_rn(sum[j], (double)(BW * BW * BW));
+#pragma unroll
+      for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+        for (int vy = 0; vy < BW; ++vy) {
+          const long long q = o + ((long long)vz * ny + vy) * nx;
+          float v[RL];
+          uint8_t m[RL];
+#pragma unroll
+          for (int i = 0; i < RL; ++i) {
+            const bool in = x0 + i < nx;
+            v[i] = in ? __ldg(y + q + i) : 0.f;
+            m[i] = in ? __ldg(ms + q + i) : (uint8_t)0;
+          }
+#pragma unroll
+          for (int vx = 0; vx < BW; ++vx)
+#pragma unroll
+            for (int j = 0; j < PX; ++j) {
+              if (m[j + vx]) {
+                const double d = __dsub_rn((double)v[j + vx], mean[j]);
+                ss[j] = __dadd_rn(ss[j], __dmul_rn(d, d));
+              } else {
+                all_in[j] = false;
+              }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PX; ++j) {
+      if (x0 + j >= nx) break;
+      if (!ok[j]) {
+        out[o + j] = make_float2(0.f, 0.f);
+      } else {
+        const float fs = (float)ss[j];
+        out[o + j] = make_float2((float)mean[j], all_in[j] ? fs : -fs);
+      }
+    }
   }
 }
 
 mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8_t *smask,
                                float2 *stats, cudaStream_t s) {
-  long long n = (long long)g.size[0] * g.size[1] * g.size[2];
+  long long n = (long long)((g.size[0] + kBoxPX - 1) / kBoxPX) * g.size[1] * g.size[2];
   int threads = 256;
   long long blocks = (n + threads - 1) / threads;
   if (blocks > 148LL * 64) blocks = 148LL * 64;

@@ -33,7 +33,7 @@ struct BmWork {
   DevBuf ncc_rec;   // per-block FP32 stage results
   DevBuf ncc_bstat; // per-block base statistics
   DevBuf ncc_pad;   // search image with 16-byte aligned rows (when its own are not)
-  DevBuf ncc_wand;  // window-AND of the footprint flags (two passes' buffers)
+  DevBuf ncc_wand;  // per-block window-AND of the footprint flags (and its passes)
 };
 
 struct BmOut {

@@ -827,21 +827,23 @@ __global__ void __launch_bounds__(C::WPC * 32, C::MINB) ncc_warp_kernel(NccArgs 
 }
 
 // ---------------------------------------------------------------------------
-// Window-AND of the footprint flags.  wand[s] (s = window start, each axis
-// from -R, stored at s + R) is 1 when every candidate of the W^3 window
-// starting at s whose footprint lies inside the volume has its footprint
-// wholly inside the search mask (box_stats: Syy sign bit clear).  Separable:
-// one pass per axis, out-of-range positions count as 1.
+// Window-AND of the footprint flags, per block: wand[b] is 1 when every
+// candidate of block b's window whose footprint lies inside the volume has its
+// footprint wholly inside the search mask (box_stats: Syy sign bit clear).
+// Separable, evaluated only at the blocks' window starts: along x for every
+// (y, z) row, then along y and z at block resolution; out-of-range positions
+// count as 1.
 // ---------------------------------------------------------------------------
-__global__ void wand_x_kernel(const float2 *stats, uint8_t *out, int nx, int ny, int nz, int W,
-                              int bw) {
-  const int R = W / 2, nxo = nx + R;
-  const long long n = (long long)nxo * ny * nz;
+__global__ void wand_x_kernel(const float2 *stats, uint8_t *out, int nx, int ny, int nz, int nbx,
+                              int stx, int G, int W, int bw) {
+  const int R = W / 2;
+  const long long n = (long long)nbx * ny * nz;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int sx = (int)(i % nxo) - R;
-    const long long yz = i / nxo;
+    const int bx = (int)(i % nbx);
+    const long long yz = i / nbx;
     const int y = (int)(yz % ny), z = (int)(yz / ny);
+    const int sx = stx + bx * G - R;
     unsigned v = 1;
     if (y <= ny - bw && z <= nz - bw) {
       const float *fy = reinterpret_cast<const float *>(stats + yz * nx) + 1;
@@ -852,17 +854,18 @@ __global__ void wand_x_kernel(const float2 *stats, uint8_t *out, int nx, int ny,
   }
 }
 
-// AND over a window of W along the middle axis of [outer][n][inner] -> [outer][n + R][inner].
+// [outer][n][inner] -> [outer][nb][inner]: AND over the window of W starting
+// at st + b G - R along the middle axis.
 __global__ void wand_axis_kernel(const uint8_t *in, uint8_t *out, long long inner, int n,
-                                 long long outer, int W) {
-  const int R = W / 2, no = n + R;
-  const long long total = outer * no * inner;
+                                 long long outer, int nb, int st, int G, int W) {
+  const int R = W / 2;
+  const long long total = outer * nb * inner;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     const long long ii = i % inner;
     const long long r = i / inner;
-    const int sa = (int)(r % no) - R;
-    const long long o = r / no;
+    const int sa = st + (int)(r % nb) * G - R;
+    const long long o = r / nb;
     unsigned v = 1;
     for (int q = sa < 0 ? 0 : sa; q < sa + W && q < n; ++q) v &= in[(o * n + q) * inner + ii];
     out[i] = (uint8_t)v;
@@ -894,7 +897,7 @@ __global__ void wand_axis_kernel(const uint8_t *in, uint8_t *out, long long inne
 constexpr int kXMinBlocks = 12;
 
 struct XArgs {
-  const uint8_t *wand;  // window-AND of the footprint flags, (nz+R) x (ny+R) x (nx+R)
+  const uint8_t *wand;  // per block: window wholly inside the search mask
   int rpu;              // union row pitch in floats (multiple of 4)
   int nch;              // 16-byte chunks per union row
   int tpr;              // warp tiles per row of the block grid
@@ -962,8 +965,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks) ncc_xlane_kernel(NccArgs a, X
 #pragma unroll
     for (int cy = 0; cy < W; ++cy)
       if (oy + cy >= 0 && oy + cy <= ny - 4) yok |= 1u << cy;
-    const bool inmask =
-        !state || xa.wand[((long long)(oz + R) * (ny + R) + (oy + R)) * (nx + R) + (ox + R)];
+    const bool inmask = !state || xa.wand[b];
     const unsigned bad = __ballot_sync(full, state && !inmask);
     if (state && (bad & seg)) {
       if (x == 0) {
@@ -1543,21 +1545,20 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
                                    (size_t)a.ny * a.nz, cudaMemcpyDeviceToDevice, s));
     a.search_al = w.ncc_pad.as<float>();
   }
-  // window-AND of the footprint flags, one pass per axis
+  // window-AND of the footprint flags per block, one pass per axis
   {
-    constexpr int R = W / 2;
-    const long long nxo = a.nx + R, nyo = a.ny + R, nzo = a.nz + R;
-    const size_t bytes = (size_t)(nxo * nyo * nzo);
-    MB2_TRY(w.ncc_wand.ensure(2 * bytes));
-    uint8_t *b0 = w.ncc_wand.as<uint8_t>(), *b1 = b0 + bytes;
+    const size_t n1 = (size_t)a.nbx * a.ny * a.nz, n2 = (size_t)a.nbx * a.nby * a.nz;
+    MB2_TRY(w.ncc_wand.ensure(n1 + n2 + (size_t)a.nblocks));
+    uint8_t *b1 = w.ncc_wand.as<uint8_t>(), *b2 = b1 + n1, *b3 = b2 + n2;
     const unsigned g = 148 * 8;
-    wand_x_kernel<<<g, 256, 0, s>>>(a.stats, b0, a.nx, a.ny, a.nz, W, 4);
+    wand_x_kernel<<<g, 256, 0, s>>>(a.stats, b1, a.nx, a.ny, a.nz, a.nbx, a.stx, a.G, W, 4);
     MB2_LAUNCH_CHECK();
-    wand_axis_kernel<<<g, 256, 0, s>>>(b0, b1, nxo, a.ny, a.nz, W);
+    wand_axis_kernel<<<g, 256, 0, s>>>(b1, b2, a.nbx, a.ny, a.nz, a.nby, a.sty, a.G, W);
     MB2_LAUNCH_CHECK();
-    wand_axis_kernel<<<g, 256, 0, s>>>(b1, b0, nxo * nyo, a.nz, 1, W);
+    wand_axis_kernel<<<g, 256, 0, s>>>(b2, b3, (long long)a.nbx * a.nby, a.nz, 1, a.nbz, a.stz,
+                                       a.G, W);
     MB2_LAUNCH_CHECK();
-    xa.wand = b0;
+    xa.wand = b3;
   }
   MB2_TRY(set_smem(ncc_xlane_kernel<W>, smem));
   const long long grid = xa.ntiles < 148LL * kXMinBlocks ? xa.ntiles : 148LL * kXMinBlocks;
