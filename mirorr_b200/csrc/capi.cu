@@ -745,6 +745,14 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float
     tfm_params(tfm, params);
   }
   tfm_set_params(tfm, params);
+  {
+    bool to = false;
+    MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
+    if (to) {
+      set_error("a bounded wait on a tensor copy of the NCC search gave up");
+      return MIRORR_ETIMEOUT;
+    }
+  }
   to_public(tfm, *result);
   if (stats) {
     stats->levels_run = nl;
@@ -1048,6 +1056,14 @@ mirorr_status mirorr_bm_get_offsets(mirorr_matcher m, size_t capacity, double *b
                                c->stream));
   MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
   for (int s = 0; s < 4; ++s) cudaEventElapsedTime(&m->timings[s], m->ev[s], m->ev[s + 1]);
+  {
+    bool to = false;
+    MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
+    if (to) {
+      set_error("a bounded wait on a tensor copy of the NCC search gave up");
+      return MIRORR_ETIMEOUT;
+    }
+  }
   m->last = g;
   m->kept = kept;
   m->has_results = true;

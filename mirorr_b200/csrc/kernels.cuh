@@ -67,6 +67,9 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
                          unsigned long long *ncc_count, cudaStream_t s,
                          cudaEvent_t *kev = nullptr, unsigned long long *xl_count = nullptr,
                          bool *xl_ran = nullptr);
+// True when a bounded device wait of the NCC stage gave up since the last
+// call (then also clears the flag).  Synchronises the stream.
+mirorr_status ncc_take_timeout(BmWork &w, cudaStream_t s, bool *timed_out);
 // Post-filter (itkBlockMatcher.txx:884-918).  Marks kept blocks (status |= 2),
 // counts them into *count_dev and, when pts != nullptr, writes the kept
 // blocks' base / match points (mm) in raster order into pts_base / pts_match

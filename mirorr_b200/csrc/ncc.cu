@@ -32,6 +32,8 @@
 //      so the block's best, second and argmax equal the FP64 reference's.
 //      Blocks whose list overflowed are re-scored entirely by
 //      ncc_fallback_kernel.
+#include <cuda.h>  // CUtensorMap (the encoder is fetched through the runtime)
+
 #include "kernels.cuh"
 
 namespace mb2 {
@@ -81,7 +83,8 @@ struct NccArgs {
   int *gen_list;    // blocks for the general kernel
   int *ovf_list;    // blocks for the fallback kernel
   unsigned int *ctl;  // [0] general blocks, [1] overflow blocks, [2] refined candidates,
-                      // [3] register-blocked blocks, [4] masked-window blocks
+                      // [3] register-blocked blocks, [4] masked-window blocks,
+                      // [5] a bounded wait on a tensor copy gave up
   const float *search_al;  // the search image with rows of spitch floats, 16-byte aligned
   int spitch;
   unsigned long long *xl_count;  // optional: candidates scored by the per-x-lane kernel
@@ -161,9 +164,42 @@ __device__ inline void cp_async8(void *dst, const void *src) {
   unsigned int d = (unsigned int)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
-__device__ inline void cp_async16(float *dst, const float *src) {
-  unsigned int d = (unsigned int)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+// Tensor-memory-access (TMA) load of a 3D box into shared memory, completing
+// on an mbarrier (no multicast).
+__device__ inline void tma_load_3d(float *dst, const CUtensorMap *map, int x, int y, int z,
+                                   uint64_t *bar) {
+  const unsigned int d = (unsigned int)__cvta_generic_to_shared(dst);
+  const unsigned int b = (unsigned int)__cvta_generic_to_shared(bar);
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(d),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(b)
+      : "memory");
+}
+__device__ inline void mbar_init(uint64_t *bar, unsigned int count) {
+  const unsigned int b = (unsigned int)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(b), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ inline void mbar_expect_tx(uint64_t *bar, unsigned int bytes) {
+  const unsigned int b = (unsigned int)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(bytes)
+               : "memory");
+}
+// Waits for phase `parity` of the barrier, at most `limit` polls; false on timeout.
+__device__ inline bool mbar_wait(uint64_t *bar, unsigned int parity, int limit) {
+  const unsigned int b = (unsigned int)__cvta_generic_to_shared(bar);
+  for (int i = 0; i < limit; ++i) {
+    unsigned int done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(b), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
 }
 __device__ inline void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
@@ -879,9 +915,10 @@ __global__ void wand_axis_kernel(const uint8_t *in, uint8_t *out, long long inne
 // A warp takes BPW = 32 / W consecutive blocks of one row of the block grid
 // (same by, bz).  Lane (k, x) scores the W x W candidates of block k whose x
 // offset in the window is x, i.e. every (cy, cz).  The blocks' windows
-// overlap along x, so the warp stages their union once, with rows starting at
-// a 16-byte aligned x (16-byte asynchronous copies); at every load the lanes
-// read consecutive floats of one row (no bank conflicts).  The lane's base
+// overlap along x, so the warp stages their union once: one tensor (TMA) copy
+// of an rpu x E x E box from a 16-byte aligned x, zero-filled outside the
+// volume, completing on an mbarrier whose wait is bounded; at every load the
+// lanes read consecutive floats of one row (no bank conflicts).  The lane's base
 // block (x~ = x - mean, 64 values) sits in registers and each window row is
 // read once, shifted by the block's constant c as it is read
 // (Sxy = sum x~ (y - c) - (mu - c) sum x~ keeps the FP32 cross term free of
@@ -898,18 +935,23 @@ constexpr int kXMinBlocks = 12;
 
 struct XArgs {
   const uint8_t *wand;  // per block: window wholly inside the search mask
-  int rpu;              // union row pitch in floats (multiple of 4)
+  int rpu;              // union row pitch in floats (multiple of 4, the box's x extent)
   int nch;              // 16-byte chunks per union row
   int tpr;              // warp tiles per row of the block grid
   long long ntiles;
 };
 
 template <int W>
-__global__ void __launch_bounds__(32, kXMinBlocks) ncc_xlane_kernel(NccArgs a, XArgs xa) {
+__global__ void __launch_bounds__(32, kXMinBlocks)
+    ncc_xlane_kernel(NccArgs a, XArgs xa, const __grid_constant__ CUtensorMap tmap) {
   constexpr int R = W / 2, E = W + 3, BPW = 32 / W;
   extern __shared__ __align__(16) float sm[];
-  float *win = sm;                      // E * E * rpu
-  float *xt = sm + E * E * xa.rpu;      // BPW * 64
+  __shared__ __align__(8) uint64_t s_bar;
+  // the tensor copy's destination starts on 128 bytes (the allocation has 128 spare)
+  float *const sma = reinterpret_cast<float *>(
+      sm + ((128u - ((unsigned int)__cvta_generic_to_shared(sm) & 127u)) & 127u) / sizeof(float));
+  float *win = sma;                     // E * E * rpu
+  float *xt = sma + E * E * xa.rpu;     // BPW * 64
   float2 *qbuf = reinterpret_cast<float2 *>(xt + BPW * 64);  // 32 * W
   __shared__ float s_red[BPW][W][2];
   __shared__ int s_deg[BPW][W][2];
@@ -921,6 +963,10 @@ __global__ void __launch_bounds__(32, kXMinBlocks) ncc_xlane_kernel(NccArgs a, X
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const unsigned full = 0xffffffffu;
   const unsigned seg = ((1u << W) - 1u) << (k < BPW ? k * W : 0);
+  if (lane == 0) mbar_init(&s_bar, 1);
+  __syncwarp();
+  unsigned int phase = 0;
+  const unsigned int win_bytes = (unsigned int)(E * E * xa.rpu * sizeof(float));
 
   for (long long tile = blockIdx.x; tile < xa.ntiles; tile += gridDim.x) {
     const long long grow = tile / xa.tpr;
@@ -976,30 +1022,14 @@ __global__ void __launch_bounds__(32, kXMinBlocks) ncc_xlane_kernel(NccArgs a, X
     }
     const unsigned act = __ballot_sync(full, state);
     if (act == 0) continue;
-    // ---- staging: union window rows and the base blocks (x~) ---------------
-    const int nch = xa.nch, rpu = xa.rpu;
-    for (int r = lane; r < E * E; r += 32) {
-      const int z = r / E, y = r - z * E;
-      const int gz = oz + z, gy = oy + y;
-      float4 *dst = reinterpret_cast<float4 *>(win + r * rpu);
-      if (gz < 0 || gz >= nz || gy < 0 || gy >= ny) {
-        for (int ch = 0; ch < nch; ++ch) dst[ch] = make_float4(0.f, 0.f, 0.f, 0.f);
-        continue;
-      }
-      const float *src = a.search_al + ((long long)gz * ny + gy) * a.spitch;
-      for (int ch = 0; ch < nch; ++ch) {
-        const int gx = xu + 4 * ch;
-        if (gx >= 0 && gx + 4 <= nx) {
-          cp_async16(reinterpret_cast<float *>(dst + ch), src + gx);
-        } else {
-          float4 v;
-          v.x = (gx >= 0 && gx < nx) ? src[gx] : 0.f;
-          v.y = (gx + 1 >= 0 && gx + 1 < nx) ? src[gx + 1] : 0.f;
-          v.z = (gx + 2 >= 0 && gx + 2 < nx) ? src[gx + 2] : 0.f;
-          v.w = (gx + 3 >= 0 && gx + 3 < nx) ? src[gx + 3] : 0.f;
-          dst[ch] = v;
-        }
-      }
+    // ---- staging: the union window by one tensor copy (zero outside the
+    // volume), the base blocks (x~) by the lanes meanwhile --------------------
+    const int rpu = xa.rpu;
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of win
+    __syncwarp();
+    if (lane == 0) {
+      mbar_expect_tx(&s_bar, win_bytes);
+      tma_load_3d(win, &tmap, xu, oy, oz, &s_bar);
     }
     for (int i = lane; i < nbt * 64; i += 32) {
       const int kk = i >> 6, v = i & 63;
@@ -1009,7 +1039,11 @@ __global__ void __launch_bounds__(32, kXMinBlocks) ncc_xlane_kernel(NccArgs a, X
       const double mk = a.bstat[brow + bx0 + kk].mean;
       xt[i] = (float)__dsub_rn((double)__ldg(&a.base[q]), mk);
     }
-    cp_async_wait_all();
+    if (!mbar_wait(&s_bar, phase, 1 << 22)) {
+      if (lane == 0) atomicExch(&a.ctl[5], 1u);
+      return;
+    }
+    phase ^= 1u;
     __syncwarp();
     // ---- FP32 scores ---------------------------------------------------------
     float l1 = -3.f, l2 = -3.f;
@@ -1515,6 +1549,26 @@ mirorr_status launch_rest(const NccArgs &a, bool all_general, cudaStream_t s) {
 
 // Per-x-lane search (block width 4) and the masked-window kernel; done is
 // false when the union window would not fit (very wide block spacing).
+// cuTensorMapEncodeTiled, fetched once through the runtime (no -lcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
 template <int W, class CM>
 mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
                            cudaEvent_t *kev) {
@@ -1532,8 +1586,8 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
   }
   xa.tpr = (a.nbx + BPW - 1) / BPW;
   xa.ntiles = (long long)xa.tpr * a.nby * a.nbz;
-  const size_t smem = sizeof(float) * ((size_t)E * E * xa.rpu + BPW * 64 + 64 * W);
-  if (xa.nch > 32 || smem > 64 * 1024) return MIRORR_OK;
+  const size_t smem = sizeof(float) * ((size_t)E * E * xa.rpu + BPW * 64 + 64 * W) + 128;
+  if (xa.rpu > 256 || smem > 64 * 1024) return MIRORR_OK;  // tensor box limit
   // rows of the search image must start on 16 bytes for the 16-byte copies
   a.search_al = a.search;
   a.spitch = a.nx;
@@ -1560,10 +1614,32 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
     MB2_LAUNCH_CHECK();
     xa.wand = b3;
   }
+  // tensor map of the search image: x extent nx (zero beyond), rows of spitch floats
+  CUtensorMap tmap;
+  {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) {
+      set_error("cuTensorMapEncodeTiled is not available from the driver");
+      return MIRORR_ECUDA;
+    }
+    const cuuint64_t gdim[3] = {(cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz};
+    const cuuint64_t gstride[2] = {(cuuint64_t)a.spitch * sizeof(float),
+                                   (cuuint64_t)a.spitch * a.ny * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)xa.rpu, (cuuint32_t)E, (cuuint32_t)E};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(a.search_al),
+                     gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+      return MIRORR_ECUDA;
+    }
+  }
   MB2_TRY(set_smem(ncc_xlane_kernel<W>, smem));
   const long long grid = xa.ntiles < 148LL * kXMinBlocks ? xa.ntiles : 148LL * kXMinBlocks;
   if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[0], s));
-  ncc_xlane_kernel<W><<<(unsigned)grid, 32, smem, s>>>(a, xa);
+  ncc_xlane_kernel<W><<<(unsigned)grid, 32, smem, s>>>(a, xa, tmap);
   MB2_LAUNCH_CHECK();
   if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[1], s));
   MB2_TRY((launch_fast1<CM, true>(a, s)));
@@ -1612,10 +1688,14 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
     return MIRORR_EINVAL;
   }
   MB2_TRY(w.ncc_lists.ensure(sizeof(int) * 3 * (g.nblocks + 1)));
+  const void *ctl_before = w.ncc_ctl.ptr;
   MB2_TRY(w.ncc_ctl.ensure(sizeof(unsigned int) * 8));
   MB2_TRY(w.ncc_rec.ensure(sizeof(NccRec) * g.nblocks));
   MB2_TRY(w.ncc_bstat.ensure(sizeof(BlockStat) * g.nblocks));
-  MB2_CUDA_TRY(cudaMemsetAsync(w.ncc_ctl.ptr, 0, sizeof(unsigned int) * 8, s));
+  // counters 0..4 restart every call; [5] (a bounded wait gave up) stays set
+  // until the host reads it (ncc_take_timeout)
+  MB2_CUDA_TRY(cudaMemsetAsync(w.ncc_ctl.ptr, 0,
+                               sizeof(unsigned int) * (w.ncc_ctl.ptr == ctl_before ? 5 : 8), s));
   NccArgs a;
   a.base = base; a.bmask = bmask; a.search = search; a.smask = smask; a.stats = stats;
   a.selected = selected;
@@ -1659,6 +1739,20 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
       set_error("block width %d not supported (1..8)", g.bw);
       return MIRORR_EINVAL;
   }
+}
+
+mirorr_status ncc_take_timeout(BmWork &w, cudaStream_t s, bool *timed_out) {
+  *timed_out = false;
+  if (!w.ncc_ctl.ptr) return MIRORR_OK;
+  unsigned int f = 0;
+  unsigned int *flag = w.ncc_ctl.as<unsigned int>() + 5;
+  MB2_CUDA_TRY(cudaMemcpyAsync(&f, flag, sizeof(f), cudaMemcpyDeviceToHost, s));
+  MB2_CUDA_TRY(cudaStreamSynchronize(s));
+  if (f) {
+    MB2_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(f), s));
+    *timed_out = true;
+  }
+  return MIRORR_OK;
 }
 
 }  // namespace mb2

@@ -28,6 +28,11 @@ CASES = [
     dict(id="bw4_w7_G4_keep05_masked", shape=(32, 32, 16), bw=4, nw=7, g=1, G=4, keep=0.5, mask="search", seed=6),
     dict(id="bw2_w5_G2", shape=(24, 20, 12), bw=2, nw=5, g=1, G=2, keep=1.0, mask=None, seed=7),
     dict(id="bw4_w6_even", shape=(28, 24, 20), bw=4, nw=6, g=1, G=3, keep=1.0, mask=None, seed=8),
+    # x extent not a multiple of 4 (search rows copied to 16-byte aligned rows)
+    # and a ragged last tile of blocks along x
+    dict(id="bw4_w9_G3_nx41_masked", shape=(41, 36, 26), bw=4, nw=9, g=1, G=3, keep=1.0,
+         mask="search", seed=9),
+    dict(id="bw4_w7_G2_nx39", shape=(39, 30, 22), bw=4, nw=7, g=1, G=2, keep=1.0, mask=None, seed=10),
 ]
 
 
