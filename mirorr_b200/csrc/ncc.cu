@@ -1410,20 +1410,6 @@ __global__ void __launch_bounds__(128) ncc_refine_kernel(NccArgs a) {
     BlockWin w;
     block_window(a, b, w);
     const long long o = lin(a, w.ox, w.oy, w.oz);
-    float x[B];
-    uint8_t mb[B];
-    double sum = 0.0;
-    for (int vz = 0; vz < BW; ++vz)
-      for (int vy = 0; vy < BW; ++vy)
-#pragma unroll
-        for (int vx = 0; vx < BW; ++vx) {
-          const int v = (vz * BW + vy) * BW + vx;
-          const long long q = o + ((long long)vz * a.ny + vy) * a.nx + vx;
-          x[v] = __ldg(&a.base[q]);
-          mb[v] = __ldg(&a.bmask[q]);
-          sum = __dadd_rn(sum, (double)x[v]);
-        }
-    const double mean_b = __ddiv_rn(sum, (double)B);
     // raster order = increasing linear index
     int n = rc.cnt;
     for (int i = 1; i < n; ++i) {
@@ -1432,7 +1418,78 @@ __global__ void __launch_bounds__(128) ncc_refine_kernel(NccArgs a) {
       rc.p[j + 1] = v;
     }
     SeqTop2 r;
-    for (int i = 0; i < n; ++i) r.push(exact_score<BW>(a, x, mb, mean_b, rc.p[i]), rc.p[i]);
+    if constexpr (B <= 64) {
+      // every voxel of the base block and of a candidate loaded into
+      // registers first (all loads in flight at once), then the reference's
+      // FP64 chains in raster order
+      // the thread's base block in a transposed shared slice (conflict-free)
+      __shared__ float xs[B][128];
+      const long long plane = (long long)a.ny * a.nx;
+      unsigned long long mbm = 0;
+      {
+        float x[B];
+#pragma unroll
+        for (int v = 0; v < B; ++v) {
+          const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+          const long long q = o + vz * plane + (long long)vy * a.nx + vx;
+          x[v] = __ldg(&a.base[q]);
+          if (__ldg(&a.bmask[q])) mbm |= 1ULL << v;
+        }
+#pragma unroll
+        for (int v = 0; v < B; ++v) xs[v][threadIdx.x] = x[v];
+      }
+      double sum = 0.0;
+#pragma unroll
+      for (int v = 0; v < B; ++v) sum = __dadd_rn(sum, (double)xs[v][threadIdx.x]);
+      const double mean_b = __ddiv_rn(sum, (double)B);
+      for (int i = 0; i < n; ++i) {
+        const long long p = rc.p[i];
+        float y[B];
+        unsigned long long msm = 0;
+#pragma unroll
+        for (int v = 0; v < B; ++v) {
+          const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+          const long long q = p + vz * plane + (long long)vy * a.nx + vx;
+          y[v] = __ldg(&a.search[q]);
+          if (__ldg(&a.smask[q])) msm |= 1ULL << v;
+        }
+        double ms = 0.0;
+#pragma unroll
+        for (int v = 0; v < B; ++v) ms = __dadd_rn(ms, (double)y[v]);
+        ms = __ddiv_rn(ms, (double)B);
+        const unsigned long long m = mbm & msm;
+        double prod = 0.0, bss = 0.0, sss = 0.0;
+#pragma unroll
+        for (int v = 0; v < B; ++v) {
+          if ((m >> v) & 1ULL) {
+            const double bb = __dsub_rn((double)xs[v][threadIdx.x], mean_b);
+            const double sb = __dsub_rn((double)y[v], ms);
+            prod = __dadd_rn(prod, __dmul_rn(bb, sb));
+            bss = __dadd_rn(bss, __dmul_rn(bb, bb));
+            sss = __dadd_rn(sss, __dmul_rn(sb, sb));
+          }
+        }
+        const double sc = (bss <= 0.0 || sss <= 0.0)
+                              ? -2.0 : __ddiv_rn(__ddiv_rn(__dmul_rn(prod, prod), bss), sss);
+        r.push(sc, (int)p);
+      }
+    } else {
+      float x[B];
+      uint8_t mb[B];
+      double sum = 0.0;
+      for (int vz = 0; vz < BW; ++vz)
+        for (int vy = 0; vy < BW; ++vy)
+#pragma unroll
+          for (int vx = 0; vx < BW; ++vx) {
+            const int v = (vz * BW + vy) * BW + vx;
+            const long long q = o + ((long long)vz * a.ny + vy) * a.nx + vx;
+            x[v] = __ldg(&a.base[q]);
+            mb[v] = __ldg(&a.bmask[q]);
+            sum = __dadd_rn(sum, (double)x[v]);
+          }
+      const double mean_b = __ddiv_rn(sum, (double)B);
+      for (int i = 0; i < n; ++i) r.push(exact_score<BW>(a, x, mb, mean_b, rc.p[i]), rc.p[i]);
+    }
     write_final(a, b, r.best, r.second, r.arg < 0 ? lin(a, w.sx, w.sy, w.sz) : r.arg, 1);
     if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)w.nc);
     atomicAdd(&a.ctl[2], (unsigned int)n);
