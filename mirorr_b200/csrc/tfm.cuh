@@ -176,18 +176,47 @@ MB2_HD void orthogonalize3(const double *m, double *o) {
   m3_mul(m, isq, o);
 }
 
-// Denman-Beavers square root of a 4x4 matrix (vnl_utils.h:46-95) with
-// EPS = 1e-14, MAX_ITER = 50 as called from itkSymMirorrRegistrationMethod.txx.
+// Inverse of a homogeneous affine 4x4 matrix [A t; 0 0 0 1] (row-major):
+// [A^-1, -A^-1 t; 0 0 0 1], with A^-1 from its cofactors.  False when A is
+// singular.
+MB2_HD bool affine4_inverse(const double *m, double *o) {
+  const double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6];
+  const double g = m[8], h = m[9], k = m[10];
+  const double c00 = e * k - f * h, c01 = f * g - d * k, c02 = d * h - e * g;
+  const double det = a * c00 + b * c01 + c * c02;
+  if (det == 0.0) return false;
+  const double r = 1.0 / det;
+  double ia[9];
+  ia[0] = c00 * r; ia[1] = (c * h - b * k) * r; ia[2] = (b * f - c * e) * r;
+  ia[3] = c01 * r; ia[4] = (a * k - c * g) * r; ia[5] = (c * d - a * f) * r;
+  ia[6] = c02 * r; ia[7] = (b * g - a * h) * r; ia[8] = (a * e - b * d) * r;
+  for (int i = 0; i < 3; ++i) {
+    o[4 * i + 0] = ia[3 * i + 0];
+    o[4 * i + 1] = ia[3 * i + 1];
+    o[4 * i + 2] = ia[3 * i + 2];
+    o[4 * i + 3] = -(ia[3 * i + 0] * m[3] + ia[3 * i + 1] * m[7] + ia[3 * i + 2] * m[11]);
+  }
+  o[12] = 0.0; o[13] = 0.0; o[14] = 0.0; o[15] = 1.0;
+  return true;
+}
+
+// Denman-Beavers square root of a homogeneous affine 4x4 matrix
+// (vnl_utils.h:46-95) with EPS = 1e-14, MAX_ITER = 50 as called from
+// itkSymMirorrRegistrationMethod.txx.  Every iterate keeps the last row
+// 0 0 0 1, so the inverses are the affine ones.
 MB2_HD void matrix_sqrt4(const double *m, double *y_out) {
-  double y[16], z[16], ny[16], nz[16], iy[16], iz[16], d[16];
+  double y[16], z[16], iy[16], iz[16], d[16];
   for (int i = 0; i < 16; ++i) { y[i] = m[i]; z[i] = (i % 5 == 0) ? 1.0 : 0.0; }
   double dd = 1.7976931348623157e308;
   int it = 0;
   while (dd > 1e-14 && it < 50) {
-    mn_inverse<4>(z, iz);
-    mn_inverse<4>(y, iy);
-    for (int i = 0; i < 16; ++i) { ny[i] = 0.5 * (y[i] + iz[i]); nz[i] = 0.5 * (z[i] + iy[i]); }
-    for (int i = 0; i < 16; ++i) { y[i] = ny[i]; z[i] = nz[i]; }
+    affine4_inverse(z, iz);
+    affine4_inverse(y, iy);
+    for (int i = 0; i < 16; ++i) {
+      const double ny = 0.5 * (y[i] + iz[i]), nz = 0.5 * (z[i] + iy[i]);
+      y[i] = ny;
+      z[i] = nz;
+    }
     ++it;
     mn_mul<4>(y, y, d);
     dd = 0.0;
@@ -668,7 +697,7 @@ MB2_HD void half_space(const Tfm &t, Tfm &f, Tfm &b) {
   }
   m[15] = 1.0;
   matrix_sqrt4(m, m12);
-  mn_inverse<4>(m, mi);
+  affine4_inverse(m, mi);
   matrix_sqrt4(mi, im12);
   tfm_identity(f, t.kind);
   tfm_identity(b, t.kind);
