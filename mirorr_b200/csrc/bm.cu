@@ -51,9 +51,11 @@ void point_geom(const double origin[3], const double spacing[3], const double di
 // ---------------------------------------------------------------------------
 // Each thread computes PX consecutive x positions of one row: every footprint
 // row of PX + BW - 1 floats is loaded once and serves all PX positions.  Per
-// position the FP64 arithmetic and its order are the two-pass loop of
-// normalizedCorrelation (mean over all voxels, then the masked sum of squares
-// in raster order, itkBlockMatcher.txx:57-95).
+// position the statistics are the two-pass ones of normalizedCorrelation
+// (mean over all voxels, then the masked sum of squares in raster order,
+// itkBlockMatcher.txx:57-95) in FP64, the squares accumulated with fused
+// multiply-adds.  They feed the FP32 search only; a sum of squares is zero
+// exactly when every masked voxel equals the mean, as in the reference.
 constexpr int kBoxPX = 4;
 
 template <int BW>
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict_
             for (int j = 0; j < PX; ++j) {
               if (m[j + vx]) {
                 const double d = __dsub_rn((double)v[j + vx], mean[j]);
-                ss[j] = __dadd_rn(ss[j], __dmul_rn(d, d));
+                ss[j] = __fma_rn(d, d, ss[j]);
               } else {
                 all_in[j] = false;
               }

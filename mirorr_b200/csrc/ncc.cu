@@ -1202,7 +1202,8 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
   const int e3 = a.emax * a.emax * a.emax;
   float *xt = reinterpret_cast<float *>(smem);  // B centred (float)
   float *yw = xt + B;                            // e3
-  uint8_t *mb = reinterpret_cast<uint8_t *>(yw + e3);
+  float *scs = yw + e3;                          // W^3 candidate scores
+  uint8_t *mb = reinterpret_cast<uint8_t *>(scs + a.W * a.W * a.W);
   uint8_t *mw = mb + B;
   __shared__ int s_cnt, s_list[kK];
   __shared__ float s_red[4][2];
@@ -1253,7 +1254,8 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
     const bool fast = bst.mmode == 1 && ms_all;
     float l1 = -3.f, l2 = -3.f;
     int d1 = -1, d2 = -1;
-    // pass 1: FP32 top-2 and the first degenerate candidates
+    // pass 0 scores every candidate (FP32 top-2, first degenerate candidates);
+    // pass 1 lists those within 2 delta of the second-best from the stored scores
     for (int pass = 0; pass < 2; ++pass) {
       float T = 0.f;
       if (pass == 1) {
@@ -1282,6 +1284,14 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
         int cx = c % w.nx, cy = (c / w.nx) % w.ny, cz = c / (w.nx * w.ny);
         int px = w.sx + cx * a.g, py = w.sy + cy * a.g, pz = w.sz + cz * a.g;
         long long p = lin(a, px, py, pz);
+        if (pass == 1) {
+          const float s = scs[c];
+          if (s > -2.f && s >= T) {
+            int pos = atomicAdd(&s_cnt, 1);
+            if (pos < kK) s_list[pos] = (int)p;
+          }
+          continue;
+        }
         float2 st = __ldg(&a.stats[p]);
         const float mu = st.x;
         const int woff = ((cz * a.g) * w.ey + cy * a.g) * w.ex + cx * a.g;
@@ -1320,13 +1330,9 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
           syy = bst.mmode == 1 ? syy_of(st.y) : ay;
         }
         float s = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
-        if (pass == 0) {
-          top2_merge(l1, l2, s, -3.f);
-          if (s == -2.f) push_deg(d1, d2, (int)p);
-        } else if (s > -2.f && s >= T) {
-          int pos = atomicAdd(&s_cnt, 1);
-          if (pos < kK) s_list[pos] = (int)p;
-        }
+        top2_merge(l1, l2, s, -3.f);
+        if (s == -2.f) push_deg(d1, d2, (int)p);
+        scs[c] = s;
       }
     }
     __syncthreads();
@@ -1584,7 +1590,7 @@ template <int BW>
 mirorr_status launch_rest(const NccArgs &a, bool all_general, cudaStream_t s) {
   constexpr int B = BW * BW * BW;
   const size_t e3 = (size_t)a.emax * a.emax * a.emax, cmax = (size_t)a.W * a.W * a.W;
-  size_t smem_g = sizeof(float) * (B + e3) + B + e3 + 16;
+  size_t smem_g = sizeof(float) * (B + e3 + cmax) + B + e3 + 16;
   size_t smem_f = sizeof(double) * cmax + 16;
   if (smem_g > 200 * 1024 || smem_f > 200 * 1024) {
     set_error("search window too large for shared memory (window %d^3, %d candidates)",
