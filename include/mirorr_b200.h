@@ -141,6 +141,13 @@ MIRORR_API mirorr_status mirorr_resample(mirorr_ctx ctx, const int32_t in_size[3
                               const uint8_t *in_mask, const int32_t out_size[3],
                               const double C[9], const double e[3], float *out_image,
                               uint8_t *out_mask);
+/* The same with itk::NearestNeighborInterpolateImageFunction (index
+ * floor(c + 0.5)), the final resampling's "nn" interpolator
+ * (itkMirorrPyramidImplement.txx:365-479). */
+MIRORR_API mirorr_status mirorr_resample_nearest(mirorr_ctx ctx, const int32_t in_size[3],
+                                      const float *in_image, const uint8_t *in_mask,
+                                      const int32_t out_size[3], const double C[9],
+                                      const double e[3], float *out_image, uint8_t *out_mask);
 /* Affine index map of the resampler from geometries and a transform
  * y = M x + offset (output grid -> input continuous index). */
 MIRORR_API mirorr_status mirorr_resample_map(const mirorr_geometry *out_grid, const mirorr_geometry *in_grid,
@@ -215,6 +222,8 @@ typedef struct mirorr_reg_params {
   mirorr_bm_params bm;    /* CLI defaults: width 4, gap 1, nhood gap 3, nhood width 7 */
   double lts_keep;        /* LTS keep fraction (reference: 0.5) */
   int32_t verbosity;      /* 1: per-iteration lines; 2: also per-call block routing */
+  int32_t last_level;     /* --pyr-end: run the schedule's levels 1..last_level (1 = the
+                             coarsest); 0 = all, negative counts back from the finest */
 } mirorr_reg_params;
 
 typedef struct mirorr_reg_stats {

@@ -102,7 +102,8 @@ class Transform(ctypes.Structure):
 class RegParams(ctypes.Structure):
     _fields_ = [("symmetric", ctypes.c_int32), ("kind", ctypes.c_int32), ("levels", ctypes.c_int32),
                 ("iterations", ctypes.c_int32), ("min_length", ctypes.c_int32), ("bm", BMParams),
-                ("lts_keep", ctypes.c_double), ("verbosity", ctypes.c_int32)]
+                ("lts_keep", ctypes.c_double), ("verbosity", ctypes.c_int32),
+                ("last_level", ctypes.c_int32)]
 
 
 class RegStats(ctypes.Structure):
@@ -160,6 +161,7 @@ def lib():
         "mirorr_bm_last_diagnostics": [vp, vp],
         "mirorr_resample": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
         "mirorr_resample_map": [P(Geometry), P(Geometry), vp, vp, vp, vp],
+        "mirorr_resample_nearest": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
         "mirorr_lts_classic": [vp, P(Transform), ctypes.c_size_t, vp, vp, ctypes.c_double,
                                P(ctypes.c_int32)],
         "mirorr_lts_symmetric": [vp, P(Transform), P(Transform), P(Transform), ctypes.c_size_t,
@@ -421,8 +423,9 @@ def resample_map(out_geom: Geometry, in_geom: Geometry, M, offset):
     return C.reshape(3, 3), e
 
 
-def resample(ctx: Context, image, mask, out_size_xyz, C, e):
-    """Linear resampling of image (float32) and/or mask (uint8) on an index map."""
+def resample(ctx: Context, image, mask, out_size_xyz, C, e, nearest=False):
+    """Linear (or nearest-neighbour) resampling of image (float32) and/or mask
+    (uint8) on an index map."""
     ref = image if image is not None else mask
     in_size = (ctypes.c_int32 * 3)(ref.shape[2], ref.shape[1], ref.shape[0])
     out_size = (ctypes.c_int32 * 3)(*[int(v) for v in out_size_xyz])
@@ -433,8 +436,9 @@ def resample(ctx: Context, image, mask, out_size_xyz, C, e):
     outm = np.zeros(shape, np.uint8) if msk is not None else None
     Cc = np.ascontiguousarray(np.asarray(C, np.float64).reshape(-1))
     ec = np.ascontiguousarray(np.asarray(e, np.float64))
-    _check(lib().mirorr_resample(ctx.handle, in_size, _ptr(img), _ptr(msk), out_size, _ptr(Cc),
-                                 _ptr(ec), _ptr(out), _ptr(outm)))
+    fn = lib().mirorr_resample_nearest if nearest else lib().mirorr_resample
+    _check(fn(ctx.handle, in_size, _ptr(img), _ptr(msk), out_size, _ptr(Cc), _ptr(ec), _ptr(out),
+              _ptr(outm)))
     return out, outm
 
 
@@ -487,7 +491,7 @@ def lts_noalloc(ctx: Context, t: Transform, n: int, init_dev: int, moved_dev: in
 
 def reg_params(symmetric=True, kind="rigid", levels=0, iterations=5, block_width=4, block_gap=1,
                nhood_gap=3, nhood_width=7, block_keep=1.0, lts_keep=0.5, min_length=32,
-               verbosity=0) -> RegParams:
+               verbosity=0, last_level=0) -> RegParams:
     p = RegParams()
     _check(lib().mirorr_reg_default_params(ctypes.byref(p)))
     p.symmetric = 1 if symmetric else 0
@@ -502,6 +506,7 @@ def reg_params(symmetric=True, kind="rigid", levels=0, iterations=5, block_width
     p.bm.block_keep = float(block_keep)
     p.lts_keep = float(lts_keep)
     p.verbosity = int(verbosity)
+    p.last_level = int(last_level)
     return p
 
 

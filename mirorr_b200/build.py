@@ -29,6 +29,30 @@ def _deps():
     return files
 
 
+CLI_SRC = os.path.join(HERE, "cli")
+CLI_OUT = os.path.join(HERE, "bin", "mirorr")
+CXX = os.environ.get("CXX", "g++")
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> str:
+    """The `mirorr` command line (mirorr_b200/cli) linked to the library."""
+    srcs = sorted(os.path.join(CLI_SRC, f) for f in os.listdir(CLI_SRC) if f.endswith(".cpp"))
+    deps = srcs + [os.path.join(CLI_SRC, f) for f in os.listdir(CLI_SRC) if f.endswith(".hpp")]
+    deps += [OUT, os.path.join(SRC, "tfm.cuh")]
+    if (not force and os.path.exists(CLI_OUT)
+            and all(os.path.getmtime(f) <= os.path.getmtime(CLI_OUT) for f in deps)):
+        return CLI_OUT
+    os.makedirs(os.path.dirname(CLI_OUT), exist_ok=True)
+    tmp = CLI_OUT + f".tmp{os.getpid()}"
+    cmd = [CXX, "-O2", "-std=c++17", "-Wall", "-o", tmp, *srcs, f"-L{HERE}", "-lmirorr_b200",
+           "-Wl,-rpath,$ORIGIN/..", "-lz"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    os.replace(tmp, CLI_OUT)
+    return CLI_OUT
+
+
 def up_to_date() -> bool:
     if not os.path.exists(OUT):
         return False
@@ -67,3 +91,4 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True, ptxas_v="--ptxas-v" in sys.argv)
     print(OUT)
+    print(build_cli(force="--force" in sys.argv, verbose=True))

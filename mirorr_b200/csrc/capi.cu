@@ -717,6 +717,8 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float
            *fg, *mg, stats, 0};
   int sm[16][3], sf[16][3];
   int nl = pyramid_schedule(*fg, *mg, pp.min_length, pp.levels, sm, sf);
+  if (pp.last_level > 0 && pp.last_level < nl) nl = pp.last_level;
+  else if (pp.last_level < 0) nl = std::max(1, nl + pp.last_level);
   Tfm tfm;
   if (init) {
     if (!from_public(*init, tfm) || init->kind != pp.kind) {
@@ -1149,9 +1151,10 @@ mirorr_status mirorr_resample_map(const mirorr_geometry *out_grid, const mirorr_
   return MIRORR_OK;
 }
 
-mirorr_status mirorr_resample(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
-                              const uint8_t *in_mask, const int32_t out_size[3], const double C[9],
-                              const double e[3], float *out_image, uint8_t *out_mask) {
+static mirorr_status resample_common(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
+                                     const uint8_t *in_mask, const int32_t out_size[3],
+                                     const double C[9], const double e[3], float *out_image,
+                                     uint8_t *out_mask, bool nearest) {
   if (!c || !in_size || !out_size || !C || !e) { set_error("null argument"); return MIRORR_EINVAL; }
   if ((in_image && !out_image) || (in_mask && !out_mask)) {
     set_error("output buffer missing");
@@ -1180,10 +1183,10 @@ mirorr_status mirorr_resample(mirorr_ctx c, const int32_t in_size[3], const floa
     memcpy(m.C, C, sizeof(m.C));
     memcpy(m.e, e, sizeof(m.e));
     if (pi && (st = launch_resample(in_size, pi, nullptr, out_size, m, oi.as<float>(), nullptr,
-                                    c->stream)) != MIRORR_OK)
+                                    c->stream, nearest)) != MIRORR_OK)
       goto done;
     if (pm && (st = launch_resample(in_size, nullptr, pm, out_size, m, nullptr, om.as<uint8_t>(),
-                                    c->stream)) != MIRORR_OK)
+                                    c->stream, nearest)) != MIRORR_OK)
       goto done;
     if (pi && cudaMemcpyAsync(out_image, oi.ptr, sizeof(float) * no, cudaMemcpyDeviceToHost,
                               c->stream) != cudaSuccess) { st = MIRORR_ECUDA; goto done; }
@@ -1200,6 +1203,19 @@ done:
   cudaStreamSynchronize(c->stream);
   di.release(); dm.release(); oi.release(); om.release();
   return st;
+}
+
+mirorr_status mirorr_resample(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
+                              const uint8_t *in_mask, const int32_t out_size[3], const double C[9],
+                              const double e[3], float *out_image, uint8_t *out_mask) {
+  return resample_common(c, in_size, in_image, in_mask, out_size, C, e, out_image, out_mask, false);
+}
+
+mirorr_status mirorr_resample_nearest(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
+                                      const uint8_t *in_mask, const int32_t out_size[3],
+                                      const double C[9], const double e[3], float *out_image,
+                                      uint8_t *out_mask) {
+  return resample_common(c, in_size, in_image, in_mask, out_size, C, e, out_image, out_mask, true);
 }
 
 // ---- LTS ---------------------------------------------------------------------------

@@ -88,7 +88,7 @@ struct ResampleMap {
 };
 mirorr_status launch_resample(const int in_size[3], const float *in, const uint8_t *in_mask,
                               const int out_size[3], const ResampleMap &map, float *out,
-                              uint8_t *out_mask, cudaStream_t s);
+                              uint8_t *out_mask, cudaStream_t s, bool nearest = false);
 // Separable Gaussian smoothing along one axis (axis 0 = x).
 mirorr_status launch_smooth_axis(const int size[3], const float *in, float *out, int axis,
                                  const double *w, int radius, cudaStream_t s);

@@ -27,6 +27,7 @@ struct ResampleArgs {
   double e[3];
   float *out;
   uint8_t *outm;
+  int nearest;  // nearest-neighbour instead of linear interpolation
 };
 
 __device__ inline double dlerp(double a, double b, double t) {
@@ -55,6 +56,21 @@ __global__ void __launch_bounds__(256) resample_kernel(ResampleArgs a) {
     if (!inside) {
       if (a.out) a.out[o] = 0.0f;
       if (a.outm) a.outm[o] = 0;
+      continue;
+    }
+    if (a.nearest) {
+      // NearestNeighborInterpolateImageFunction: index = floor(c + 0.5)
+      long long q = 0, stride = 1;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        int b = (int)floor(__dadd_rn(c[r], 0.5));
+        if (b < 0) b = 0;
+        if (b > nn[r] - 1) b = nn[r] - 1;
+        q += (long long)b * stride;
+        stride *= nn[r];
+      }
+      if (a.out) a.out[o] = __ldg(a.in + q);
+      if (a.outm) a.outm[o] = __ldg(a.inm + q);
       continue;
     }
     int i0[3], i1[3];
@@ -106,8 +122,9 @@ __global__ void __launch_bounds__(256) resample_kernel(ResampleArgs a) {
 
 mirorr_status launch_resample(const int in_size[3], const float *in, const uint8_t *in_mask,
                               const int out_size[3], const ResampleMap &map, float *out,
-                              uint8_t *out_mask, cudaStream_t s) {
+                              uint8_t *out_mask, cudaStream_t s, bool nearest) {
   ResampleArgs a;
+  a.nearest = nearest ? 1 : 0;
   a.in = in; a.inm = in_mask;
   a.inx = in_size[0]; a.iny = in_size[1]; a.inz = in_size[2];
   a.onx = out_size[0]; a.ony = out_size[1]; a.onz = out_size[2];

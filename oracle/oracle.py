@@ -266,6 +266,31 @@ def resample(in_data, in_mask, out_size, C, e):
     return out, outm
 
 
+def resample_nearest(in_data, in_mask, out_size, C, e):
+    """Nearest-neighbour resampling on an explicit index map, as
+    itk::NearestNeighborInterpolateImageFunction inside ResampleImageFilter:
+    c = e + C idx evaluated left to right in FP64, inside test
+    -0.5 <= c < n - 0.5 (otherwise 0), index floor(c + 0.5)."""
+    ref = in_data if in_data is not None else in_mask
+    n = (ref.shape[2], ref.shape[1], ref.shape[0])
+    k, j, i = np.meshgrid(np.arange(out_size[2], dtype=np.float64),
+                          np.arange(out_size[1], dtype=np.float64),
+                          np.arange(out_size[0], dtype=np.float64), indexing="ij")
+    C = np.asarray(C, np.float64).reshape(3, 3)
+    c = [((e[r] + C[r, 0] * i) + C[r, 1] * j) + C[r, 2] * k for r in range(3)]
+    inside = np.ones(k.shape, bool)
+    idx = []
+    for r in range(3):
+        inside &= (c[r] >= -0.5) & (c[r] < n[r] - 0.5)
+        idx.append(np.clip(np.floor(c[r] + 0.5), 0, n[r] - 1).astype(np.int64))
+    out = outm = None
+    if in_data is not None:
+        out = np.where(inside, np.asarray(in_data, np.float32)[idx[2], idx[1], idx[0]], 0).astype(np.float32)
+    if in_mask is not None:
+        outm = np.where(inside, np.asarray(in_mask, np.uint8)[idx[2], idx[1], idx[0]], 0).astype(np.uint8)
+    return out, outm
+
+
 # ---------------------------------------------------------------------------
 # ITK transform semantics (restated)
 # ---------------------------------------------------------------------------

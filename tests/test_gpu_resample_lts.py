@@ -37,6 +37,23 @@ def test_resample_bit_exact(ctx, seed):
     np.testing.assert_allclose(eg, e, atol=1e-12)
 
 
+@pytest.mark.parametrize("seed", [3, 4])
+def test_resample_nearest_bit_exact(ctx, seed):
+    rng = np.random.default_rng(seed)
+    img = rng.random((21, 26, 30)).astype(np.float32)
+    msk = (rng.random(img.shape) > 0.4).astype(np.uint8) * 255
+    M = random_rotation(rng, 12.0) @ np.diag(rng.uniform(0.85, 1.15, 3))
+    off = rng.uniform(-4, 4, 3)
+    gin = O.Image(img, np.array([1.0, 0.8, 1.1]), np.array([0.0, 1.0, -2.0]))
+    gout = O.Image(np.zeros((19, 25, 31), np.float32), np.array([1.1, 0.9, 1.0]),
+                   np.array([0.5, 0.0, -1.0]))
+    C, e = O.resample_map(gout, gin, M, off)
+    out_o, outm_o = O.resample_nearest(img, msk, gout.size, C, e)
+    out_g, outm_g = mb.resample(ctx, img, msk, gout.size, C, e, nearest=True)
+    np.testing.assert_array_equal(out_g, out_o)
+    np.testing.assert_array_equal(outm_g, outm_o)
+
+
 @pytest.mark.parametrize("factors", [(2, 2, 2), (4, 4, 2), (2, 2, 1), (8, 8, 4)])
 def test_pyramid_level_bit_exact(ctx, factors):
     ph = make_phantom((64, 48, 40), n_gauss=10, seed=3)
