@@ -18,11 +18,12 @@
 //      and the list of candidates whose FP32 score lies within 2*delta of the
 //      FP32 second-best (delta bounds |FP32 - FP64|), plus the first two
 //      degenerate candidates when fewer than two are non-degenerate.
-//        * ncc_fast_kernel: blocks whose base block and search window are
-//          wholly inside both masks, block gap 1.  Several blocks per CTA;
-//          each thread keeps a TY x W tile of candidates in registers and
-//          streams window rows from shared memory (cross term only: one FMA
-//          per voxel and candidate).
+//        * ncc_xlane_kernel (block width 4, window 7 or 9) and
+//          ncc_warp_kernel (other widths): blocks whose base block and search
+//          window are wholly inside both masks, block gap 1; cross term only,
+//          one FMA per voxel and candidate.  They route the other blocks.
+//        * ncc_masked_kernel: base block inside its mask, window partly
+//          masked, block gap 1; three correlations.
 //        * ncc_general_kernel: every other block (any mask pattern, any gap),
 //          one CTA per block.
 //   2. ncc_refine_kernel, one thread per block: the listed candidates are
@@ -271,19 +272,16 @@ __global__ void block_stat_kernel(NccArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Register-blocked FP32 search, block gap 1.  Several blocks per CTA; each
-// thread owns a TY x W tile of candidates (one z plane) and streams window
-// rows from shared memory.  The window is staged as y - c with c the mean of
-// the block's own candidate (a per-block constant that keeps the FP32 cross
-// term free of cancellation): Sxy = sum x~ (y - c) - (mu - c) sum x~.
-//   MASKED = false: base block and whole window inside both masks,
-//                   Sxy from one correlation, Syy from box_stats.
-//   MASKED = true : base block inside its mask, window partly masked (m = ms):
-//                   C1 = sum x~ ms (y - c), C2 = sum x~ ms, C3 = sum x~^2 ms,
-//                   Sxy = C1 - (mu - c) C2, Sxx = C3, Syy from box_stats.
-// The unmasked kernel runs over every block and routes the others: blocks
-// with a partly masked window to the masked kernel, blocks with a partly
-// masked base block to the general kernel.
+// Register-blocked FP32 search for blocks whose base block lies inside its
+// mask but whose window is partly masked (block gap 1).  The unmasked search
+// kernels route these blocks here through the list after gen_list[nblocks].
+// Several blocks per CTA; each thread owns a TY x W tile of candidates (one
+// z plane) and streams window rows from shared memory.  The window is staged
+// as (y - c) ms, with ms the search mask and c the mean of the block's own
+// candidate (a per-block constant that keeps the FP32 cross term free of
+// cancellation), next to ms itself:
+//   C1 = sum x~ ms (y - c),  C2 = sum x~ ms,  C3 = sum x~^2 ms,
+//   Sxy = C1 - (mu - c) C2,  Sxx = C3,  Syy from box_stats.
 // ---------------------------------------------------------------------------
 template <int BW_, int W_, int TY_, int BPC_>
 struct FastCfg {
@@ -302,15 +300,15 @@ struct FastCfg {
   static_assert(WIN % 4 == 0 && EXP % 4 == 0 && PS % 4 == 0 && B > 0, "alignment");
 };
 
-template <class C, bool MASKED>
-__global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
+template <class C>
+__global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
   constexpr int BW = C::BW, W = C::W, TY = C::TY, BPC = C::BPC, B = C::B, R = C::R, E = C::E;
   constexpr int EY = C::EY, EXP = C::EXP, PS = C::PS, WIN = C::WIN, TPB = C::TPB, NYG = C::NYG;
-  constexpr int NWIN = E * EY * E;
+  constexpr int NROW = E * EY;
   extern __shared__ __align__(16) float sm[];
-  float *win = sm;                                  // BPC * WIN: y - c
-  float *mwin = win + BPC * WIN;                    // BPC * WIN: ms != 0 (MASKED only)
-  float *xt = win + (MASKED ? 2 : 1) * BPC * WIN;   // BPC * B
+  float *win = sm;                    // BPC * WIN: (y - c) ms
+  float *mwin = win + BPC * WIN;      // BPC * WIN: ms != 0
+  float *xt = win + 2 * BPC * WIN;    // BPC * B: x - mu
   __shared__ float s_red[BPC][TPB][2];
   __shared__ int s_deg[BPC][TPB][2];
   __shared__ float s_f[BPC][2];
@@ -318,12 +316,9 @@ __global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
   __shared__ int s_cnt[BPC];
   __shared__ int s_list[BPC][kK];
   __shared__ int s_state[BPC];           // 1 compute, 0 skip
-  __shared__ int s_inmask[BPC];
   __shared__ int s_b[BPC];
   __shared__ int s_o[BPC][3];            // window origin (block origin - R)
   __shared__ float s_c[BPC];
-  __shared__ float s_sxt[BPC];
-  __shared__ float s_sxx[BPC];
   __shared__ double s_mean[BPC];
   const int tid = threadIdx.x;
   const int slot = tid / TPB;
@@ -332,17 +327,16 @@ __global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
   const int cz = lt / NYG;
   const int cy0 = (lt - cz * NYG) * TY;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const long long nlist = MASKED ? (long long)*(volatile unsigned int *)&a.ctl[4] : a.nblocks;
+  const long long nlist = (long long)*(volatile unsigned int *)&a.ctl[4];
 
   for (long long base = (long long)blockIdx.x * BPC; base < nlist; base += (long long)gridDim.x * BPC) {
     __syncthreads();
     if (tid < BPC) {
       long long i = base + tid;
       int state = 0;
-      s_inmask[tid] = 1;
       s_cnt[tid] = 0;
       if (i < nlist) {
-        const int b = MASKED ? a.gen_list[a.nblocks + 1 + i] : (int)i;
+        const int b = a.gen_list[a.nblocks + 1 + i];
         s_b[tid] = b;
         const int bx = b % a.nbx, by = (b / a.nbx) % a.nby, bz = b / (a.nbx * a.nby);
         const int ox = a.stx + bx * a.G, oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
@@ -350,52 +344,46 @@ __global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
         s_o[tid][1] = oy - R;
         s_o[tid][2] = oz - R;
         const long long o = ((long long)oz * ny + oy) * nx + ox;
-        bool ok = true;
-        if (!MASKED) {
-          BlockWin w;
-          ok = block_window(a, b, w);
-          if (a.selected && !a.selected[b]) {
-            write_final(a, b, -3.f, -3.f, o, 0);
-            a.rec[b].cnt = -1;
-            ok = false;
-          } else if (!ok) {
-            write_final(a, b, -3.f, -3.f, o, 1);
-            a.rec[b].cnt = -1;
-          }
-        }
-        if (ok) {
-          BlockStat st = a.bstat[b];
-          if (st.mmode == 1) {
-            state = 1;
-            s_sxt[tid] = st.sxt;
-            s_sxx[tid] = st.sxx;
-            s_mean[tid] = st.mean;
-            s_c[tid] = __ldg(&a.stats[o]).x;  // the block's own position is a candidate
-          } else {
-            unsigned int p = atomicAdd(&a.ctl[0], 1u);
-            a.gen_list[p] = b;
-          }
+        const BlockStat st = a.bstat[b];
+        if (st.mmode == 1) {
+          state = 1;
+          s_mean[tid] = st.mean;
+          s_c[tid] = __ldg(&a.stats[o]).x;  // the block's own position is a candidate
+        } else {
+          unsigned int p = atomicAdd(&a.ctl[0], 1u);
+          a.gen_list[p] = b;
         }
       }
       s_state[tid] = state;
     }
     __syncthreads();
-    // stage windows (zero outside the image), masks and the raw base blocks
-    // with asynchronous copies; test the candidates' mask flags
-    for (int i = tid; i < BPC * NWIN; i += blockDim.x) {
-      const int s = i / NWIN;
+    // stage the windows, one thread per window row: (y - c) ms and ms, zero
+    // outside the image and in the padding; the base blocks as x - mu
+    for (int i = tid; i < BPC * NROW; i += blockDim.x) {
+      const int s = i / NROW;
       if (!s_state[s]) continue;
-      const int r = i - s * NWIN;
-      const int x = r % E, y = (r / E) % EY, z = r / (E * EY);
-      const int gx = s_o[s][0] + x, gy = s_o[s][1] + y, gz = s_o[s][2] + z;
-      const int off = s * WIN + z * PS + y * EXP + x;
-      if (y < E && gx >= 0 && gy >= 0 && gz >= 0 && gx < nx && gy < ny && gz < nz) {
-        const long long q = ((long long)gz * ny + gy) * nx + gx;
-        cp_async4(&win[off], &a.search[q]);
-        if (MASKED) mwin[off] = __ldg(&a.smask[q]) ? 1.f : 0.f;
-      } else {
-        win[off] = 0.f;
-        if (MASKED) mwin[off] = 0.f;
+      const int rr = i - s * NROW;
+      const int z = rr / EY, y = rr - z * EY;
+      const int gx0 = s_o[s][0], gy = s_o[s][1] + y, gz = s_o[s][2] + z;
+      const float c = s_c[s];
+      const bool rowin = y < E && gy >= 0 && gz >= 0 && gy < ny && gz < nz;
+      const long long q0 = ((long long)gz * ny + gy) * nx + gx0;
+      float4 *wr = reinterpret_cast<float4 *>(win + s * WIN + z * PS + y * EXP);
+      float4 *mr = reinterpret_cast<float4 *>(mwin + s * WIN + z * PS + y * EXP);
+#pragma unroll
+      for (int k = 0; k < EXP / 4; ++k) {
+        float v[4], mv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int x = 4 * k + e;
+          const bool in = rowin && x < E && gx0 + x >= 0 && gx0 + x < nx;
+          const float yv = in ? __ldg(&a.search[q0 + x]) : 0.f;
+          const bool ms = in && __ldg(&a.smask[q0 + x]) != 0;
+          v[e] = ms ? yv - c : 0.f;
+          mv[e] = ms ? 1.f : 0.f;
+        }
+        wr[k] = make_float4(v[0], v[1], v[2], v[3]);
+        mr[k] = make_float4(mv[0], mv[1], mv[2], mv[3]);
       }
     }
     for (int i = tid; i < BPC * B; i += blockDim.x) {
@@ -405,92 +393,40 @@ __global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
       const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
       const long long q = ((long long)(s_o[s][2] + R + vz) * ny + (s_o[s][1] + R + vy)) * nx +
                           (s_o[s][0] + R + vx);
-      cp_async4(&xt[i], &a.base[q]);
-    }
-    if (!MASKED && worker && s_state[slot]) {
-      const int px0 = s_o[slot][0], py0 = s_o[slot][1] + cy0, pz = s_o[slot][2] + cz;
-      bool ok = true;
-      if (pz >= 0 && pz <= nz - BW) {
-#pragma unroll
-        for (int j = 0; j < TY; ++j) {
-          const int py = py0 + j;
-          if (cy0 + j >= W || py < 0 || py > ny - BW) continue;
-#pragma unroll
-          for (int x = 0; x < W; ++x) {
-            const int px = px0 + x;
-            if (px < 0 || px > nx - BW) continue;
-            if (!footprint_in_mask(__ldg(&a.stats[((long long)pz * ny + py) * nx + px]).y)) ok = false;
-          }
-        }
-      }
-      if (!ok) s_inmask[slot] = 0;
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    for (int i = tid; i < BPC * NWIN; i += blockDim.x) {
-      const int s = i / NWIN;
-      if (!s_state[s]) continue;
-      const int r = i - s * NWIN;
-      const int x = r % E, y = (r / E) % EY, z = r / (E * EY);
-      const int off = s * WIN + z * PS + y * EXP + x;
-      if (MASKED) {
-        if (mwin[off] != 0.f) win[off] = win[off] - s_c[s];
-        else win[off] = 0.f;
-      } else {
-        win[off] = win[off] - s_c[s];
-      }
-    }
-    for (int i = tid; i < BPC * B; i += blockDim.x) {
-      const int s = i / B;
-      if (!s_state[s]) continue;
-      xt[i] = (float)__dsub_rn((double)xt[i], s_mean[s]);
-    }
-    if (!MASKED && tid < BPC && s_state[tid] && !s_inmask[tid]) {
-      // partly masked window: the masked kernel takes it
-      unsigned int p = atomicAdd(&a.ctl[4], 1u);
-      a.gen_list[a.nblocks + 1 + p] = s_b[tid];
-      s_state[tid] = 0;
+      xt[i] = (float)__dsub_rn((double)__ldg(&a.base[q]), s_mean[s]);
     }
     __syncthreads();
     const bool active = worker && s_state[slot];
-    float sc[TY][W];
-    float c2[MASKED ? TY : 1][MASKED ? W : 1];
-    float c3[MASKED ? TY : 1][MASKED ? W : 1];
+    float sc[TY][W], c2[TY][W], c3[TY][W];
     float l1 = -3.f, l2 = -3.f;
     int d1 = -1, d2 = -1;
     if (active) {
 #pragma unroll
       for (int j = 0; j < TY; ++j)
 #pragma unroll
-        for (int x = 0; x < W; ++x) {
-          sc[j][x] = 0.f;
-          if (MASKED) { c2[j][x] = 0.f; c3[j][x] = 0.f; }
-        }
+        for (int x = 0; x < W; ++x) { sc[j][x] = 0.f; c2[j][x] = 0.f; c3[j][x] = 0.f; }
       const int wo = slot * WIN + cz * PS + cy0 * EXP;
       const float *tp = xt + slot * B;
 #pragma unroll 1
       for (int vz = 0; vz < BW; ++vz) {
-        float t[BW][BW];
+        float t[BW][BW], t2[BW][BW];
 #pragma unroll
         for (int vy = 0; vy < BW; ++vy)
 #pragma unroll
-          for (int vx = 0; vx < BW; ++vx) t[vy][vx] = tp[(vz * BW + vy) * BW + vx];
+          for (int vx = 0; vx < BW; ++vx) {
+            t[vy][vx] = tp[(vz * BW + vy) * BW + vx];
+            t2[vy][vx] = t[vy][vx] * t[vy][vx];
+          }
 #pragma unroll
         for (int j = 0; j < TY + BW - 1; ++j) {
-          float r[EXP], m[MASKED ? EXP : 1];
+          float r[EXP], m[EXP];
           const float4 *rp = reinterpret_cast<const float4 *>(win + wo + vz * PS + j * EXP);
+          const float4 *mp = reinterpret_cast<const float4 *>(mwin + wo + vz * PS + j * EXP);
 #pragma unroll
           for (int k = 0; k < EXP / 4; ++k) {
-            float4 q = rp[k];
+            const float4 q = rp[k], u = mp[k];
             r[4 * k] = q.x; r[4 * k + 1] = q.y; r[4 * k + 2] = q.z; r[4 * k + 3] = q.w;
-          }
-          if (MASKED) {
-            const float4 *mp = reinterpret_cast<const float4 *>(mwin + wo + vz * PS + j * EXP);
-#pragma unroll
-            for (int k = 0; k < EXP / 4; ++k) {
-              float4 q = mp[k];
-              m[4 * k] = q.x; m[4 * k + 1] = q.y; m[4 * k + 2] = q.z; m[4 * k + 3] = q.w;
-            }
+            m[4 * k] = u.x; m[4 * k + 1] = u.y; m[4 * k + 2] = u.z; m[4 * k + 3] = u.w;
           }
 #pragma unroll
           for (int vy = 0; vy < BW; ++vy) {
@@ -498,27 +434,22 @@ __global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
             if (jj < 0 || jj >= TY) continue;
 #pragma unroll
             for (int x = 0; x < W; ++x) {
-              float acc = sc[jj][x];
+              float a1 = sc[jj][x], a2 = c2[jj][x], a3 = c3[jj][x];
 #pragma unroll
-              for (int vx = 0; vx < BW; ++vx) acc = fmaf(t[vy][vx], r[x + vx], acc);
-              sc[jj][x] = acc;
-              if (MASKED) {
-                float a2 = c2[jj][x], a3 = c3[jj][x];
-#pragma unroll
-                for (int vx = 0; vx < BW; ++vx) {
-                  const float tm = t[vy][vx] * m[x + vx];
-                  a2 += tm;
-                  a3 = fmaf(tm, t[vy][vx], a3);
-                }
-                c2[jj][x] = a2;
-                c3[jj][x] = a3;
+              for (int vx = 0; vx < BW; ++vx) {
+                a1 = fmaf(t[vy][vx], r[x + vx], a1);
+                a2 = fmaf(t[vy][vx], m[x + vx], a2);
+                a3 = fmaf(t2[vy][vx], m[x + vx], a3);
               }
+              sc[jj][x] = a1;
+              c2[jj][x] = a2;
+              c3[jj][x] = a3;
             }
           }
         }
       }
       // scores
-      const float sxt = s_sxt[slot], sxx_b = s_sxx[slot], cc = s_c[slot];
+      const float cc = s_c[slot];
       const int pz = s_o[slot][2] + cz;
 #pragma unroll
       for (int j = 0; j < TY; ++j) {
@@ -533,15 +464,8 @@ __global__ void __launch_bounds__(C::NT) ncc_fast_kernel(NccArgs a) {
             const long long p = ((long long)pz * ny + py) * nx + px;
             const float2 st = __ldg(&a.stats[p]);
             const float syy = syy_of(st.y);
-            const float dm = st.x - cc;
-            float sxy, sxx;
-            if (MASKED) {
-              sxy = sc[j][x] - dm * c2[j][x];
-              sxx = c3[j][x];
-            } else {
-              sxy = sc[j][x] - dm * sxt;
-              sxx = sxx_b;
-            }
+            const float sxy = sc[j][x] - (st.x - cc) * c2[j][x];
+            const float sxx = c3[j][x];
             s = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
             if (s == -2.f) push_deg(d1, d2, (int)p);
             top2_merge(l1, l2, s, -3.f);
@@ -1557,13 +1481,13 @@ mirorr_status set_smem(K kernel, size_t smem) {
   return MIRORR_OK;
 }
 
-template <class C, bool MASKED>
-mirorr_status launch_fast1(const NccArgs &a, cudaStream_t s) {
-  size_t smem = sizeof(float) * (size_t)C::BPC * ((MASKED ? 2 : 1) * C::WIN + C::B);
-  MB2_TRY(set_smem(ncc_fast_kernel<C, MASKED>, smem));
+template <class C>
+mirorr_status launch_masked(const NccArgs &a, cudaStream_t s) {
+  size_t smem = sizeof(float) * (size_t)C::BPC * (2 * C::WIN + C::B);
+  MB2_TRY(set_smem(ncc_masked_kernel<C>, smem));
   long long need = (a.nblocks + C::BPC - 1) / C::BPC;
   long long grid = need < 148LL * 8 ? need : 148LL * 8;
-  ncc_fast_kernel<C, MASKED><<<(unsigned)grid, C::NT, smem, s>>>(a);
+  ncc_masked_kernel<C><<<(unsigned)grid, C::NT, smem, s>>>(a);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
@@ -1582,7 +1506,7 @@ mirorr_status launch_warp(const NccArgs &a, cudaStream_t s) {
 template <class CW, class CM>
 mirorr_status launch_fast(const NccArgs &a, cudaStream_t s) {
   MB2_TRY((launch_warp<CW>(a, s)));
-  MB2_TRY((launch_fast1<CM, true>(a, s)));
+  MB2_TRY((launch_masked<CM>(a, s)));
   return MIRORR_OK;
 }
 
@@ -1705,7 +1629,7 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
   ncc_xlane_kernel<W><<<(unsigned)grid, 32, smem, s>>>(a, xa, tmap);
   MB2_LAUNCH_CHECK();
   if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[1], s));
-  MB2_TRY((launch_fast1<CM, true>(a, s)));
+  MB2_TRY((launch_masked<CM>(a, s)));
   done = true;
   return MIRORR_OK;
 }
