@@ -279,9 +279,16 @@ __global__ void block_stat_kernel(NccArgs a) {
 // z plane) and streams window rows from shared memory.  The window is staged
 // as (y - c) ms, with ms the search mask and c the mean of the block's own
 // candidate (a per-block constant that keeps the FP32 cross term free of
-// cancellation), next to ms itself:
+// cancellation), and with
 //   C1 = sum x~ ms (y - c),  C2 = sum x~ ms,  C3 = sum x~^2 ms,
-//   Sxy = C1 - (mu - c) C2,  Sxx = C3,  Syy from box_stats.
+//   Sxy = C1 - (mu - c) C2,  Sxx = C3,  Syy from box_stats
+// every candidate gets C1 from the register tiles.  C2 and C3 are needed only
+// where the footprint straddles the mask edge: wholly inside it they are the
+// block's own sums, wholly outside it Syy = 0 and the score is -2.  Those
+// candidates are listed in shared memory and finished by the whole CTA from
+// per-row mask bits and per-block tables of partial sums (for each base row
+// (vy, vz) and each pattern of BW mask bits along x, the sums of x~ and x~^2
+// over the set bits).
 // ---------------------------------------------------------------------------
 template <int BW_, int W_, int TY_, int BPC_>
 struct FastCfg {
@@ -297,18 +304,33 @@ struct FastCfg {
   static constexpr int WIN = E * PS;                   // floats per block window
   static constexpr int TPB = W * NYG;                  // threads per block
   static constexpr int NT = ((BPC * TPB + 31) / 32) * 32;
+  static constexpr int NC = W * W * W;                 // candidates per block
+  static constexpr int NROW = E * EY;                  // window rows per block
+  static constexpr int NPAT = 1 << BW;                 // mask patterns of one base row
+  static constexpr int NTAB = BW * BW * NPAT;          // table entries per block
+  // dynamic shared memory, in floats: windows, base blocks, row bits, tables
+  static constexpr int OFF_XT = BPC * WIN;
+  static constexpr int OFF_BITS = OFF_XT + ((BPC * B + 3) & ~3);
+  static constexpr int OFF_TAB = OFF_BITS + ((BPC * NROW + 3) & ~3);
+  static constexpr int SMEM_FLOATS = OFF_TAB + 2 * BPC * NTAB;
   static_assert(WIN % 4 == 0 && EXP % 4 == 0 && PS % 4 == 0 && B > 0, "alignment");
+  static_assert(2 * NC <= WIN, "scores and straddler list reuse the window");
+  static_assert(E <= 16 && NT % 32 == 0, "a window row fits 16 lanes");
 };
 
 template <class C>
 __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
   constexpr int BW = C::BW, W = C::W, TY = C::TY, BPC = C::BPC, B = C::B, R = C::R, E = C::E;
   constexpr int EY = C::EY, EXP = C::EXP, PS = C::PS, WIN = C::WIN, TPB = C::TPB, NYG = C::NYG;
-  constexpr int NROW = E * EY;
+  constexpr int NC = C::NC, NROW = C::NROW, NPAT = C::NPAT, NTAB = C::NTAB;
   extern __shared__ __align__(16) float sm[];
-  float *win = sm;                    // BPC * WIN: (y - c) ms
-  float *mwin = win + BPC * WIN;      // BPC * WIN: ms != 0
-  float *xt = win + 2 * BPC * WIN;    // BPC * B: x - mu
+  float *win = sm;                                                // BPC * WIN: (y - c) ms
+  float *xt = sm + C::OFF_XT;                                     // BPC * B: x - mu
+  unsigned int *bits = reinterpret_cast<unsigned int *>(sm + C::OFF_BITS);  // BPC * NROW
+  float2 *tab = reinterpret_cast<float2 *>(sm + C::OFF_TAB);      // BPC * NTAB
+  // after the correlation pass the windows hold the scores and the list
+  float *scs = sm;                                                // BPC * NC
+  int *slist = reinterpret_cast<int *>(sm + BPC * NC);           // BPC * NC
   __shared__ float s_red[BPC][TPB][2];
   __shared__ int s_deg[BPC][TPB][2];
   __shared__ float s_f[BPC][2];
@@ -319,7 +341,10 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
   __shared__ int s_b[BPC];
   __shared__ int s_o[BPC][3];            // window origin (block origin - R)
   __shared__ float s_c[BPC];
+  __shared__ float s_sxt[BPC];
+  __shared__ float s_sxx[BPC];
   __shared__ double s_mean[BPC];
+  __shared__ int s_nstr;
   const int tid = threadIdx.x;
   const int slot = tid / TPB;
   const int lt = tid - slot * TPB;
@@ -348,6 +373,8 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
         if (st.mmode == 1) {
           state = 1;
           s_mean[tid] = st.mean;
+          s_sxt[tid] = st.sxt;
+          s_sxx[tid] = st.sxx;
           s_c[tid] = __ldg(&a.stats[o]).x;  // the block's own position is a candidate
         } else {
           unsigned int p = atomicAdd(&a.ctl[0], 1u);
@@ -356,34 +383,33 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
       }
       s_state[tid] = state;
     }
+    if (tid == 0) s_nstr = 0;
     __syncthreads();
-    // stage the windows, one thread per window row: (y - c) ms and ms, zero
-    // outside the image and in the padding; the base blocks as x - mu
-    for (int i = tid; i < BPC * NROW; i += blockDim.x) {
-      const int s = i / NROW;
-      if (!s_state[s]) continue;
-      const int rr = i - s * NROW;
-      const int z = rr / EY, y = rr - z * EY;
-      const int gx0 = s_o[s][0], gy = s_o[s][1] + y, gz = s_o[s][2] + z;
-      const float c = s_c[s];
-      const bool rowin = y < E && gy >= 0 && gz >= 0 && gy < ny && gz < nz;
-      const long long q0 = ((long long)gz * ny + gy) * nx + gx0;
-      float4 *wr = reinterpret_cast<float4 *>(win + s * WIN + z * PS + y * EXP);
-      float4 *mr = reinterpret_cast<float4 *>(mwin + s * WIN + z * PS + y * EXP);
-#pragma unroll
-      for (int k = 0; k < EXP / 4; ++k) {
-        float v[4], mv[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int x = 4 * k + e;
-          const bool in = rowin && x < E && gx0 + x >= 0 && gx0 + x < nx;
-          const float yv = in ? __ldg(&a.search[q0 + x]) : 0.f;
-          const bool ms = in && __ldg(&a.smask[q0 + x]) != 0;
-          v[e] = ms ? yv - c : 0.f;
-          mv[e] = ms ? 1.f : 0.f;
+    // stage the windows, 16 lanes per window row (consecutive x): (y - c) ms,
+    // zero outside the image and in the padding, and the row's mask bits
+    // (warp ballot); the base blocks as x - mu
+    {
+      constexpr int LPR = 16, RPI = C::NT / LPR;  // rows per pass
+      constexpr int NPASS = (BPC * NROW + RPI - 1) / RPI;
+      const int xl = tid & (LPR - 1);
+#pragma unroll 2
+      for (int it = 0; it < NPASS; ++it) {
+        const int i = it * RPI + tid / LPR;
+        const int s = i < BPC * NROW ? i / NROW : 0;
+        const bool rowact = i < BPC * NROW && s_state[s];
+        const int rr = i - s * NROW;
+        const int z = rr / EY, y = rr - z * EY;
+        const int gx = s_o[s][0] + xl, gy = s_o[s][1] + y, gz = s_o[s][2] + z;
+        const bool in = rowact && xl < E && y < E && gx >= 0 && gy >= 0 && gz >= 0 && gx < nx &&
+                        gy < ny && gz < nz;
+        const long long q = ((long long)gz * ny + gy) * nx + gx;
+        const float yv = in ? __ldg(&a.search[q]) : 0.f;
+        const bool ms = in && __ldg(&a.smask[q]) != 0;
+        const unsigned int bal = __ballot_sync(0xffffffffu, ms);
+        if (rowact) {
+          if (xl < EXP) win[s * WIN + z * PS + y * EXP + xl] = ms ? yv - s_c[s] : 0.f;
+          if (xl == 0) bits[i] = (bal >> (tid & LPR)) & 0xFFFFu;
         }
-        wr[k] = make_float4(v[0], v[1], v[2], v[3]);
-        mr[k] = make_float4(mv[0], mv[1], mv[2], mv[3]);
       }
     }
     for (int i = tid; i < BPC * B; i += blockDim.x) {
@@ -396,37 +422,47 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
       xt[i] = (float)__dsub_rn((double)__ldg(&a.base[q]), s_mean[s]);
     }
     __syncthreads();
+    // partial-sum tables: entry (vz, vy, pattern) = sums of x~ and x~^2 over
+    // the x offsets set in the pattern
+    for (int i = tid; i < BPC * NTAB; i += blockDim.x) {
+      const int s = i / NTAB;
+      if (!s_state[s]) continue;
+      const int e = i - s * NTAB;
+      const int row = e / NPAT, pat = e - row * NPAT;
+      const float *xr = xt + s * B + row * BW;
+      float s2 = 0.f, s3 = 0.f;
+#pragma unroll
+      for (int vx = 0; vx < BW; ++vx)
+        if ((pat >> vx) & 1) {
+          s2 += xr[vx];
+          s3 = fmaf(xr[vx], xr[vx], s3);
+        }
+      tab[i] = make_float2(s2, s3);
+    }
     const bool active = worker && s_state[slot];
-    float sc[TY][W], c2[TY][W], c3[TY][W];
-    float l1 = -3.f, l2 = -3.f;
-    int d1 = -1, d2 = -1;
+    float sc[TY][W];
     if (active) {
 #pragma unroll
       for (int j = 0; j < TY; ++j)
 #pragma unroll
-        for (int x = 0; x < W; ++x) { sc[j][x] = 0.f; c2[j][x] = 0.f; c3[j][x] = 0.f; }
+        for (int x = 0; x < W; ++x) sc[j][x] = 0.f;
       const int wo = slot * WIN + cz * PS + cy0 * EXP;
       const float *tp = xt + slot * B;
 #pragma unroll 1
       for (int vz = 0; vz < BW; ++vz) {
-        float t[BW][BW], t2[BW][BW];
+        float t[BW][BW];
 #pragma unroll
         for (int vy = 0; vy < BW; ++vy)
 #pragma unroll
-          for (int vx = 0; vx < BW; ++vx) {
-            t[vy][vx] = tp[(vz * BW + vy) * BW + vx];
-            t2[vy][vx] = t[vy][vx] * t[vy][vx];
-          }
+          for (int vx = 0; vx < BW; ++vx) t[vy][vx] = tp[(vz * BW + vy) * BW + vx];
 #pragma unroll
         for (int j = 0; j < TY + BW - 1; ++j) {
-          float r[EXP], m[EXP];
+          float r[EXP];
           const float4 *rp = reinterpret_cast<const float4 *>(win + wo + vz * PS + j * EXP);
-          const float4 *mp = reinterpret_cast<const float4 *>(mwin + wo + vz * PS + j * EXP);
 #pragma unroll
           for (int k = 0; k < EXP / 4; ++k) {
-            const float4 q = rp[k], u = mp[k];
+            const float4 q = rp[k];
             r[4 * k] = q.x; r[4 * k + 1] = q.y; r[4 * k + 2] = q.z; r[4 * k + 3] = q.w;
-            m[4 * k] = u.x; m[4 * k + 1] = u.y; m[4 * k + 2] = u.z; m[4 * k + 3] = u.w;
           }
 #pragma unroll
           for (int vy = 0; vy < BW; ++vy) {
@@ -434,45 +470,92 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
             if (jj < 0 || jj >= TY) continue;
 #pragma unroll
             for (int x = 0; x < W; ++x) {
-              float a1 = sc[jj][x], a2 = c2[jj][x], a3 = c3[jj][x];
+              float acc = sc[jj][x];
 #pragma unroll
-              for (int vx = 0; vx < BW; ++vx) {
-                a1 = fmaf(t[vy][vx], r[x + vx], a1);
-                a2 = fmaf(t[vy][vx], m[x + vx], a2);
-                a3 = fmaf(t2[vy][vx], m[x + vx], a3);
-              }
-              sc[jj][x] = a1;
-              c2[jj][x] = a2;
-              c3[jj][x] = a3;
+              for (int vx = 0; vx < BW; ++vx) acc = fmaf(t[vy][vx], r[x + vx], acc);
+              sc[jj][x] = acc;
             }
           }
         }
       }
-      // scores
-      const float cc = s_c[slot];
+    }
+    __syncthreads();  // the windows are free: scores and the straddler list go there
+    if (active) {
+      const float sxt = s_sxt[slot], sxx_b = s_sxx[slot], cc = s_c[slot];
       const int pz = s_o[slot][2] + cz;
 #pragma unroll
       for (int j = 0; j < TY; ++j) {
         const int cy = cy0 + j;
+        if (cy >= W) continue;
         const int py = s_o[slot][1] + cy;
-        const bool rowok = cy < W && py >= 0 && py <= ny - BW && pz >= 0 && pz <= nz - BW;
+        const bool rowok = py >= 0 && py <= ny - BW && pz >= 0 && pz <= nz - BW;
 #pragma unroll
         for (int x = 0; x < W; ++x) {
           const int px = s_o[slot][0] + x;
+          const int ci = slot * NC + (cz * W + cy) * W + x;
           float s = -4.f;  // not a candidate
           if (rowok && px >= 0 && px <= nx - BW) {
-            const long long p = ((long long)pz * ny + py) * nx + px;
-            const float2 st = __ldg(&a.stats[p]);
+            const float2 st = __ldg(&a.stats[((long long)pz * ny + py) * nx + px]);
             const float syy = syy_of(st.y);
-            const float sxy = sc[j][x] - (st.x - cc) * c2[j][x];
-            const float sxx = c3[j][x];
-            s = (sxx <= 0.f || syy <= 0.f) ? -2.f : (sxy * sxy) / sxx / syy;
-            if (s == -2.f) push_deg(d1, d2, (int)p);
+            if (syy <= 0.f) {
+              s = -2.f;
+            } else if (footprint_in_mask(st.y)) {
+              const float sxy = sc[j][x] - (st.x - cc) * sxt;
+              s = sxx_b <= 0.f ? -2.f : (sxy * sxy) / sxx_b / syy;
+            } else {
+              // footprint across the mask edge: finished below from C1
+              s = sc[j][x];
+              slist[atomicAdd(&s_nstr, 1)] = ci;
+            }
+          }
+          scs[ci] = s;
+        }
+      }
+    }
+    __syncthreads();
+    // straddling candidates: C2 and C3 from the row bits and the tables
+    const int nstr = s_nstr;
+    for (int i = tid; i < nstr; i += blockDim.x) {
+      const int ci = slist[i];
+      const int s = ci / NC;
+      const int cl = ci - s * NC;
+      const int x = cl % W, cy = (cl / W) % W, czz = cl / (W * W);
+      const unsigned int *rb = bits + s * NROW;
+      const float2 *tb = tab + s * NTAB;
+      float c2 = 0.f, c3 = 0.f;
+#pragma unroll
+      for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+        for (int vy = 0; vy < BW; ++vy) {
+          const unsigned int pat = (rb[(czz + vz) * EY + cy + vy] >> x) & (NPAT - 1);
+          const float2 q = tb[(vz * BW + vy) * NPAT + pat];
+          c2 += q.x;
+          c3 += q.y;
+        }
+      const int px = s_o[s][0] + x, py = s_o[s][1] + cy, pz = s_o[s][2] + czz;
+      const float2 st = __ldg(&a.stats[((long long)pz * ny + py) * nx + px]);
+      const float syy = syy_of(st.y);
+      const float sxy = scs[ci] - (st.x - s_c[s]) * c2;
+      scs[ci] = c3 <= 0.f ? -2.f : (sxy * sxy) / c3 / syy;
+    }
+    __syncthreads();
+    float l1 = -3.f, l2 = -3.f;
+    int d1 = -1, d2 = -1;
+    if (active) {
+      const int pz = s_o[slot][2] + cz;
+#pragma unroll
+      for (int j = 0; j < TY; ++j)
+#pragma unroll
+        for (int x = 0; x < W; ++x) {
+          const int cy = cy0 + j;
+          const float s = cy < W ? scs[slot * NC + (cz * W + cy) * W + x] : -4.f;
+          if (s > -4.f) {
+            if (s == -2.f)
+              push_deg(d1, d2, (int)(((long long)pz * ny + s_o[slot][1] + cy) * nx + s_o[slot][0] + x));
             top2_merge(l1, l2, s, -3.f);
           }
           sc[j][x] = s;
         }
-      }
     }
     if (worker) {
       s_red[slot][lt][0] = l1;
@@ -1483,7 +1566,7 @@ mirorr_status set_smem(K kernel, size_t smem) {
 
 template <class C>
 mirorr_status launch_masked(const NccArgs &a, cudaStream_t s) {
-  size_t smem = sizeof(float) * (size_t)C::BPC * (2 * C::WIN + C::B);
+  size_t smem = sizeof(float) * (size_t)C::SMEM_FLOATS;
   MB2_TRY(set_smem(ncc_masked_kernel<C>, smem));
   long long need = (a.nblocks + C::BPC - 1) / C::BPC;
   long long grid = need < 148LL * 8 ? need : 148LL * 8;
