@@ -319,7 +319,7 @@ struct FastCfg {
 };
 
 template <class C>
-__global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
+__global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
   constexpr int BW = C::BW, W = C::W, TY = C::TY, BPC = C::BPC, B = C::B, R = C::R, E = C::E;
   constexpr int EY = C::EY, EXP = C::EXP, PS = C::PS, WIN = C::WIN, TPB = C::TPB, NYG = C::NYG;
   constexpr int NC = C::NC, NROW = C::NROW, NPAT = C::NPAT, NTAB = C::NTAB;
@@ -328,7 +328,8 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
   float *xt = sm + C::OFF_XT;                                     // BPC * B: x - mu
   unsigned int *bits = reinterpret_cast<unsigned int *>(sm + C::OFF_BITS);  // BPC * NROW
   float2 *tab = reinterpret_cast<float2 *>(sm + C::OFF_TAB);      // BPC * NTAB
-  // after the correlation pass the windows hold the scores and the list
+  // after the correlation pass the windows hold the scores and, per block,
+  // the list of candidates whose footprint straddles the mask edge
   float *scs = sm;                                                // BPC * NC
   int *slist = reinterpret_cast<int *>(sm + BPC * NC);           // BPC * NC
   __shared__ float s_red[BPC][TPB][2];
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
   __shared__ float s_sxt[BPC];
   __shared__ float s_sxx[BPC];
   __shared__ double s_mean[BPC];
-  __shared__ int s_nstr;
+  __shared__ int s_nstr[BPC];
   const int tid = threadIdx.x;
   const int slot = tid / TPB;
   const int lt = tid - slot * TPB;
@@ -383,7 +384,7 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
       }
       s_state[tid] = state;
     }
-    if (tid == 0) s_nstr = 0;
+    if (tid < BPC) s_nstr[tid] = 0;
     __syncthreads();
     // stage the windows, 16 lanes per window row (consecutive x): (y - c) ms,
     // zero outside the image and in the padding, and the row's mask bits
@@ -479,7 +480,9 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
         }
       }
     }
-    __syncthreads();  // the windows are free: scores and the straddler list go there
+    __syncthreads();  // the windows are free: scores and the straddler lists go there
+    float l1 = -3.f, l2 = -3.f;
+    int d1 = -1, d2 = -1;
     if (active) {
       const float sxt = s_sxt[slot], sxx_b = s_sxx[slot], cc = s_c[slot];
       const int pz = s_o[slot][2] + cz;
@@ -489,73 +492,63 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
         if (cy >= W) continue;
         const int py = s_o[slot][1] + cy;
         const bool rowok = py >= 0 && py <= ny - BW && pz >= 0 && pz <= nz - BW;
+        const long long prow = ((long long)pz * ny + py) * nx + s_o[slot][0];
 #pragma unroll
         for (int x = 0; x < W; ++x) {
           const int px = s_o[slot][0] + x;
-          const int ci = slot * NC + (cz * W + cy) * W + x;
+          const int cl = (cz * W + cy) * W + x;
           float s = -4.f;  // not a candidate
           if (rowok && px >= 0 && px <= nx - BW) {
-            const float2 st = __ldg(&a.stats[((long long)pz * ny + py) * nx + px]);
+            const float2 st = __ldg(&a.stats[prow + x]);
             const float syy = syy_of(st.y);
             if (syy <= 0.f) {
               s = -2.f;
             } else if (footprint_in_mask(st.y)) {
               const float sxy = sc[j][x] - (st.x - cc) * sxt;
-              s = sxx_b <= 0.f ? -2.f : (sxy * sxy) / sxx_b / syy;
+              s = sxx_b <= 0.f ? -2.f : __fdividef(__fdividef(sxy * sxy, sxx_b), syy);
             } else {
-              // footprint across the mask edge: finished below from C1
-              s = sc[j][x];
-              slist[atomicAdd(&s_nstr, 1)] = ci;
+              // footprint across the mask edge: C1 kept, finished below
+              slist[slot * NC + atomicAdd(&s_nstr[slot], 1)] = cl;
+              scs[slot * NC + cl] = sc[j][x];
+              continue;
             }
+            if (s == -2.f) push_deg(d1, d2, (int)(prow + x));
+            top2_merge(l1, l2, s, -3.f);
           }
-          scs[ci] = s;
+          scs[slot * NC + cl] = s;
         }
       }
     }
     __syncthreads();
-    // straddling candidates: C2 and C3 from the row bits and the tables
-    const int nstr = s_nstr;
-    for (int i = tid; i < nstr; i += blockDim.x) {
-      const int ci = slist[i];
-      const int s = ci / NC;
-      const int cl = ci - s * NC;
-      const int x = cl % W, cy = (cl / W) % W, czz = cl / (W * W);
-      const unsigned int *rb = bits + s * NROW;
-      const float2 *tb = tab + s * NTAB;
-      float c2 = 0.f, c3 = 0.f;
-#pragma unroll
-      for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-        for (int vy = 0; vy < BW; ++vy) {
-          const unsigned int pat = (rb[(czz + vz) * EY + cy + vy] >> x) & (NPAT - 1);
-          const float2 q = tb[(vz * BW + vy) * NPAT + pat];
-          c2 += q.x;
-          c3 += q.y;
-        }
-      const int px = s_o[s][0] + x, py = s_o[s][1] + cy, pz = s_o[s][2] + czz;
-      const float2 st = __ldg(&a.stats[((long long)pz * ny + py) * nx + px]);
-      const float syy = syy_of(st.y);
-      const float sxy = scs[ci] - (st.x - s_c[s]) * c2;
-      scs[ci] = c3 <= 0.f ? -2.f : (sxy * sxy) / c3 / syy;
-    }
-    __syncthreads();
-    float l1 = -3.f, l2 = -3.f;
-    int d1 = -1, d2 = -1;
     if (active) {
-      const int pz = s_o[slot][2] + cz;
+      // this block's straddling candidates: C2 and C3 from the row bits and
+      // the tables
+      const int nstr = s_nstr[slot];
+      const unsigned int *rb = bits + slot * NROW;
+      const float2 *tb = tab + slot * NTAB;
+      const float cc = s_c[slot];
+      for (int i = lt; i < nstr; i += TPB) {
+        const int cl = slist[slot * NC + i];
+        const int x = cl % W, cy = (cl / W) % W, czz = cl / (W * W);
+        float c2 = 0.f, c3 = 0.f;
 #pragma unroll
-      for (int j = 0; j < TY; ++j)
+        for (int vz = 0; vz < BW; ++vz)
 #pragma unroll
-        for (int x = 0; x < W; ++x) {
-          const int cy = cy0 + j;
-          const float s = cy < W ? scs[slot * NC + (cz * W + cy) * W + x] : -4.f;
-          if (s > -4.f) {
-            if (s == -2.f)
-              push_deg(d1, d2, (int)(((long long)pz * ny + s_o[slot][1] + cy) * nx + s_o[slot][0] + x));
-            top2_merge(l1, l2, s, -3.f);
+          for (int vy = 0; vy < BW; ++vy) {
+            const unsigned int pat = (rb[(czz + vz) * EY + cy + vy] >> x) & (NPAT - 1);
+            const float2 q = tb[(vz * BW + vy) * NPAT + pat];
+            c2 += q.x;
+            c3 += q.y;
           }
-          sc[j][x] = s;
-        }
+        const long long p = ((long long)(s_o[slot][2] + czz) * ny + s_o[slot][1] + cy) * nx +
+                            s_o[slot][0] + x;
+        const float2 st = __ldg(&a.stats[p]);
+        const float sxy = scs[slot * NC + cl] - (st.x - cc) * c2;
+        const float s = c3 <= 0.f ? -2.f : __fdividef(__fdividef(sxy * sxy, c3), syy_of(st.y));
+        scs[slot * NC + cl] = s;
+        if (s == -2.f) min2_merge(d1, d2, (int)p, -1);  // list order: keep the two smallest
+        top2_merge(l1, l2, s, -3.f);
+      }
     }
     if (worker) {
       s_red[slot][lt][0] = l1;
@@ -564,33 +557,51 @@ __global__ void __launch_bounds__(C::NT) ncc_masked_kernel(NccArgs a) {
       s_deg[slot][lt][1] = d2;
     }
     __syncthreads();
-    if (active && lt == 0) {
-      float f1 = -3.f, f2 = -3.f;
-      int e1 = -1, e2 = -1;
-      for (int k = 0; k < TPB; ++k) {
-        top2_merge(f1, f2, s_red[slot][k][0], s_red[slot][k][1]);
-        min2_merge(e1, e2, s_deg[slot][k][0], s_deg[slot][k][1]);
+    {
+      // block-level top-2 and first degenerate candidates: one warp per block
+      const int wp = tid >> 5, ln = tid & 31;
+      if (wp < BPC && s_state[wp]) {
+        float f1 = -3.f, f2 = -3.f;
+        int e1 = -1, e2 = -1;
+        for (int k = ln; k < TPB; k += 32) {
+          top2_merge(f1, f2, s_red[wp][k][0], s_red[wp][k][1]);
+          min2_merge(e1, e2, s_deg[wp][k][0], s_deg[wp][k][1]);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const float o1 = __shfl_down_sync(0xffffffffu, f1, off);
+          const float o2 = __shfl_down_sync(0xffffffffu, f2, off);
+          const int g1 = __shfl_down_sync(0xffffffffu, e1, off);
+          const int g2 = __shfl_down_sync(0xffffffffu, e2, off);
+          top2_merge(f1, f2, o1, o2);
+          min2_merge(e1, e2, g1, g2);
+        }
+        if (ln == 0) {
+          s_f[wp][0] = f1;
+          s_f[wp][1] = f2;
+          s_d[wp][0] = e1;
+          s_d[wp][1] = e2;
+        }
       }
-      s_f[slot][0] = f1;
-      s_f[slot][1] = f2;
-      s_d[slot][0] = e1;
-      s_d[slot][1] = e2;
     }
     __syncthreads();
     if (active) {
       const float T = s_f[slot][1] - 2.f * kDelta;
       const int pz = s_o[slot][2] + cz;
 #pragma unroll
-      for (int j = 0; j < TY; ++j)
+      for (int j = 0; j < TY; ++j) {
+        const int cy = cy0 + j;
+        if (cy >= W) continue;
 #pragma unroll
         for (int x = 0; x < W; ++x) {
-          float s = sc[j][x];
+          const float s = scs[slot * NC + (cz * W + cy) * W + x];
           if (s > -2.f && s >= T) {
             int pos = atomicAdd(&s_cnt[slot], 1);
             if (pos < kK)
-              s_list[slot][pos] = (int)(((long long)pz * ny + s_o[slot][1] + cy0 + j) * nx + s_o[slot][0] + x);
+              s_list[slot][pos] = (int)(((long long)pz * ny + s_o[slot][1] + cy) * nx + s_o[slot][0] + x);
           }
         }
+      }
     }
     __syncthreads();
     if (active && lt == 0) {
