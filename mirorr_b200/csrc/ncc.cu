@@ -315,7 +315,7 @@ struct FastCfg {
   static constexpr int SMEM_FLOATS = OFF_TAB + 2 * BPC * NTAB;
   static_assert(WIN % 4 == 0 && EXP % 4 == 0 && PS % 4 == 0 && B > 0, "alignment");
   static_assert(2 * NC <= WIN, "scores and straddler list reuse the window");
-  static_assert(E <= 16 && NT % 32 == 0, "a window row fits 16 lanes");
+  static_assert(E <= 16 && EY <= NT / 16 && NT % 32 == 0, "a window plane fits the CTA");
 };
 
 template <class C>
@@ -386,30 +386,33 @@ __global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
     }
     if (tid < BPC) s_nstr[tid] = 0;
     __syncthreads();
-    // stage the windows, 16 lanes per window row (consecutive x): (y - c) ms,
-    // zero outside the image and in the padding, and the row's mask bits
-    // (warp ballot); the base blocks as x - mu
+    // stage the windows one plane per pass, a 16-lane group per window row
+    // (consecutive x): (y - c) ms, zero outside the image and in the padding,
+    // and the row's mask bits (warp ballot); the base blocks as x - mu
     {
-      constexpr int LPR = 16, RPI = C::NT / LPR;  // rows per pass
-      constexpr int NPASS = (BPC * NROW + RPI - 1) / RPI;
-      const int xl = tid & (LPR - 1);
+      constexpr int LPR = 16;
+      const int xl = tid & (LPR - 1), yl = tid / LPR;
+      const long long plane = (long long)nx * ny;
+      for (int s = 0; s < BPC; ++s) {
+        if (!s_state[s]) continue;
+        const int gx = s_o[s][0] + xl, gy = s_o[s][1] + yl, gz0 = s_o[s][2];
+        const bool xyin = xl < E && yl < E && gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+        const float c = s_c[s];
+        const long long q0 = ((long long)gz0 * ny + gy) * nx + gx;
+        float *wd = win + s * WIN + yl * EXP + xl;
+        unsigned int *bd = bits + s * NROW + yl;
 #pragma unroll 2
-      for (int it = 0; it < NPASS; ++it) {
-        const int i = it * RPI + tid / LPR;
-        const int s = i < BPC * NROW ? i / NROW : 0;
-        const bool rowact = i < BPC * NROW && s_state[s];
-        const int rr = i - s * NROW;
-        const int z = rr / EY, y = rr - z * EY;
-        const int gx = s_o[s][0] + xl, gy = s_o[s][1] + y, gz = s_o[s][2] + z;
-        const bool in = rowact && xl < E && y < E && gx >= 0 && gy >= 0 && gz >= 0 && gx < nx &&
-                        gy < ny && gz < nz;
-        const long long q = ((long long)gz * ny + gy) * nx + gx;
-        const float yv = in ? __ldg(&a.search[q]) : 0.f;
-        const bool ms = in && __ldg(&a.smask[q]) != 0;
-        const unsigned int bal = __ballot_sync(0xffffffffu, ms);
-        if (rowact) {
-          if (xl < EXP) win[s * WIN + z * PS + y * EXP + xl] = ms ? yv - s_c[s] : 0.f;
-          if (xl == 0) bits[i] = (bal >> (tid & LPR)) & 0xFFFFu;
+        for (int z = 0; z < E; ++z) {
+          const int gz = gz0 + z;
+          const bool in = xyin && gz >= 0 && gz < nz;
+          const long long q = q0 + z * plane;
+          const float yv = in ? __ldg(&a.search[q]) : 0.f;
+          const bool ms = in && __ldg(&a.smask[q]) != 0;
+          const unsigned int bal = __ballot_sync(0xffffffffu, ms);
+          if (yl < EY) {
+            if (xl < EXP) wd[z * PS] = ms ? yv - c : 0.f;
+            if (xl == 0) bd[z * EY] = (bal >> (tid & LPR)) & 0xFFFFu;
+          }
         }
       }
     }
