@@ -318,6 +318,102 @@ struct FastCfg {
   static_assert(E <= 16 && EY <= NT / 16 && NT % 32 == 0, "a window plane fits the CTA");
 };
 
+// Shared state of the per-block reduction that ends a CTA tile.
+template <int BPC, int TPB>
+struct TileTail {
+  float red[BPC][TPB][2];
+  int deg[BPC][TPB][2];
+  float f[BPC][2];
+  int d[BPC][2];
+  int cnt[BPC];
+  int list[BPC][kK];
+};
+
+// End of a CTA tile of BPC blocks: per block, the FP32 best and second and
+// the first two degenerate candidates over the threads' partials (one warp
+// per block), then the candidates within 2 delta of the second-best from the
+// stored scores (scs: W^3 per block, -4 where not a candidate), then the
+// block's record.  count_fast adds the block to the register-blocked count.
+template <class C>
+__device__ void finish_tile(const NccArgs &a, TileTail<C::BPC, C::TPB> &tt, const float *scs,
+                            const int *s_b, const int (*s_o)[3], const int *s_state, float l1,
+                            float l2, int d1, int d2, bool count_fast) {
+  constexpr int BPC = C::BPC, TPB = C::TPB, TY = C::TY, W = C::W, NC = C::NC, NYG = C::NYG;
+  const int tid = threadIdx.x, slot = tid / TPB, lt = tid - slot * TPB;
+  const bool worker = slot < BPC;
+  const bool active = worker && s_state[slot];
+  const int cz = lt / NYG, cy0 = (lt - cz * NYG) * TY;
+  const int nx = a.nx, ny = a.ny;
+  if (worker) {
+    tt.red[slot][lt][0] = l1;
+    tt.red[slot][lt][1] = l2;
+    tt.deg[slot][lt][0] = d1;
+    tt.deg[slot][lt][1] = d2;
+  }
+  __syncthreads();
+  {
+    const int wp = tid >> 5, ln = tid & 31;
+    if (wp < BPC && s_state[wp]) {
+      float f1 = -3.f, f2 = -3.f;
+      int e1 = -1, e2 = -1;
+      for (int k = ln; k < TPB; k += 32) {
+        top2_merge(f1, f2, tt.red[wp][k][0], tt.red[wp][k][1]);
+        min2_merge(e1, e2, tt.deg[wp][k][0], tt.deg[wp][k][1]);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const float o1 = __shfl_down_sync(0xffffffffu, f1, off);
+        const float o2 = __shfl_down_sync(0xffffffffu, f2, off);
+        const int g1 = __shfl_down_sync(0xffffffffu, e1, off);
+        const int g2 = __shfl_down_sync(0xffffffffu, e2, off);
+        top2_merge(f1, f2, o1, o2);
+        min2_merge(e1, e2, g1, g2);
+      }
+      if (ln == 0) {
+        tt.f[wp][0] = f1;
+        tt.f[wp][1] = f2;
+        tt.d[wp][0] = e1;
+        tt.d[wp][1] = e2;
+      }
+    }
+  }
+  __syncthreads();
+  if (active) {
+    const float T = tt.f[slot][1] - 2.f * kDelta;
+    const int pz = s_o[slot][2] + cz;
+#pragma unroll
+    for (int j = 0; j < TY; ++j) {
+      const int cy = cy0 + j;
+      if (cy >= W) continue;
+#pragma unroll
+      for (int x = 0; x < W; ++x) {
+        const float s = scs[slot * NC + (cz * W + cy) * W + x];
+        if (s > -2.f && s >= T) {
+          int pos = atomicAdd(&tt.cnt[slot], 1);
+          if (pos < kK)
+            tt.list[slot][pos] = (int)(((long long)pz * ny + s_o[slot][1] + cy) * nx + s_o[slot][0] + x);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (active && lt == 0) {
+    NccRec &rc = a.rec[s_b[slot]];
+    int cnt = tt.cnt[slot];
+    rc.f1 = tt.f[slot][0];
+    rc.f2 = tt.f[slot][1];
+    if (cnt <= kK) {
+      for (int k = 0; k < cnt; ++k) rc.p[k] = tt.list[slot][k];
+      if (tt.f[slot][1] <= -2.f) {
+        if (tt.d[slot][0] >= 0) rc.p[cnt++] = tt.d[slot][0];
+        if (tt.d[slot][1] >= 0) rc.p[cnt++] = tt.d[slot][1];
+      }
+    }
+    rc.cnt = cnt;
+    if (count_fast) atomicAdd(&a.ctl[3], 1u);
+  }
+}
+
 template <class C>
 __global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
   constexpr int BW = C::BW, W = C::W, TY = C::TY, BPC = C::BPC, B = C::B, R = C::R, E = C::E;
@@ -332,12 +428,7 @@ __global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
   // the list of candidates whose footprint straddles the mask edge
   float *scs = sm;                                                // BPC * NC
   int *slist = reinterpret_cast<int *>(sm + BPC * NC);           // BPC * NC
-  __shared__ float s_red[BPC][TPB][2];
-  __shared__ int s_deg[BPC][TPB][2];
-  __shared__ float s_f[BPC][2];
-  __shared__ int s_d[BPC][2];
-  __shared__ int s_cnt[BPC];
-  __shared__ int s_list[BPC][kK];
+  __shared__ TileTail<BPC, TPB> tt;
   __shared__ int s_state[BPC];           // 1 compute, 0 skip
   __shared__ int s_b[BPC];
   __shared__ int s_o[BPC][3];            // window origin (block origin - R)
@@ -360,7 +451,7 @@ __global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
     if (tid < BPC) {
       long long i = base + tid;
       int state = 0;
-      s_cnt[tid] = 0;
+      tt.cnt[tid] = 0;
       if (i < nlist) {
         const int b = a.gen_list[a.nblocks + 1 + i];
         s_b[tid] = b;
@@ -553,75 +644,193 @@ __global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
         top2_merge(l1, l2, s, -3.f);
       }
     }
-    if (worker) {
-      s_red[slot][lt][0] = l1;
-      s_red[slot][lt][1] = l2;
-      s_deg[slot][lt][0] = d1;
-      s_deg[slot][lt][1] = d2;
+    finish_tile<C>(a, tt, scs, s_b, s_o, s_state, l1, l2, d1, d2, true);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Register-blocked FP32 search for blocks whose base block is partly masked
+// (block gap 1); the unmasked search kernels route them here through
+// gen_list[0 .. ctl[0]).  With m = mb ms (base and search mask), mu the
+// unmasked mean of the candidate footprint and x~ = x - mean of the base
+// block:
+//   Sxy = sum m x~ (y - mu),  Sxx = sum m x~^2,  Syy = sum m (y - mu)^2,
+// each summed directly (no expansion around a constant, so no cancellation).
+// The window is staged as y ms and ms, the base block as (mb x~, mb x~^2, mb);
+// per candidate voxel, md = ms (y - mu) is one FMA and the three sums take
+// one FMA each plus a multiply for mb md.  Tile layout as the masked kernel.
+// ---------------------------------------------------------------------------
+template <class C>
+__global__ void __launch_bounds__(C::NT, 2) ncc_basemask_kernel(NccArgs a) {
+  constexpr int BW = C::BW, W = C::W, TY = C::TY, BPC = C::BPC, B = C::B, R = C::R, E = C::E;
+  constexpr int EY = C::EY, EXP = C::EXP, PS = C::PS, WIN = C::WIN, TPB = C::TPB, NYG = C::NYG;
+  constexpr int NC = C::NC;
+  extern __shared__ __align__(16) float sm[];
+  float *win = sm;                                               // BPC * WIN: y ms
+  float *mwin = sm + BPC * WIN;                                  // BPC * WIN: ms
+  float4 *xb = reinterpret_cast<float4 *>(sm + 2 * BPC * WIN);  // BPC * B: mb x~, mb x~^2, mb
+  float *scs = sm;  // after the correlation pass: BPC * NC scores
+  __shared__ TileTail<BPC, TPB> tt;
+  __shared__ int s_state[BPC];
+  __shared__ int s_b[BPC];
+  __shared__ int s_o[BPC][3];
+  __shared__ double s_mean[BPC];
+  const int tid = threadIdx.x;
+  const int slot = tid / TPB;
+  const int lt = tid - slot * TPB;
+  const bool worker = slot < BPC;
+  const int cz = lt / NYG;
+  const int cy0 = (lt - cz * NYG) * TY;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long long nlist = (long long)*(volatile unsigned int *)&a.ctl[0];
+
+  for (long long base = (long long)blockIdx.x * BPC; base < nlist; base += (long long)gridDim.x * BPC) {
+    __syncthreads();
+    if (tid < BPC) {
+      long long i = base + tid;
+      int state = 0;
+      tt.cnt[tid] = 0;
+      if (i < nlist) {
+        const int b = a.gen_list[i];
+        s_b[tid] = b;
+        const int bx = b % a.nbx, by = (b / a.nbx) % a.nby, bz = b / (a.nbx * a.nby);
+        s_o[tid][0] = a.stx + bx * a.G - R;
+        s_o[tid][1] = a.sty + by * a.G - R;
+        s_o[tid][2] = a.stz + bz * a.G - R;
+        const BlockStat st = a.bstat[b];
+        if (st.mmode == 2) {
+          finish_unmasked_block(a, b);
+        } else {
+          state = 1;
+          s_mean[tid] = st.mean;
+        }
+      }
+      s_state[tid] = state;
     }
     __syncthreads();
+    // stage the windows one plane per pass, a 16-lane group per window row:
+    // y ms and ms, zero outside the image and in the padding
     {
-      // block-level top-2 and first degenerate candidates: one warp per block
-      const int wp = tid >> 5, ln = tid & 31;
-      if (wp < BPC && s_state[wp]) {
-        float f1 = -3.f, f2 = -3.f;
-        int e1 = -1, e2 = -1;
-        for (int k = ln; k < TPB; k += 32) {
-          top2_merge(f1, f2, s_red[wp][k][0], s_red[wp][k][1]);
-          min2_merge(e1, e2, s_deg[wp][k][0], s_deg[wp][k][1]);
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          const float o1 = __shfl_down_sync(0xffffffffu, f1, off);
-          const float o2 = __shfl_down_sync(0xffffffffu, f2, off);
-          const int g1 = __shfl_down_sync(0xffffffffu, e1, off);
-          const int g2 = __shfl_down_sync(0xffffffffu, e2, off);
-          top2_merge(f1, f2, o1, o2);
-          min2_merge(e1, e2, g1, g2);
-        }
-        if (ln == 0) {
-          s_f[wp][0] = f1;
-          s_f[wp][1] = f2;
-          s_d[wp][0] = e1;
-          s_d[wp][1] = e2;
+      constexpr int LPR = 16;
+      const int xl = tid & (LPR - 1), yl = tid / LPR;
+      const long long plane = (long long)nx * ny;
+      for (int s = 0; s < BPC; ++s) {
+        if (!s_state[s]) continue;
+        const int gx = s_o[s][0] + xl, gy = s_o[s][1] + yl, gz0 = s_o[s][2];
+        const bool xyin = xl < E && yl < E && gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+        const long long q0 = ((long long)gz0 * ny + gy) * nx + gx;
+        float *wd = win + s * WIN + yl * EXP + xl;
+        float *md = mwin + s * WIN + yl * EXP + xl;
+        if (yl < EY && xl < EXP) {
+#pragma unroll 2
+          for (int z = 0; z < E; ++z) {
+            const int gz = gz0 + z;
+            const bool in = xyin && gz >= 0 && gz < nz;
+            const long long q = q0 + z * plane;
+            const float yv = in ? __ldg(&a.search[q]) : 0.f;
+            const bool ms = in && __ldg(&a.smask[q]) != 0;
+            wd[z * PS] = ms ? yv : 0.f;
+            md[z * PS] = ms ? 1.f : 0.f;
+          }
         }
       }
     }
+    for (int i = tid; i < BPC * B; i += blockDim.x) {
+      const int s = i / B;
+      if (!s_state[s]) continue;
+      const int v = i - s * B;
+      const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
+      const long long q = ((long long)(s_o[s][2] + R + vz) * ny + (s_o[s][1] + R + vy)) * nx +
+                          (s_o[s][0] + R + vx);
+      const float xv = (float)__dsub_rn((double)__ldg(&a.base[q]), s_mean[s]);
+      const float mb = __ldg(&a.bmask[q]) ? 1.f : 0.f;
+      xb[i] = make_float4(mb * xv, mb * (xv * xv), mb, 0.f);
+    }
     __syncthreads();
+    const bool active = worker && s_state[slot];
+    float s1[TY][W], s2[TY][W], s3[TY][W], nmu[TY][W];
     if (active) {
-      const float T = s_f[slot][1] - 2.f * kDelta;
+      const int pz = s_o[slot][2] + cz;
+#pragma unroll
+      for (int j = 0; j < TY; ++j)
+#pragma unroll
+        for (int x = 0; x < W; ++x) {
+          const int py = s_o[slot][1] + cy0 + j, px = s_o[slot][0] + x;
+          const bool ok = cy0 + j < W && px >= 0 && px <= nx - BW && py >= 0 && py <= ny - BW &&
+                          pz >= 0 && pz <= nz - BW;
+          nmu[j][x] = ok ? -__ldg(&a.stats[((long long)pz * ny + py) * nx + px]).x : 0.f;
+          s1[j][x] = 0.f;
+          s2[j][x] = 0.f;
+          s3[j][x] = 0.f;
+        }
+      const int wo = slot * WIN + cz * PS + cy0 * EXP;
+      const float4 *tp = xb + slot * B;
+#pragma unroll 1
+      for (int vz = 0; vz < BW; ++vz) {
+#pragma unroll
+        for (int j = 0; j < TY + BW - 1; ++j) {
+          float r[EXP], m[EXP];
+          const float4 *rp = reinterpret_cast<const float4 *>(win + wo + vz * PS + j * EXP);
+          const float4 *mp = reinterpret_cast<const float4 *>(mwin + wo + vz * PS + j * EXP);
+#pragma unroll
+          for (int k = 0; k < EXP / 4; ++k) {
+            const float4 q = rp[k], u = mp[k];
+            r[4 * k] = q.x; r[4 * k + 1] = q.y; r[4 * k + 2] = q.z; r[4 * k + 3] = q.w;
+            m[4 * k] = u.x; m[4 * k + 1] = u.y; m[4 * k + 2] = u.z; m[4 * k + 3] = u.w;
+          }
+#pragma unroll
+          for (int vy = 0; vy < BW; ++vy) {
+            const int jj = j - vy;
+            if (jj < 0 || jj >= TY) continue;
+            // the base row (vy, vz), read where it is used (fewer live registers)
+            float4 t[BW];
+#pragma unroll
+            for (int vx = 0; vx < BW; ++vx) t[vx] = tp[(vz * BW + vy) * BW + vx];
+#pragma unroll
+            for (int x = 0; x < W; ++x) {
+              float a1 = s1[jj][x], a2 = s2[jj][x], a3 = s3[jj][x];
+#pragma unroll
+              for (int vx = 0; vx < BW; ++vx) {
+                const float md = fmaf(nmu[jj][x], m[x + vx], r[x + vx]);  // ms (y - mu)
+                a1 = fmaf(t[vx].x, md, a1);
+                a2 = fmaf(t[vx].y, m[x + vx], a2);
+                a3 = fmaf(t[vx].z * md, md, a3);
+              }
+              s1[jj][x] = a1;
+              s2[jj][x] = a2;
+              s3[jj][x] = a3;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // the windows are free: the scores go there
+    float l1 = -3.f, l2 = -3.f;
+    int d1 = -1, d2 = -1;
+    if (active) {
       const int pz = s_o[slot][2] + cz;
 #pragma unroll
       for (int j = 0; j < TY; ++j) {
         const int cy = cy0 + j;
         if (cy >= W) continue;
+        const int py = s_o[slot][1] + cy;
+        const bool rowok = py >= 0 && py <= ny - BW && pz >= 0 && pz <= nz - BW;
+        const long long prow = ((long long)pz * ny + py) * nx + s_o[slot][0];
 #pragma unroll
         for (int x = 0; x < W; ++x) {
-          const float s = scs[slot * NC + (cz * W + cy) * W + x];
-          if (s > -2.f && s >= T) {
-            int pos = atomicAdd(&s_cnt[slot], 1);
-            if (pos < kK)
-              s_list[slot][pos] = (int)(((long long)pz * ny + s_o[slot][1] + cy) * nx + s_o[slot][0] + x);
+          const int px = s_o[slot][0] + x;
+          float s = -4.f;  // not a candidate
+          if (rowok && px >= 0 && px <= nx - BW) {
+            const float sxy = s1[j][x], sxx = s2[j][x], syy = s3[j][x];
+            s = (sxx <= 0.f || syy <= 0.f) ? -2.f : __fdividef(__fdividef(sxy * sxy, sxx), syy);
+            if (s == -2.f) push_deg(d1, d2, (int)(prow + x));
+            top2_merge(l1, l2, s, -3.f);
           }
+          scs[slot * NC + (cz * W + cy) * W + x] = s;
         }
       }
     }
-    __syncthreads();
-    if (active && lt == 0) {
-      NccRec &rc = a.rec[s_b[slot]];
-      int cnt = s_cnt[slot];
-      rc.f1 = s_f[slot][0];
-      rc.f2 = s_f[slot][1];
-      if (cnt <= kK) {
-        for (int k = 0; k < cnt; ++k) rc.p[k] = s_list[slot][k];
-        if (s_f[slot][1] <= -2.f) {
-          if (s_d[slot][0] >= 0) rc.p[cnt++] = s_d[slot][0];
-          if (s_d[slot][1] >= 0) rc.p[cnt++] = s_d[slot][1];
-        }
-      }
-      rc.cnt = cnt;
-      atomicAdd(&a.ctl[3], 1u);
-    }
+    finish_tile<C>(a, tt, scs, s_b, s_o, s_state, l1, l2, d1, d2, false);
   }
 }
 
@@ -1214,10 +1423,11 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
 }
 
 // ---------------------------------------------------------------------------
-// General FP32 search: one CTA (128 threads) per block, any mask pattern.
+// General FP32 search: one CTA (128 threads) per block, any mask pattern and
+// block gap, for geometries without the register-blocked kernels.
 // ---------------------------------------------------------------------------
 template <int BW>
-__global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_list) {
+__global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a) {
   constexpr int B = BW * BW * BW;
   extern __shared__ __align__(16) unsigned char smem[];
   const int e3 = a.emax * a.emax * a.emax;
@@ -1230,23 +1440,19 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a, int use_lis
   __shared__ float s_red[4][2];
   __shared__ int s_deg[4][2];
   const int tid = threadIdx.x;
-  const long long n = use_list ? (long long)*(volatile unsigned int *)&a.ctl[0] : a.nblocks;
 
-  for (long long i = blockIdx.x; i < n; i += gridDim.x) {
+  for (long long b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
     __syncthreads();
-    const long long b = use_list ? (long long)a.gen_list[i] : i;
     BlockWin w;
     bool ok = block_window(a, b, w);
     const long long obase = lin(a, w.ox, w.oy, w.oz);
-    if (!use_list) {
-      if (a.selected && !a.selected[b]) {
-        if (tid == 0) { write_final(a, b, -3.f, -3.f, obase, 0); a.rec[b].cnt = -1; }
-        continue;
-      }
-      if (!ok) {
-        if (tid == 0) { write_final(a, b, -3.f, -3.f, obase, 1); a.rec[b].cnt = -1; }
-        continue;
-      }
+    if (a.selected && !a.selected[b]) {
+      if (tid == 0) { write_final(a, b, -3.f, -3.f, obase, 0); a.rec[b].cnt = -1; }
+      continue;
+    }
+    if (!ok) {
+      if (tid == 0) { write_final(a, b, -3.f, -3.f, obase, 1); a.rec[b].cnt = -1; }
+      continue;
     }
     const BlockStat bst = a.bstat[b];
     if (bst.mmode == 2) {
@@ -1586,6 +1792,13 @@ mirorr_status launch_masked(const NccArgs &a, cudaStream_t s) {
   long long grid = need < 148LL * 8 ? need : 148LL * 8;
   ncc_masked_kernel<C><<<(unsigned)grid, C::NT, smem, s>>>(a);
   MB2_LAUNCH_CHECK();
+  // then the blocks with a partly masked base block (the list grows in both
+  // kernels above)
+  const size_t smem_b = sizeof(float) * (size_t)C::BPC * (2 * C::WIN + 4 * C::B);
+  MB2_TRY(set_smem(ncc_basemask_kernel<C>, smem_b));
+  const long long grid_b = need < 148LL * 4 ? need : 148LL * 4;
+  ncc_basemask_kernel<C><<<(unsigned)grid_b, C::NT, smem_b, s>>>(a);
+  MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
 
@@ -1620,9 +1833,12 @@ mirorr_status launch_rest(const NccArgs &a, bool all_general, cudaStream_t s) {
   }
   MB2_TRY(set_smem(ncc_general_kernel<BW>, smem_g));
   MB2_TRY(set_smem(ncc_fallback_kernel<BW>, smem_f));
-  long long grid = a.nblocks < 148LL * 16 ? a.nblocks : 148LL * 16;
-  ncc_general_kernel<BW><<<(unsigned)grid, 128, smem_g, s>>>(a, all_general ? 0 : 1);
-  MB2_LAUNCH_CHECK();
+  if (all_general) {
+    // no register-blocked kernels for this geometry: every block here
+    long long grid = a.nblocks < 148LL * 16 ? a.nblocks : 148LL * 16;
+    ncc_general_kernel<BW><<<(unsigned)grid, 128, smem_g, s>>>(a);
+    MB2_LAUNCH_CHECK();
+  }
   long long rgrid = (a.nblocks + 127) / 128;
   ncc_refine_kernel<BW><<<(unsigned)rgrid, 128, 0, s>>>(a);
   MB2_LAUNCH_CHECK();

@@ -1,13 +1,14 @@
 """One block-matching call (GetOffsets) on the benchmark's 256x256x128
 phantom pair, for kernel profiling.
 
-    python -m mirorr_b200.matcher_workload [--calls N] [--masked]
+    python -m mirorr_b200.matcher_workload [--calls N] [--masked] [--base-masked]
 
 Block width 4, search radius 4 (9^3 = 729 candidates), block spacing 3: the
 finest-level matcher call of the symmetric affine benchmark.  --masked gives
 the search image a field-of-view border (mask 0 on a 10-voxel shell), as a
 resampled image has.  Prints the per-stage CUDA-event timings and the
-fast/general path split.
+fast/general path split.  --base-masked gives the base image a 12-voxel
+shell (blocks across its edge take the general search kernel).
 """
 from __future__ import annotations
 
@@ -24,6 +25,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--calls", type=int, default=3)
     ap.add_argument("--masked", action="store_true")
+    ap.add_argument("--base-masked", action="store_true")
     ap.add_argument("--shape", default="256,256,128")
     args = ap.parse_args()
     shape = tuple(int(v) for v in args.shape.split(","))
@@ -40,6 +42,10 @@ def main():
         sm = np.zeros(ph.fixed.shape, np.uint8)
         sm[10:-10, 10:-10, 10:-10] = 255
         m.SetSearchMask(sm)
+    if args.base_masked:
+        bm = np.zeros(ph.moving.shape, np.uint8)
+        bm[12:-12, 12:-12, 12:-12] = 255
+        m.SetBaseMask(bm)
     out = []
     for _ in range(args.calls):
         bp, _ = m.GetOffsets()

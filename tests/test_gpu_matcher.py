@@ -35,6 +35,11 @@ CASES = [
     dict(id="bw4_w7_G2_nx39", shape=(39, 30, 22), bw=4, nw=7, g=1, G=2, keep=1.0, mask=None, seed=10),
     dict(id="bw5_w11_G3_masked", shape=(40, 36, 30), bw=5, nw=11, g=1, G=3, keep=1.0, mask="search",
          seed=11),
+    # partly masked base blocks with the other register-blocked geometries
+    dict(id="bw4_w7_G2_basemask", shape=(34, 30, 24), bw=4, nw=7, g=1, G=2, keep=1.0, mask="both",
+         seed=12),
+    dict(id="bw5_w11_G3_basemask", shape=(40, 36, 30), bw=5, nw=11, g=1, G=3, keep=1.0, mask="both",
+         seed=13),
 ]
 
 
