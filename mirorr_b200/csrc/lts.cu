@@ -6,11 +6,11 @@
 //   residuals r_i (FP64) under the current final transform(s);
 //   the threshold r_nth: the maximum on the first iteration, otherwise the
 //     exact value of rank min(floor(f N), N-1) by an MSD radix select on the
-//     residual bit patterns (grid-wide histograms, then the few keys left in
-//     the chosen bucket are sorted in shared memory);
-//   subset {r_i <= r_nth}: barycentres, then the 6x6 second moments of the
-//     centred (initial, moved) pairs, reduced per CTA and summed in a fixed
-//     order (deterministic);
+//     residual bit patterns (grid-wide histograms until at most one CTA's
+//     worth of keys share the prefix, then those keys ranked by counting);
+//   subset {r_i <= r_nth}: count, first and second moments of the
+//     (initial, moved) pairs about the first pair in one sweep, reduced per
+//     CTA and summed in a fixed order (deterministic), then centred;
 //   the FP64 solve (affine normal equations / Horn quaternion, symmetric
 //     half-space algebra) in one thread, and the loop test.
 // CTAs meet at a software grid barrier whose wait is bounded (about one
@@ -27,7 +27,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kBins = 4096;
-constexpr int kCandMax = 2048;
+constexpr int kCandMax = kThreads;  // keys left for the final rank (one per thread)
 constexpr int kPartial = 32;  // doubles per CTA partial
 
 struct LtsCtl {
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
   __shared__ __align__(16) LtsState s;
   __shared__ unsigned int h[kBins];
   __shared__ unsigned long long ck[kCandMax];
-  __shared__ double red_n[21 * 32];
+  __shared__ double red_n[28 * 32];
   __shared__ double s_nth;
   __shared__ unsigned long long s_key;
   __shared__ unsigned long long s_pair[2];
@@ -268,6 +268,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         mask |= ((1ULL << bits) - 1ULL) << shift;
         __syncthreads();
         if (bucket <= (unsigned long long)kCandMax || shift == 0) break;
+        // more than one CTA's worth of keys share the prefix: refine it
         // next pass
         ++pass;
         bits = shift >= 12 ? 12 : shift;
@@ -288,21 +289,24 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
           if (h[i]) atomicAdd(&gh2[i], h[i]);
         if (!grid_sync(a.ctl)) return;
       }
-      // ---- gather the bucket's keys and pick rank k -----------------------
-      for (long long i = gtid; i < n; i += gstride) {
-        unsigned long long key = (unsigned long long)__double_as_longlong(a.resid[i]);
-        if ((key & mask) == prefix) {
-          unsigned long long pos = atomicAdd(&a.ctl->ncand, 1ULL);
-          if (pos < (unsigned long long)kCandMax) a.cand[pos] = key;
+      if (shift == 0) {
+        // every bit fixed: the bucket's keys all equal the prefix
+        nth = __longlong_as_double((long long)prefix);
+      } else {
+        // ---- gather the bucket's keys (at most one per thread) and rank them
+        for (long long i = gtid; i < n; i += gstride) {
+          unsigned long long key = (unsigned long long)__double_as_longlong(a.resid[i]);
+          if ((key & mask) == prefix) {
+            unsigned long long pos = atomicAdd(&a.ctl->ncand, 1ULL);
+            if (pos < (unsigned long long)kCandMax) a.cand[pos] = key;
+          }
         }
-      }
-      if (!grid_sync(a.ctl)) return;
-      if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->ncand);
-      __syncthreads();
-      int nc = (int)(s_key < (unsigned long long)kCandMax ? s_key : kCandMax);
-      const unsigned long long kk = k < (unsigned long long)nc ? k : (nc > 0 ? nc - 1 : 0);
-      if (nc <= kThreads) {
-        // rank by counting: key i has rank k iff lo_i <= k < lo_i + eq_i
+        if (!grid_sync(a.ctl)) return;
+        if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->ncand);
+        __syncthreads();
+        const int nc = (int)(s_key < (unsigned long long)kCandMax ? s_key : kCandMax);
+        const unsigned long long kk = k < (unsigned long long)nc ? k : (nc > 0 ? nc - 1 : 0);
+        // rank by counting: key i has rank kk iff lo_i <= kk < lo_i + eq_i
         for (int i = threadIdx.x; i < nc; i += blockDim.x) ck[i] = __ldcg(&a.cand[i]);
         __syncthreads();
         if (threadIdx.x < nc) {
@@ -318,77 +322,55 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         }
         __syncthreads();
         nth = s_nth;
-      } else {
-      for (int i = threadIdx.x; i < kCandMax; i += blockDim.x)
-        ck[i] = (i < nc) ? __ldcg(&a.cand[i]) : ~0ULL;
-      __syncthreads();
-      // bitonic sort of kCandMax keys
-      for (int size = 2; size <= kCandMax; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-          for (int i = threadIdx.x; i < kCandMax; i += blockDim.x) {
-            int j = i ^ stride;
-            if (j > i) {
-              bool up = (i & size) == 0;
-              unsigned long long x = ck[i], y = ck[j];
-              if ((x > y) == up) { ck[i] = y; ck[j] = x; }
-            }
-          }
-          __syncthreads();
-        }
-      if (threadIdx.x == 0) s_nth = __longlong_as_double((long long)ck[kk]);
-      __syncthreads();
-      nth = s_nth;
       }
     }
-    // ---- subset barycentres ---------------------------------------------
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (long long i = gtid; i < n; i += gstride) {
-      if (a.resid[i] <= nth) {
-        acc[0] += 1.0;
-        for (int c = 0; c < 3; ++c) {
-          acc[1 + c] += a.init[3 * i + c];
-          acc[4 + c] += a.moved[3 * i + c];
-        }
-      }
+    // ---- subset moments in one sweep: count, first and second moments of
+    // the pairs z = (initial, moved) about the first pair z0 (near the data,
+    // so centring afterwards loses nothing in FP64) ------------------------
+    double z0[6];
+    for (int c = 0; c < 3; ++c) {
+      z0[c] = __ldg(&a.init[c]);
+      z0[3 + c] = __ldg(&a.moved[c]);
     }
-    __shared__ double s_out[21];
-    block_sums<7>(acc, red_n, s_out);
-    if (threadIdx.x < 7) a.partial[(long long)blockIdx.x * kPartial + threadIdx.x] = s_out[threadIdx.x];
-    if (!grid_sync(a.ctl)) return;
-    __shared__ double s_mean[7];
-    grid_partial_sums(a.partial, 0, 7, s_mean);
-    const double cnt = s_mean[0];
-    double mi[3], mm[3];
-    for (int c = 0; c < 3; ++c) { mi[c] = s_mean[1 + c] / cnt; mm[c] = s_mean[4 + c] / cnt; }
-    // ---- centred second moments (21 unique of the 6x6) -------------------
-    double z2[21];
-    for (int q = 0; q < 21; ++q) z2[q] = 0.0;
+    double acc[28];
+#pragma unroll
+    for (int q = 0; q < 28; ++q) acc[q] = 0.0;
     for (long long i = gtid; i < n; i += gstride) {
       if (a.resid[i] <= nth) {
         double z[6];
         for (int c = 0; c < 3; ++c) {
-          z[c] = a.init[3 * i + c] - mi[c];
-          z[3 + c] = a.moved[3 * i + c] - mm[c];
+          z[c] = a.init[3 * i + c] - z0[c];
+          z[3 + c] = a.moved[3 * i + c] - z0[3 + c];
         }
-        int q = 0;
+        acc[0] += 1.0;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) acc[1 + r] += z[r];
+        int q = 7;
+#pragma unroll
         for (int r = 0; r < 6; ++r)
-          for (int c = r; c < 6; ++c) z2[q++] += z[r] * z[c];
+#pragma unroll
+          for (int c = r; c < 6; ++c) acc[q++] += z[r] * z[c];
       }
     }
-    __syncthreads();
-    block_sums<21>(z2, red_n, s_out);
-    if (threadIdx.x < 21) a.partial[(long long)blockIdx.x * kPartial + 8 + threadIdx.x] = s_out[threadIdx.x];
+    __shared__ double s_out[28];
+    block_sums<28>(acc, red_n, s_out);
+    if (threadIdx.x < 28) a.partial[(long long)blockIdx.x * kPartial + threadIdx.x] = s_out[threadIdx.x];
     if (!grid_sync(a.ctl)) return;
-    if (blockIdx.x == 0) grid_partial_sums(a.partial, 8, 21, s_out);
+    if (blockIdx.x == 0) grid_partial_sums(a.partial, 0, 28, s_out);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       LtsMoments mo;
+      const double cnt = s_out[0];
+      double m[6];
+      for (int r = 0; r < 6; ++r) m[r] = s_out[1 + r] / cnt;
       mo.n = cnt;
-      for (int c = 0; c < 3; ++c) { mo.mean_i[c] = mi[c]; mo.mean_m[c] = mm[c]; }
-      double zz[21];
-      for (int q = 0; q < 21; ++q) zz[q] = s_out[q];
-      int q = 0;
+      for (int c = 0; c < 3; ++c) { mo.mean_i[c] = z0[c] + m[c]; mo.mean_m[c] = z0[3 + c] + m[3 + c]; }
+      int q = 7;
       for (int r = 0; r < 6; ++r)
-        for (int c = r; c < 6; ++c) { mo.Z[6 * r + c] = zz[q]; mo.Z[6 * c + r] = zz[q]; ++q; }
+        for (int c = r; c < 6; ++c) {
+          const double zz = s_out[q++] - cnt * m[r] * m[c];
+          mo.Z[6 * r + c] = zz;
+          mo.Z[6 * c + r] = zz;
+        }
       if (s.symmetric) lts_symmetric_step(s, mo);
       else lts_classic_step(s, mo);
       s.fraction = s.lts_keep;
@@ -488,7 +470,7 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
 //   [4096, 4352)     LtsCtl (zeroed each call)
 //   [4352, 4608)     point-pair counters {n, 0} (uploaded each call)
 //   [4608, +48 KB)   3 radix histograms of 4096 bins (zeroed each call)
-//   then             2048 candidate keys, kNaMaxCtas * 32 partial sums,
+//   then             256 candidate keys, kNaMaxCtas * 32 partial sums,
 //                    MIRORR_LTS_NOALLOC_MAX_POINTS residuals.
 // Two calls in flight on one device share the array and race.
 
