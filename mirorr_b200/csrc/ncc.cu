@@ -143,6 +143,12 @@ __device__ inline void top2_merge(float &a1, float &a2, float b1, float b2) {
   a2 = m2;
 }
 
+// top2_merge(a1, a2, b, -3) for a running pair with a2 >= -3.
+__device__ inline void top2_push(float &a1, float &a2, float b) {
+  a2 = fmaxf(a2, fminf(a1, b));
+  a1 = fmaxf(a1, b);
+}
+
 __device__ inline void min2_merge(int &a1, int &a2, int b1, int b2) {
   // two smallest non-negative values of {a1, a2, b1, b2} (negative = none)
   int v[4] = {a1, a2, b1, b2};
@@ -492,7 +498,7 @@ __global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
         const long long q0 = ((long long)gz0 * ny + gy) * nx + gx;
         float *wd = win + s * WIN + yl * EXP + xl;
         unsigned int *bd = bits + s * NROW + yl;
-#pragma unroll 2
+#pragma unroll
         for (int z = 0; z < E; ++z) {
           const int gz = gz0 + z;
           const bool in = xyin && gz >= 0 && gz < nz;
@@ -722,7 +728,7 @@ __global__ void __launch_bounds__(C::NT, 2) ncc_basemask_kernel(NccArgs a) {
         float *wd = win + s * WIN + yl * EXP + xl;
         float *md = mwin + s * WIN + yl * EXP + xl;
         if (yl < EY && xl < EXP) {
-#pragma unroll 2
+#pragma unroll
           for (int z = 0; z < E; ++z) {
             const int gz = gz0 + z;
             const bool in = xyin && gz >= 0 && gz < nz;
@@ -1288,6 +1294,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
         t[4 * i] = q.x; t[4 * i + 1] = q.y; t[4 * i + 2] = q.z; t[4 * i + 3] = q.w;
       }
       const float c = st.c, sxt = st.sxt, sxx = st.sxx;
+      const float rsxx = sxx > 0.f ? 1.f / sxx : 0.f;
       float2 *qb = qbuf + lane * W;
       const float2 *st0 = a.stats + (((long long)oz * ny + oy) * nx + px);
       const float *rp = win + (ox - xu) + x;
@@ -1340,9 +1347,8 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
               if (!((yok >> cy) & 1u)) continue;
               const float2 q = qb[cy];
               const float sxy = acc[0][cy] - (q.x - c) * sxt;
-              const float s = (sxx <= 0.f || q.y <= 0.f)
-                                  ? -2.f : __fdividef(__fdividef(sxy * sxy, sxx), q.y);
-              top2_merge(l1, l2, s, -3.f);
+              const float s = (sxx <= 0.f || q.y <= 0.f) ? -2.f : __fdividef(sxy * sxy * rsxx, q.y);
+              top2_push(l1, l2, s);
               if (s == -2.f) push_deg(d1, d2, (int)(prow + (long long)cy * nx));
               sc[cy] = s;
             }
