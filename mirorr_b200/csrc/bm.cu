@@ -52,11 +52,36 @@ void point_geom(const double origin[3], const double spacing[3], const double di
 // Each thread computes PX consecutive x positions of one row: every footprint
 // row of PX + BW - 1 floats is loaded once and serves all PX positions.  Per
 // position the statistics are the two-pass ones of normalizedCorrelation
-// (mean over all voxels, then the masked sum of squares in raster order,
-// itkBlockMatcher.txx:57-95) in FP64, the squares accumulated with fused
-// multiply-adds.  They feed the FP32 search only; a sum of squares is zero
-// exactly when every masked voxel equals the mean, as in the reference.
+// (mean over all voxels, then the masked sum of squares,
+// itkBlockMatcher.txx:57-95).  The mean is an FP64 sum (exact for float
+// inputs of ordinary range, so a flat footprint's mean is its value); the
+// sum of squares is taken in FP32 about the FP32 mean.  They feed the FP32
+// search only, where the one decision that must be exact is Syy = 0.  When
+// the FP64 mean is a float, a masked voxel differs from it in FP32 exactly
+// when it does in FP64; otherwise an FP32 sum of at least 1e-30 implies a
+// non-zero FP64 one, and below that the position is recomputed with the FP64
+// two-pass sum, zero exactly when every masked voxel equals the mean, as in
+// the reference.
 constexpr int kBoxPX = 4;
+
+// FP64 masked sum of squares about mean of the footprint at linear index o
+// (raster order, fused multiply-adds); the footprint lies inside the volume.
+template <int BW>
+__device__ __noinline__ double box_ss64(const float *__restrict__ y,
+                                        const uint8_t *__restrict__ ms, long long o, int nx,
+                                        int ny, double mean) {
+  double ss = 0.0;
+  for (int vz = 0; vz < BW; ++vz)
+    for (int vy = 0; vy < BW; ++vy) {
+      const long long q = o + ((long long)vz * ny + vy) * nx;
+      for (int vx = 0; vx < BW; ++vx)
+        if (__ldg(ms + q + vx)) {
+          const double d = __dsub_rn((double)__ldg(y + q + vx), mean);
+          ss = __fma_rn(d, d, ss);
+        }
+    }
+  return ss;
+}
 
 template <int BW>
 __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict__ y,
@@ -95,33 +120,57 @@ __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict_
 #pragma unroll
             for (int j = 0; j < PX; ++j) sum[j] = __dadd_rn(sum[j], (double)v[j + vx]);
         }
+      constexpr int B = BW * BW * BW;
 #pragma unroll
-      for (int j = 0; j < PX; ++j) mean[j] = __ddiv_rn(sum[j], (double)(BW * BW * BW));
+      for (int j = 0; j < PX; ++j)
+        mean[j] = (B & (B - 1)) == 0 ? sum[j] * (1.0 / B) : __ddiv_rn(sum[j], (double)B);
+      float mu[PX], s32[PX];
+#pragma unroll
+      for (int j = 0; j < PX; ++j) { mu[j] = (float)mean[j]; s32[j] = 0.f; }
+      // mask columns of the PX + BW - 1 wide footprint rows: in the mask in
+      // every row (allb) and in some row (anyb)
+      unsigned int allb = ~0u, anyb = 0u;
 #pragma unroll
       for (int vz = 0; vz < BW; ++vz)
 #pragma unroll
         for (int vy = 0; vy < BW; ++vy) {
           const long long q = o + ((long long)vz * ny + vy) * nx;
           float v[RL];
-          uint8_t m[RL];
+          bool m[RL];
+          unsigned int mb = 0u;
 #pragma unroll
           for (int i = 0; i < RL; ++i) {
             const bool in = x0 + i < nx;
             v[i] = in ? __ldg(y + q + i) : 0.f;
-            m[i] = in ? __ldg(ms + q + i) : (uint8_t)0;
+            m[i] = in && __ldg(ms + q + i) != 0;
+            mb |= (m[i] ? 1u : 0u) << i;
           }
+          allb &= mb;
+          anyb |= mb;
 #pragma unroll
           for (int vx = 0; vx < BW; ++vx)
 #pragma unroll
             for (int j = 0; j < PX; ++j) {
-              if (m[j + vx]) {
-                const double d = __dsub_rn((double)v[j + vx], mean[j]);
-                ss[j] = __fma_rn(d, d, ss[j]);
-              } else {
-                all_in[j] = false;
-              }
+              const float d = m[j + vx] ? v[j + vx] - mu[j] : 0.f;
+              s32[j] = fmaf(d, d, s32[j]);
             }
         }
+      constexpr unsigned int kRow = (1u << BW) - 1u;
+      bool any_in[PX];
+#pragma unroll
+      for (int j = 0; j < PX; ++j) {
+        all_in[j] = ((allb >> j) & kRow) == kRow;
+        any_in[j] = ((anyb >> j) & kRow) != 0u;
+      }
+#pragma unroll
+      for (int j = 0; j < PX; ++j) {
+        ss[j] = (double)s32[j];
+        // no masked voxel: zero; with a mean that is a float, v - mean is zero
+        // in FP32 exactly when it is in FP64; otherwise a tiny FP32 sum is
+        // recomputed in FP64
+        if (ok[j] && any_in[j] && s32[j] < 1e-30f && (double)mu[j] != mean[j])
+          ss[j] = box_ss64<BW>(y, ms, o + j, nx, ny, mean[j]);
+      }
     }
 #pragma unroll
     for (int j = 0; j < PX; ++j) {
