@@ -148,6 +148,21 @@ MIRORR_API mirorr_status mirorr_resample_nearest(mirorr_ctx ctx, const int32_t i
                                       const float *in_image, const uint8_t *in_mask,
                                       const int32_t out_size[3], const double C[9],
                                       const double e[3], float *out_image, uint8_t *out_mask);
+/* Final resampling with itk::BSplineInterpolateImageFunction of order 3, the
+ * "bspline" interpolator (and the reference command line's default) of
+ * GetInterpolatorFromString / GetResampledImage
+ * (itkMirorrPyramidImplement.txx:365-479): FP64 coefficients by the recursive
+ * prefilter with mirror boundaries, evaluation on the 4x4x4 support.  Index
+ * map and outside value as mirorr_resample.  Image only; host pointers. */
+MIRORR_API mirorr_status mirorr_resample_bspline(mirorr_ctx ctx, const int32_t in_size[3],
+                                      const float *in_image, const int32_t out_size[3],
+                                      const double C[9], const double e[3], float *out_image);
+/* The same with itk::WindowedSincInterpolateImageFunction of radius 5 with the
+ * Welch window and clamp-to-edge neighbours, the "sinc" interpolator of
+ * GetInterpolatorFromString (itkMirorrPyramidImplement.txx:416-425). */
+MIRORR_API mirorr_status mirorr_resample_sinc(mirorr_ctx ctx, const int32_t in_size[3],
+                                   const float *in_image, const int32_t out_size[3],
+                                   const double C[9], const double e[3], float *out_image);
 /* Affine index map of the resampler from geometries and a transform
  * y = M x + offset (output grid -> input continuous index). */
 MIRORR_API mirorr_status mirorr_resample_map(const mirorr_geometry *out_grid, const mirorr_geometry *in_grid,

@@ -162,6 +162,8 @@ def lib():
         "mirorr_resample": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
         "mirorr_resample_map": [P(Geometry), P(Geometry), vp, vp, vp, vp],
         "mirorr_resample_nearest": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
+        "mirorr_resample_bspline": [vp, vp, vp, vp, vp, vp, vp],
+        "mirorr_resample_sinc": [vp, vp, vp, vp, vp, vp, vp],
         "mirorr_lts_classic": [vp, P(Transform), ctypes.c_size_t, vp, vp, ctypes.c_double,
                                P(ctypes.c_int32)],
         "mirorr_lts_symmetric": [vp, P(Transform), P(Transform), P(Transform), ctypes.c_size_t,
@@ -440,6 +442,26 @@ def resample(ctx: Context, image, mask, out_size_xyz, C, e, nearest=False):
     _check(fn(ctx.handle, in_size, _ptr(img), _ptr(msk), out_size, _ptr(Cc), _ptr(ec), _ptr(out),
               _ptr(outm)))
     return out, outm
+
+
+def resample_final(ctx: Context, image, out_size_xyz, C, e, interpolator="bspline"):
+    """Final resampling of image (float32, z, y, x) on an index map with the
+    cubic B-spline ("bspline") or the radius-5 Welch-windowed sinc ("sinc")
+    interpolator of GetResampledImage."""
+    img = _f32(image)
+    in_size = (ctypes.c_int32 * 3)(img.shape[2], img.shape[1], img.shape[0])
+    out_size = (ctypes.c_int32 * 3)(*[int(v) for v in out_size_xyz])
+    out = np.zeros((int(out_size_xyz[2]), int(out_size_xyz[1]), int(out_size_xyz[0])), np.float32)
+    Cc = np.ascontiguousarray(np.asarray(C, np.float64).reshape(-1))
+    ec = np.ascontiguousarray(np.asarray(e, np.float64))
+    if interpolator == "bspline":
+        fn = lib().mirorr_resample_bspline
+    elif interpolator == "sinc":
+        fn = lib().mirorr_resample_sinc
+    else:
+        raise ValueError("interpolator must be 'bspline' or 'sinc'")
+    _check(fn(ctx.handle, in_size, _ptr(img), out_size, _ptr(Cc), _ptr(ec), _ptr(out)))
+    return out
 
 
 def lts_classic(ctx: Context, t: Transform, init, moved, lts_keep=0.5):

@@ -6,8 +6,7 @@
 // pyramid levels, block parameters, masks, and the final resampled outputs.
 // Options of the reference that select machinery outside this path (other
 // block metrics, inner resampling modes other than "middle", crop and
-// reorientation, b-spline and sinc final interpolators) are rejected with a
-// message rather than silently changed.
+// reorientation) are rejected with a message rather than silently changed.
 #include <sys/stat.h>
 
 #include <cstdio>
@@ -39,7 +38,7 @@ const char *kUsage =
     "  -R, --do-not-register      only resample with the given transform\n"
     "      --save-resampled-moving FILE   moving image on the fixed grid\n"
     "      --save-resampled-fixed FILE    fixed image on the moving grid\n"
-    "      --final-interpolator I nn | linear (default linear)\n"
+    "      --final-interpolator I nn | linear | bspline | sinc (default bspline)\n"
     "  -M, --moving-mask FILE     moving image mask\n"
     "  -F, --fixed-mask FILE      fixed image mask\n"
     "  -I, --invert-last-tfm      write the inverse of the result\n"
@@ -191,17 +190,45 @@ std::vector<uint8_t> read_mask(const std::string &path, const mirorr_geometry &l
 
 // Resamples `in` (on grid gin) onto grid gout through y = M x + offset
 // (an output physical point maps to an input physical point).
+enum class Interp { kNearest, kLinear, kBspline, kSinc };
+
+// GetInterpolatorFromString (itkMirorrPyramidImplement.txx:365-390): the first
+// of "nn", "linear", "bspline", "sinc" contained in the name; otherwise
+// bspline, with a note.
+Interp interpolator_from_string(const std::string &name, bool quiet) {
+  if (name.find("nn") != std::string::npos) return Interp::kNearest;
+  if (name.find("linear") != std::string::npos) return Interp::kLinear;
+  if (name.find("bspline") != std::string::npos) return Interp::kBspline;
+  if (name.find("sinc") != std::string::npos) return Interp::kSinc;
+  if (!quiet)
+    std::printf("Unspecified or unknown interpolator name '%s'. Defaulting to bspline.\n",
+                name.c_str());
+  return Interp::kBspline;
+}
+
 std::vector<float> resample_to(mirorr_ctx ctx, const Volume &in, const mirorr_geometry &gout,
-                               const mb2::Tfm &t, bool nearest) {
+                               const mb2::Tfm &t, Interp interp) {
   double C[9], e[3];
   check(mirorr_resample_map(&gout, &in.geom, t.M, t.off, C, e), "resample map");
   std::vector<float> out((size_t)gout.size[0] * gout.size[1] * gout.size[2]);
-  if (nearest)
-    check(mirorr_resample_nearest(ctx, in.geom.size, in.data.data(), nullptr, gout.size, C, e,
-                                  out.data(), nullptr), "resample");
-  else
-    check(mirorr_resample(ctx, in.geom.size, in.data.data(), nullptr, gout.size, C, e,
-                          out.data(), nullptr), "resample");
+  switch (interp) {
+    case Interp::kNearest:
+      check(mirorr_resample_nearest(ctx, in.geom.size, in.data.data(), nullptr, gout.size, C, e,
+                                    out.data(), nullptr), "resample");
+      break;
+    case Interp::kLinear:
+      check(mirorr_resample(ctx, in.geom.size, in.data.data(), nullptr, gout.size, C, e,
+                            out.data(), nullptr), "resample");
+      break;
+    case Interp::kBspline:
+      check(mirorr_resample_bspline(ctx, in.geom.size, in.data.data(), gout.size, C, e,
+                                    out.data()), "resample");
+      break;
+    case Interp::kSinc:
+      check(mirorr_resample_sinc(ctx, in.geom.size, in.data.data(), gout.size, C, e, out.data()),
+            "resample");
+      break;
+  }
   return out;
 }
 
@@ -235,9 +262,7 @@ int run(int argc, char **argv) {
     throw std::runtime_error("only the normalised correlation block metric (nc) is available");
   if (a.get("resampling-mode", "middle") != "middle")
     throw std::runtime_error("only the middle inner resampling mode is available");
-  const std::string interp = a.get("final-interpolator", "linear");
-  if (interp != "linear" && interp != "nn")
-    throw std::runtime_error("final interpolator '" + interp + "' is not available; use linear or nn");
+  const Interp interp = interpolator_from_string(a.get("final-interpolator", "bspline"), quiet);
   if (!a.has("moving") || !a.has("fixed")) throw std::runtime_error("moving and fixed images are required");
 
   const std::string tt = a.get("tfm-type", "rigid");
@@ -324,15 +349,14 @@ int run(int argc, char **argv) {
     if (!quiet) std::printf("mirorr: wrote %s\n", last.c_str());
   }
   // final resampling: the transform maps moving points to fixed points
-  const bool nearest = interp == "nn";
   if (a.has("save-resampled-moving")) {
     mb2::Tfm inv;
     if (!mb2::tfm_inverse(result, inv)) throw std::runtime_error("transform is singular");
-    std::vector<float> out = resample_to(context(), moving, fixed.geom, inv, nearest);
+    std::vector<float> out = resample_to(context(), moving, fixed.geom, inv, interp);
     write_nifti_float(a.get("save-resampled-moving", ""), fixed.geom, out.data());
   }
   if (a.has("save-resampled-fixed")) {
-    std::vector<float> out = resample_to(context(), fixed, moving.geom, result, nearest);
+    std::vector<float> out = resample_to(context(), fixed, moving.geom, result, interp);
     write_nifti_float(a.get("save-resampled-fixed", ""), moving.geom, out.data());
   }
   if (ctx) mirorr_ctx_destroy(ctx);

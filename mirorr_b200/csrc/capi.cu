@@ -1218,6 +1218,59 @@ mirorr_status mirorr_resample_nearest(mirorr_ctx c, const int32_t in_size[3], co
   return resample_common(c, in_size, in_image, in_mask, out_size, C, e, out_image, out_mask, true);
 }
 
+// Final resampling with the B-spline (bspline) or windowed-sinc interpolator:
+// image only, host buffers in and out.
+static mirorr_status resample_final(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
+                                    const int32_t out_size[3], const double C[9],
+                                    const double e[3], float *out_image, bool bspline) {
+  if (!c || !in_size || !out_size || !C || !e || !in_image || !out_image) {
+    set_error("null argument");
+    return MIRORR_EINVAL;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (in_size[d] <= 0 || out_size[d] <= 0) { set_error("empty volume"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  const long long ni = vox(in_size), no = vox(out_size);
+  DevBuf di, coef, oi;
+  auto run = [&]() -> mirorr_status {
+    MB2_TRY(upload(c, di, in_image, sizeof(float) * ni));
+    MB2_TRY(oi.ensure(sizeof(float) * no));
+    ResampleMap m;
+    memcpy(m.C, C, sizeof(m.C));
+    memcpy(m.e, e, sizeof(m.e));
+    if (bspline) {
+      MB2_TRY(coef.ensure(sizeof(double) * ni));
+      MB2_TRY(launch_resample_bspline(in_size, di.as<float>(), out_size, m, coef.as<double>(),
+                                      oi.as<float>(), c->stream));
+    } else {
+      MB2_TRY(launch_resample_sinc(in_size, di.as<float>(), out_size, m, oi.as<float>(),
+                                   c->stream));
+    }
+    MB2_CUDA_TRY(cudaMemcpyAsync(out_image, oi.ptr, sizeof(float) * no, cudaMemcpyDeviceToHost,
+                                 c->stream));
+    MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MIRORR_OK;
+  };
+  const mirorr_status st = run();
+  cudaStreamSynchronize(c->stream);  // nothing in flight uses the buffers below
+  di.release();
+  coef.release();
+  oi.release();
+  return st;
+}
+
+mirorr_status mirorr_resample_bspline(mirorr_ctx c, const int32_t in_size[3],
+                                      const float *in_image, const int32_t out_size[3],
+                                      const double C[9], const double e[3], float *out_image) {
+  return resample_final(c, in_size, in_image, out_size, C, e, out_image, true);
+}
+
+mirorr_status mirorr_resample_sinc(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
+                                   const int32_t out_size[3], const double C[9],
+                                   const double e[3], float *out_image) {
+  return resample_final(c, in_size, in_image, out_size, C, e, out_image, false);
+}
+
 // ---- LTS ---------------------------------------------------------------------------
 static mirorr_status lts_common(mirorr_ctx c, mirorr_transform *t, mirorr_transform *t12f,
                                 mirorr_transform *t12b, size_t n, const double *init,

@@ -89,6 +89,13 @@ struct ResampleMap {
 mirorr_status launch_resample(const int in_size[3], const float *in, const uint8_t *in_mask,
                               const int out_size[3], const ResampleMap &map, float *out,
                               uint8_t *out_mask, cudaStream_t s, bool nearest = false);
+// Final-resampling interpolators (interp.cu): cubic B-spline (coef: FP64
+// scratch of the input's size) and Welch-windowed sinc of radius 5.
+mirorr_status launch_resample_bspline(const int in_size[3], const float *in, const int out_size[3],
+                                      const ResampleMap &map, double *coef, float *out,
+                                      cudaStream_t s);
+mirorr_status launch_resample_sinc(const int in_size[3], const float *in, const int out_size[3],
+                                   const ResampleMap &map, float *out, cudaStream_t s);
 // Separable Gaussian smoothing along one axis (axis 0 = x).
 mirorr_status launch_smooth_axis(const int size[3], const float *in, float *out, int axis,
                                  const double *w, int radius, cudaStream_t s);

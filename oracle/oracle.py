@@ -291,6 +291,147 @@ def resample_nearest(in_data, in_mask, out_size, C, e):
     return out, outm
 
 
+def _index_map(out_size, C, e, n):
+    """c = e + C idx (FP64, left to right) and the buffer test
+    -0.5 <= c < n - 0.5, for every output voxel (arrays in z, y, x order)."""
+    k, j, i = np.meshgrid(np.arange(out_size[2], dtype=np.float64),
+                          np.arange(out_size[1], dtype=np.float64),
+                          np.arange(out_size[0], dtype=np.float64), indexing="ij")
+    C = np.asarray(C, np.float64).reshape(3, 3)
+    c = [((e[r] + C[r, 0] * i) + C[r, 1] * j) + C[r, 2] * k for r in range(3)]
+    inside = np.ones(k.shape, bool)
+    for r in range(3):
+        inside &= (c[r] >= -0.5) & (c[r] < n[r] - 0.5)
+    return c, inside
+
+
+def bspline_coefficients(data):
+    """Cubic B-spline coefficients of a (z, y, x) volume in FP64, restating
+    itk::BSplineDecompositionImageFilter of order 3 (Unser's recursive
+    prefilter, pole z = sqrt(3) - 2, mirror boundaries, tolerance 1e-10), as
+    used by BSplineInterpolateImageFunction for GetResampledImage's
+    "bspline" interpolator (itkMirorrPyramidImplement.txx:409-415).  Axes x,
+    y, z in turn; per line c[0 .. N): c *= lambda; causal initial value
+    (truncated sum over the horizon, or the mirror-symmetric full sum when
+    the line is shorter, z^(N-1) as a product); c[n] += z c[n-1];
+    c[N-1] = z / (z^2 - 1) (z c[N-2] + c[N-1]); c[n] = z (c[n+1] - c[n])."""
+    c = np.array(data, np.float64)
+    z = math.sqrt(3.0) - 2.0
+    lam = (1.0 - z) * (1.0 - 1.0 / z)
+    iz = 1.0 / z
+    anti = z / (z * z - 1.0)
+    horizon = int(math.ceil(math.log(1e-10) / math.log(abs(z))))
+    for axis in (2, 1, 0):
+        a = np.moveaxis(c, axis, 0)
+        N = a.shape[0]
+        if N == 1:
+            continue
+        a *= lam
+        zn = z
+        if horizon < N:
+            s = a[0].copy()
+            for n in range(1, horizon):
+                s = s + zn * a[n]
+                zn = zn * z
+            a[0] = s
+        else:
+            z2n = 1.0
+            for _ in range(N - 1):
+                z2n = z2n * z
+            s = a[0] + z2n * a[N - 1]
+            z2n = z2n * (z2n * iz)
+            for n in range(1, N - 1):
+                s = s + (zn + z2n) * a[n]
+                zn = zn * z
+                z2n = z2n * iz
+            a[0] = s / (1.0 - zn * zn)
+        for n in range(1, N):
+            a[n] = a[n] + z * a[n - 1]
+        a[N - 1] = anti * (z * a[N - 2] + a[N - 1])
+        for n in range(N - 2, -1, -1):
+            a[n] = z * (a[n + 1] - a[n])
+    return c
+
+
+def _mirror(idx, n):
+    """Mirror boundary of the B-spline evaluation (period 2N - 2; 0 for N = 1)."""
+    if n == 1:
+        return np.zeros_like(idx)
+    l2 = 2 * n - 2
+    idx = np.where(idx < 0, -idx - l2 * ((-idx) // l2), idx - l2 * (idx // l2))
+    return np.where(n <= idx, l2 - idx, idx)
+
+
+def resample_bspline(in_data, out_size, C, e):
+    """Final resampling with BSplineInterpolateImageFunction of order 3
+    (itkMirorrPyramidImplement.txx:365-479): per axis the support starts at
+    floor(c) - 1 with weights, for w = c - floor(c),
+    w3 = w^3/6, w0 = 1/6 + w (w - 1)/2 - w3, w2 = w + w0 - 2 w3,
+    w1 = 1 - w0 - w2 - w3; the 64 products ((wx wy) wz) coef summed with x
+    fastest; 0 outside the buffer; float output."""
+    coef = bspline_coefficients(in_data)
+    n = (coef.shape[2], coef.shape[1], coef.shape[0])
+    c, inside = _index_map(out_size, C, e, n)
+    sixth = 1.0 / 6.0
+    wt, ix = [], []
+    for r in range(3):
+        b = np.floor(c[r])
+        w = c[r] - b
+        b = b.astype(np.int64)
+        w3 = ((sixth * w) * w) * w
+        w0 = (sixth + (0.5 * w) * (w - 1.0)) - w3
+        w2 = (w + w0) - 2.0 * w3
+        w1 = ((1.0 - w0) - w2) - w3
+        wt.append([w0, w1, w2, w3])
+        ix.append([_mirror(b - 1 + k, n[r]) for k in range(4)])
+    v = np.zeros(inside.shape, np.float64)
+    for kz in range(4):
+        for ky in range(4):
+            for kx in range(4):
+                w = (wt[0][kx] * wt[1][ky]) * wt[2][kz]
+                v = v + w * coef[ix[2][kz], ix[1][ky], ix[0][kx]]
+    return np.where(inside, v, 0.0).astype(np.float32)
+
+
+def resample_sinc(in_data, out_size, C, e, radius=5):
+    """Final resampling with WindowedSincInterpolateImageFunction (radius 5,
+    Welch window, zero-flux Neumann boundary: indices clamp to the image),
+    GetInterpolatorFromString's "sinc" (itkMirorrPyramidImplement.txx:416-425).
+    Per axis, base floor(c), d = c - floor(c); the 2R taps at offsets
+    1-R .. R weigh (1 - x^2/R^2) sin(pi x)/(pi x) for x = d + R - 1 - i
+    (a delta at offset 0 when d = 0); the products (((p wx) wy) wz) summed with
+    x fastest; 0 outside the buffer; float output."""
+    data = np.asarray(in_data, np.float32)
+    n = (data.shape[2], data.shape[1], data.shape[0])
+    c, inside = _index_map(out_size, C, e, n)
+    R, T = radius, 2 * radius
+    f = 1.0 / (R * R)
+    wt, ix = [], []
+    for r in range(3):
+        b = np.floor(c[r])
+        d = c[r] - b
+        b = b.astype(np.int64)
+        x = d + float(R)
+        ws, xs = [], []
+        for i in range(T):
+            xs.append(np.clip(b + i - (R - 1), 0, n[r] - 1))
+            x = x - 1.0
+            welch = 1.0 - (x * f) * x
+            px = math.pi * x
+            with np.errstate(invalid="ignore", divide="ignore"):
+                tap = np.where(x == 0.0, welch, welch * (np.sin(px) / px))
+            ws.append(np.where(d == 0.0, 1.0 if i == R - 1 else 0.0, tap))
+        wt.append(ws)
+        ix.append(xs)
+    v = np.zeros(inside.shape, np.float64)
+    for kz in range(T):
+        for ky in range(T):
+            for kx in range(T):
+                p = data[ix[2][kz], ix[1][ky], ix[0][kx]].astype(np.float64)
+                v = v + ((p * wt[0][kx]) * wt[1][ky]) * wt[2][kz]
+    return np.where(inside, v, 0.0).astype(np.float32)
+
+
 # ---------------------------------------------------------------------------
 # ITK transform semantics (restated)
 # ---------------------------------------------------------------------------

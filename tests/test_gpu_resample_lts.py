@@ -54,6 +54,42 @@ def test_resample_nearest_bit_exact(ctx, seed):
     np.testing.assert_array_equal(outm_g, outm_o)
 
 
+@pytest.mark.parametrize("shape", [(17, 19, 23), (9, 2, 14), (6, 11, 1)])
+def test_resample_bspline_bit_exact(ctx, shape):
+    # final resampling, cubic B-spline: FP64 prefilter and evaluation restated
+    # with explicit rounding on both sides; axes of length 2 and 1 included
+    rng = np.random.default_rng(sum(shape))
+    img = (rng.random(shape) * 100.0).astype(np.float32)
+    M = random_rotation(rng, 9.0) @ np.diag(rng.uniform(0.9, 1.1, 3))
+    off = rng.uniform(-2, 2, 3)
+    gin = O.Image(img, np.array([1.0, 0.9, 1.1]), np.array([0.5, -1.0, 2.0]))
+    gout = O.Image(np.zeros((15, 18, 20), np.float32), np.array([1.05, 1.0, 0.95]),
+                   np.array([1.0, 0.0, 1.5]))
+    C, e = O.resample_map(gout, gin, M, off)
+    want = O.resample_bspline(img, gout.size, C, e)
+    got = mb.resample_final(ctx, img, gout.size, C, e, "bspline")
+    np.testing.assert_array_equal(got, want)
+
+
+def test_resample_sinc_matches_oracle(ctx):
+    # windowed sinc: the taps call sin(), so CUDA's and the host's results may
+    # differ in the last FP64 bits; after the float cast they agree to 1e-5
+    rng = np.random.default_rng(7)
+    img = (rng.random((14, 16, 18)) * 100.0).astype(np.float32)
+    M = random_rotation(rng, 7.0)
+    off = rng.uniform(-2, 2, 3)
+    gin = O.Image(img, np.array([1.0, 1.0, 1.0]), np.array([0.0, 0.0, 0.0]))
+    gout = O.Image(np.zeros((12, 15, 17), np.float32), np.array([1.1, 0.95, 1.0]),
+                   np.array([0.3, 0.2, -0.4]))
+    C, e = O.resample_map(gout, gin, M, off)
+    want = O.resample_sinc(img, gout.size, C, e)
+    got = mb.resample_final(ctx, img, gout.size, C, e, "sinc")
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-4)
+    # on the grid the weights are a delta: an exact copy
+    same = mb.resample_final(ctx, img, (18, 16, 14), np.eye(3), np.zeros(3), "sinc")
+    np.testing.assert_array_equal(same, img)
+
+
 @pytest.mark.parametrize("factors", [(2, 2, 2), (4, 4, 2), (2, 2, 1), (8, 8, 4)])
 def test_pyramid_level_bit_exact(ctx, factors):
     ph = make_phantom((64, 48, 40), n_gauss=10, seed=3)
