@@ -5,10 +5,12 @@
 // ITK transform files in and out, classic / symmetric, rigid / affine,
 // pyramid levels, block parameters, masks, and the final resampled outputs.
 // Options of the reference that select machinery outside this path (other
-// block metrics, inner resampling modes other than "middle", crop and
-// reorientation) are rejected with a message rather than silently changed.
+// block metrics, inner resampling modes other than "middle", the experimental
+// --reorient-fixed / --reorient-moving identity-space mode) are rejected with a
+// message rather than silently changed.
 #include <sys/stat.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -39,6 +41,7 @@ const char *kUsage =
     "      --save-resampled-moving FILE   moving image on the fixed grid\n"
     "      --save-resampled-fixed FILE    fixed image on the moving grid\n"
     "      --final-interpolator I nn | linear | bspline | sinc (default bspline)\n"
+    "      --crop mX,mY,fX,fY     crop moving / fixed by voxels on both sides of x and y\n"
     "  -M, --moving-mask FILE     moving image mask\n"
     "  -F, --fixed-mask FILE      fixed image mask\n"
     "  -I, --invert-last-tfm      write the inverse of the result\n"
@@ -232,6 +235,101 @@ std::vector<float> resample_to(mirorr_ctx ctx, const Volume &in, const mirorr_ge
   return out;
 }
 
+// OrientImageFilter towards ARI with the image's own direction, which the
+// reference applies to both images and both masks before registering
+// (itkMirorrPyramidWrapper.txx:79-92, :208-211): every voxel axis is matched
+// to the physical axis its direction column points along most (largest
+// |component|), and the buffer is permuted and flipped so that axis 0 runs
+// along +y (towards posterior), axis 1 along +x (left) and axis 2 along +z
+// (superior) in ITK's LPS space.  Spacing, direction columns and origin
+// follow, so every voxel keeps its physical position (an oblique direction
+// stays oblique).  A direction whose columns share a dominant axis is left
+// as it is.
+template <class T>
+std::vector<T> permute_flip(const std::vector<T> &in, const int32_t n[3], const int p[3],
+                            const int f[3]) {
+  const int32_t m[3] = {n[p[0]], n[p[1]], n[p[2]]};
+  std::vector<T> out(in.size());
+  size_t o = 0;
+  for (int k = 0; k < m[2]; ++k)
+    for (int j = 0; j < m[1]; ++j)
+      for (int i = 0; i < m[0]; ++i, ++o) {
+        const int ni[3] = {i, j, k};
+        long long idx[3];
+        for (int a = 0; a < 3; ++a) idx[p[a]] = f[a] > 0 ? ni[a] : m[a] - 1 - ni[a];
+        out[o] = in[(size_t)((idx[2] * n[1] + idx[1]) * n[0] + idx[0])];
+      }
+  return out;
+}
+
+void reorient_ari(Volume &v, std::vector<uint8_t> &mask) {
+  const double *D = v.geom.direction;
+  int dom[3], sgn[3];
+  for (int c = 0; c < 3; ++c) {
+    int r = 0;
+    for (int q = 1; q < 3; ++q)
+      if (std::fabs(D[3 * q + c]) > std::fabs(D[3 * r + c])) r = q;
+    dom[c] = r;
+    sgn[c] = D[3 * r + c] < 0 ? -1 : 1;
+  }
+  const int target[3] = {1, 0, 2};  // ARI: axis 0 along y, axis 1 along x, axis 2 along z
+  int p[3], f[3];
+  for (int a = 0; a < 3; ++a) {
+    p[a] = -1;
+    for (int c = 0; c < 3; ++c)
+      if (dom[c] == target[a]) {
+        if (p[a] >= 0) return;  // two axes share a dominant direction
+        p[a] = c;
+      }
+    if (p[a] < 0) return;
+    f[a] = sgn[p[a]];
+  }
+  mirorr_geometry g = v.geom;
+  double origin[3] = {v.geom.origin[0], v.geom.origin[1], v.geom.origin[2]};
+  for (int a = 0; a < 3; ++a) {
+    const int c = p[a];
+    g.size[a] = v.geom.size[c];
+    g.spacing[a] = v.geom.spacing[c];
+    for (int r = 0; r < 3; ++r) g.direction[3 * r + a] = f[a] * D[3 * r + c];
+    if (f[a] < 0)  // the new first voxel is the old last one along this axis
+      for (int r = 0; r < 3; ++r)
+        origin[r] += D[3 * r + c] * v.geom.spacing[c] * (double)(v.geom.size[c] - 1);
+  }
+  for (int r = 0; r < 3; ++r) g.origin[r] = origin[r];
+  v.data = permute_flip(v.data, v.geom.size, p, f);
+  if (!mask.empty()) mask = permute_flip(mask, v.geom.size, p, f);
+  v.geom = g;
+}
+
+// CropImageFilter with equal lower and upper crop sizes cx, cy along voxel
+// axes 0 and 1 (itkMirorrPyramidWrapper.txx:243-296): the kept voxels keep
+// their physical positions.
+template <class T>
+std::vector<T> crop_xy(const std::vector<T> &in, const int32_t n[3], int cx, int cy) {
+  std::vector<T> out;
+  out.reserve((size_t)(n[0] - 2 * cx) * (n[1] - 2 * cy) * n[2]);
+  for (int k = 0; k < n[2]; ++k)
+    for (int j = cy; j < n[1] - cy; ++j)
+      for (int i = cx; i < n[0] - cx; ++i)
+        out.push_back(in[((size_t)k * n[1] + j) * n[0] + i]);
+  return out;
+}
+
+void crop_volume(Volume &v, std::vector<uint8_t> &mask, int cx, int cy) {
+  if (cx <= 0 && cy <= 0) return;
+  cx = cx > 0 ? cx : 0;
+  cy = cy > 0 ? cy : 0;
+  if (v.geom.size[0] <= 2 * cx || v.geom.size[1] <= 2 * cy)
+    throw std::runtime_error("--crop removes the whole image");
+  v.data = crop_xy(v.data, v.geom.size, cx, cy);
+  if (!mask.empty()) mask = crop_xy(mask, v.geom.size, cx, cy);
+  const double *D = v.geom.direction;
+  for (int r = 0; r < 3; ++r)
+    v.geom.origin[r] += D[3 * r] * v.geom.spacing[0] * cx + D[3 * r + 1] * v.geom.spacing[1] * cy;
+  v.geom.size[0] -= 2 * cx;
+  v.geom.size[1] -= 2 * cy;
+}
+
 int run(int argc, char **argv) {
   Args a = parse(argc, argv);
   if (a.has("help") || argc == 1) {
@@ -248,6 +346,16 @@ int run(int argc, char **argv) {
     double s = 0.0;
     for (float x : v.data) s += x;
     std::printf("\nsum %.9g\n", s);
+    // the geometry the registration sees (reoriented to ARI) and its first voxel
+    Volume r = v;
+    std::vector<uint8_t> none;
+    reorient_ari(r, none);
+    const mirorr_geometry &h = r.geom;
+    std::printf("ari_size %d %d %d\nari_spacing %.9g %.9g %.9g\nari_origin %.9g %.9g %.9g\n"
+                "ari_direction", h.size[0], h.size[1], h.size[2], h.spacing[0], h.spacing[1],
+                h.spacing[2], h.origin[0], h.origin[1], h.origin[2]);
+    for (int i = 0; i < 9; ++i) std::printf(" %.9g", h.direction[i]);
+    std::printf("\nari_first %.9g %.9g\n", r.data.front(), r.data.back());
     return 0;
   }
   const bool quiet = a.has("quiet"), verbose = a.has("verbose");
@@ -255,7 +363,7 @@ int run(int argc, char **argv) {
     for (int i = 0; i < argc; ++i) std::printf("%s%s", i ? " " : "", argv[i]);
     std::printf("\n");
   }
-  for (const char *k : {"crop", "reorient-fixed", "reorient-moving", "save-fixed", "save-moving",
+  for (const char *k : {"reorient-fixed", "reorient-moving", "save-fixed", "save-moving",
                         "save-reoriented-fixed", "save-reoriented-moving", "switch-images"})
     if (a.has(k)) throw std::runtime_error(std::string("--") + k + " is outside this build's path");
   if (a.get("blockmetric", "nc") != "nc")
@@ -306,6 +414,21 @@ int run(int argc, char **argv) {
     have_init = true;
   }
 
+  // the images the registration sees: reoriented to ARI, then cropped; the
+  // final resampling uses the inputs as read (GetResampledImage is given
+  // fixedImage_in / movingImage_in, itkMirorrPyramidWrapper.txx:745,801)
+  Volume reg_moving = moving, reg_fixed = fixed;
+  std::vector<uint8_t> reg_mmask = mmask, reg_fmask = fmask;
+  reorient_ari(reg_moving, reg_mmask);
+  reorient_ari(reg_fixed, reg_fmask);
+  if (a.has("crop") && !a.get("crop", "").empty()) {
+    int c[4] = {0, 0, 0, 0};
+    if (std::sscanf(a.get("crop", "").c_str(), "%d,%d,%d,%d", &c[0], &c[1], &c[2], &c[3]) != 4)
+      throw std::runtime_error("--crop takes movingX,movingY,fixedX,fixedY");
+    crop_volume(reg_moving, reg_mmask, c[0], c[1]);
+    crop_volume(reg_fixed, reg_fmask, c[2], c[3]);
+  }
+
   mb2::Tfm result = init;
   if (!a.has("do-not-register")) {
     mirorr_reg_params p;
@@ -327,8 +450,9 @@ int run(int argc, char **argv) {
     p.verbosity = verbose ? 1 : 0;
     mirorr_transform init_pub = from_tfm(init), res;
     mirorr_reg_stats st;
-    check(mirorr_register(context(), &fixed.geom, fixed.data.data(), fmask.empty() ? nullptr : fmask.data(),
-                          &moving.geom, moving.data.data(), mmask.empty() ? nullptr : mmask.data(),
+    check(mirorr_register(context(), &reg_fixed.geom, reg_fixed.data.data(),
+                          reg_fmask.empty() ? nullptr : reg_fmask.data(), &reg_moving.geom,
+                          reg_moving.data.data(), reg_mmask.empty() ? nullptr : reg_mmask.data(),
                           &p, have_init ? &init_pub : nullptr, &res, &st),
           "registration");
     result = to_tfm(res);

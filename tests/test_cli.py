@@ -83,9 +83,12 @@ def test_help_and_errors(cli, tmp_path):
     assert r.returncode == 1 and "unknown option" in r.stderr
     img = tmp_path / "a.nii"
     write_nifti(str(img), np.zeros((4, 5, 6), np.float32))
-    r = subprocess.run([cli, "-m", str(img), "-f", str(img), "--crop", "4"],
+    r = subprocess.run([cli, "-m", str(img), "-f", str(img), "--reorient-fixed"],
                        capture_output=True, text=True)
     assert r.returncode == 1 and "outside" in r.stderr
+    r = subprocess.run([cli, "-m", str(img), "-f", str(img), "--crop", "4"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "movingX,movingY,fixedX,fixedY" in r.stderr
     r = subprocess.run([cli, "-m", str(img), "-f", str(img), "--blockmetric", "mi"],
                        capture_output=True, text=True)
     assert r.returncode == 1 and "nc" in r.stderr
@@ -191,7 +194,10 @@ def test_cli_registration_matches_library(cli, tmp_path):
                                       g["direction"].reshape(3, 3))
     ctx = mb.Context(0)
     p = mb.reg_params(symmetric=True, kind="rigid", levels=2, iterations=3)
-    t, _ = mb.register(ctx, ph.fixed, ph.moving, p, geom(gf), geom(gm))
+    # the command line registers the images reoriented to ARI
+    fa, gfa = _ari_geometry(mb, ph.fixed, gf)
+    ma, gma = _ari_geometry(mb, ph.moving, gm)
+    t, _ = mb.register(ctx, fa, ma, p, gfa, gma)
     d = _read_tfm(out)
     np.testing.assert_allclose([float(v) for v in d["Parameters"]], t.param_vector(), rtol=0,
                                atol=1e-12)
@@ -242,3 +248,83 @@ def test_cli_final_interpolators(cli, tmp_path, interp):
     want = mb.resample_final(mb.Context(0), img, g["size"].astype(int), C, e,
                              "sinc" if interp == "sinc" else "bspline")
     assert abs(info(cli, res)["sum"][0] - float(want.astype(np.float64).sum())) < 1e-2
+
+
+def _ari_of(data_zyx, D, origin, spacing):
+    """Expected ARI reorientation: axis 0 along +y, 1 along +x, 2 along +z
+    (LPS), each voxel keeping its physical position."""
+    D = np.asarray(D, float)
+    dom = [int(np.argmax(np.abs(D[:, c]))) for c in range(3)]
+    p = [dom.index(t) for t in (1, 0, 2)]
+    f = [1 if D[dom[c], c] > 0 else -1 for c in p]
+    a = np.transpose(data_zyx, (2, 1, 0))  # (x, y, z) = axes 0, 1, 2
+    a = np.transpose(a, p)
+    for k in range(3):
+        if f[k] < 0:
+            a = np.flip(a, axis=k)
+    n = data_zyx.shape[::-1]
+    first_old = [0 if f[p.index(c)] > 0 else n[c] - 1 for c in range(3)]
+    org = np.asarray(origin, float) + D @ (np.asarray(spacing, float) * first_old)
+    Dn = np.stack([f[k] * D[:, p[k]] for k in range(3)], axis=1)
+    return np.transpose(a, (2, 1, 0)), org, Dn, [n[c] for c in p]
+
+
+def _ari_geometry(mb, data_zyx, g):
+    """The ARI-reoriented array and its library geometry for an --info record."""
+    D = g["direction"].reshape(3, 3)
+    arr, org, Dn, size = _ari_of(data_zyx, D, g["origin"], g["spacing"])
+    dom = [int(np.argmax(np.abs(D[:, c]))) for c in range(3)]
+    sp = [g["spacing"][dom.index(t)] for t in (1, 0, 2)]
+    return np.ascontiguousarray(arr), mb.Geometry.make(np.array(size), sp, org, Dn)
+
+
+@pytest.mark.parametrize("perm", [(0, 1, 2), (1, 0, 2), (2, 0, 1)])
+def test_ari_reorientation_geometry(cli, tmp_path, perm):
+    rng = np.random.default_rng(3)
+    data = rng.random((5, 6, 7)).astype(np.float32)
+    # sform (RAS): axis c along RAS axis perm[c], alternating signs
+    S = np.zeros((3, 4))
+    sp = [0.9, 1.2, 1.5]
+    for c in range(3):
+        S[perm[c], c] = sp[c] * (1 if c % 2 == 0 else -1)
+    S[:, 3] = [3.0, -2.0, 5.5]
+    path = str(tmp_path / "o.nii")
+    write_nifti(path, data, sform=S)
+    g = info(cli, path)
+    D = g["direction"].reshape(3, 3)
+    want, org, Dn, size = _ari_of(data, D, g["origin"], g["spacing"])
+    np.testing.assert_array_equal(g["ari_size"], size)
+    np.testing.assert_allclose(g["ari_direction"].reshape(3, 3), Dn, atol=1e-9)
+    np.testing.assert_allclose(np.abs(g["ari_direction"].reshape(3, 3)),
+                               [[0, 1, 0], [1, 0, 0], [0, 0, 1]], atol=1e-9)
+    np.testing.assert_allclose(g["ari_origin"], org, atol=1e-6)
+    np.testing.assert_allclose(g["ari_first"], [want[0, 0, 0], want[-1, -1, -1]], rtol=1e-7)
+
+
+@pytest.mark.gpu
+def test_cli_registration_independent_of_storage_orientation(cli, tmp_path):
+    # the same physical images stored in two voxel orders register alike: the
+    # registration sees both reoriented to ARI
+    from mirorr_b200.phantom import make_phantom
+    ph = make_phantom((40, 36, 32), n_gauss=12, kind="rigid", seed=17, max_angle_deg=4.0,
+                      max_shift_vox=3.0)
+    outs = []
+    for storage in ("ras", "ari"):
+        if storage == "ras":
+            S = np.array([[1.0, 0, 0, 2.0], [0, 1.0, 0, -3.0], [0, 0, 1.0, 1.0]])
+            fix_d, mov_d = ph.fixed, ph.moving
+        else:
+            # the ARI voxel order of the RAS-stored images, with its sform
+            D = np.diag([-1.0, -1.0, 1.0])
+            fix_d, org, Dn, _ = _ari_of(ph.fixed, D, np.array([-2.0, 3.0, 1.0]), [1, 1, 1])
+            mov_d, _, _, _ = _ari_of(ph.moving, D, np.array([-2.0, 3.0, 1.0]), [1, 1, 1])
+            flip = np.diag([-1.0, -1.0, 1.0])
+            S = np.concatenate([flip @ Dn, (flip @ org)[:, None]], axis=1)
+        fix, mov = str(tmp_path / f"f_{storage}.nii"), str(tmp_path / f"m_{storage}.nii")
+        write_nifti(fix, np.ascontiguousarray(fix_d), sform=S)
+        write_nifti(mov, np.ascontiguousarray(mov_d), sform=S)
+        out = str(tmp_path / f"{storage}.tfm")
+        subprocess.run([cli, "-q", "-m", mov, "-f", fix, "-l", out, "-t", "rigid", "-d", "2",
+                        "-c", "0", "-n", "3"], check=True)
+        outs.append(np.array([float(v) for v in _read_tfm(out)["Parameters"]]))
+    np.testing.assert_allclose(outs[0], outs[1], atol=1e-6)
