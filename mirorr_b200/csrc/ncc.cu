@@ -1148,10 +1148,11 @@ __global__ void wand_axis_kernel(const uint8_t *in, uint8_t *out, long long inne
 // Lane-per-x-offset FP32 search, block width 4, block gap 1, for blocks whose
 // base block and window lie wholly inside both masks.
 //
-// A warp takes BPW = 32 / W consecutive blocks of one row of the block grid
-// (same by, bz).  Lane (k, x) scores the W x W candidates of block k whose x
-// offset in the window is x, i.e. every (cy, cz).  The blocks' windows
-// overlap along x, so the warp stages their union once: one tensor (TMA) copy
+// A CTA of NW warps (NL = 32 NW lanes) takes BPW = NL / W consecutive blocks
+// of one row of the block grid (same by, bz); with two warps and W = 9 that
+// is 7 blocks on 63 of 64 lanes.  Lane (k, x) scores the W x W candidates of
+// block k whose x offset in the window is x, i.e. every (cy, cz).  The
+// blocks' windows overlap along x, so the CTA stages their union once: one tensor (TMA) copy
 // of an rpu x E x E box from a 16-byte aligned x, zero-filled outside the
 // volume, completing on an mbarrier whose wait is bounded; at every load the
 // lanes read consecutive floats of one row (no bank conflicts).  The lane's base
@@ -1161,13 +1162,16 @@ __global__ void wand_axis_kernel(const uint8_t *in, uint8_t *out, long long inne
 // cancellation).  A window plane wz feeds the candidate planes wz - 3 .. wz;
 // their accumulators rotate through four register sets and a plane is scored
 // once its last window plane has been read.  The scores go to the shared
-// memory of a window plane already consumed; after the block-level top-2
+// memory of a window plane every warp has consumed (a CTA barrier per plane
+// makes sure of it; lanes without a block run the loop on placeholder data
+// and write nothing); after the block-level top-2
 // reduction one pass over them lists the candidates within 2 delta of the
 // block's FP32 second-best.  Blocks whose window is partly masked (window-AND
 // of the footprint flags) go to the masked kernel, blocks with a partly
-// masked base block to the general kernel.
+// masked base block to the base-mask kernel.
 // ---------------------------------------------------------------------------
-constexpr int kXMinBlocks = 12;
+constexpr int kXWarpsPerSM = 12;  // resident warps per SM aimed for
+constexpr int kXWarps = 2;        // warps per CTA
 
 struct XArgs {
   const uint8_t *wand;  // per block: window wholly inside the search mask
@@ -1177,10 +1181,10 @@ struct XArgs {
   long long ntiles;
 };
 
-template <int W>
-__global__ void __launch_bounds__(32, kXMinBlocks)
+template <int W, int NW>
+__global__ void __launch_bounds__(32 * NW, kXWarpsPerSM / NW)
     ncc_xlane_kernel(NccArgs a, XArgs xa, const __grid_constant__ CUtensorMap tmap) {
-  constexpr int R = W / 2, E = W + 3, BPW = 32 / W;
+  constexpr int R = W / 2, E = W + 3, NL = 32 * NW, BPW = NL / W;
   extern __shared__ __align__(16) float sm[];
   __shared__ __align__(8) uint64_t s_bar;
   // the tensor copy's destination starts on 128 bytes (the allocation has 128 spare)
@@ -1188,7 +1192,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
       sm + ((128u - ((unsigned int)__cvta_generic_to_shared(sm) & 127u)) & 127u) / sizeof(float));
   float *win = sma;                     // E * E * rpu
   float *xt = sma + E * E * xa.rpu;     // BPW * 64
-  float2 *qbuf = reinterpret_cast<float2 *>(xt + BPW * 64);  // 32 * W
+  float2 *qbuf = reinterpret_cast<float2 *>(xt + BPW * 64);  // NL * W
   __shared__ float s_red[BPW][W][2];
   __shared__ int s_deg[BPW][W][2];
   __shared__ float s_f[BPW][2];
@@ -1197,10 +1201,8 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
   const int lane = threadIdx.x;
   const int k = lane / W, x = lane - k * W;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const unsigned full = 0xffffffffu;
-  const unsigned seg = ((1u << W) - 1u) << (k < BPW ? k * W : 0);
   if (lane == 0) mbar_init(&s_bar, 1);
-  __syncwarp();
+  __syncthreads();
   unsigned int phase = 0;
   const unsigned int win_bytes = (unsigned int)(E * E * xa.rpu * sizeof(float));
 
@@ -1247,27 +1249,26 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
 #pragma unroll
     for (int cy = 0; cy < W; ++cy)
       if (oy + cy >= 0 && oy + cy <= ny - 4) yok |= 1u << cy;
-    const bool inmask = !state || xa.wand[b];
-    const unsigned bad = __ballot_sync(full, state && !inmask);
-    if (state && (bad & seg)) {
+    // a partly masked window sends the block (all of its lanes read the same
+    // flag) to the masked kernel
+    if (state && !xa.wand[b]) {
       if (x == 0) {
         unsigned int p = atomicAdd(&a.ctl[4], 1u);
         a.gen_list[a.nblocks + 1 + p] = (int)b;
       }
       state = 0;
     }
-    const unsigned act = __ballot_sync(full, state);
-    if (act == 0) continue;
+    if (!__syncthreads_or(state)) continue;
     // ---- staging: the union window by one tensor copy (zero outside the
     // volume), the base blocks (x~) by the lanes meanwhile --------------------
     const int rpu = xa.rpu;
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of win
-    __syncwarp();
+    __syncthreads();
     if (lane == 0) {
       mbar_expect_tx(&s_bar, win_bytes);
       tma_load_3d(win, &tmap, xu, oy, oz, &s_bar);
     }
-    for (int i = lane; i < nbt * 64; i += 32) {
+    for (int i = lane; i < nbt * 64; i += NL) {
       const int kk = i >> 6, v = i & 63;
       const int vx = v & 3, vy = (v >> 2) & 3, vz = v >> 4;
       const long long q = ((long long)(oz + R + vz) * ny + (oy + R + vy)) * nx +
@@ -1275,19 +1276,24 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
       const double mk = a.bstat[brow + bx0 + kk].mean;
       xt[i] = (float)__dsub_rn((double)__ldg(&a.base[q]), mk);
     }
-    if (!mbar_wait(&s_bar, phase, 1 << 22)) {
+    // the give-up decision is the CTA's, so no thread is left at a barrier
+    const bool landed = mbar_wait(&s_bar, phase, 1 << 22);
+    if (__syncthreads_or(!landed)) {
       if (lane == 0) atomicExch(&a.ctl[5], 1u);
       return;
     }
     phase ^= 1u;
-    __syncwarp();
+    __syncthreads();
     // ---- FP32 scores ---------------------------------------------------------
     float l1 = -3.f, l2 = -3.f;
     int d1 = -1, d2 = -1;
     const int E_rpu = E * rpu;
-    if (state) {
+    {
+      // every thread runs the plane loop (it holds CTA barriers); a lane
+      // without a block computes on its own placeholder data and writes nothing
+      const bool real = state != 0;
       float t[64];
-      const float4 *tp = reinterpret_cast<const float4 *>(xt + k * 64);
+      const float4 *tp = reinterpret_cast<const float4 *>(xt + (real ? k : 0) * 64);
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const float4 q = tp[i];
@@ -1297,7 +1303,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
       const float rsxx = sxx > 0.f ? 1.f / sxx : 0.f;
       float2 *qb = qbuf + lane * W;
       const float2 *st0 = a.stats + (((long long)oz * ny + oy) * nx + px);
-      const float *rp = win + (ox - xu) + x;
+      const float *rp = win + (real ? ox - xu : 0) + x;
       // acc[j]: candidate plane cz = wz - 3 + j.  Window plane wz feeds the
       // planes wz - 3 .. wz (j = 3 - vz); planes outside 0 .. W-1, fed at the
       // first and last three window planes, are never scored.
@@ -1309,7 +1315,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
 #pragma unroll 1
       for (int wz = 0; wz < E; ++wz) {
         const int cz = wz - 3;
-        const bool zok = cz >= 0 && xok && oz + cz >= 0 && oz + cz <= nz - 4;
+        const bool zok = real && cz >= 0 && xok && oz + cz >= 0 && oz + cz <= nz - 4;
         if (zok) {
           // statistics of the plane completed below, fetched meanwhile
 #pragma unroll
@@ -1335,9 +1341,9 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
               }
         }
         if (cz >= 0) {
-          // window plane cz was read three planes ago: its rows now hold the
-          // scores of candidate plane cz (lane-major, W per lane)
-          __syncwarp(act);
+          // window plane cz was read three planes ago by every warp: its rows
+          // now hold the scores of candidate plane cz (lane-major, W per lane)
+          __syncthreads();
           if (zok) {
             asm volatile("cp.async.wait_group 0;\n" ::: "memory");
             float *sc = win + cz * E_rpu + lane * W;
@@ -1369,7 +1375,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
       s_red[k][x][0] = l1; s_red[k][x][1] = l2;
       s_deg[k][x][0] = d1; s_deg[k][x][1] = d2;
     }
-    __syncwarp();
+    __syncthreads();
     if (state && x == 0) {
       float f1 = -3.f, f2 = -3.f;
       int e1 = -1, e2 = -1;
@@ -1380,7 +1386,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
       s_f[k][0] = f1; s_f[k][1] = f2;
       s_deg[k][0][0] = e1; s_deg[k][0][1] = e2;
     }
-    __syncwarp();
+    __syncthreads();
     if (state && xok) {
       // candidates within 2 delta of the block's FP32 second-best
       const float T2 = s_f[k][1] - 2.f * kDelta;
@@ -1399,7 +1405,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
         }
       }
     }
-    __syncwarp();
+    __syncthreads();
     if (state && x == 0) {
       NccRec &rc = a.rec[b];
       const float f1 = s_f[k][0], f2 = s_f[k][1];
@@ -1424,7 +1430,7 @@ __global__ void __launch_bounds__(32, kXMinBlocks)
         atomicAdd(a.xl_count, (unsigned long long)nval(ox, nx) * nval(oy, ny) * nval(oz, nz));
       }
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
@@ -1878,21 +1884,21 @@ EncodeTiledFn encode_tiled() {
 template <int W, class CM>
 mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
                            cudaEvent_t *kev) {
-  constexpr int E = W + 3, BPW = 32 / W;
+  constexpr int E = W + 3, NL = 32 * kXWarps, BPW = NL / W;
   done = false;
   const long long u = (long long)(BPW - 1) * a.G + E;   // union row length
   XArgs xa;
   xa.nch = (int)((u + 6) / 4);
   xa.rpu = 4 * xa.nch;
   // each window plane must hold one plane of scores (W per lane) once read
-  const int min_rpu = ((BPW * W + E - 1) / E + 3) & ~3;
+  const int min_rpu = ((BPW * W * W + E - 1) / E + 3) & ~3;
   if (xa.rpu < min_rpu) {
     xa.rpu = min_rpu;
     xa.nch = min_rpu / 4;
   }
   xa.tpr = (a.nbx + BPW - 1) / BPW;
   xa.ntiles = (long long)xa.tpr * a.nby * a.nbz;
-  const size_t smem = sizeof(float) * ((size_t)E * E * xa.rpu + BPW * 64 + 64 * W) + 128;
+  const size_t smem = sizeof(float) * ((size_t)E * E * xa.rpu + BPW * 64 + 2 * NL * W) + 128;
   if (xa.rpu > 256 || smem > 64 * 1024) return MIRORR_OK;  // tensor box limit
   // rows of the search image must start on 16 bytes for the 16-byte copies
   a.search_al = a.search;
@@ -1942,10 +1948,11 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
       return MIRORR_ECUDA;
     }
   }
-  MB2_TRY(set_smem(ncc_xlane_kernel<W>, smem));
-  const long long grid = xa.ntiles < 148LL * kXMinBlocks ? xa.ntiles : 148LL * kXMinBlocks;
+  MB2_TRY(set_smem(ncc_xlane_kernel<W, kXWarps>, smem));
+  constexpr long long kCtas = 148LL * (kXWarpsPerSM / kXWarps);
+  const long long grid = xa.ntiles < kCtas ? xa.ntiles : kCtas;
   if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[0], s));
-  ncc_xlane_kernel<W><<<(unsigned)grid, 32, smem, s>>>(a, xa, tmap);
+  ncc_xlane_kernel<W, kXWarps><<<(unsigned)grid, NL, smem, s>>>(a, xa, tmap);
   MB2_LAUNCH_CHECK();
   if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[1], s));
   MB2_TRY((launch_masked<CM>(a, s)));

@@ -35,6 +35,9 @@ CASES = [
     dict(id="bw4_w7_G2_nx39", shape=(39, 30, 22), bw=4, nw=7, g=1, G=2, keep=1.0, mask=None, seed=10),
     dict(id="bw5_w11_G3_masked", shape=(40, 36, 30), bw=5, nw=11, g=1, G=3, keep=1.0, mask="search",
          seed=11),
+    # block spacing 1: the densest union window (scores fill whole window planes)
+    dict(id="bw4_w9_G1", shape=(30, 26, 22), bw=4, nw=9, g=1, G=1, keep=1.0, mask="search", seed=14),
+    dict(id="bw4_w7_G1", shape=(28, 24, 20), bw=4, nw=7, g=1, G=1, keep=1.0, mask=None, seed=15),
     # partly masked base blocks with the other register-blocked geometries
     dict(id="bw4_w7_G2_basemask", shape=(34, 30, 24), bw=4, nw=7, g=1, G=2, keep=1.0, mask="both",
          seed=12),
