@@ -92,9 +92,9 @@ __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict_
   const long long n = (long long)ngx * ny * nz;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
        p += (long long)gridDim.x * blockDim.x) {
-    const int x0 = (int)(p % ngx) * PX;
-    const int yy = (int)((p / ngx) % ny);
-    const int z = (int)(p / ((long long)ngx * ny));
+    int gx, yy, z;
+    split3(p, ngx, ny, gx, yy, z);
+    const int x0 = gx * PX;
     const long long o = ((long long)z * ny + yy) * nx + x0;
     const bool rowok = yy <= ny - BW && z <= nz - BW;
     double sum[PX], mean[PX], ss[PX];

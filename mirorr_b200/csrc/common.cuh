@@ -106,4 +106,22 @@ struct HostBuf {
 
 inline int64_t vox(const int32_t s[3]) { return (int64_t)s[0] * s[1] * s[2]; }
 
+#ifdef __CUDACC__
+// Splits a linear index o of an (n0, n1, ...) grid, x fastest, into i (along
+// n0), j (along n1) and k (the rest); 32-bit division when o fits.
+__device__ __forceinline__ void split3(long long o, int n0, int n1, int &i, int &j, int &k) {
+  if (o < 0x7fffffffLL) {
+    const unsigned int u = (unsigned int)o, t = u / (unsigned int)n0;
+    i = (int)(u - t * (unsigned int)n0);
+    j = (int)(t % (unsigned int)n1);
+    k = (int)(t / (unsigned int)n1);
+  } else {
+    const long long t = o / n0;
+    i = (int)(o - t * n0);
+    j = (int)(t % n1);
+    k = (int)(t / n1);
+  }
+}
+#endif
+
 }  // namespace mb2

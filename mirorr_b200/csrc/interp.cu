@@ -21,9 +21,8 @@ __device__ inline double dsub(double a, double b) { return __dsub_rn(a, b); }
 
 __device__ inline void continuous_index(const ResampleMap &m, long long o, const int *on,
                                         double c[3]) {
-  const int i = (int)(o % on[0]);
-  const int j = (int)((o / on[0]) % on[1]);
-  const int k = (int)(o / ((long long)on[0] * on[1]));
+  int i, j, k;
+  split3(o, on[0], on[1], i, j, k);
   const double di = (double)i, dj = (double)j, dk = (double)k;
 #pragma unroll
   for (int r = 0; r < 3; ++r)

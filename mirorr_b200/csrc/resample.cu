@@ -38,9 +38,8 @@ __global__ void __launch_bounds__(256) resample_kernel(ResampleArgs a) {
   long long n = (long long)a.onx * a.ony * a.onz;
   for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n;
        o += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(o % a.onx);
-    const int j = (int)((o / a.onx) % a.ony);
-    const int k = (int)(o / ((long long)a.onx * a.ony));
+    int i, j, k;
+    split3(o, a.onx, a.ony, i, j, k);
     const double di = (double)i, dj = (double)j, dk = (double)k;
     double c[3];
 #pragma unroll
