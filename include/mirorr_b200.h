@@ -295,8 +295,10 @@ MIRORR_API mirorr_status mirorr_bm_last_timings(mirorr_matcher m, float ms[4]);
 /* Diagnostics of the last GetOffsets: [0] candidates re-scored in FP64 by the
  * exact refinement, [1] blocks re-scored entirely in FP64 (refinement list
  * overflow), [2] kept blocks, [3] blocks of the grid, [4] blocks searched by
- * the register-blocked FP32 kernel, [5] blocks searched by the general
- * (masked) FP32 kernel. */
+ * the register-blocked FP32 kernels with a base block inside its mask (window
+ * wholly or partly masked), [5] blocks with a partly masked base block (0 for
+ * geometries without register-blocked kernels, which search every block with
+ * the general kernel). */
 MIRORR_API mirorr_status mirorr_bm_last_diagnostics(mirorr_matcher m, int64_t out[6]);
 /* Count of kernels launched by this context since creation. */
 MIRORR_API int64_t mirorr_ctx_kernel_launches(mirorr_ctx ctx);

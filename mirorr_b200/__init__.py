@@ -396,7 +396,8 @@ class BlockMatcher:
 
     def LastDiagnostics(self):
         """(FP64-refined candidates, fully re-scored blocks, kept blocks, grid blocks,
-        fast-path blocks, general-path blocks)."""
+        blocks scored by the register-blocked kernels (unmasked and masked
+        window), blocks with a partly masked base block)."""
         d = np.zeros(6, np.int64)
         _check(lib().mirorr_bm_last_diagnostics(self._h, _ptr(d)))
         return tuple(int(v) for v in d)

@@ -525,7 +525,7 @@ mirorr_status match_into(RegRun &r, const float *base, const uint8_t *bmask, con
     unsigned int ctl[8] = {0};
     MB2_CUDA_TRY(cudaMemcpyAsync(ctl, c->bmw.ncc_ctl.ptr, sizeof(ctl), cudaMemcpyDeviceToHost, c->stream));
     MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    printf("  matcher: %lld blocks, register-blocked %u, masked-window %u, general %u, "
+    printf("  matcher: %lld blocks, register-blocked %u, masked-window %u, base-mask %u, "
            "refined candidates %u, overflowed %u\n",
            g.nblocks, ctl[3], ctl[4], ctl[0], ctl[2], ctl[1]);
   }

@@ -81,9 +81,10 @@ struct NccArgs {
   uint8_t *status;
   unsigned long long *ncc_count;
   NccRec *rec;
-  int *gen_list;    // blocks for the general kernel
+  int *gen_list;    // [0, ctl[0]): partly masked base blocks (base-mask kernel);
+                    // after nblocks + 1: partly masked windows (masked kernel)
   int *ovf_list;    // blocks for the fallback kernel
-  unsigned int *ctl;  // [0] general blocks, [1] overflow blocks, [2] refined candidates,
+  unsigned int *ctl;  // [0] base-mask blocks, [1] overflow blocks, [2] refined candidates,
                       // [3] register-blocked blocks, [4] masked-window blocks,
                       // [5] a bounded wait on a tensor copy gave up
   const float *search_al;  // the search image with rows of spitch floats, 16-byte aligned
@@ -851,7 +852,7 @@ __global__ void __launch_bounds__(C::NT, 2) ncc_basemask_kernel(NccArgs a) {
 // staged as y - c (c: mean of the block's own candidate), so
 // Sxy = sum x~ (y - c) - (mu - c) sum x~ has no FP32 cancellation.  Blocks
 // with a partly masked window go to the masked kernel, blocks with a partly
-// masked base block to the general kernel.
+// masked base block to the base-mask kernel.
 // ---------------------------------------------------------------------------
 template <int BW_, int W_, int TY_, int SPW_, int WPC_, int MINB_>
 struct WarpCfg {

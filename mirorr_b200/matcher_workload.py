@@ -54,7 +54,7 @@ def main():
         out.append({"kept": int(bp.shape[0]), "ms_box_stats": float(t[0]),
                     "ms_selection": float(t[1]), "ms_ncc": float(t[2]),
                     "ms_postfilter": float(t[3]), "refined": d[0], "fallback_blocks": d[1],
-                    "fast_blocks": d[4], "general_blocks": d[5], "blocks": d[3]})
+                    "fast_blocks": d[4], "basemask_blocks": d[5], "blocks": d[3]})
     print(json.dumps(out[-1]))
     m.close()
     ctx.close()

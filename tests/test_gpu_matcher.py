@@ -108,7 +108,7 @@ def test_matcher_matches_oracle(ctx, c):
     assert kept == gp[0].shape[0] and nblocks == res.best.size
     assert refined >= int(res.status.sum()) - full
     print(f"{c['id']}: {refined} candidates refined in FP64 over {nblocks} blocks, "
-          f"{full} blocks fully re-scored, {nfast} fast-path / {ngen} general-path blocks")
+          f"{full} blocks fully re-scored, {nfast} register-blocked / {ngen} base-mask blocks")
 
 
 def test_swap_image_order(ctx):
