@@ -44,3 +44,14 @@ def test_sinc_copies_on_the_grid_and_follows_a_smooth_signal():
     out = O.resample_sinc(s, (40, 12, 12), np.eye(3), [0.5, 0.0, 0.0])
     np.testing.assert_allclose(out[6, 6, 8:30], np.sin(2 * np.pi * (x[8:30] + 0.5) / 16.0),
                                atol=5e-3)
+
+
+def test_bspline_short_lines_interpolate_the_samples():
+    # lines of length 1 and 2 (the full mirror-symmetric initial sum; the
+    # mirror boundary with period 2N - 2) still pass through the samples
+    rng = np.random.default_rng(2)
+    for shape in [(1, 2, 5), (2, 1, 3), (1, 1, 2)]:
+        img = rng.random(shape).astype(np.float32)
+        size = (shape[2], shape[1], shape[0])
+        out = O.resample_bspline(img, size, np.eye(3), [0.0, 0.0, 0.0])
+        np.testing.assert_allclose(out, img, rtol=0, atol=2e-6)
