@@ -11,14 +11,21 @@ Workload (one "step" = one full registration, the reference's
 Arms:
   default       the CUDA path.  `value` = registrations/s with the inputs
                 already in HBM (device-timed with CUDA events on the library's
-                stream, max over ranks); `e2e` = the same through the C ABI
-                from pinned host buffers (uploads inside the timed step,
-                result read back).
+                stream, max over ranks, in-library profiling off); `e2e` = the
+                same through the C ABI from pinned host buffers (uploads inside
+                the timed step, result read back).  After the timed steps: a
+                profiled pass (kernel rooflines), the selector leg, and on
+                rank 0 at N=1 the FP64 oracle's registration of the same pair
+                (matrix error, TRE, argmax agreement; its time is the CPU
+                baseline).
   --impl reference
-                the reference's CPU block matcher, restated in C
-                (oracle/mirorr_oracle.c, threaded with the reference's slab
-                split) on all host cores, on a bounded sample of the workload;
-                registrations/s extrapolated from its block-NCC rate.
+                the reference's CPU path restated (oracle/: the C block
+                matcher threaded with the reference's slab split, FP64 LTS,
+                resampler and loop) running full registrations of the same pair
+                on all host cores, as many as fit a time budget.
+
+Profiling legs (`--leg matcher|resample`): one finest-level matcher call or
+the final-resampling interpolators on the same pair, for ncu captures.
 
 Multi-GPU: registrations are independent, so N ranks run N replicas, each its
 own pair (weak scaling, no collective on the data path).
@@ -51,6 +58,16 @@ BASELINE_METRIC = ("registrations/s & p50/p99 latency at ≤1e-4 matrix err; "
 WORKLOAD = ("symmetric affine registration, 256x256x128 float32 phantom pair (80 Gaussians), "
             "3 pyramid levels, block 4, radius 4 (729 candidates), block spacing 3, "
             "LTS keep 0.5, 10 iterations/level")
+# seconds of full CPU registrations the reference arm times at most (at least one)
+REFERENCE_BUDGET_S = 240.0
+
+
+def config():
+    """The workload description both arms print (identical by construction)."""
+    return {"workload": WORKLOAD, "shape": list(SHAPE), "levels": LEVELS,
+            "iterations_per_level": ITERS, "block_width": BW, "nhood_width": NW,
+            "nhood_gap": G, "block_keep": 1.0, "lts_keep": LTS_KEEP, "mode": "symmetric",
+            "transform": "affine", "baseline_metric": BASELINE_METRIC}
 
 
 def traffic_bytes_per_candidate():
@@ -139,6 +156,10 @@ def reg_params(mb):
                          lts_keep=LTS_KEEP)
 
 
+def oracle_params(O):
+    return O.RegParams("symmetric", "affine", ITERS, O.BMParams(BW, 1, G, NW, 1.0), LTS_KEEP)
+
+
 def dist_setup(n):
     if n <= 1 or "RANK" not in os.environ:
         return 0, 1, None
@@ -149,6 +170,19 @@ def dist_setup(n):
     torch.cuda.set_device(local)
     dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     return dist.get_rank(), dist.get_world_size(), dist
+
+
+def cpu_info():
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return os.cpu_count() or 1, model
 
 
 def run_cuda(args):
@@ -189,14 +223,15 @@ def run_cuda(args):
         if dist is not None:
             dist.barrier()
 
-    def timed(fn, profile):
+    def timed(fn, steps, profile):
         times, stats, res = [], [], None
         ctx.set_profiling(profile)
         ctx.stage_times()
         if profile:
             ctx.search_kernel_times()
+            ctx.resample_times()
         l0 = ctx.kernel_launches()
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.fill_(1.0)  # L2 flush between steps, outside the events
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
@@ -210,15 +245,16 @@ def run_cuda(args):
         launches = ctx.kernel_launches() - l0
         stage_ms, calls = ctx.stage_times()
         kern = ctx.search_kernel_times() if profile else (0.0, 0, 0)
+        rs = ctx.resample_times() if profile else (0.0, 0, 0)
         ctx.set_profiling(False)
-        return times, stats, res, launches, (stage_ms, kern), calls
+        return times, stats, res, launches, (stage_ms, kern, rs), calls
 
     sampler = ClockSampler(dev)
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    t_dev, st_dev, res_dev, launches, (stage_ms, kern), calls = timed(step_device, True)
-    t_e2e, st_e2e, res_e2e, _, _, _ = timed(step_e2e, False)
+    t_dev, st_dev, res_dev, launches, _, _ = timed(step_device, args.steps, False)
+    t_e2e, st_e2e, res_e2e, _, _, _ = timed(step_e2e, args.steps, False)
     clocks = sampler.stop()
     torch.cuda.synchronize()
     barrier()
@@ -233,12 +269,16 @@ def run_cuda(args):
     value = regs / (total_dev / 1e3)
     e2e_value = regs / (total_e2e / 1e3)
     ncc = st_dev[-1].block_ncc_evaluated
+
+    # ---- profiled pass (not part of `value`): kernel rooflines ----------------
+    n_prof = max(1, min(3, args.steps))
+    _, _, _, _, (stage_ms, kern, rs), calls = timed(step_device, n_prof, True)
     peaks, peak_src = load_peaks()
-    # Roofline of the dominant kernel, the per-x-lane FP32 NCC search: FP32 FMA
-    # bound, 2*B algorithmic flops per block-NCC (the cross term; mean and sum
-    # of squares come from box_stats).  Its launches are bracketed by CUDA
-    # events on the context's stream and a device counter adds up the
-    # candidates it scores.
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    # The dominant kernel, the per-x-lane FP32 NCC search: FP32 FMA bound, 2*B
+    # algorithmic flops per block-NCC (the cross term; mean and sum of squares
+    # come from box_stats).  Its launches are bracketed by CUDA events on the
+    # context's stream and a device counter adds up the candidates it scores.
     flops_per_ncc = 2 * BW ** 3
     k_ms, k_launches, k_cands = kern
     k_avg_ms = k_ms / max(k_launches, 1)
@@ -248,26 +288,25 @@ def run_cuda(args):
     bpc = traffic_bytes_per_candidate()
     traffic = round(bpc * k_cands_per_launch) if bpc else None
     ncc_ms_per_call = stage_ms[2] / max(calls, 1)
-    ncc_per_call = sum(s.block_ncc_evaluated for s in st_dev) / max(
-        sum(s.matcher_calls for s in st_dev), 1)
-    err = tre(res_dev.M, res_dev.off, ph.true_matrix, ph.true_offset, SHAPE, ph.spacing)
-    d_e2e = np.max(np.abs(res_e2e.M - res_dev.M))
+    # resampler: 10 algorithmic bytes per output voxel of an image + mask pass
+    # (float32 image 4 B read + 4 B written, uint8 mask 1 B + 1 B)
+    rs_ms, rs_passes, rs_vox = rs
+    rs_gbs = 10.0 * rs_vox / (rs_ms / 1e3) / 1e9 if rs_ms > 0 else 0.0
+
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": "registrations/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total_dev / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "shape": list(SHAPE), "levels": LEVELS,
-                   "iterations_per_level": ITERS, "block_width": BW, "nhood_width": NW,
-                   "nhood_gap": G, "lts_keep": LTS_KEEP, "mode": "symmetric", "transform": "affine",
-                   "parallelism": f"replicas{world}", "l2": "flushed (256 MB write) between steps",
-                   "baseline_metric": BASELINE_METRIC},
+        "config": config(),
+        "parallelism": f"replicas{world}", "l2": "flushed (256 MB write) between steps",
         "latency_ms": {"p50": round(float(np.percentile(t_dev, 50)), 3),
                        "p99": round(float(np.percentile(t_dev, 99)), 3)},
         "gblock_ncc_per_s": round(ncc * args.steps * world / (total_dev / 1e3) / 1e9, 3),
         "block_ncc_per_registration": int(ncc),
-        "tre_mm": round(err, 4),
-        "e2e_vs_device_max_matrix_diff": float(d_e2e),
+        "tre_mm": round(tre(res_dev.M, res_dev.off, ph.true_matrix, ph.true_offset, SHAPE,
+                            ph.spacing), 4),
+        "e2e_vs_device_max_matrix_diff": float(np.max(np.abs(res_e2e.M - res_dev.M))),
         "e2e": {"value": round(e2e_value, 4), "unit": "registrations/s",
                 "h2d_bytes_per_step": int(st_e2e[-1].h2d_bytes),
                 "d2h_bytes_per_step": int(st_e2e[-1].d2h_bytes),
@@ -287,14 +326,30 @@ def run_cuda(args):
                                        "capture in profiles/ncc_xlane_kernel_256x256x128.md, "
                                        "times this run's candidates per launch",
                      "ncc_stage_ms_per_call": round(ncc_ms_per_call, 4),
-                     "ncc_stage_block_ncc_per_call": round(ncc_per_call)},
-        "stage_ms_per_registration": {k: round(v / args.steps, 3) for k, v in
+                     "timed_in": f"a separate profiled pass of {n_prof} registrations"},
+        "roofline_secondary": [
+            {"kernel": "resample_kernel (image + mask pass, all levels)", "bound": "hbm",
+             "achieved": round(rs_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+             "frac": round(rs_gbs / hbm_peak, 4), "passes": int(rs_passes),
+             "avg_pass_ms": round(rs_ms / max(rs_passes, 1), 4),
+             "voxels_per_pass": round(rs_vox / max(rs_passes, 1)),
+             "bytes_per_voxel": 10, "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_src})"},
+        ],
+        "stage_ms_per_registration": {k: round(v / n_prof, 3) for k, v in
                                       zip(["box_stats", "selection", "ncc", "postfilter"], stage_ms)},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
-    if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args, sample_only=True)
+    if rank == 0:
+        sel = selector_leg(mb, ctx, ph, hbm_peak, peak_src)
+        if sel:
+            out["roofline_secondary"].append(sel)
+        out["roofline_secondary"].append(resample_finest_leg(mb, ctx, ph, dev, hbm_peak,
+                                                             peak_src))
+    if rank == 0 and world == 1 and not args.no_parity:
+        par, cpu = parity_leg(mb, ctx, ph, res_dev, args)
+        out["parity"] = par
+        out["cpu_baseline"] = cpu
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -302,85 +357,236 @@ def run_cuda(args):
         dist.destroy_process_group()
 
 
-def registration_ncc_counts():
-    """Block-NCC evaluations per matcher call at each level (all blocks)."""
-    from oracle import oracle as O
-    out = []
-    ms, _ = O.pyramid_schedule(SHAPE, SHAPE, np.ones(3), np.ones(3), 32, LEVELS)
-    for f in ms:
-        size = tuple(int(s // fi) for s, fi in zip(SHAPE, f))
-        nb, st = O.block_grid(size, BW, G)
-        per_axis = []
-        for d in range(3):
-            tot = 0
-            for b in range(nb[d]):
-                o = st[d] + b * G
-                lo = max(0, o - NW // 2)
-                hi = min(size[d] - BW, o + NW // 2)
-                tot += hi - lo + 1
-            per_axis.append(tot)
-        out.append(per_axis[0] * per_axis[1] * per_axis[2])
-    return out
+def selector_leg(mb, ctx, ph, hbm_peak, peak_src, calls=5):
+    """Block-variance selection (keep the top half of the blocks by variance)
+    on the 256x256x128 pair at block 4, spacing 3: the selection stage's
+    CUDA-event time per call.  Algorithmic bytes: 4 per base voxel read + 8 per
+    block key."""
+    m = mb.BlockMatcher(ctx)
+    m.SetBlockWidth(BW)
+    m.SetNhoodWidth(NW)
+    m.SetNhoodGap(G)
+    m.SetBlockKeep(0.5)
+    m.SetBaseImage(ph.moving, ph.spacing, ph.origin)
+    m.SetSearchImage(ph.fixed, ph.spacing, ph.origin)
+    ts = []
+    for i in range(calls + 1):
+        m.GetOffsets()
+        if i:
+            ts.append(float(m.LastTimings()[1]))
+    nb = int(np.prod(m.Grid()[0]))
+    m.close()
+    ms = statistics.median(ts)
+    nbytes = 4 * ph.moving.size + 8 * nb
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"kernel": "variance selection (block_variance_kernel + radix select passes)",
+            "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(gbs / hbm_peak, 4), "ms_per_call": round(ms, 4), "blocks": nb,
+            "algorithmic_bytes": int(nbytes), "block_keep": 0.5,
+            "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_src})"}
 
 
-def cpu_baseline(args, sample_only=False):
-    """The reference CPU matcher (oracle/mirorr_oracle.c restatement, threaded
-    as itkBlockMatcherThreaded) timed on a bounded sample: the finest level's
-    matcher on a 16-slice slab of the pair.  Registrations/s are extrapolated
-    from the measured block-NCC rate (10 iterations x 2 matcher calls per level)."""
+def resample_finest_leg(mb, ctx, ph, dev, hbm_peak, peak_src, reps=10):
+    """One image + mask resampling pass at the finest level's size (the pass a
+    symmetric iteration makes twice): 256x256x128 float32 image and uint8 mask
+    through an affine map, device buffers, CUDA events; 10 algorithmic bytes
+    per output voxel."""
+    import torch
+    from mirorr_b200.phantom import random_rotation
+    rng = np.random.default_rng(5)
+    g = mb.Geometry.of(ph.moving, ph.spacing, ph.origin)
+    C, e = mb.resample_map(g, g, random_rotation(rng, 4.0) @ np.diag([1.02, 0.98, 1.0]),
+                           rng.uniform(-3, 3, 3))
+    img = torch.from_numpy(ph.moving).to(f"cuda:{dev}")
+    msk = torch.full(ph.moving.shape, 255, dtype=torch.uint8, device=f"cuda:{dev}")
+    out = torch.empty_like(img)
+    outm = torch.empty_like(msk)
+    size = (SHAPE[0], SHAPE[1], SHAPE[2])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    ts = []
+    for i in range(reps + 2):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mb.resample_device(ctx, img.data_ptr(), msk.data_ptr(), size, size, C, e,
+                           out.data_ptr(), outm.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        if i >= 2:
+            ts.append(e0.elapsed_time(e1))
+    ms = statistics.median(ts)
+    nbytes = 10 * ph.moving.size
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"kernel": "resample_kernel, image + mask in one launch, 256x256x128 (finest level)",
+            "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(gbs / hbm_peak, 4), "ms_per_launch": round(ms, 4),
+            "voxels": int(ph.moving.size), "bytes_per_voxel": 10, "l2": "flushed before each",
+            "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_src})"}
+
+
+def parity_leg(mb, ctx, ph, res_dev, args):
+    """The FP64 oracle's registration of the same pair on all host cores
+    (outside every timed region): final matrix and offset error of the GPU
+    result against it, both TREs, and the argmax agreement of one
+    finest-size matcher call.  The oracle's wall time is the CPU baseline."""
     from oracle import oracle as O
-    ph = make_pair(seed=1000)
-    threads = os.cpu_count() or 1
-    slab = slice(56, 72)
-    base = np.ascontiguousarray(ph.moving[slab])
-    search = np.ascontiguousarray(ph.fixed[slab])
-    p = O.BMParams(BW, 1, G, NW, 1.0)
-    O.lib()
+    from mirorr_b200.phantom import tre
+    threads, model = cpu_info()
+    fixed = O.Image(ph.fixed, ph.spacing, ph.origin)
+    moving = O.Image(ph.moving, ph.spacing, ph.origin)
     t0 = time.perf_counter()
-    r = O.match_blocks(base, search, None, None, p, threads=threads)
+    to = O.register(fixed, moving, oracle_params(O), LEVELS, threads=threads)
     dt = time.perf_counter() - t0
-    nb = r.best.size
-    # candidates evaluated in the sample
-    size = (base.shape[2], base.shape[1], base.shape[0])
-    per_axis = []
-    for d in range(3):
-        tot = 0
-        for b in range(r.nblocks[d]):
-            o = r.start[d] + b * G
-            tot += min(size[d] - BW, o + NW // 2) - max(0, o - NW // 2) + 1
-        per_axis.append(tot)
-    sample_ncc = per_axis[0] * per_axis[1] * per_axis[2]
-    rate = sample_ncc / dt
-    per_reg = sum(registration_ncc_counts()) * ITERS * 2
-    value = rate / per_reg
-    return {"value": round(value, 6), "unit": "registrations/s", "cores": threads, "kind": "port",
-            "sample": f"finest-level matcher on a 16-slice slab ({nb} blocks, {sample_ncc} "
-                      f"block-NCCs) in {dt:.2f} s; extrapolated to {per_reg} block-NCCs per "
-                      "registration (3 levels x 10 iterations x 2 calls)",
-            "block_ncc_per_s": round(rate, 1)}
+    dM = float(np.max(np.abs(res_dev.M - to.M)))
+    doff = float(np.max(np.abs(res_dev.off - to.off)))
+    # argmax agreement on a finest-size call (base = moving, search = fixed)
+    m = mb.BlockMatcher(ctx)
+    m.SetBlockWidth(BW)
+    m.SetNhoodWidth(NW)
+    m.SetNhoodGap(G)
+    m.SetBaseImage(ph.moving, ph.spacing, ph.origin)
+    m.SetSearchImage(ph.fixed, ph.spacing, ph.origin)
+    m.GetOffsets()
+    mi, best, second, status = m.BlockResults()
+    m.close()
+    ref = O.match_blocks(ph.moving, ph.fixed, None, None, O.BMParams(BW, 1, G, NW, 1.0),
+                         threads=threads)
+    s = ref.status == 1
+    same = np.all(mi == ref.match, axis=1)[s]
+    gap = (ref.best.astype(np.float64) - ref.second)[s]
+    clear = gap > 1e-4
+    par = {"oracle": "FP64 CPU restatement (oracle/), same inputs and parameters",
+           "max_abs_dM_vs_oracle": dM, "max_abs_doffset_mm_vs_oracle": doff,
+           "within_1e-4": bool(dM <= 1e-4),
+           "tre_mm_gpu": round(tre(res_dev.M, res_dev.off, ph.true_matrix, ph.true_offset, SHAPE,
+                                   ph.spacing), 5),
+           "tre_mm_oracle": round(tre(to.M, to.off, ph.true_matrix, ph.true_offset, SHAPE,
+                                      ph.spacing), 5),
+           "finest_call_blocks": int(s.sum()),
+           "finest_call_argmax_agreement": round(float(same.mean()), 6),
+           "finest_call_argmax_agreement_gap_gt_1e-4": round(float(same[clear].mean()), 6),
+           "finest_call_scores_bit_identical": bool(np.array_equal(best[s], ref.best[s]) and
+                                                    np.array_equal(second[s], ref.second[s]))}
+    cpu = {"value": round(1.0 / dt, 6), "unit": "registrations/s", "cores": threads,
+           "kind": "port", "cpu_model": model,
+           "sample": f"one full registration of the same pair by the FP64 oracle in {dt:.1f} s "
+                     f"({threads} threads in the block matcher)"}
+    return par, cpu
 
 
 def run_reference(args):
+    """Full CPU registrations of the workload by the reference's path restated
+    (oracle/), as many as fit REFERENCE_BUDGET_S (at least one, at most
+    --steps); the warm-up is one small registration that loads the code."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    samples = []
-    for _ in range(max(args.warmup, 0)):
-        cpu_baseline(args)
-    for _ in range(args.steps):
-        samples.append(cpu_baseline(args))
-    v = statistics.median([s["value"] for s in samples])
-    out = {"metric": METRIC, "value": v, "unit": "registrations/s", "impl": "reference",
-           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": round(1e3 / v, 1) if v else None, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "shape": list(SHAPE), "levels": LEVELS,
-                      "iterations_per_level": ITERS, "block_width": BW, "nhood_width": NW,
-                      "nhood_gap": G, "parallelism": "cpu threads"},
-           "cpu_baseline": dict(samples[-1], value=v),
-           "e2e": {"value": v, "unit": "registrations/s", "h2d_bytes_per_step": 0,
+    from oracle import oracle as O
+    from mirorr_b200.phantom import make_phantom
+    threads, model = cpu_info()
+    O.lib()
+    if args.warmup > 0:
+        w = make_phantom((48, 48, 32), n_gauss=10, kind="affine", seed=1)
+        O.register(O.Image(w.fixed), O.Image(w.moving), oracle_params(O), 1, threads=threads)
+    ph = make_pair(seed=1000)
+    fixed = O.Image(ph.fixed, ph.spacing, ph.origin)
+    moving = O.Image(ph.moving, ph.spacing, ph.origin)
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max(args.steps, 1):
+        t0 = time.perf_counter()
+        O.register(fixed, moving, oracle_params(O), LEVELS, threads=threads)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start + times[-1] > REFERENCE_BUDGET_S:
+            break
+    total = sum(times)
+    v = len(times) / total
+    out = {"metric": METRIC, "value": round(v, 6), "unit": "registrations/s", "impl": "reference",
+           "n_gpus": args.gpus, "steps": len(times), "steps_requested": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(1e3 * total / len(times), 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": config(), "parallelism": f"cpu threads ({threads})",
+           "latency_ms": {"p50": round(1e3 * float(np.percentile(times, 50)), 1),
+                          "p99": round(1e3 * float(np.percentile(times, 99)), 1)},
+           "cpu_baseline": {"value": round(v, 6), "unit": "registrations/s", "cores": threads,
+                            "kind": "port", "cpu_model": model,
+                            "sample": f"{len(times)} full registrations of the workload "
+                                      f"({total:.1f} s); the steps that fit "
+                                      f"{REFERENCE_BUDGET_S:.0f} s of the {args.steps} asked for"},
+           "e2e": {"value": round(v, 6), "unit": "registrations/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+def run_leg(args):
+    """Profiling legs for ncu captures (one GPU, small and bounded)."""
+    import mirorr_b200 as mb
+    from mirorr_b200.phantom import make_phantom
+    shape = tuple(int(v) for v in args.shape.split(","))
+    ph = make_phantom(shape, n_gauss=80, kind="affine", seed=1000, max_angle_deg=8.0,
+                      max_shift_vox=12.0)
+    ctx = mb.Context(0)
+    if args.leg == "matcher":
+        # one finest-level matcher call of the benchmark (block 4, radius 4,
+        # spacing 3); --masked gives the search image a 10-voxel field-of-view
+        # shell of mask 0, --base-masked the base image a 12-voxel one
+        m = mb.BlockMatcher(ctx)
+        m.SetBlockWidth(BW)
+        m.SetNhoodWidth(NW)
+        m.SetNhoodGap(G)
+        m.SetBlockKeep(args.block_keep)
+        m.SetBaseImage(ph.moving)
+        m.SetSearchImage(ph.fixed)
+        if args.masked:
+            sm = np.zeros(ph.fixed.shape, np.uint8)
+            sm[10:-10, 10:-10, 10:-10] = 255
+            m.SetSearchMask(sm)
+        if args.base_masked:
+            bm = np.zeros(ph.moving.shape, np.uint8)
+            bm[12:-12, 12:-12, 12:-12] = 255
+            m.SetBaseMask(bm)
+        res = None
+        for _ in range(args.calls):
+            bp, _ = m.GetOffsets()
+            t = m.LastTimings()
+            d = m.LastDiagnostics()
+            res = {"kept": int(bp.shape[0]), "ms_box_stats": float(t[0]),
+                   "ms_selection": float(t[1]), "ms_ncc": float(t[2]),
+                   "ms_postfilter": float(t[3]), "refined": d[0], "fallback_blocks": d[1],
+                   "fast_blocks": d[4], "basemask_blocks": d[5], "blocks": d[3]}
+        print(json.dumps(res))
+        m.close()
+    elif args.leg == "resample":
+        # final resampling through a small rigid transform with each
+        # interpolator, host buffers (upload and read-back included)
+        from mirorr_b200.phantom import random_rotation
+        img = ph.moving
+        rng = np.random.default_rng(3)
+        M = random_rotation(rng, 6.0)
+        geom = mb.Geometry.of(img, ph.spacing, ph.origin)
+        C, e = mb.resample_map(geom, geom, M, rng.uniform(-3, 3, 3))
+        size = (img.shape[2], img.shape[1], img.shape[0])
+        calls = {
+            "nn": lambda: mb.resample(ctx, img, None, size, C, e, nearest=True),
+            "linear": lambda: mb.resample(ctx, img, None, size, C, e),
+            "bspline": lambda: mb.resample_final(ctx, img, size, C, e, "bspline"),
+            "sinc": lambda: mb.resample_final(ctx, img, size, C, e, "sinc"),
+        }
+        out = {"shape_xyz": list(size), "voxels": int(img.size)}
+        for name, fn in calls.items():
+            fn()
+            ts = []
+            for _ in range(args.calls):
+                t0 = time.perf_counter()
+                fn()
+                ts.append(time.perf_counter() - t0)
+            ms = float(np.median(ts) * 1e3)
+            out[name] = {"ms_per_call": round(ms, 3), "voxels_per_s": float(img.size / (ms * 1e-3))}
+        print(json.dumps(out))
+    ctx.close()
 
 
 def main():
@@ -389,9 +595,18 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the FP64 oracle registration (parity and CPU baseline)")
+    ap.add_argument("--leg", choices=["matcher", "resample"], default=None)
+    ap.add_argument("--calls", type=int, default=3)
+    ap.add_argument("--shape", default="256,256,128")
+    ap.add_argument("--masked", action="store_true")
+    ap.add_argument("--base-masked", action="store_true")
+    ap.add_argument("--block-keep", type=float, default=1.0)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.leg:
+        run_leg(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_cuda(args)

@@ -141,6 +141,15 @@ MIRORR_API mirorr_status mirorr_resample(mirorr_ctx ctx, const int32_t in_size[3
                               const uint8_t *in_mask, const int32_t out_size[3],
                               const double C[9], const double e[3], float *out_image,
                               uint8_t *out_mask);
+/* mirorr_resample (nearest != 0: mirorr_resample_nearest) on device buffers
+ * of the context's device: in_image / out_image float32, in_mask / out_mask
+ * uint8, either pair may be NULL; out_image 16-byte and out_mask 4-byte
+ * aligned.  Issued on the context's stream; returns without waiting for it. */
+MIRORR_API mirorr_status mirorr_resample_device(mirorr_ctx ctx, const int32_t in_size[3],
+                                     const float *in_image, const uint8_t *in_mask,
+                                     const int32_t out_size[3], const double C[9],
+                                     const double e[3], float *out_image, uint8_t *out_mask,
+                                     int32_t nearest);
 /* The same with itk::NearestNeighborInterpolateImageFunction (index
  * floor(c + 0.5)), the final resampling's "nn" interpolator
  * (itkMirorrPyramidImplement.txx:365-479). */
@@ -207,15 +216,20 @@ MIRORR_API mirorr_status mirorr_lts_symmetric(mirorr_ctx ctx, mirorr_transform *
  * when another allocator (the caching allocator of a serving process, say)
  * already holds the free memory.  Results equal mirorr_lts_classic /
  * mirorr_lts_symmetric on the same pairs.
- *   - The first call on a device does the set-up (it looks up the array's
- *     address and the cooperative-launch size); make it before any stream
- *     capture.
- *   - n > MIRORR_LTS_NOALLOC_MAX_POINTS returns MIRORR_ERANGE; host pointers
- *     or pointers on another device return MIRORR_EINVAL.
+ *   - The first call on a device does the set-up: it loads the library's
+ *     device code on that device if nothing has yet (which is when the
+ *     array's memory is reserved), looks up the array's address and the
+ *     cooperative-launch size.  Make that first call early, before a caching
+ *     allocator takes the free device memory; later calls reserve nothing.
+ *   - n > MIRORR_LTS_NOALLOC_MAX_POINTS returns MIRORR_ERANGE; host pointers,
+ *     pointers on another device, and arrays shorter than n x 3 doubles
+ *     return MIRORR_EINVAL.
  *   - All calls on one device share the array: calls that overlap in time
  *     (several threads, contexts or streams) race and give wrong results.
- *   - Like the other LTS entry points it copies the fit state in and out and
- *     synchronises the context's stream before returning. */
+ *   - Like the other LTS entry points it copies the fit state in and out
+ *     through pageable host memory and synchronises the context's stream
+ *     before returning, so it cannot be called while that stream is being
+ *     captured into a CUDA graph. */
 #define MIRORR_LTS_NOALLOC_MAX_POINTS 524288
 MIRORR_API mirorr_status mirorr_lts_noalloc(mirorr_ctx ctx, mirorr_transform *t, mirorr_transform *t12f,
                                  mirorr_transform *t12b, size_t n, const double *initial_dev,
@@ -318,6 +332,21 @@ MIRORR_API mirorr_status mirorr_ctx_stage_times(mirorr_ctx ctx, double ms[4], in
  * profiling aid with no counterpart in the reference. */
 MIRORR_API mirorr_status mirorr_ctx_search_kernel_times(mirorr_ctx ctx, double *ms, int64_t *launches,
                                              int64_t *candidates);
+/* With profiling on, CUDA events also bracket each resampling pass of a
+ * registration (an image and its mask into the middle-space grid; one launch
+ * when both share an input grid, two otherwise).  Returns the accumulated
+ * milliseconds, passes and output voxels, and resets them.  A profiling aid
+ * with no counterpart in the reference. */
+MIRORR_API mirorr_status mirorr_ctx_resample_times(mirorr_ctx ctx, double *ms, int64_t *passes,
+                                        int64_t *voxels);
+/* A test aid with no counterpart in the reference: the number of polls a
+ * grid-barrier wait of the LTS kernel makes before it gives up (0 restores the
+ * default of 2^23 polls, about 0.84 s).  When a wait gives up, every CTA of the
+ * launch returns, the call returns MIRORR_ETIMEOUT, the caller's transforms
+ * are left as they were, and the context stays usable.  A tiny limit makes the
+ * waits give up on CTAs that are merely late, which is how the tests reach
+ * that path without a fault. */
+MIRORR_API mirorr_status mirorr_ctx_set_wait_limit(mirorr_ctx ctx, int64_t polls);
 
 #ifdef __cplusplus
 }

@@ -163,6 +163,7 @@ def lib():
         "mirorr_resample_map": [P(Geometry), P(Geometry), vp, vp, vp, vp],
         "mirorr_resample_nearest": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
         "mirorr_resample_bspline": [vp, vp, vp, vp, vp, vp, vp],
+        "mirorr_resample_device": [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int32],
         "mirorr_resample_sinc": [vp, vp, vp, vp, vp, vp, vp],
         "mirorr_lts_classic": [vp, P(Transform), ctypes.c_size_t, vp, vp, ctypes.c_double,
                                P(ctypes.c_int32)],
@@ -197,6 +198,11 @@ def lib():
     L.mirorr_ctx_search_kernel_times.restype = st
     L.mirorr_ctx_search_kernel_times.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_int64),
                                                  P(ctypes.c_int64)]
+    L.mirorr_ctx_resample_times.restype = st
+    L.mirorr_ctx_resample_times.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_int64),
+                                            P(ctypes.c_int64)]
+    L.mirorr_ctx_set_wait_limit.restype = st
+    L.mirorr_ctx_set_wait_limit.argtypes = [vp, ctypes.c_int64]
     _lib = L
     return L
 
@@ -257,6 +263,20 @@ class Context:
         _check(lib().mirorr_ctx_search_kernel_times(self._h, ctypes.byref(ms), ctypes.byref(launches),
                                                     ctypes.byref(cands)))
         return ms.value, launches.value, cands.value
+
+    def resample_times(self):
+        """(ms, passes, output voxels) of the registrations' resampling passes
+        since the last read (profiling on)."""
+        ms = ctypes.c_double(0.0)
+        passes = ctypes.c_int64(0)
+        voxels = ctypes.c_int64(0)
+        _check(lib().mirorr_ctx_resample_times(self._h, ctypes.byref(ms), ctypes.byref(passes),
+                                               ctypes.byref(voxels)))
+        return ms.value, passes.value, voxels.value
+
+    def set_wait_limit(self, polls: int):
+        """Polls of an LTS grid-barrier wait before it gives up (0: the default)."""
+        _check(lib().mirorr_ctx_set_wait_limit(self._h, int(polls)))
 
     def close(self):
         if self._h:
@@ -445,6 +465,23 @@ def resample(ctx: Context, image, mask, out_size_xyz, C, e, nearest=False):
     return out, outm
 
 
+def resample_device(ctx: Context, in_image_ptr, in_mask_ptr, in_size_xyz, out_size_xyz, C, e,
+                    out_image_ptr, out_mask_ptr, nearest=False):
+    """Linear (or nearest) resampling of device buffers (integer addresses on
+    the context's device; either image or mask may be None), issued on the
+    context's stream without waiting for it."""
+    in_size = (ctypes.c_int32 * 3)(*[int(v) for v in in_size_xyz])
+    out_size = (ctypes.c_int32 * 3)(*[int(v) for v in out_size_xyz])
+    Cc = np.ascontiguousarray(np.asarray(C, np.float64).reshape(-1))
+    ec = np.ascontiguousarray(np.asarray(e, np.float64))
+    vp = ctypes.c_void_p
+    _check(lib().mirorr_resample_device(
+        ctx.handle, in_size, vp(in_image_ptr) if in_image_ptr else None,
+        vp(in_mask_ptr) if in_mask_ptr else None, out_size, _ptr(Cc), _ptr(ec),
+        vp(out_image_ptr) if out_image_ptr else None, vp(out_mask_ptr) if out_mask_ptr else None,
+        1 if nearest else 0))
+
+
 def resample_final(ctx: Context, image, out_size_xyz, C, e, interpolator="bspline"):
     """Final resampling of image (float32, z, y, x) on an index map with the
     cubic B-spline ("bspline") or the radius-5 Welch-windowed sinc ("sinc")
@@ -500,8 +537,10 @@ def lts_noalloc(ctx: Context, t: Transform, n: int, init_dev: int, moved_dev: in
     both are given; the results equal lts_classic / lts_symmetric.  The
     scratch is a static device array sized for LTS_NOALLOC_MAX_POINTS pairs
     (larger n raises MirorrError with MIRORR_ERANGE).  The first call on a
-    device does the set-up; make it before any stream capture.  Calls on one
-    device share the scratch, so calls that overlap in time race.
+    device does the set-up (loading the device code reserves the array), so
+    make it before a caching allocator takes the free memory.  Every call
+    synchronises the context's stream, so none can run under stream capture.
+    Calls on one device share the scratch, so calls that overlap in time race.
     Returns the number of LTS inner iterations."""
     it = ctypes.c_int32(0)
     pf = None if t12f is None else ctypes.byref(t12f)

@@ -190,7 +190,7 @@ mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8
   long long n = (long long)((g.size[0] + kBoxPX - 1) / kBoxPX) * g.size[1] * g.size[2];
   int threads = 256;
   long long blocks = (n + threads - 1) / threads;
-  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  if (blocks > (long long)sm_count() * 64) blocks = (long long)sm_count() * 64;
   switch (g.bw) {
 #define CASE(B) \
   case B: box_stats_kernel<B><<<(unsigned)blocks, threads, 0, s>>>(search, smask, g.size[0], g.size[1], g.size[2], stats); break;
@@ -308,7 +308,7 @@ mirorr_status launch_variance_selection(const BmGeom &g, const float *base, doub
   unsigned long long *key = reinterpret_cast<unsigned long long *>(var + n);
   int threads = 256;
   long long blocks = (n + threads - 1) / threads;
-  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  if (blocks > (long long)sm_count() * 32) blocks = (long long)sm_count() * 32;
   block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
       base, g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2], g.st[0], g.st[1], g.st[2], g.ngap,
       g.bw, var, key);

@@ -4,11 +4,15 @@
 // (MirorrPyramidImplement::RunMirorr + the classic / symmetric iteration loops).
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 #include <vector>
+
+#include <cuda.h>
 
 #include "kernels.cuh"
 
@@ -26,6 +30,26 @@ void set_error(const char *fmt, ...) {
 void clear_error() { t_err[0] = 0; }
 const char *get_error() { return t_err; }
 
+int sm_count() {
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 148;
+  }
+  if (dev >= 0 && dev < 64) {
+    int v = cached[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+  }
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    n = 148;
+  }
+  if (dev >= 0 && dev < 64) cached[dev].store(n, std::memory_order_relaxed);
+  return n;
+}
+
 }  // namespace mb2
 
 using namespace mb2;
@@ -41,6 +65,23 @@ struct StageTimer {
   double search_ms = 0.0;     // the FP32 search kernel (events 5, 6 of a call)
   long long search_calls = 0;
   std::vector<char> ran;      // per call: the search kernel ran (events 5, 6 recorded)
+  // resampler passes (an image and its mask into one middle-space grid)
+  std::vector<cudaEvent_t> rpool;
+  size_t rused = 0;
+  std::vector<long long> rvox;
+  double resample_ms = 0.0;
+  long long resample_passes = 0, resample_voxels = 0;
+  cudaEvent_t *take_resample(long long voxels) {
+    while (rpool.size() < rused + 2) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      rpool.push_back(e);
+    }
+    cudaEvent_t *p = &rpool[rused];
+    rused += 2;
+    rvox.push_back(voxels);
+    return p;
+  }
   cudaEvent_t *take(size_t k) {
     while (pool.size() < used + k) {
       cudaEvent_t e;
@@ -69,10 +110,24 @@ struct StageTimer {
     }
     ran.clear();
     used = 0;
+    for (size_t i = 0; i + 2 <= rused; i += 2) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, rpool[i], rpool[i + 1]) == cudaSuccess) {
+        resample_ms += t;
+        ++resample_passes;
+        resample_voxels += rvox[i / 2];
+      }
+    }
+    rused = 0;
+    rvox.clear();
     cudaGetLastError();
   }
   void release() {
     for (auto e : pool) cudaEventDestroy(e);
+    for (auto e : rpool) cudaEventDestroy(e);
+    rpool.clear();
+    rvox.clear();
+    rused = 0;
     pool.clear();
     ran.clear();
     used = 0;
@@ -456,18 +511,40 @@ mirorr_status resample_into(mirorr_ctx c, const RegImage &src, const uint8_t *ma
   long long n = vox(grid.size);
   MB2_TRY(img.ensure(sizeof(float) * n));
   MB2_TRY(msk.ensure(n));
-  MB2_TRY(launch_resample(src.g.size, src.img, nullptr, grid.size, mi, img.as<float>(), nullptr,
-                          c->stream));
-  MB2_TRY(launch_resample(mask_g.size, nullptr, mask, grid.size, mm, nullptr, msk.as<uint8_t>(),
-                          c->stream));
+  cudaEvent_t *ev = c->timer.on ? c->timer.take_resample(n) : nullptr;
+  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], c->stream));
+  const bool same_grid = src.g.size[0] == mask_g.size[0] && src.g.size[1] == mask_g.size[1] &&
+                         src.g.size[2] == mask_g.size[2] && memcmp(&mi, &mm, sizeof(mi)) == 0;
+  if (same_grid) {
+    // image and mask on one input grid (the finest level): one pass computes
+    // each voxel's index map once for both
+    MB2_TRY(launch_resample(src.g.size, src.img, mask, grid.size, mi, img.as<float>(),
+                            msk.as<uint8_t>(), c->stream));
+  } else {
+    MB2_TRY(launch_resample(src.g.size, src.img, nullptr, grid.size, mi, img.as<float>(), nullptr,
+                            c->stream));
+    MB2_TRY(launch_resample(mask_g.size, nullptr, mask, grid.size, mm, nullptr,
+                            msk.as<uint8_t>(), c->stream));
+  }
+  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], c->stream));
   return MIRORR_OK;
 }
 
 mirorr_status run_lts(RegRun &r, LtsState &hs, long long nmax, long long *n_used) {
   int inner = 0;
   mirorr_ctx c = r.c;
+  unsigned int gave_up = 0;
   MB2_TRY(lts_run(c->ltsw, hs, c->pts_i.as<double>(), c->pts_m.as<double>(),
-                  c->counts.as<long long>(), nmax, c->stream, &inner, n_used));
+                  c->counts.as<long long>(), nmax, c->stream, &inner, n_used,
+                  ncc_timeout_flag(c->bmw), &gave_up));
+  if (gave_up) {
+    // a CTA of the search gave up its bounded wait on a tensor copy: that
+    // call's scores (and so this fit) cannot be trusted; the registration stops
+    bool to = false;
+    MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
+    set_error("a bounded wait on a tensor copy of the NCC search gave up");
+    return MIRORR_ETIMEOUT;
+  }
   if (r.stats) {
     r.stats->h2d_bytes += (int64_t)sizeof(LtsState);
     r.stats->d2h_bytes += (int64_t)(sizeof(LtsState) + 2 * sizeof(long long) + 32);
@@ -857,6 +934,27 @@ mirorr_status mirorr_ctx_search_kernel_times(mirorr_ctx c, double *ms, int64_t *
   return MIRORR_OK;
 }
 
+mirorr_status mirorr_ctx_resample_times(mirorr_ctx c, double *ms, int64_t *passes,
+                                        int64_t *voxels) {
+  if (!c || !ms) { set_error("null argument"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->timer.harvest();
+  *ms = c->timer.resample_ms;
+  if (passes) *passes = c->timer.resample_passes;
+  if (voxels) *voxels = c->timer.resample_voxels;
+  c->timer.resample_ms = 0.0;
+  c->timer.resample_passes = 0;
+  c->timer.resample_voxels = 0;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_ctx_set_wait_limit(mirorr_ctx c, int64_t polls) {
+  if (!c || polls < 0) { set_error("null context or negative limit"); return MIRORR_EINVAL; }
+  c->ltsw.spin_limit = polls;
+  return MIRORR_OK;
+}
+
 mirorr_status mirorr_ctx_stage_times(mirorr_ctx c, double ms[4], int64_t *calls) {
   if (!c || !ms) { set_error("null argument"); return MIRORR_EINVAL; }
   MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1182,11 +1280,9 @@ static mirorr_status resample_common(mirorr_ctx c, const int32_t in_size[3], con
     ResampleMap m;
     memcpy(m.C, C, sizeof(m.C));
     memcpy(m.e, e, sizeof(m.e));
-    if (pi && (st = launch_resample(in_size, pi, nullptr, out_size, m, oi.as<float>(), nullptr,
-                                    c->stream, nearest)) != MIRORR_OK)
-      goto done;
-    if (pm && (st = launch_resample(in_size, nullptr, pm, out_size, m, nullptr, om.as<uint8_t>(),
-                                    c->stream, nearest)) != MIRORR_OK)
+    // image and mask share the input grid and the map: one launch for both
+    if ((st = launch_resample(in_size, pi, pm, out_size, m, pi ? oi.as<float>() : nullptr,
+                              pm ? om.as<uint8_t>() : nullptr, c->stream, nearest)) != MIRORR_OK)
       goto done;
     if (pi && cudaMemcpyAsync(out_image, oi.ptr, sizeof(float) * no, cudaMemcpyDeviceToHost,
                               c->stream) != cudaSuccess) { st = MIRORR_ECUDA; goto done; }
@@ -1259,6 +1355,25 @@ static mirorr_status resample_final(mirorr_ctx c, const int32_t in_size[3], cons
   return st;
 }
 
+mirorr_status mirorr_resample_device(mirorr_ctx c, const int32_t in_size[3], const float *in_image,
+                                     const uint8_t *in_mask, const int32_t out_size[3],
+                                     const double C[9], const double e[3], float *out_image,
+                                     uint8_t *out_mask, int32_t nearest) {
+  if (!c || !in_size || !out_size || !C || !e || (!in_image && !in_mask) ||
+      (in_image && !out_image) || (in_mask && !out_mask)) {
+    set_error("null argument");
+    return MIRORR_EINVAL;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (in_size[d] <= 0 || out_size[d] <= 0) { set_error("empty volume"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  ResampleMap m;
+  memcpy(m.C, C, sizeof(m.C));
+  memcpy(m.e, e, sizeof(m.e));
+  return launch_resample(in_size, in_image, in_mask, out_size, m, in_image ? out_image : nullptr,
+                         in_mask ? out_mask : nullptr, c->stream, nearest != 0);
+}
+
 mirorr_status mirorr_resample_bspline(mirorr_ctx c, const int32_t in_size[3],
                                       const float *in_image, const int32_t out_size[3],
                                       const double C[9], const double e[3], float *out_image) {
@@ -1324,15 +1439,37 @@ mirorr_status mirorr_lts_symmetric(mirorr_ctx c, mirorr_transform *t, mirorr_tra
   return lts_common(c, t, t12f, t12b, n, init, moved, lts_keep, inner, true);
 }
 
-// True when p is device memory (or managed memory) usable on device dev.
-static bool device_pointer_on(const void *p, int dev) {
+// True when [p, p + bytes) lies inside one device (or managed) allocation
+// usable on device dev.  The allocation's extent comes from the driver's
+// cuMemGetAddressRange, looked up through the runtime's entry-point query so
+// the library needs no link-time dependency on libcuda.
+typedef CUresult (*GetAddressRangeFn)(CUdeviceptr *, size_t *, CUdeviceptr);
+
+static bool device_range_on(const void *p, size_t bytes, int dev) {
   cudaPointerAttributes at;
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  if (at.type == cudaMemoryTypeManaged) return true;
-  return at.type == cudaMemoryTypeDevice && at.device == dev;
+  if (at.type != cudaMemoryTypeManaged && !(at.type == cudaMemoryTypeDevice && at.device == dev))
+    return false;
+  static GetAddressRangeFn range_fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      range_fn = reinterpret_cast<GetAddressRangeFn>(fn);
+    cudaGetLastError();
+  });
+  if (!range_fn) return false;
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (range_fn(&base, &size, (CUdeviceptr)(uintptr_t)p) != CUDA_SUCCESS) return false;
+  const uintptr_t lo = (uintptr_t)p, end = (uintptr_t)base + size;
+  return lo >= (uintptr_t)base && bytes <= end - lo;
 }
 
 mirorr_status mirorr_lts_noalloc(mirorr_ctx c, mirorr_transform *t, mirorr_transform *t12f,
@@ -1355,8 +1492,10 @@ mirorr_status mirorr_lts_noalloc(mirorr_ctx c, mirorr_transform *t, mirorr_trans
       set_error("point arrays must be 8-byte aligned");
       return MIRORR_EINVAL;
     }
-    if (!device_pointer_on(init, c->device) || !device_pointer_on(moved, c->device)) {
-      set_error("point arrays must be device memory on the context's device %d", c->device);
+    if (!device_range_on(init, sizeof(double) * 3 * n, c->device) ||
+        !device_range_on(moved, sizeof(double) * 3 * n, c->device)) {
+      set_error("point arrays must be device memory on the context's device %d, each holding "
+                "at least n x 3 doubles", c->device);
       return MIRORR_EINVAL;
     }
   }

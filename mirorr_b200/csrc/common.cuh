@@ -18,6 +18,11 @@ void clear_error();
 // context).  Incremented on the host right after every launch.
 extern int64_t g_launches;
 
+// Multiprocessor count of the calling thread's current device (queried once
+// per device, then cached); grids of the grid-stride kernels are sized in
+// multiples of it.
+int sm_count();
+
 struct Status {
   mirorr_status code = MIRORR_OK;
   explicit operator bool() const { return code != MIRORR_OK; }

@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(128) sinc_eval_kernel(const float *img, int nx
 
 long long grid_for(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
-  return b > 148LL * 64 ? 148LL * 64 : (b < 1 ? 1 : b);
+  return b > (long long)sm_count() * 64 ? (long long)sm_count() * 64 : (b < 1 ? 1 : b);
 }
 
 }  // namespace

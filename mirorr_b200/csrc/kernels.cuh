@@ -110,13 +110,19 @@ struct LtsWork {
   DevBuf ctrl;      // barrier + select control
   DevBuf cand;      // candidate keys
   int max_ctas = 0;
+  long long spin_limit = 0;  // grid-barrier polls before giving up (0: the default)
 };
 // n_dev: two device counters whose sum is the number of point pairs; n_max is
 // an upper bound used for sizing.  Runs lts_begin / the inner loop /
-// lts_finish on host_state.
+// lts_finish on host_state.  watch_dev (optional): a device word read back in
+// the same synchronisation into *watch_host (the NCC stage's give-up flag).
 mirorr_status lts_run(LtsWork &w, LtsState &host_state, const double *init_dev,
                       const double *moved_dev, const long long *n_dev, long long n_max,
-                      cudaStream_t s, int *inner_iters, long long *n_used);
+                      cudaStream_t s, int *inner_iters, long long *n_used,
+                      const unsigned int *watch_dev = nullptr,
+                      unsigned int *watch_host = nullptr);
+// The NCC stage's give-up flag (device word), or nullptr before any search.
+const unsigned int *ncc_timeout_flag(const BmWork &w);
 // lts_run with every scratch buffer in a static device array sized for
 // MIRORR_LTS_NOALLOC_MAX_POINTS pairs: allocates no device memory.  n is the
 // number of pairs (no device counters).  Calls on one device must not overlap.

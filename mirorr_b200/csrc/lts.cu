@@ -29,6 +29,9 @@ constexpr int kThreads = 256;
 constexpr int kBins = 4096;
 constexpr int kCandMax = kThreads;  // keys left for the final rank (one per thread)
 constexpr int kPartial = 32;  // doubles per CTA partial
+// Polls of a grid-barrier wait (about 0.84 s with the 100 ns back-off) before
+// the wait gives up, raises the error flag and every CTA returns.
+constexpr long long kDefaultSpinLimit = 1LL << 23;
 
 struct LtsCtl {
   unsigned int bar_count;
@@ -49,9 +52,10 @@ struct LtsArgs {
   unsigned int *hist;     // 3 * kBins
   unsigned long long *cand;
   LtsCtl *ctl;
+  long long spin_limit;   // polls of a grid-barrier wait before it gives up
 };
 
-__device__ bool grid_sync(LtsCtl *ctl) {
+__device__ bool grid_sync(LtsCtl *ctl, long long spin_limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -68,7 +72,7 @@ __device__ bool grid_sync(LtsCtl *ctl) {
       long long spins = 0;
       while (*genp == gen && *errp == 0) {
         if (spins > 256) __nanosleep(100);
-        if (++spins > (1LL << 23)) {
+        if (++spins > spin_limit) {
           atomicExch(&ctl->err, 1);
           break;
         }
@@ -240,7 +244,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
       for (int i = threadIdx.x; i < kBins; i += blockDim.x)
         if (h[i]) atomicAdd(&a.hist[i], h[i]);
     }
-    if (!grid_sync(a.ctl)) return;
+    if (!grid_sync(a.ctl, a.spin_limit)) return;
     double nth;
     if (first) {
       if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->maxkey);
@@ -287,7 +291,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         unsigned int *gh2 = a.hist + (pass % 3) * kBins;
         for (int i = threadIdx.x; i < kBins; i += blockDim.x)
           if (h[i]) atomicAdd(&gh2[i], h[i]);
-        if (!grid_sync(a.ctl)) return;
+        if (!grid_sync(a.ctl, a.spin_limit)) return;
       }
       if (shift == 0) {
         // every bit fixed: the bucket's keys all equal the prefix
@@ -301,7 +305,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
             if (pos < (unsigned long long)kCandMax) a.cand[pos] = key;
           }
         }
-        if (!grid_sync(a.ctl)) return;
+        if (!grid_sync(a.ctl, a.spin_limit)) return;
         if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->ncand);
         __syncthreads();
         const int nc = (int)(s_key < (unsigned long long)kCandMax ? s_key : kCandMax);
@@ -355,7 +359,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
     __shared__ double s_out[28];
     block_sums<28>(acc, red_n, s_out);
     if (threadIdx.x < 28) a.partial[(long long)blockIdx.x * kPartial + threadIdx.x] = s_out[threadIdx.x];
-    if (!grid_sync(a.ctl)) return;
+    if (!grid_sync(a.ctl, a.spin_limit)) return;
     if (blockIdx.x == 0) grid_partial_sums(a.partial, 0, 28, s_out);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       LtsMoments mo;
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
       __syncthreads();
       for (int i = threadIdx.x; i < kBins; i += blockDim.x) a.hist[i] = 0;
     }
-    if (!grid_sync(a.ctl)) return;
+    if (!grid_sync(a.ctl, a.spin_limit)) return;
   }
 }
 
@@ -395,7 +399,9 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
 
 mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const double *moved_dev,
                       const long long *n_dev, long long n, cudaStream_t st, int *inner_iters,
-                      long long *n_used) {
+                      long long *n_used, const unsigned int *watch_dev,
+                      unsigned int *watch_host) {
+  if (watch_host) *watch_host = 0;
   lts_begin(hs);
   if (n <= 0) {
     lts_finish(hs);
@@ -441,6 +447,7 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
   a.hist = w.hist.as<unsigned int>();
   a.cand = w.cand.as<unsigned long long>();
   a.ctl = w.ctrl.as<LtsCtl>();
+  a.spin_limit = w.spin_limit > 0 ? w.spin_limit : kDefaultSpinLimit;
   void *args[] = {&a};
   MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)lts_kernel, dim3(grid), dim3(kThreads), args, 0, st));
   ++g_launches;
@@ -449,6 +456,9 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
   MB2_CUDA_TRY(cudaMemcpyAsync(&hs, w.state.ptr, sizeof(LtsState), cudaMemcpyDeviceToHost, st));
   MB2_CUDA_TRY(cudaMemcpyAsync(&ctl, w.ctrl.ptr, sizeof(LtsCtl), cudaMemcpyDeviceToHost, st));
   MB2_CUDA_TRY(cudaMemcpyAsync(nn, n_dev, sizeof(nn), cudaMemcpyDeviceToHost, st));
+  if (watch_dev && watch_host)
+    MB2_CUDA_TRY(cudaMemcpyAsync(watch_host, watch_dev, sizeof(unsigned int),
+                                 cudaMemcpyDeviceToHost, st));
   MB2_CUDA_TRY(cudaStreamSynchronize(st));
   if (n_used) *n_used = nn[0] + nn[1];
   if (ctl.err) {
@@ -572,6 +582,7 @@ mirorr_status lts_run_noalloc(LtsState &hs, const double *init_dev, const double
   a.hist = reinterpret_cast<unsigned int *>(base + kNaHist);
   a.cand = reinterpret_cast<unsigned long long *>(base + kNaCand);
   a.ctl = reinterpret_cast<LtsCtl *>(base + kNaCtl);
+  a.spin_limit = kDefaultSpinLimit;
   void *args[] = {&a};
   MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)lts_kernel, dim3(grid), dim3(kThreads), args, 0, st));
   ++g_launches;

@@ -1802,14 +1802,14 @@ mirorr_status launch_masked(const NccArgs &a, cudaStream_t s) {
   size_t smem = sizeof(float) * (size_t)C::SMEM_FLOATS;
   MB2_TRY(set_smem(ncc_masked_kernel<C>, smem));
   long long need = (a.nblocks + C::BPC - 1) / C::BPC;
-  long long grid = need < 148LL * 8 ? need : 148LL * 8;
+  long long grid = need < (long long)sm_count() * 8 ? need : (long long)sm_count() * 8;
   ncc_masked_kernel<C><<<(unsigned)grid, C::NT, smem, s>>>(a);
   MB2_LAUNCH_CHECK();
   // then the blocks with a partly masked base block (the list grows in both
   // kernels above)
   const size_t smem_b = sizeof(float) * (size_t)C::BPC * (2 * C::WIN + 4 * C::B);
   MB2_TRY(set_smem(ncc_basemask_kernel<C>, smem_b));
-  const long long grid_b = need < 148LL * 4 ? need : 148LL * 4;
+  const long long grid_b = need < (long long)sm_count() * 4 ? need : (long long)sm_count() * 4;
   ncc_basemask_kernel<C><<<(unsigned)grid_b, C::NT, smem_b, s>>>(a);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
@@ -1820,7 +1820,7 @@ mirorr_status launch_warp(const NccArgs &a, cudaStream_t s) {
   size_t smem = sizeof(float) * (size_t)CW::WPC * CW::SPW * CW::SLOT;
   MB2_TRY(set_smem(ncc_warp_kernel<CW>, smem));
   long long need = (a.nblocks + CW::WPC * CW::SPW - 1) / (CW::WPC * CW::SPW);
-  long long grid = need < 148LL * CW::MINB * 4 ? need : 148LL * CW::MINB * 4;
+  long long grid = need < (long long)sm_count() * CW::MINB * 4 ? need : (long long)sm_count() * CW::MINB * 4;
   ncc_warp_kernel<CW><<<(unsigned)grid, CW::WPC * 32, smem, s>>>(a);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
@@ -1848,14 +1848,14 @@ mirorr_status launch_rest(const NccArgs &a, bool all_general, cudaStream_t s) {
   MB2_TRY(set_smem(ncc_fallback_kernel<BW>, smem_f));
   if (all_general) {
     // no register-blocked kernels for this geometry: every block here
-    long long grid = a.nblocks < 148LL * 16 ? a.nblocks : 148LL * 16;
+    long long grid = a.nblocks < (long long)sm_count() * 16 ? a.nblocks : (long long)sm_count() * 16;
     ncc_general_kernel<BW><<<(unsigned)grid, 128, smem_g, s>>>(a);
     MB2_LAUNCH_CHECK();
   }
   long long rgrid = (a.nblocks + 127) / 128;
   ncc_refine_kernel<BW><<<(unsigned)rgrid, 128, 0, s>>>(a);
   MB2_LAUNCH_CHECK();
-  ncc_fallback_kernel<BW><<<148, 128, smem_f, s>>>(a);
+  ncc_fallback_kernel<BW><<<(unsigned)sm_count(), 128, smem_f, s>>>(a);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
@@ -1917,7 +1917,7 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
     const size_t n1 = (size_t)a.nbx * a.ny * a.nz, n2 = (size_t)a.nbx * a.nby * a.nz;
     MB2_TRY(w.ncc_wand.ensure(n1 + n2 + (size_t)a.nblocks));
     uint8_t *b1 = w.ncc_wand.as<uint8_t>(), *b2 = b1 + n1, *b3 = b2 + n2;
-    const unsigned g = 148 * 8;
+    const unsigned g = (unsigned)sm_count() * 8;
     wand_x_kernel<<<g, 256, 0, s>>>(a.stats, b1, a.nx, a.ny, a.nz, a.nbx, a.stx, a.G, W, 4);
     MB2_LAUNCH_CHECK();
     wand_axis_kernel<<<g, 256, 0, s>>>(b1, b2, a.nbx, a.ny, a.nz, a.nby, a.sty, a.G, W);
@@ -1950,7 +1950,7 @@ mirorr_status launch_xlane(NccArgs &a, BmWork &w, cudaStream_t s, bool &done,
     }
   }
   MB2_TRY(set_smem(ncc_xlane_kernel<W, kXWarps>, smem));
-  constexpr long long kCtas = 148LL * (kXWarpsPerSM / kXWarps);
+  const long long kCtas = (long long)sm_count() * (kXWarpsPerSM / kXWarps);
   const long long grid = xa.ntiles < kCtas ? xa.ntiles : kCtas;
   if (kev) MB2_CUDA_TRY(cudaEventRecord(kev[0], s));
   ncc_xlane_kernel<W, kXWarps><<<(unsigned)grid, NL, smem, s>>>(a, xa, tmap);
@@ -2031,7 +2031,7 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
   a.xl_count = xl_count;
   {
     long long grid = (g.nblocks + 127) / 128;
-    if (grid > 148LL * 16) grid = 148LL * 16;
+    if (grid > (long long)sm_count() * 16) grid = (long long)sm_count() * 16;
     block_stat_kernel<<<(unsigned)grid, 128, 0, s>>>(a);
     MB2_LAUNCH_CHECK();
   }
@@ -2053,6 +2053,10 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
       set_error("block width %d not supported (1..8)", g.bw);
       return MIRORR_EINVAL;
   }
+}
+
+const unsigned int *ncc_timeout_flag(const BmWork &w) {
+  return w.ncc_ctl.ptr ? w.ncc_ctl.as<unsigned int>() + 5 : nullptr;
 }
 
 mirorr_status ncc_take_timeout(BmWork &w, cudaStream_t s, bool *timed_out) {

@@ -12,6 +12,8 @@
 //   * lerp chain x -> y -> z, a + (b - a) t, in FP64;
 //   * float output rounded to nearest; uint8 output clamped to [0, 255] and
 //     truncated (ResampleImageFilter::CastPixelWithBoundsChecking).
+// An image and its mask on the same input grid go through one launch, which
+// computes each voxel's index map once for both.
 // The FP64 arithmetic is written with explicit round-to-nearest intrinsics so
 // results are bit-identical to a plain C evaluation of the same expressions.
 #include "kernels.cuh"
@@ -34,87 +36,143 @@ __device__ inline double dlerp(double a, double b, double t) {
   return __dadd_rn(a, __dmul_rn(__dsub_rn(b, a), t));
 }
 
-__global__ void __launch_bounds__(256) resample_kernel(ResampleArgs a) {
-  long long n = (long long)a.onx * a.ony * a.onz;
-  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n;
-       o += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    split3(o, a.onx, a.ony, i, j, k);
-    const double di = (double)i, dj = (double)j, dk = (double)k;
-    double c[3];
+// Linear or nearest resampling of one output voxel (i, j, k); cj, ck hold
+// C[r][1] * j and C[r][2] * k (products the whole x-run shares).  Writes the
+// image value to *v and the mask value to *m when the respective input exists.
+template <bool IMG, bool MSK>
+__device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, const double cj[3],
+                                               const double ck[3], float *v, uint8_t *m) {
+  const double di = (double)i;
+  double c[3];
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
-      c[r] = __dadd_rn(__dadd_rn(__dadd_rn(a.e[r], __dmul_rn(a.C[3 * r], di)),
-                                 __dmul_rn(a.C[3 * r + 1], dj)),
-                       __dmul_rn(a.C[3 * r + 2], dk));
-    const int nn[3] = {a.inx, a.iny, a.inz};
-    bool inside = true;
+  for (int r = 0; r < 3; ++r)
+    c[r] = __dadd_rn(__dadd_rn(__dadd_rn(a.e[r], __dmul_rn(a.C[3 * r], di)), cj[r]), ck[r]);
+  const int nn[3] = {a.inx, a.iny, a.inz};
+  bool inside = true;
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
-      if (!(c[r] >= -0.5 && c[r] < (double)nn[r] - 0.5)) inside = false;
-    if (!inside) {
-      if (a.out) a.out[o] = 0.0f;
-      if (a.outm) a.outm[o] = 0;
-      continue;
-    }
-    if (a.nearest) {
-      // NearestNeighborInterpolateImageFunction: index = floor(c + 0.5)
-      long long q = 0, stride = 1;
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        int b = (int)floor(__dadd_rn(c[r], 0.5));
-        if (b < 0) b = 0;
-        if (b > nn[r] - 1) b = nn[r] - 1;
-        q += (long long)b * stride;
-        stride *= nn[r];
-      }
-      if (a.out) a.out[o] = __ldg(a.in + q);
-      if (a.outm) a.outm[o] = __ldg(a.inm + q);
-      continue;
-    }
-    int i0[3], i1[3];
-    double t[3];
+  for (int r = 0; r < 3; ++r)
+    if (!(c[r] >= -0.5 && c[r] < (double)nn[r] - 0.5)) inside = false;
+  if (!inside) {
+    if (IMG) *v = 0.0f;
+    if (MSK) *m = 0;
+    return;
+  }
+  if (a.nearest) {
+    // NearestNeighborInterpolateImageFunction: index = floor(c + 0.5)
+    long long q = 0, stride = 1;
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      int b = (int)floor(c[r]);
+      int b = (int)floor(__dadd_rn(c[r], 0.5));
       if (b < 0) b = 0;
-      double d = __dsub_rn(c[r], (double)b);
-      if (d <= 0.0) d = 0.0;
-      i0[r] = b;
-      i1[r] = (b + 1 > nn[r] - 1) ? b : b + 1;
-      t[r] = d;
+      if (b > nn[r] - 1) b = nn[r] - 1;
+      q += (long long)b * stride;
+      stride *= nn[r];
     }
-    const long long sx = 1, sy = a.inx, sz = (long long)a.inx * a.iny;
-    const long long q000 = i0[2] * sz + i0[1] * sy + i0[0] * sx;
-    const long long q100 = i0[2] * sz + i0[1] * sy + i1[0] * sx;
-    const long long q010 = i0[2] * sz + i1[1] * sy + i0[0] * sx;
-    const long long q110 = i0[2] * sz + i1[1] * sy + i1[0] * sx;
-    const long long q001 = i1[2] * sz + i0[1] * sy + i0[0] * sx;
-    const long long q101 = i1[2] * sz + i0[1] * sy + i1[0] * sx;
-    const long long q011 = i1[2] * sz + i1[1] * sy + i0[0] * sx;
-    const long long q111 = i1[2] * sz + i1[1] * sy + i1[0] * sx;
-    if (a.out) {
-      const float *p = a.in;
-      double x00 = dlerp((double)__ldg(p + q000), (double)__ldg(p + q100), t[0]);
-      double x10 = dlerp((double)__ldg(p + q010), (double)__ldg(p + q110), t[0]);
-      double x01 = dlerp((double)__ldg(p + q001), (double)__ldg(p + q101), t[0]);
-      double x11 = dlerp((double)__ldg(p + q011), (double)__ldg(p + q111), t[0]);
-      double xx0 = dlerp(x00, x10, t[1]);
-      double xx1 = dlerp(x01, x11, t[1]);
-      a.out[o] = __double2float_rn(dlerp(xx0, xx1, t[2]));
+    if (IMG) *v = __ldg(a.in + q);
+    if (MSK) *m = __ldg(a.inm + q);
+    return;
+  }
+  int i0[3], i1[3];
+  double t[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    int b = (int)floor(c[r]);
+    if (b < 0) b = 0;
+    double d = __dsub_rn(c[r], (double)b);
+    if (d <= 0.0) d = 0.0;
+    i0[r] = b;
+    i1[r] = (b + 1 > nn[r] - 1) ? b : b + 1;
+    t[r] = d;
+  }
+  const long long sy = a.inx, sz = (long long)a.inx * a.iny;
+  const long long z0 = i0[2] * sz, z1 = i1[2] * sz, y0 = i0[1] * sy, y1 = i1[1] * sy;
+  const long long q000 = z0 + y0 + i0[0], q100 = z0 + y0 + i1[0];
+  const long long q010 = z0 + y1 + i0[0], q110 = z0 + y1 + i1[0];
+  const long long q001 = z1 + y0 + i0[0], q101 = z1 + y0 + i1[0];
+  const long long q011 = z1 + y1 + i0[0], q111 = z1 + y1 + i1[0];
+  if (IMG) {
+    const float *p = a.in;
+    const double x00 = dlerp((double)__ldg(p + q000), (double)__ldg(p + q100), t[0]);
+    const double x10 = dlerp((double)__ldg(p + q010), (double)__ldg(p + q110), t[0]);
+    const double x01 = dlerp((double)__ldg(p + q001), (double)__ldg(p + q101), t[0]);
+    const double x11 = dlerp((double)__ldg(p + q011), (double)__ldg(p + q111), t[0]);
+    *v = __double2float_rn(dlerp(dlerp(x00, x10, t[1]), dlerp(x01, x11, t[1]), t[2]));
+  }
+  if (MSK) {
+    const uint8_t *p = a.inm;
+    const uint8_t m000 = __ldg(p + q000), m100 = __ldg(p + q100), m010 = __ldg(p + q010),
+                  m110 = __ldg(p + q110), m001 = __ldg(p + q001), m101 = __ldg(p + q101),
+                  m011 = __ldg(p + q011), m111 = __ldg(p + q111);
+    if (m000 == m100 && m000 == m010 && m000 == m110 && m000 == m001 && m000 == m101 &&
+        m000 == m011 && m000 == m111) {
+      // every lerp of equal values returns that value exactly
+      *m = m000;
+    } else {
+      const double x00 = dlerp((double)m000, (double)m100, t[0]);
+      const double x10 = dlerp((double)m010, (double)m110, t[0]);
+      const double x01 = dlerp((double)m001, (double)m101, t[0]);
+      const double x11 = dlerp((double)m011, (double)m111, t[0]);
+      double w = dlerp(dlerp(x00, x10, t[1]), dlerp(x01, x11, t[1]), t[2]);
+      if (w < 0.0) w = 0.0;
+      if (w > 255.0) w = 255.0;
+      *m = (uint8_t)(int)w;
     }
-    if (a.outm) {
-      const uint8_t *p = a.inm;
-      double x00 = dlerp((double)__ldg(p + q000), (double)__ldg(p + q100), t[0]);
-      double x10 = dlerp((double)__ldg(p + q010), (double)__ldg(p + q110), t[0]);
-      double x01 = dlerp((double)__ldg(p + q001), (double)__ldg(p + q101), t[0]);
-      double x11 = dlerp((double)__ldg(p + q011), (double)__ldg(p + q111), t[0]);
-      double xx0 = dlerp(x00, x10, t[1]);
-      double xx1 = dlerp(x01, x11, t[1]);
-      double v = dlerp(xx0, xx1, t[2]);
-      if (v < 0.0) v = 0.0;
-      if (v > 255.0) v = 255.0;
-      a.outm[o] = (uint8_t)(int)v;
+  }
+}
+
+// Each thread produces a run of 4 consecutive output voxels (linear order, so
+// a run may cross a row) and stores them with one 16-byte image store and one
+// 4-byte mask store.  The output buffers are 16-byte aligned (checked by the
+// launcher).  Per voxel the index map is the same FP64 expression as a plain
+// evaluation; only the j and k products are shared along the run.
+template <bool IMG, bool MSK>
+__global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
+  const long long n = (long long)a.onx * a.ony * a.onz;
+  const long long nrun = (n + 3) >> 2;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nrun;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long o0 = g << 2;
+    int i, j, k;
+    split3(o0, a.onx, a.ony, i, j, k);
+    double cj[3], ck[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      cj[r] = __dmul_rn(a.C[3 * r + 1], (double)j);
+      ck[r] = __dmul_rn(a.C[3 * r + 2], (double)k);
+    }
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    uint8_t m[4] = {0, 0, 0, 0};
+    const int cnt = n - o0 < 4 ? (int)(n - o0) : 4;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (u < cnt) {
+        resample_voxel<IMG, MSK>(a, i, cj, ck, &v[u], &m[u]);
+        if (++i == a.onx) {
+          i = 0;
+          if (++j == a.ony) {
+            j = 0;
+            ++k;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) ck[r] = __dmul_rn(a.C[3 * r + 2], (double)k);
+          }
+#pragma unroll
+          for (int r = 0; r < 3; ++r) cj[r] = __dmul_rn(a.C[3 * r + 1], (double)j);
+        }
+      }
+    }
+    if (cnt == 4) {
+      if (IMG) *reinterpret_cast<float4 *>(a.out + o0) = make_float4(v[0], v[1], v[2], v[3]);
+      if (MSK)
+        *reinterpret_cast<uint32_t *>(a.outm + o0) =
+            (uint32_t)m[0] | ((uint32_t)m[1] << 8) | ((uint32_t)m[2] << 16) | ((uint32_t)m[3] << 24);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (u < cnt) {
+          if (IMG) a.out[o0 + u] = v[u];
+          if (MSK) a.outm[o0 + u] = m[u];
+        }
+      }
     }
   }
 }
@@ -132,10 +190,17 @@ mirorr_status launch_resample(const int in_size[3], const float *in, const uint8
   a.out = in ? out : nullptr;
   a.outm = in_mask ? out_mask : nullptr;
   long long n = (long long)out_size[0] * out_size[1] * out_size[2];
-  if (n <= 0) return MIRORR_OK;
-  long long blocks = (n + 255) / 256;
-  if (blocks > 148LL * 64) blocks = 148LL * 64;
-  resample_kernel<<<(unsigned)blocks, 256, 0, s>>>(a);
+  if (n <= 0 || (!a.out && !a.outm)) return MIRORR_OK;
+  if (((uintptr_t)a.out & 15u) || ((uintptr_t)a.outm & 3u)) {
+    set_error("resampler output buffers must be 16-byte (image) and 4-byte (mask) aligned");
+    return MIRORR_EINVAL;
+  }
+  long long blocks = ((n + 3) / 4 + 255) / 256;
+  const long long cap = (long long)sm_count() * 8;
+  if (blocks > cap) blocks = cap;
+  if (a.out && a.outm) resample_kernel<true, true><<<(unsigned)blocks, 256, 0, s>>>(a);
+  else if (a.out) resample_kernel<true, false><<<(unsigned)blocks, 256, 0, s>>>(a);
+  else resample_kernel<false, true><<<(unsigned)blocks, 256, 0, s>>>(a);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
@@ -166,7 +231,7 @@ mirorr_status launch_smooth_axis(const int size[3], const float *in, float *out,
                                  const double *w, int radius, cudaStream_t s) {
   long long n = (long long)size[0] * size[1] * size[2];
   long long blocks = (n + 255) / 256;
-  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  if (blocks > (long long)sm_count() * 64) blocks = (long long)sm_count() * 64;
   smooth_axis_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, out, size[0], size[1], size[2], axis, w,
                                                       radius);
   MB2_LAUNCH_CHECK();
@@ -182,7 +247,7 @@ __global__ void fill_u8_kernel(uint8_t *p, long long n, uint8_t v) {
 mirorr_status launch_fill_u8(uint8_t *p, long long n, uint8_t v, cudaStream_t s) {
   if (n <= 0) return MIRORR_OK;
   long long blocks = (n + 255) / 256;
-  if (blocks > 148LL * 16) blocks = 148LL * 16;
+  if (blocks > (long long)sm_count() * 16) blocks = (long long)sm_count() * 16;
   fill_u8_kernel<<<(unsigned)blocks, 256, 0, s>>>(p, n, v);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;

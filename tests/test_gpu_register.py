@@ -53,3 +53,31 @@ def test_registration_matches_oracle(ctx, c):
     assert abs(err - err_o) < 1e-3
     if c.get("improves", True):
         assert err < err_0
+
+
+def test_registration_matches_oracle_at_classic_rigid_128x128x64(ctx):
+    """The classic rigid configuration at its full size: 128x128x64 pair of 40
+    Gaussians (intensity-mapped moving image, rotation up to 5 degrees,
+    translation up to 8 voxels), 2 pyramid levels, block 4, block spacing 4,
+    radius 3 (343 candidates), top 50 % of blocks by variance, LTS keep 0.5,
+    10 iterations per level.  Same bars as the small cases."""
+    shape = (128, 128, 64)
+    ph = make_phantom(shape, n_gauss=40, kind="rigid", seed=0, max_angle_deg=5.0,
+                      max_shift_vox=8.0)
+    rp = O.RegParams("classic", "rigid", 10, O.BMParams(4, 1, 4, 7, 0.5), 0.5)
+    fixed = O.Image(ph.fixed, ph.spacing, ph.origin)
+    moving = O.Image(ph.moving, ph.spacing, ph.origin)
+    to = O.register(fixed, moving, rp, 2)
+    p = mb.reg_params(symmetric=False, kind="rigid", levels=2, iterations=10, nhood_gap=4,
+                      nhood_width=7, block_keep=0.5, lts_keep=0.5)
+    tg, st = mb.register(ctx, ph.fixed, ph.moving, p)
+    assert st.levels_run == 2
+    np.testing.assert_allclose(tg.M, to.M, atol=1e-4, rtol=0)
+    np.testing.assert_allclose(tg.off, to.off, atol=1e-3, rtol=0)
+    err = tre(tg.M, tg.off, ph.true_matrix, ph.true_offset, shape, ph.spacing)
+    err_o = tre(to.M, to.off, ph.true_matrix, ph.true_offset, shape, ph.spacing)
+    err_0 = tre(np.eye(3), np.zeros(3), ph.true_matrix, ph.true_offset, shape, ph.spacing)
+    print(f"128x128x64 classic rigid: TRE gpu {err:.4f} mm, oracle {err_o:.4f} mm, initial "
+          f"{err_0:.4f} mm, max |dM| {np.max(np.abs(tg.M - to.M)):.2e}")
+    assert abs(err - err_o) < 1e-3
+    assert err < err_0

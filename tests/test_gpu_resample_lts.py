@@ -37,6 +37,24 @@ def test_resample_bit_exact(ctx, seed):
     np.testing.assert_allclose(eg, e, atol=1e-12)
 
 
+def test_resample_image_only_and_mask_only(ctx):
+    # separate launches for an image alone and a mask alone, an output size
+    # that is not a multiple of the 4-voxel run (ragged last run)
+    rng = np.random.default_rng(5)
+    img = rng.random((13, 17, 19)).astype(np.float32)
+    msk = (rng.random(img.shape) > 0.5).astype(np.uint8) * 255
+    M = random_rotation(rng, 7.0)
+    gin = O.Image(img, np.array([1.0, 1.0, 1.0]), np.zeros(3))
+    gout = O.Image(np.zeros((11, 15, 21), np.float32), np.array([1.1, 1.0, 0.9]),
+                   np.array([0.5, 0.5, 0.0]))
+    C, e = O.resample_map(gout, gin, M, rng.uniform(-2, 2, 3))
+    out_o, outm_o = O.resample(img, msk, gout.size, C, e)
+    out_g, _ = mb.resample(ctx, img, None, gout.size, C, e)
+    _, outm_g = mb.resample(ctx, None, msk, gout.size, C, e)
+    np.testing.assert_array_equal(out_g, out_o)
+    np.testing.assert_array_equal(outm_g, outm_o)
+
+
 @pytest.mark.parametrize("seed", [3, 4])
 def test_resample_nearest_bit_exact(ctx, seed):
     rng = np.random.default_rng(seed)
@@ -160,3 +178,28 @@ def test_lts_large_point_set(ctx):
     assert it_g == it_o
     np.testing.assert_allclose(tg.M, t.M, atol=1e-9)
     np.testing.assert_allclose(tg.off, t.off, atol=1e-8)
+
+
+def test_lts_barrier_wait_gives_up_and_context_recovers(ctx):
+    """The LTS kernel's grid-barrier waits are bounded.  With a limit of one
+    poll the CTAs that reach a barrier before the others give up, every CTA
+    returns, and the call reports ETIMEOUT without touching the transform; the
+    default limit then fits the same pairs as the oracle (the context and the
+    GPU are still usable).  Nothing faults: the waits just end early."""
+    x, y = _pairs("affine", 13, n=400000)  # many CTAs, so arrivals are spread out
+    t0 = O.Tfm("affine")
+    tg = _to_mb(t0)
+    before = (tg.M.copy(), tg.off.copy())
+    ctx.set_wait_limit(1)
+    try:
+        with pytest.raises(mb.MirorrError) as e:
+            mb.lts_classic(ctx, tg, x, y, 0.5)
+        assert e.value.name == "ETIMEOUT"
+        np.testing.assert_array_equal(tg.M, before[0])
+        np.testing.assert_array_equal(tg.off, before[1])
+    finally:
+        ctx.set_wait_limit(0)
+    it_o = O.lts_classic(t0, x, y, 0.5)
+    it_g = mb.lts_classic(ctx, tg, x, y, 0.5)
+    assert it_g == it_o
+    np.testing.assert_allclose(tg.M, t0.M, atol=1e-9)

@@ -73,6 +73,13 @@ def test_noalloc_classic_matches(ctx, kind, n):
         it_b = mb.lts_noalloc(ctx, tb, n, xd.data_ptr(), yd.data_ptr(), 0.5)
         assert it_b == it_a
         _same(tb, ta)
+    # the defining property: once set up, a call takes no device memory
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        mb.lts_noalloc(ctx, _start(kind), n, xd.data_ptr(), yd.data_ptr(), 0.5)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
 
 
 @pytest.mark.parametrize("kind", ["rigid", "affine"])
@@ -109,6 +116,21 @@ def test_noalloc_rejects(ctx):
     with pytest.raises(mb.MirorrError) as e:  # host memory is refused before any launch
         mb.lts_noalloc(ctx, _start("affine"), 64, x.ctypes.data, y.ctypes.data, 0.5)
     assert e.value.name == "EINVAL"
+    # arrays shorter than n x 3 doubles: an allocation of its own (not a slice
+    # of a caching allocator's segment) holding 64 pairs, asked for 65
+    from cuda.bindings import runtime as cudart
+    err, raw = cudart.cudaMalloc(64 * 3 * 8)
+    assert err == cudart.cudaError_t.cudaSuccess
+    try:
+        err, = cudart.cudaMemcpy(raw, x.ctypes.data, 64 * 3 * 8,
+                                 cudart.cudaMemcpyKind.cudaMemcpyHostToDevice)
+        assert err == cudart.cudaError_t.cudaSuccess
+        assert mb.lts_noalloc(ctx, _start("affine"), 64, raw, yd.data_ptr(), 0.5) >= 0
+        with pytest.raises(mb.MirorrError) as e:
+            mb.lts_noalloc(ctx, _start("affine"), 65, raw, yd.data_ptr(), 0.5)
+        assert e.value.name == "EINVAL"
+    finally:
+        cudart.cudaFree(raw)
     with pytest.raises(mb.MirorrError) as e:  # only one half-space transform
         mb.lts_noalloc(ctx, _start("affine"), 64, xd.data_ptr(), yd.data_ptr(), 0.5,
                        t12f=_start("affine"))
