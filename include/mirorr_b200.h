@@ -7,7 +7,8 @@
  *
  * Layout conventions (those of itk::Image<float,3> / itk::Image<unsigned char,3>):
  *   volumes are x-fastest, size = {nx, ny, nz}; voxel (x, y, z) sits at
- *   data[(z * ny + y) * nx + x].  Images are float32, masks uint8 (0 = outside).
+ *   data[(z * ny + y) * nx + x].  Images are float32 (or 16-bit where a
+ *   storage type says so, see mirorr_dtype), masks uint8 (0 = outside).
  *   Physical point of index i: origin + direction * diag(spacing) * i,
  *   direction row-major.
  *
@@ -25,7 +26,7 @@
 extern "C" {
 #endif
 
-#define MIRORR_ABI_VERSION 1
+#define MIRORR_ABI_VERSION 2
 
 #if defined(MIRORR_BUILD)
 #define MIRORR_API __attribute__((visibility("default")))
@@ -44,6 +45,16 @@ typedef enum mirorr_status {
   MIRORR_ESTATE = 6,     /* call out of order (e.g. GetOffsets before images are set) */
   MIRORR_ERANGE = 7      /* output buffer too small; *_needed reports the size */
 } mirorr_status;
+
+/* Element type of stored volumes.  F32 is the plain path (the drop-in); BF16
+ * and F16 store images in 16 bits (round to nearest even from float) and run
+ * the block search's cross term on the tensor cores; U8 is the masks' type. */
+typedef enum mirorr_dtype {
+  MIRORR_DTYPE_F32 = 0,
+  MIRORR_DTYPE_BF16 = 1,
+  MIRORR_DTYPE_F16 = 2,
+  MIRORR_DTYPE_U8 = 3
+} mirorr_dtype;
 
 typedef struct mirorr_ctx_s *mirorr_ctx;
 typedef struct mirorr_matcher_s *mirorr_matcher;
@@ -109,6 +120,19 @@ MIRORR_API mirorr_status mirorr_bm_set_search_image_device(mirorr_matcher m, con
                                                 const float *dev);
 MIRORR_API mirorr_status mirorr_bm_set_base_mask_device(mirorr_matcher m, const uint8_t *dev);
 MIRORR_API mirorr_status mirorr_bm_set_search_mask_device(mirorr_matcher m, const uint8_t *dev);
+/* No reference counterpart: the element type the matcher stores its images in
+ * (MIRORR_DTYPE_F32, the default, or _BF16 / _F16).  Set it before the images;
+ * changing it drops the images set so far.  With 16-bit storage the float32
+ * setters above convert (round to nearest even) into device copies, the
+ * block search runs on the tensor cores (block width 4, block gap 1, window
+ * up to 7; other windows up to 13 through a direct FP32 search) and scores
+ * are FP32 sums over the stored values rather than the reference's FP64. */
+MIRORR_API mirorr_status mirorr_bm_set_storage(mirorr_matcher m, int32_t dtype);
+/* 16-bit device images in the storage type (borrowed, no copy). */
+MIRORR_API mirorr_status mirorr_bm_set_base_image_device16(mirorr_matcher m, const mirorr_geometry *g,
+                                                const void *dev);
+MIRORR_API mirorr_status mirorr_bm_set_search_image_device16(mirorr_matcher m,
+                                                  const mirorr_geometry *g, const void *dev);
 /* SwapImageOrder (itkAbstractBlockMatcher.txx:101-112; the GPU matcher keeps
  * its device buffers, itkBlockMatcherGPU.txx:186-202). */
 MIRORR_API mirorr_status mirorr_bm_swap_image_order(mirorr_matcher m);
@@ -253,6 +277,9 @@ typedef struct mirorr_reg_params {
   int32_t verbosity;      /* 1: per-iteration lines; 2: also per-call block routing */
   int32_t last_level;     /* --pyr-end: run the schedule's levels 1..last_level (1 = the
                              coarsest); 0 = all, negative counts back from the finest */
+  int32_t storage;        /* element type of the input images and of the middle-space
+                             images (mirorr_dtype; no reference counterpart): F32 (the
+                             drop-in) or BF16 / F16, whose search runs on the tensor cores */
 } mirorr_reg_params;
 
 typedef struct mirorr_reg_stats {
@@ -266,20 +293,21 @@ typedef struct mirorr_reg_stats {
 } mirorr_reg_stats;
 
 MIRORR_API mirorr_status mirorr_reg_default_params(mirorr_reg_params *p);
-/* Full registration from host buffers (the e2e path: uploads inside).  Masks
- * may be NULL (all 255).  init may be NULL: centred initialisation
+/* Full registration from host buffers (the e2e path: uploads inside).  fixed
+ * and moving hold elements of p->storage (float32, or 16-bit patterns of
+ * BF16 / F16).  Masks may be NULL (all 255).  init may be NULL: centred initialisation
  * (CenteredTransformInitializer GeometryOn, itkMirorrPyramidWrapper.txx:611-623).
  * The result maps moving-image physical points to fixed-image points. */
 MIRORR_API mirorr_status mirorr_register(mirorr_ctx ctx, const mirorr_geometry *fixed_geom,
-                              const float *fixed, const uint8_t *fixed_mask,
-                              const mirorr_geometry *moving_geom, const float *moving,
+                              const void *fixed, const uint8_t *fixed_mask,
+                              const mirorr_geometry *moving_geom, const void *moving,
                               const uint8_t *moving_mask, const mirorr_reg_params *p,
                               const mirorr_transform *init, mirorr_transform *result,
                               mirorr_reg_stats *stats);
 /* Same with device-resident inputs (caller-owned device pointers). */
 MIRORR_API mirorr_status mirorr_register_device(mirorr_ctx ctx, const mirorr_geometry *fixed_geom,
-                                     const float *fixed, const uint8_t *fixed_mask,
-                                     const mirorr_geometry *moving_geom, const float *moving,
+                                     const void *fixed, const uint8_t *fixed_mask,
+                                     const mirorr_geometry *moving_geom, const void *moving,
                                      const uint8_t *moving_mask, const mirorr_reg_params *p,
                                      const mirorr_transform *init, mirorr_transform *result,
                                      mirorr_reg_stats *stats);
@@ -312,7 +340,8 @@ MIRORR_API mirorr_status mirorr_bm_last_timings(mirorr_matcher m, float ms[4]);
  * the register-blocked FP32 kernels with a base block inside its mask (window
  * wholly or partly masked), [5] blocks with a partly masked base block (0 for
  * geometries without register-blocked kernels, which search every block with
- * the general kernel). */
+ * the general kernel).  With 16-bit storage: [0], [1] are 0, [4] blocks searched by
+ * the tensor cores, [5] blocks searched by the direct FP32 search. */
 MIRORR_API mirorr_status mirorr_bm_last_diagnostics(mirorr_matcher m, int64_t out[6]);
 /* Count of kernels launched by this context since creation. */
 MIRORR_API int64_t mirorr_ctx_kernel_launches(mirorr_ctx ctx);

@@ -103,7 +103,44 @@ class RegParams(ctypes.Structure):
     _fields_ = [("symmetric", ctypes.c_int32), ("kind", ctypes.c_int32), ("levels", ctypes.c_int32),
                 ("iterations", ctypes.c_int32), ("min_length", ctypes.c_int32), ("bm", BMParams),
                 ("lts_keep", ctypes.c_double), ("verbosity", ctypes.c_int32),
-                ("last_level", ctypes.c_int32)]
+                ("last_level", ctypes.c_int32), ("storage", ctypes.c_int32)]
+
+
+# element types of stored volumes (mirorr_dtype)
+F32, BF16, F16 = 0, 1, 2
+_DTYPES = {"f32": F32, "float32": F32, "bf16": BF16, "bfloat16": BF16, "f16": F16, "float16": F16}
+
+
+def dtype_code(d) -> int:
+    if isinstance(d, int):
+        return d
+    return _DTYPES[str(d).lower()]
+
+
+def to_storage(a, dtype):
+    """float32 array -> its 16-bit storage bit patterns (uint16, round to
+    nearest even), as the library's conversion does; float32 arrays pass
+    through for F32."""
+    d = dtype_code(dtype)
+    a = np.ascontiguousarray(a, np.float32)
+    if d == F32:
+        return a
+    if d == F16:
+        return a.astype(np.float16).view(np.uint16)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return r.astype(np.uint16)
+
+
+def from_storage(bits, dtype):
+    """16-bit storage bit patterns -> float32 values."""
+    d = dtype_code(dtype)
+    if d == F32:
+        return np.ascontiguousarray(bits, np.float32)
+    b = np.ascontiguousarray(bits, np.uint16)
+    if d == F16:
+        return b.view(np.float16).astype(np.float32)
+    return (b.astype(np.uint32) << 16).view(np.float32)
 
 
 class RegStats(ctypes.Structure):
@@ -154,6 +191,9 @@ def lib():
         "mirorr_bm_set_base_mask_device": [vp, vp],
         "mirorr_bm_set_search_mask_device": [vp, vp],
         "mirorr_bm_swap_image_order": [vp],
+        "mirorr_bm_set_storage": [vp, ctypes.c_int32],
+        "mirorr_bm_set_base_image_device16": [vp, P(Geometry), vp],
+        "mirorr_bm_set_search_image_device16": [vp, P(Geometry), vp],
         "mirorr_bm_grid": [vp, vp, vp],
         "mirorr_bm_get_offsets": [vp, ctypes.c_size_t, vp, vp, P(ctypes.c_size_t)],
         "mirorr_bm_block_results": [vp, ctypes.c_size_t, vp, vp, vp, vp, P(ctypes.c_size_t)],
@@ -376,6 +416,19 @@ class BlockMatcher:
     def SetSearchMaskDevice(self, dev_ptr):
         _check(lib().mirorr_bm_set_search_mask_device(self._h, ctypes.c_void_p(dev_ptr) if dev_ptr else None))
 
+    def SetStorage(self, dtype):
+        """Element type of the stored images: "f32" (default), "bf16" or "f16"
+        (no reference counterpart); set it before the images."""
+        _check(lib().mirorr_bm_set_storage(self._h, dtype_code(dtype)))
+
+    def SetBaseImageDevice16(self, geom: Geometry, dev_ptr: int):
+        _check(lib().mirorr_bm_set_base_image_device16(self._h, ctypes.byref(geom),
+                                                       ctypes.c_void_p(dev_ptr)))
+
+    def SetSearchImageDevice16(self, geom: Geometry, dev_ptr: int):
+        _check(lib().mirorr_bm_set_search_image_device16(self._h, ctypes.byref(geom),
+                                                         ctypes.c_void_p(dev_ptr)))
+
     def SwapImageOrder(self):
         _check(lib().mirorr_bm_swap_image_order(self._h))
 
@@ -553,7 +606,7 @@ def lts_noalloc(ctx: Context, t: Transform, n: int, init_dev: int, moved_dev: in
 
 def reg_params(symmetric=True, kind="rigid", levels=0, iterations=5, block_width=4, block_gap=1,
                nhood_gap=3, nhood_width=7, block_keep=1.0, lts_keep=0.5, min_length=32,
-               verbosity=0, last_level=0) -> RegParams:
+               verbosity=0, last_level=0, storage="f32") -> RegParams:
     p = RegParams()
     _check(lib().mirorr_reg_default_params(ctypes.byref(p)))
     p.symmetric = 1 if symmetric else 0
@@ -569,15 +622,24 @@ def reg_params(symmetric=True, kind="rigid", levels=0, iterations=5, block_width
     p.lts_keep = float(lts_keep)
     p.verbosity = int(verbosity)
     p.last_level = int(last_level)
+    p.storage = dtype_code(storage)
     return p
 
 
 def register(ctx: Context, fixed, moving, params: RegParams, fixed_geom: Geometry | None = None,
              moving_geom: Geometry | None = None, fixed_mask=None, moving_mask=None,
              init: Transform | None = None):
-    """Full registration from host arrays.  Returns (Transform, RegStats)."""
-    f = _f32(fixed)
-    m = _f32(moving)
+    """Full registration from host arrays.  Returns (Transform, RegStats).
+    With 16-bit storage (params.storage) float32 arrays are converted with
+    to_storage() first; uint16 arrays are taken as storage bit patterns."""
+    if params.storage == F32:
+        f = _f32(fixed)
+        m = _f32(moving)
+    else:
+        f = fixed if np.asarray(fixed).dtype == np.uint16 else to_storage(fixed, params.storage)
+        m = moving if np.asarray(moving).dtype == np.uint16 else to_storage(moving, params.storage)
+        f = np.ascontiguousarray(f)
+        m = np.ascontiguousarray(m)
     fg = fixed_geom or Geometry.of(f)
     mg = moving_geom or Geometry.of(m)
     res = Transform()

@@ -14,6 +14,9 @@
 //   4. postfilter:  best > 1e-7 && |best - second| > 1e-4 (itkBlockMatcher.txx:884-918),
 //                   deterministic raster-order compaction and block -> mm points
 //                   (itkAbstractBlockMatcher.h:271-287).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "kernels.cuh"
 
 namespace mb2 {
@@ -212,7 +215,12 @@ __device__ inline unsigned long long order_key(double v) {
   return (u & 0x8000000000000000ULL) ? ~u : (u | 0x8000000000000000ULL);
 }
 
-__global__ void block_variance_kernel(const float *__restrict__ img, int nx, int ny, int nbx,
+__device__ __forceinline__ float to_float(float v) { return v; }
+__device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
+
+template <typename T>
+__global__ void block_variance_kernel(const T *__restrict__ img, int nx, int ny, int nbx,
                                       int nby, int nbz, int stx, int sty, int stz, int G, int bw,
                                       double *__restrict__ var, unsigned long long *__restrict__ key) {
   long long nb = (long long)nbx * nby * nbz;
@@ -224,7 +232,7 @@ __global__ void block_variance_kernel(const float *__restrict__ img, int nx, int
     for (int z = 0; z < bw; ++z)
       for (int y = 0; y < bw; ++y)
         for (int x = 0; x < bw; ++x) {
-          float v = __ldg(&img[o + ((long long)z * ny + y) * nx + x]);
+          float v = to_float(img[o + ((long long)z * ny + y) * nx + x]);
           cnt = __dadd_rn(cnt, 1.0);
           sum = __dadd_rn(sum, (double)v);
           float sq = __fmul_rn(v, v);  // float * float in the reference
@@ -294,9 +302,9 @@ __global__ void select_flags_kernel(const double *__restrict__ var, long long n,
     selected[i] = var[i] > cutoff ? 1 : 0;
 }
 
-mirorr_status launch_variance_selection(const BmGeom &g, const float *base, double keep,
+mirorr_status launch_variance_selection(const BmGeom &g, const void *base, double keep,
                                         BmWork &w, const uint8_t **selected_out,
-                                        cudaStream_t s) {
+                                        cudaStream_t s, int dtype) {
   *selected_out = nullptr;
   if (!(keep < 1.0)) return MIRORR_OK;
   long long n = g.nblocks;
@@ -309,9 +317,20 @@ mirorr_status launch_variance_selection(const BmGeom &g, const float *base, doub
   int threads = 256;
   long long blocks = (n + threads - 1) / threads;
   if (blocks > (long long)sm_count() * 32) blocks = (long long)sm_count() * 32;
-  block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
-      base, g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2], g.st[0], g.st[1], g.st[2], g.ngap,
-      g.bw, var, key);
+  // the reference's FP64 variance (exact k-th value, so the selected blocks
+  // are the reference's for any storage type)
+  if (dtype == MIRORR_DTYPE_BF16)
+    block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
+        static_cast<const __nv_bfloat16 *>(base), g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2],
+        g.st[0], g.st[1], g.st[2], g.ngap, g.bw, var, key);
+  else if (dtype == MIRORR_DTYPE_F16)
+    block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
+        static_cast<const __half *>(base), g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2],
+        g.st[0], g.st[1], g.st[2], g.ngap, g.bw, var, key);
+  else
+    block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
+        static_cast<const float *>(base), g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2],
+        g.st[0], g.st[1], g.st[2], g.ngap, g.bw, var, key);
   MB2_LAUNCH_CHECK();
   // cut-off index (unsigned)((1 - keep) * N); index >= N -> the maximum
   unsigned long long idx = (unsigned long long)(unsigned int)((1.0 - keep) * (double)n);

@@ -139,6 +139,7 @@ struct mirorr_ctx_s {
   cudaStream_t stream = nullptr;
   int64_t launches0 = 0;
   BmWork bmw;
+  Bm16Work bm16;
   LtsWork ltsw;
   DevBuf counts;      // long long[4]
   DevBuf ncc_count;   // unsigned long long
@@ -155,7 +156,8 @@ struct mirorr_ctx_s {
 };
 
 struct Vol {
-  const float *img = nullptr;
+  const void *img = nullptr;     // element type: the matcher's storage
+
   const uint8_t *mask = nullptr;
   DevBuf own_img, own_mask;
   bool has = false;
@@ -166,6 +168,7 @@ struct Vol {
 struct mirorr_matcher_s {
   mirorr_ctx ctx = nullptr;
   mirorr_bm_params p{};
+  int storage = MIRORR_DTYPE_F32;  // element type of the stored images
   Vol base, search;
   DevBuf best, second, match, status, pts_b, pts_m;
   BmGeom last{};
@@ -176,6 +179,9 @@ struct mirorr_matcher_s {
 };
 
 namespace {
+
+size_t elem_size(int dtype) { return dtype == MIRORR_DTYPE_F32 ? 4 : (dtype == MIRORR_DTYPE_U8 ? 1 : 2); }
+bool is16(int dtype) { return dtype == MIRORR_DTYPE_BF16 || dtype == MIRORR_DTYPE_F16; }
 
 mirorr_status check_device(int device) {
   int n = 0;
@@ -291,7 +297,8 @@ mirorr_status check_bm_params(const mirorr_bm_params &p) {
 
 // ---- one matcher call on device data ---------------------------------------
 struct MatchCall {
-  const float *base, *search;
+  const void *base, *search;   // element type `dtype`
+  int dtype;
   const uint8_t *bmask, *smask;
   int size[3];
   mirorr_geometry point_geom;  // base image geometry (blockPositionToPoint)
@@ -309,23 +316,38 @@ mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall
     return MIRORR_EINVAL;
   }
   long long nvox = (long long)mc.size[0] * mc.size[1] * mc.size[2];
-  MB2_TRY(c->bmw.stats.ensure(sizeof(float2) * nvox));
+  if (!is16(mc.dtype)) MB2_TRY(c->bmw.stats.ensure(sizeof(float2) * nvox));
   MB2_TRY(best.ensure(sizeof(float) * g.nblocks));
   MB2_TRY(second.ensure(sizeof(float) * g.nblocks));
   MB2_TRY(match.ensure(sizeof(int32_t) * g.nblocks));
   MB2_TRY(status.ensure(g.nblocks));
   cudaStream_t s = c->stream;
-  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], s));
-  MB2_TRY(launch_box_stats(g, mc.search, mc.smask, c->bmw.stats.as<float2>(), s));
-  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], s));
-  const uint8_t *sel = nullptr;
-  MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s));
-  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
   BmOut out{best.as<float>(), second.as<float>(), match.as<int32_t>(), status.as<uint8_t>()};
-  MB2_TRY(launch_ncc(g, mc.base, mc.bmask, mc.search, mc.smask, c->bmw.stats.as<float2>(), sel,
-                     out, c->bmw, c->ncc_count.as<unsigned long long>(), s, kev, xl_count,
-                     xl_ran));
-  if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[3], s));
+  if (is16(mc.dtype)) {
+    // 16-bit storage: box statistics, selection and search of tc.cu
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], s));
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], s));
+    const uint8_t *sel = nullptr;
+    MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s, mc.dtype));
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
+    MB2_TRY(launch_match16(mc.dtype, g, mc.base, mc.bmask, mc.search, mc.smask, sel, out, c->bm16,
+                           c->ncc_count.as<unsigned long long>(), s));
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[3], s));
+    if (xl_ran) *xl_ran = false;
+  } else {
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], s));
+    MB2_TRY(launch_box_stats(g, static_cast<const float *>(mc.search), mc.smask,
+                             c->bmw.stats.as<float2>(), s));
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], s));
+    const uint8_t *sel = nullptr;
+    MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s));
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
+    MB2_TRY(launch_ncc(g, static_cast<const float *>(mc.base), mc.bmask,
+                       static_cast<const float *>(mc.search), mc.smask, c->bmw.stats.as<float2>(),
+                       sel, out, c->bmw, c->ncc_count.as<unsigned long long>(), s, kev, xl_count,
+                       xl_ran));
+    if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[3], s));
+  }
   PointGeom pg;
   point_geom(mc.point_geom.origin, mc.point_geom.spacing, mc.point_geom.direction,
              (int)p.block_width, pg);
@@ -439,12 +461,16 @@ void level_geometry(const mirorr_geometry &in, const int f[3], mirorr_geometry &
 }
 
 // Builds one pyramid level on the device.  When every factor is 1 the input
-// itself is the level (*out_ptr = in, no copy).
-mirorr_status make_level(mirorr_ctx c, const mirorr_geometry &ig, const float *in,
-                         const int f[3], mirorr_geometry &og, DevBuf &out, const float **out_ptr) {
+// itself is the level (*out_ptr = in, no copy, the input's element type);
+// otherwise the level is float32 (the first smoothing pass reads the input's
+// type).
+mirorr_status make_level(mirorr_ctx c, const mirorr_geometry &ig, const void *in, int in_dtype,
+                         const int f[3], mirorr_geometry &og, DevBuf &out, const void **out_ptr,
+                         int *out_dtype) {
   level_geometry(ig, f, og);
   if (f[0] == 1 && f[1] == 1 && f[2] == 1) {
     *out_ptr = in;
+    *out_dtype = in_dtype;
     return MIRORR_OK;
   }
   cudaStream_t s = c->stream;
@@ -462,14 +488,16 @@ mirorr_status make_level(mirorr_ctx c, const mirorr_geometry &ig, const float *i
     rad[d] = gaussian_weights(f[d], w[d]);
   }
   MB2_CUDA_TRY(cudaMemcpyAsync(c->weights.ptr, w, sizeof(w), cudaMemcpyHostToDevice, s));
-  const float *cur = in;
+  const void *cur = in;
+  int cur_t = in_dtype;
   float *bufs[2] = {c->tmp_a.as<float>(), c->tmp_b.as<float>()};
   int bi = 0;
   for (int d = 0; d < 3; ++d) {
     if (f[d] <= 1) continue;
     MB2_TRY(launch_smooth_axis(ig.size, cur, bufs[bi], d, c->weights.as<double>() + 64 * d,
-                               rad[d], s));
+                               rad[d], s, cur_t));
     cur = bufs[bi];
+    cur_t = MIRORR_DTYPE_F32;
     bi ^= 1;
   }
   MB2_TRY(out.ensure(sizeof(float) * vox(og.size)));
@@ -479,14 +507,20 @@ mirorr_status make_level(mirorr_ctx c, const mirorr_geometry &ig, const float *i
     m.C[4 * d] = (double)f[d];
     m.e[d] = ((double)f[d] - 1.0) / 2.0;
   }
+  if (cur_t != MIRORR_DTYPE_F32) {
+    set_error("a pyramid factor above 1 on some axis is required to smooth a 16-bit level");
+    return MIRORR_EINVAL;
+  }
   MB2_TRY(launch_resample(ig.size, cur, nullptr, og.size, m, out.as<float>(), nullptr, s));
   *out_ptr = out.as<float>();
+  *out_dtype = MIRORR_DTYPE_F32;
   return MIRORR_OK;
 }
 
 // ---- registration ----------------------------------------------------------
 struct RegImage {
-  const float *img;
+  const void *img;
+  int dtype;        // element type of img
   mirorr_geometry g;
 };
 
@@ -502,14 +536,14 @@ struct RegRun {
 
 mirorr_status resample_into(mirorr_ctx c, const RegImage &src, const uint8_t *mask,
                             const mirorr_geometry &mask_g, const mirorr_geometry &grid,
-                            const Tfm &t, DevBuf &img, DevBuf &msk) {
+                            const Tfm &t, DevBuf &img, DevBuf &msk, int out_dtype) {
   ResampleMap mi, mm;
   if (!make_map(grid, src.g, t.M, t.off, mi) || !make_map(grid, mask_g, t.M, t.off, mm)) {
     set_error("singular image geometry");
     return MIRORR_EINVAL;
   }
   long long n = vox(grid.size);
-  MB2_TRY(img.ensure(sizeof(float) * n));
+  MB2_TRY(img.ensure(elem_size(out_dtype) * n));
   MB2_TRY(msk.ensure(n));
   cudaEvent_t *ev = c->timer.on ? c->timer.take_resample(n) : nullptr;
   if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], c->stream));
@@ -518,11 +552,11 @@ mirorr_status resample_into(mirorr_ctx c, const RegImage &src, const uint8_t *ma
   if (same_grid) {
     // image and mask on one input grid (the finest level): one pass computes
     // each voxel's index map once for both
-    MB2_TRY(launch_resample(src.g.size, src.img, mask, grid.size, mi, img.as<float>(),
-                            msk.as<uint8_t>(), c->stream));
+    MB2_TRY(launch_resample(src.g.size, src.img, mask, grid.size, mi, img.ptr, msk.as<uint8_t>(),
+                            c->stream, false, src.dtype, out_dtype));
   } else {
-    MB2_TRY(launch_resample(src.g.size, src.img, nullptr, grid.size, mi, img.as<float>(), nullptr,
-                            c->stream));
+    MB2_TRY(launch_resample(src.g.size, src.img, nullptr, grid.size, mi, img.ptr, nullptr,
+                            c->stream, false, src.dtype, out_dtype));
     MB2_TRY(launch_resample(mask_g.size, nullptr, mask, grid.size, mm, nullptr,
                             msk.as<uint8_t>(), c->stream));
   }
@@ -534,14 +568,17 @@ mirorr_status run_lts(RegRun &r, LtsState &hs, long long nmax, long long *n_used
   int inner = 0;
   mirorr_ctx c = r.c;
   unsigned int gave_up = 0;
+  const unsigned int *watch = is16(r.p->storage)
+                                  ? (c->bm16.ctl.ptr ? c->bm16.ctl.as<unsigned int>() + 2 : nullptr)
+                                  : ncc_timeout_flag(c->bmw);
   MB2_TRY(lts_run(c->ltsw, hs, c->pts_i.as<double>(), c->pts_m.as<double>(),
-                  c->counts.as<long long>(), nmax, c->stream, &inner, n_used,
-                  ncc_timeout_flag(c->bmw), &gave_up));
+                  c->counts.as<long long>(), nmax, c->stream, &inner, n_used, watch, &gave_up));
   if (gave_up) {
     // a CTA of the search gave up its bounded wait on a tensor copy: that
     // call's scores (and so this fit) cannot be trusted; the registration stops
     bool to = false;
-    MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
+    if (is16(r.p->storage)) MB2_CUDA_TRY(cudaMemsetAsync(c->bm16.ctl.ptr, 0, 16, c->stream));
+    else MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
     set_error("a bounded wait on a tensor copy of the NCC search gave up");
     return MIRORR_ETIMEOUT;
   }
@@ -583,12 +620,12 @@ void grid_geom(const double *origin, const double *spacing, const int *size,
   for (int i = 0; i < 9; ++i) g.direction[i] = direction[i];
 }
 
-mirorr_status match_into(RegRun &r, const float *base, const uint8_t *bmask, const float *search,
+mirorr_status match_into(RegRun &r, const void *base, const uint8_t *bmask, const void *search,
                          const uint8_t *smask, const mirorr_geometry &base_g, double *pts_b,
                          double *pts_m, int count_slot, const long long *offset_dev) {
   mirorr_ctx c = r.c;
-  MatchCall mc{base, search, bmask, smask, {base_g.size[0], base_g.size[1], base_g.size[2]},
-               base_g};
+  MatchCall mc{base, search, r.p->storage, bmask, smask,
+               {base_g.size[0], base_g.size[1], base_g.size[2]}, base_g};
   BmGeom g;
   cudaEvent_t *ev = c->timer.on ? c->timer.take(StageTimer::kPerCall) : nullptr;
   bool xl_ran = false;
@@ -626,7 +663,7 @@ mirorr_status classic_level(RegRun &r, const RegImage &fl, const RegImage &ml, T
   grid_geom(origin, spacing, size, ml.g.direction, grid_m);
   Tfm ident;
   tfm_identity(ident, KIND_AFFINE);
-  MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, ident, c->img_b, c->msk_b));
+  MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, ident, c->img_b, c->msk_b, p.storage));
   BmGeom g;
   if (!bm_geometry(size, (int)p.bm.block_width, (int)p.bm.block_gap, (int)p.bm.nhood_gap,
                    (int)p.bm.nhood_width, g)) {
@@ -639,9 +676,9 @@ mirorr_status classic_level(RegRun &r, const RegImage &fl, const RegImage &ml, T
   int np = tfm_nparams(tfm);
   int it = 0;
   for (; it < std::abs(p.iterations); ++it) {
-    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, tfm, c->img_s, c->msk_s));
+    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, tfm, c->img_s, c->msk_s, p.storage));
     MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
-    MB2_TRY(match_into(r, c->img_b.as<float>(), c->msk_b.as<uint8_t>(), c->img_s.as<float>(),
+    MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
                        c->msk_s.as<uint8_t>(), grid_m, c->pts_i.as<double>(),
                        c->pts_m.as<double>(), 0, nullptr));
     LtsState hs;
@@ -716,16 +753,16 @@ mirorr_status symmetric_level(RegRun &r, const RegImage &fl, const RegImage &ml,
   for (; it < std::abs(p.iterations); ++it) {
     Tfm cF, cB;
     centered(cF, cB);
-    MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, cB, c->img_b, c->msk_b));
-    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, cF, c->img_s, c->msk_s));
+    MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, cB, c->img_b, c->msk_b, p.storage));
+    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, cF, c->img_s, c->msk_s, p.storage));
     MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
     double *pi = c->pts_i.as<double>(), *pmv = c->pts_m.as<double>();
     // forward: base = moving, search = fixed
-    MB2_TRY(match_into(r, c->img_b.as<float>(), c->msk_b.as<uint8_t>(), c->img_s.as<float>(),
+    MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
                        c->msk_s.as<uint8_t>(), grid_m, pi, pmv, 0, nullptr));
     // swapped: base = fixed, search = moving; its lists are appended with
     // roles reversed (itkSymMirorrRegistrationMethod.txx:595-602)
-    MB2_TRY(match_into(r, c->img_s.as<float>(), c->msk_s.as<uint8_t>(), c->img_b.as<float>(),
+    MB2_TRY(match_into(r, c->img_s.ptr, c->msk_s.as<uint8_t>(), c->img_b.ptr,
                        c->msk_b.as<uint8_t>(), grid_f, pmv, pi, 1, c->counts.as<long long>()));
     LtsState hs;
     memset(&hs, 0, sizeof(hs));
@@ -758,8 +795,8 @@ mirorr_status symmetric_level(RegRun &r, const RegImage &fl, const RegImage &ml,
   return MIRORR_OK;
 }
 
-mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float *fixed,
-                            const uint8_t *fmask, const mirorr_geometry *mg, const float *moving,
+mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const void *fixed,
+                            const uint8_t *fmask, const mirorr_geometry *mg, const void *moving,
                             const uint8_t *mmask, const mirorr_reg_params *p,
                             const mirorr_transform *init, mirorr_transform *result,
                             mirorr_reg_stats *stats) {
@@ -776,6 +813,10 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float
     return MIRORR_EINVAL;
   }
   MB2_TRY(check_bm_params(p->bm));
+  if (p->storage != MIRORR_DTYPE_F32 && !is16(p->storage)) {
+    set_error("storage must be MIRORR_DTYPE_F32, _BF16 or _F16 (got %d)", p->storage);
+    return MIRORR_EINVAL;
+  }
   if (!(p->lts_keep > 0.0 && p->lts_keep <= 1.0)) {
     set_error("lts_keep must lie in (0, 1]");
     return MIRORR_EINVAL;
@@ -815,8 +856,8 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float
   tfm_params(tfm, params);
   for (int lev = 0; lev < nl; ++lev) {
     RegImage fl, ml;
-    MB2_TRY(make_level(c, *fg, fixed, sf[lev], fl.g, c->lvl_f, &fl.img));
-    MB2_TRY(make_level(c, *mg, moving, sm[lev], ml.g, c->lvl_m, &ml.img));
+    MB2_TRY(make_level(c, *fg, fixed, pp.storage, sf[lev], fl.g, c->lvl_f, &fl.img, &fl.dtype));
+    MB2_TRY(make_level(c, *mg, moving, pp.storage, sm[lev], ml.g, c->lvl_m, &ml.img, &ml.dtype));
     tfm_set_params(tfm, params);
     r.level = lev;
     if (pp.symmetric) MB2_TRY(symmetric_level(r, fl, ml, tfm));
@@ -825,9 +866,10 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const float
   }
   tfm_set_params(tfm, params);
   {
-    bool to = false;
+    bool to = false, to16 = false;
     MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
-    if (to) {
+    MB2_TRY(match16_take_timeout(c->bm16, c->stream, &to16));
+    if (to || to16) {
       set_error("a bounded wait on a tensor copy of the NCC search gave up");
       return MIRORR_ETIMEOUT;
     }
@@ -892,7 +934,9 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
                     &c->ncc_count, &c->ones, &c->lvl_f, &c->lvl_m, &c->tmp_a, &c->tmp_b,
                     &c->weights, &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best,
                     &c->second, &c->match, &c->status, &c->pts_i, &c->pts_m, &c->up_f,
-                    &c->up_m, &c->up_fm, &c->up_mm};
+                    &c->up_m, &c->up_fm, &c->up_mm, &c->bm16.stats, &c->bm16.wand,
+                    &c->bm16.prep, &c->bm16.xs, &c->bm16.ctl, &c->bm16.fb_list,
+                    &c->bm16.chunked};
   for (DevBuf *b : bufs) b->release();
   c->timer.release();
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1023,18 +1067,42 @@ mirorr_status mirorr_bm_set_metric(mirorr_matcher m, const char *name) {
   return MIRORR_EINVAL;
 }
 
+// Sets an image.  host: float32 copied to the device; dev32: a float32 device
+// buffer; dev16: a device buffer already in the 16-bit storage type.  With
+// 16-bit storage, float32 input is converted (round to nearest) into a copy
+// the matcher owns; with float32 storage a device buffer is borrowed.
+enum class ImgSrc { host, dev32, dev16 };
+
 static mirorr_status set_image(mirorr_matcher m, Vol &v, const mirorr_geometry *g,
-                               const float *p, bool host) {
+                               const void *p, ImgSrc src) {
   if (!m || !g || !p) { set_error("null argument"); return MIRORR_EINVAL; }
   if (!valid_geom(g)) { set_error("invalid geometry"); return MIRORR_EINVAL; }
   MB2_CUDA_TRY(cudaSetDevice(m->ctx->device));
-  if (host) {
-    MB2_TRY(upload(m->ctx, v.own_img, p, sizeof(float) * vox(g->size)));
-    v.img = v.own_img.as<float>();
-  } else {
+  const long long n = vox(g->size);
+  if (src == ImgSrc::dev16) {
+    if (!is16(m->storage)) {
+      set_error("16-bit images need BF16 or F16 storage (mirorr_bm_set_storage)");
+      return MIRORR_ESTATE;
+    }
     v.img = p;
+  } else if (!is16(m->storage)) {
+    if (src == ImgSrc::host) {
+      MB2_TRY(upload(m->ctx, v.own_img, p, sizeof(float) * n));
+      v.img = v.own_img.ptr;
+    } else {
+      v.img = p;
+    }
+  } else {
+    const float *f32 = static_cast<const float *>(p);
+    if (src == ImgSrc::host) {
+      MB2_TRY(upload(m->ctx, m->ctx->up_f, p, sizeof(float) * n));
+      f32 = m->ctx->up_f.as<float>();
+    }
+    MB2_TRY(v.own_img.ensure(2 * n));
+    MB2_TRY(launch_to16(f32, v.own_img.ptr, n, m->storage, m->ctx->stream));
+    v.img = v.own_img.ptr;
   }
-  if (v.has && vox(v.geom.size) != vox(g->size) && v.has_mask) {
+  if (v.has && vox(v.geom.size) != n && v.has_mask) {
     v.has_mask = false;  // a mask of the old size no longer applies
     v.mask = nullptr;
   }
@@ -1065,18 +1133,41 @@ static mirorr_status set_mask(mirorr_matcher m, Vol &v, const uint8_t *p, bool h
 }
 
 mirorr_status mirorr_bm_set_base_image(mirorr_matcher m, const mirorr_geometry *g, const float *h) {
-  return set_image(m, m->base, g, h, true);
+  return m ? set_image(m, m->base, g, h, ImgSrc::host) : MIRORR_EINVAL;
 }
 mirorr_status mirorr_bm_set_search_image(mirorr_matcher m, const mirorr_geometry *g, const float *h) {
-  return set_image(m, m->search, g, h, true);
+  return m ? set_image(m, m->search, g, h, ImgSrc::host) : MIRORR_EINVAL;
 }
 mirorr_status mirorr_bm_set_base_image_device(mirorr_matcher m, const mirorr_geometry *g,
                                               const float *d) {
-  return set_image(m, m->base, g, d, false);
+  return m ? set_image(m, m->base, g, d, ImgSrc::dev32) : MIRORR_EINVAL;
 }
 mirorr_status mirorr_bm_set_search_image_device(mirorr_matcher m, const mirorr_geometry *g,
                                                 const float *d) {
-  return set_image(m, m->search, g, d, false);
+  return m ? set_image(m, m->search, g, d, ImgSrc::dev32) : MIRORR_EINVAL;
+}
+mirorr_status mirorr_bm_set_storage(mirorr_matcher m, int32_t dtype) {
+  if (!m) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (dtype != MIRORR_DTYPE_F32 && !is16(dtype)) {
+    set_error("storage must be MIRORR_DTYPE_F32, _BF16 or _F16 (got %d)", dtype);
+    return MIRORR_EINVAL;
+  }
+  if (dtype != m->storage) {
+    // images of the old type no longer apply
+    m->base.has = m->search.has = false;
+    m->base.img = m->search.img = nullptr;
+    m->has_results = false;
+  }
+  m->storage = dtype;
+  return MIRORR_OK;
+}
+mirorr_status mirorr_bm_set_base_image_device16(mirorr_matcher m, const mirorr_geometry *g,
+                                                const void *d) {
+  return m ? set_image(m, m->base, g, d, ImgSrc::dev16) : MIRORR_EINVAL;
+}
+mirorr_status mirorr_bm_set_search_image_device16(mirorr_matcher m, const mirorr_geometry *g,
+                                                  const void *d) {
+  return m ? set_image(m, m->search, g, d, ImgSrc::dev16) : MIRORR_EINVAL;
 }
 mirorr_status mirorr_bm_set_base_mask(mirorr_matcher m, const uint8_t *h) {
   return m ? set_mask(m, m->base, h, true) : MIRORR_EINVAL;
@@ -1145,7 +1236,7 @@ mirorr_status mirorr_bm_get_offsets(mirorr_matcher m, size_t capacity, double *b
   MB2_TRY(m->pts_b.ensure(sizeof(double) * 3 * g.nblocks));
   MB2_TRY(m->pts_m.ensure(sizeof(double) * 3 * g.nblocks));
   MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
-  MatchCall mc{m->base.img, m->search.img, bmask, smask,
+  MatchCall mc{m->base.img, m->search.img, m->storage, bmask, smask,
                {m->base.geom.size[0], m->base.geom.size[1], m->base.geom.size[2]},
                m->base.geom};
   MB2_TRY(run_match(c, m->p, mc, g, m->best, m->second, m->match, m->status,
@@ -1158,7 +1249,8 @@ mirorr_status mirorr_bm_get_offsets(mirorr_matcher m, size_t capacity, double *b
   for (int s = 0; s < 4; ++s) cudaEventElapsedTime(&m->timings[s], m->ev[s], m->ev[s + 1]);
   {
     bool to = false;
-    MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
+    if (is16(m->storage)) MB2_TRY(match16_take_timeout(c->bm16, c->stream, &to));
+    else MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
     if (to) {
       set_error("a bounded wait on a tensor copy of the NCC search gave up");
       return MIRORR_ETIMEOUT;
@@ -1215,6 +1307,17 @@ mirorr_status mirorr_bm_last_diagnostics(mirorr_matcher m, int64_t out[6]) {
   if (!m->has_results) { set_error("no results: call GetOffsets first"); return MIRORR_ESTATE; }
   unsigned int ctl[8] = {0};
   MB2_CUDA_TRY(cudaSetDevice(m->ctx->device));
+  if (is16(m->storage)) {
+    unsigned int c16[2] = {0, 0};
+    MB2_TRY(match16_counts(m->ctx->bm16, m->ctx->stream, c16));
+    out[0] = 0;
+    out[1] = 0;
+    out[2] = m->kept;
+    out[3] = m->last.nblocks;
+    out[4] = c16[0];
+    out[5] = c16[1];
+    return MIRORR_OK;
+  }
   MB2_CUDA_TRY(cudaMemcpy(ctl, m->ctx->bmw.ncc_ctl.ptr, sizeof(ctl), cudaMemcpyDeviceToHost));
   out[0] = ctl[2];
   out[1] = ctl[1];
@@ -1538,9 +1641,9 @@ mirorr_status mirorr_reg_default_params(mirorr_reg_params *p) {
   return MIRORR_OK;
 }
 
-mirorr_status mirorr_register_device(mirorr_ctx c, const mirorr_geometry *fg, const float *fixed,
+mirorr_status mirorr_register_device(mirorr_ctx c, const mirorr_geometry *fg, const void *fixed,
                                      const uint8_t *fmask, const mirorr_geometry *mg,
-                                     const float *moving, const uint8_t *mmask,
+                                     const void *moving, const uint8_t *mmask,
                                      const mirorr_reg_params *p, const mirorr_transform *init,
                                      mirorr_transform *result, mirorr_reg_stats *stats) {
   if (!c) { set_error("null argument"); return MIRORR_EINVAL; }
@@ -1548,25 +1651,30 @@ mirorr_status mirorr_register_device(mirorr_ctx c, const mirorr_geometry *fg, co
   return register_impl(c, fg, fixed, fmask, mg, moving, mmask, p, init, result, stats);
 }
 
-mirorr_status mirorr_register(mirorr_ctx c, const mirorr_geometry *fg, const float *fixed,
-                              const uint8_t *fmask, const mirorr_geometry *mg, const float *moving,
+mirorr_status mirorr_register(mirorr_ctx c, const mirorr_geometry *fg, const void *fixed,
+                              const uint8_t *fmask, const mirorr_geometry *mg, const void *moving,
                               const uint8_t *mmask, const mirorr_reg_params *p,
                               const mirorr_transform *init, mirorr_transform *result,
                               mirorr_reg_stats *stats) {
-  if (!c || !fg || !mg || !fixed || !moving) { set_error("null argument"); return MIRORR_EINVAL; }
+  if (!c || !fg || !mg || !fixed || !moving || !p) { set_error("null argument"); return MIRORR_EINVAL; }
   if (!valid_geom(fg) || !valid_geom(mg)) { set_error("invalid image geometry"); return MIRORR_EINVAL; }
+  if (p->storage != MIRORR_DTYPE_F32 && !is16(p->storage)) {
+    set_error("storage must be MIRORR_DTYPE_F32, _BF16 or _F16 (got %d)", p->storage);
+    return MIRORR_EINVAL;
+  }
   MB2_CUDA_TRY(cudaSetDevice(c->device));
   auto t0 = std::chrono::steady_clock::now();
-  MB2_TRY(upload(c, c->up_f, fixed, sizeof(float) * vox(fg->size)));
-  MB2_TRY(upload(c, c->up_m, moving, sizeof(float) * vox(mg->size)));
+  const size_t es = elem_size(p->storage);
+  MB2_TRY(upload(c, c->up_f, fixed, es * vox(fg->size)));
+  MB2_TRY(upload(c, c->up_m, moving, es * vox(mg->size)));
   const uint8_t *dfm = nullptr, *dmm = nullptr;
   if (fmask) { MB2_TRY(upload(c, c->up_fm, fmask, vox(fg->size))); dfm = c->up_fm.as<uint8_t>(); }
   if (mmask) { MB2_TRY(upload(c, c->up_mm, mmask, vox(mg->size))); dmm = c->up_mm.as<uint8_t>(); }
-  mirorr_status s = register_impl(c, fg, c->up_f.as<float>(), dfm, mg, c->up_m.as<float>(), dmm, p,
-                                  init, result, stats);
+  mirorr_status s = register_impl(c, fg, c->up_f.ptr, dfm, mg, c->up_m.ptr, dmm, p, init, result,
+                                  stats);
   if (s == MIRORR_OK && stats) {
     stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    stats->h2d_bytes += (int64_t)(sizeof(float) * (vox(fg->size) + vox(mg->size)) +
+    stats->h2d_bytes += (int64_t)(es * (vox(fg->size) + vox(mg->size)) +
                                   (fmask ? vox(fg->size) : 0) + (mmask ? vox(mg->size) : 0));
   }
   return s;
@@ -1604,8 +1712,9 @@ mirorr_status mirorr_pyramid_level(mirorr_ctx c, const mirorr_geometry *ig, cons
     return MIRORR_ERANGE;
   }
   MB2_TRY(upload(c, c->up_f, in, sizeof(float) * vox(ig->size)));
-  const float *lp = nullptr;
-  MB2_TRY(make_level(c, *ig, c->up_f.as<float>(), factors, g, c->lvl_f, &lp));
+  const void *lp = nullptr;
+  int lt = MIRORR_DTYPE_F32;
+  MB2_TRY(make_level(c, *ig, c->up_f.ptr, MIRORR_DTYPE_F32, factors, g, c->lvl_f, &lp, &lt));
   MB2_CUDA_TRY(cudaMemcpyAsync(out, lp, sizeof(float) * vox(g.size), cudaMemcpyDeviceToHost, c->stream));
   MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
   *og = g;

@@ -54,9 +54,10 @@ void point_geom(const double origin[3], const double spacing[3], const double di
 
 mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8_t *smask,
                                float2 *stats, cudaStream_t s);
-mirorr_status launch_variance_selection(const BmGeom &g, const float *base, double keep,
+// base: float32, or 16-bit when dtype is MIRORR_DTYPE_BF16 / _F16.
+mirorr_status launch_variance_selection(const BmGeom &g, const void *base, double keep,
                                         BmWork &w, const uint8_t **selected_out,
-                                        cudaStream_t s);
+                                        cudaStream_t s, int dtype = MIRORR_DTYPE_F32);
 // ncc_count (optional): device counter incremented by the number of candidate
 // scores evaluated.  Profiling (optional): kev[0], kev[1] are recorded around
 // the per-x-lane search kernel's launch and xl_count adds up the candidates it
@@ -81,14 +82,44 @@ mirorr_status launch_postfilter(const BmGeom &g, const BmOut &out, BmWork &w,
                                 long long *count_dev, const long long *offset_dev,
                                 cudaStream_t s);
 
+// Scratch of the 16-bit storage search (tc.cu).
+struct Bm16Work {
+  DevBuf stats;    // float2 per search position: (mean, Syy), Syy sign bit = footprint leaves the mask
+  DevBuf wand;     // window-AND passes and the per-block flags
+  DevBuf prep;     // per-block base statistics
+  DevBuf xs;       // per-block 16-bit parts of the centred base block
+  DevBuf ctl;      // [0] tensor blocks, [1] direct blocks, [2] a bounded wait gave up
+  DevBuf fb_list;  // blocks of the direct search
+  DevBuf chunked;  // x-chunked copy of the search image for the window tensor copies
+};
+// One matcher call on 16-bit images (dtype MIRORR_DTYPE_BF16 or _F16): box
+// statistics, base-block preparation, the tensor-core search and the direct
+// FP32 search of the blocks the tensor form does not take.  Writes `out` for
+// every block (the post-filter follows as for the FP32 path).
+mirorr_status launch_match16(int dtype, const BmGeom &g, const void *base, const uint8_t *bmask,
+                             const void *search, const uint8_t *smask, const uint8_t *selected,
+                             const BmOut &out, Bm16Work &w, unsigned long long *ncc_count,
+                             cudaStream_t s);
+// True when a bounded wait of the 16-bit search gave up (synchronises).
+mirorr_status match16_take_timeout(Bm16Work &w, cudaStream_t s, bool *timed_out);
+// Blocks of the last 16-bit search taken by [0] the tensor form, [1] the
+// direct search (synchronises).
+mirorr_status match16_counts(Bm16Work &w, cudaStream_t s, unsigned int out[2]);
+
 // Linear resampling with an explicit affine index map (see mirorr_b200.h).
 struct ResampleMap {
   double C[9];
   double e[3];
 };
-mirorr_status launch_resample(const int in_size[3], const float *in, const uint8_t *in_mask,
-                              const int out_size[3], const ResampleMap &map, float *out,
-                              uint8_t *out_mask, cudaStream_t s, bool nearest = false);
+// in / out: float32, or 16-bit per in_dtype / out_dtype (MIRORR_DTYPE_*):
+// F32 -> F32, F32 -> BF16/F16, and BF16 -> BF16 / F16 -> F16.  A 16-bit output
+// is the float result rounded to the storage type.
+mirorr_status launch_resample(const int in_size[3], const void *in, const uint8_t *in_mask,
+                              const int out_size[3], const ResampleMap &map, void *out,
+                              uint8_t *out_mask, cudaStream_t s, bool nearest = false,
+                              int in_dtype = MIRORR_DTYPE_F32, int out_dtype = MIRORR_DTYPE_F32);
+// float32 -> BF16 / F16 (round to nearest even).
+mirorr_status launch_to16(const float *in, void *out, long long n, int dtype, cudaStream_t s);
 // Final-resampling interpolators (interp.cu): cubic B-spline (coef: FP64
 // scratch of the input's size) and Welch-windowed sinc of radius 5.
 mirorr_status launch_resample_bspline(const int in_size[3], const float *in, const int out_size[3],
@@ -97,8 +128,9 @@ mirorr_status launch_resample_bspline(const int in_size[3], const float *in, con
 mirorr_status launch_resample_sinc(const int in_size[3], const float *in, const int out_size[3],
                                    const ResampleMap &map, float *out, cudaStream_t s);
 // Separable Gaussian smoothing along one axis (axis 0 = x).
-mirorr_status launch_smooth_axis(const int size[3], const float *in, float *out, int axis,
-                                 const double *w, int radius, cudaStream_t s);
+mirorr_status launch_smooth_axis(const int size[3], const void *in, float *out, int axis,
+                                 const double *w, int radius, cudaStream_t s,
+                                 int in_dtype = MIRORR_DTYPE_F32);
 mirorr_status launch_fill_u8(uint8_t *p, long long n, uint8_t v, cudaStream_t s);
 
 // LTS fit on device (one cooperative launch for the whole inner loop).
@@ -121,6 +153,11 @@ mirorr_status lts_run(LtsWork &w, LtsState &host_state, const double *init_dev,
                       cudaStream_t s, int *inner_iters, long long *n_used,
                       const unsigned int *watch_dev = nullptr,
                       unsigned int *watch_host = nullptr);
+// Window-AND of the footprint-in-mask flags of box statistics (sign bit of
+// the second field), per block of g: 1 when every candidate footprint of the
+// block's window that lies in the volume is wholly inside the search mask.
+mirorr_status launch_window_and(const BmGeom &g, const float2 *stats, DevBuf &buf,
+                                const uint8_t **wand, cudaStream_t s);
 // The NCC stage's give-up flag (device word), or nullptr before any search.
 const unsigned int *ncc_timeout_flag(const BmWork &w);
 // lts_run with every scratch buffer in a static device array sized for

@@ -2055,6 +2055,24 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
   }
 }
 
+mirorr_status launch_window_and(const BmGeom &g, const float2 *stats, DevBuf &buf,
+                                const uint8_t **wand, cudaStream_t s) {
+  const int nx = g.size[0], ny = g.size[1], nz = g.size[2];
+  const size_t n1 = (size_t)g.nb[0] * ny * nz, n2 = (size_t)g.nb[0] * g.nb[1] * nz;
+  MB2_TRY(buf.ensure(n1 + n2 + (size_t)g.nblocks));
+  uint8_t *b1 = buf.as<uint8_t>(), *b2 = b1 + n1, *b3 = b2 + n2;
+  const unsigned grid = (unsigned)sm_count() * 8;
+  wand_x_kernel<<<grid, 256, 0, s>>>(stats, b1, nx, ny, nz, g.nb[0], g.st[0], g.ngap, g.nw, g.bw);
+  MB2_LAUNCH_CHECK();
+  wand_axis_kernel<<<grid, 256, 0, s>>>(b1, b2, g.nb[0], ny, nz, g.nb[1], g.st[1], g.ngap, g.nw);
+  MB2_LAUNCH_CHECK();
+  wand_axis_kernel<<<grid, 256, 0, s>>>(b2, b3, (long long)g.nb[0] * g.nb[1], nz, 1, g.nb[2],
+                                        g.st[2], g.ngap, g.nw);
+  MB2_LAUNCH_CHECK();
+  *wand = b3;
+  return MIRORR_OK;
+}
+
 const unsigned int *ncc_timeout_flag(const BmWork &w) {
   return w.ncc_ctl.ptr ? w.ncc_ctl.as<unsigned int>() + 5 : nullptr;
 }

@@ -16,21 +16,42 @@
 // computes each voxel's index map once for both.
 // The FP64 arithmetic is written with explicit round-to-nearest intrinsics so
 // results are bit-identical to a plain C evaluation of the same expressions.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "kernels.cuh"
 
 namespace mb2 {
 
 struct ResampleArgs {
-  const float *in;
+  const void *in;  // float32, or 16-bit (kernel template type)
   const uint8_t *inm;
   int inx, iny, inz;
   int onx, ony, onz;
   double C[9];
   double e[3];
-  float *out;
+  void *out;       // float32, or 16-bit
   uint8_t *outm;
   int nearest;  // nearest-neighbour instead of linear interpolation
 };
+
+__device__ __forceinline__ float ld_f(const float *p, long long i) { return __ldg(p + i); }
+__device__ __forceinline__ float ld_f(const __nv_bfloat16 *p, long long i) {
+  return __bfloat162float(p[i]);
+}
+__device__ __forceinline__ float ld_f(const __half *p, long long i) { return __half2float(p[i]); }
+// An interpolated FP64 value as stored: rounded to float, then (16-bit
+// storage) rounded again to the storage type.
+__device__ __forceinline__ void st_v(float &d, double v) { d = __double2float_rn(v); }
+__device__ __forceinline__ void st_v(__nv_bfloat16 &d, double v) {
+  d = __float2bfloat16_rn(__double2float_rn(v));
+}
+__device__ __forceinline__ void st_v(__half &d, double v) {
+  d = __float2half_rn(__double2float_rn(v));
+}
+__device__ __forceinline__ void st_copy(float &d, float v) { d = v; }
+__device__ __forceinline__ void st_copy(__nv_bfloat16 &d, float v) { d = __float2bfloat16_rn(v); }
+__device__ __forceinline__ void st_copy(__half &d, float v) { d = __float2half_rn(v); }
 
 __device__ inline double dlerp(double a, double b, double t) {
   return __dadd_rn(a, __dmul_rn(__dsub_rn(b, a), t));
@@ -39,9 +60,10 @@ __device__ inline double dlerp(double a, double b, double t) {
 // Linear or nearest resampling of one output voxel (i, j, k); cj, ck hold
 // C[r][1] * j and C[r][2] * k (products the whole x-run shares).  Writes the
 // image value to *v and the mask value to *m when the respective input exists.
-template <bool IMG, bool MSK>
+template <bool IMG, bool MSK, typename TI, typename TO>
 __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, const double cj[3],
-                                               const double ck[3], float *v, uint8_t *m) {
+                                               const double ck[3], TO *v, uint8_t *m) {
+  const TI *in = static_cast<const TI *>(a.in);
   const double di = (double)i;
   double c[3];
 #pragma unroll
@@ -53,7 +75,7 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
   for (int r = 0; r < 3; ++r)
     if (!(c[r] >= -0.5 && c[r] < (double)nn[r] - 0.5)) inside = false;
   if (!inside) {
-    if (IMG) *v = 0.0f;
+    if (IMG) st_copy(*v, 0.0f);
     if (MSK) *m = 0;
     return;
   }
@@ -68,7 +90,7 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
       q += (long long)b * stride;
       stride *= nn[r];
     }
-    if (IMG) *v = __ldg(a.in + q);
+    if (IMG) st_copy(*v, ld_f(in, q));
     if (MSK) *m = __ldg(a.inm + q);
     return;
   }
@@ -91,12 +113,11 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
   const long long q001 = z1 + y0 + i0[0], q101 = z1 + y0 + i1[0];
   const long long q011 = z1 + y1 + i0[0], q111 = z1 + y1 + i1[0];
   if (IMG) {
-    const float *p = a.in;
-    const double x00 = dlerp((double)__ldg(p + q000), (double)__ldg(p + q100), t[0]);
-    const double x10 = dlerp((double)__ldg(p + q010), (double)__ldg(p + q110), t[0]);
-    const double x01 = dlerp((double)__ldg(p + q001), (double)__ldg(p + q101), t[0]);
-    const double x11 = dlerp((double)__ldg(p + q011), (double)__ldg(p + q111), t[0]);
-    *v = __double2float_rn(dlerp(dlerp(x00, x10, t[1]), dlerp(x01, x11, t[1]), t[2]));
+    const double x00 = dlerp((double)ld_f(in, q000), (double)ld_f(in, q100), t[0]);
+    const double x10 = dlerp((double)ld_f(in, q010), (double)ld_f(in, q110), t[0]);
+    const double x01 = dlerp((double)ld_f(in, q001), (double)ld_f(in, q101), t[0]);
+    const double x11 = dlerp((double)ld_f(in, q011), (double)ld_f(in, q111), t[0]);
+    st_v(*v, dlerp(dlerp(x00, x10, t[1]), dlerp(x01, x11, t[1]), t[2]));
   }
   if (MSK) {
     const uint8_t *p = a.inm;
@@ -125,8 +146,9 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
 // 4-byte mask store.  The output buffers are 16-byte aligned (checked by the
 // launcher).  Per voxel the index map is the same FP64 expression as a plain
 // evaluation; only the j and k products are shared along the run.
-template <bool IMG, bool MSK>
+template <bool IMG, bool MSK, typename TI, typename TO>
 __global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
+  TO *const out = static_cast<TO *>(a.out);
   const long long n = (long long)a.onx * a.ony * a.onz;
   const long long nrun = (n + 3) >> 2;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nrun;
@@ -140,13 +162,14 @@ __global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
       cj[r] = __dmul_rn(a.C[3 * r + 1], (double)j);
       ck[r] = __dmul_rn(a.C[3 * r + 2], (double)k);
     }
-    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    TO v[4];
     uint8_t m[4] = {0, 0, 0, 0};
     const int cnt = n - o0 < 4 ? (int)(n - o0) : 4;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
+      st_copy(v[u], 0.0f);
       if (u < cnt) {
-        resample_voxel<IMG, MSK>(a, i, cj, ck, &v[u], &m[u]);
+        resample_voxel<IMG, MSK, TI, TO>(a, i, cj, ck, &v[u], &m[u]);
         if (++i == a.onx) {
           i = 0;
           if (++j == a.ony) {
@@ -161,7 +184,17 @@ __global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
       }
     }
     if (cnt == 4) {
-      if (IMG) *reinterpret_cast<float4 *>(a.out + o0) = make_float4(v[0], v[1], v[2], v[3]);
+      if (IMG) {
+        if (sizeof(TO) == 4) {
+          *reinterpret_cast<float4 *>(out + o0) =
+              make_float4(*reinterpret_cast<float *>(&v[0]), *reinterpret_cast<float *>(&v[1]),
+                          *reinterpret_cast<float *>(&v[2]), *reinterpret_cast<float *>(&v[3]));
+        } else {
+          const unsigned short *h = reinterpret_cast<const unsigned short *>(v);
+          *reinterpret_cast<uint2 *>(out + o0) =
+              make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
+        }
+      }
       if (MSK)
         *reinterpret_cast<uint32_t *>(a.outm + o0) =
             (uint32_t)m[0] | ((uint32_t)m[1] << 8) | ((uint32_t)m[2] << 16) | ((uint32_t)m[3] << 24);
@@ -169,7 +202,7 @@ __global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         if (u < cnt) {
-          if (IMG) a.out[o0 + u] = v[u];
+          if (IMG) out[o0 + u] = v[u];
           if (MSK) a.outm[o0 + u] = m[u];
         }
       }
@@ -177,9 +210,17 @@ __global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
   }
 }
 
-mirorr_status launch_resample(const int in_size[3], const float *in, const uint8_t *in_mask,
-                              const int out_size[3], const ResampleMap &map, float *out,
-                              uint8_t *out_mask, cudaStream_t s, bool nearest) {
+template <typename TI, typename TO>
+void launch_rs(const ResampleArgs &a, unsigned blocks, cudaStream_t s) {
+  if (a.out && a.outm) resample_kernel<true, true, TI, TO><<<blocks, 256, 0, s>>>(a);
+  else if (a.out) resample_kernel<true, false, TI, TO><<<blocks, 256, 0, s>>>(a);
+  else resample_kernel<false, true, float, float><<<blocks, 256, 0, s>>>(a);
+}
+
+mirorr_status launch_resample(const int in_size[3], const void *in, const uint8_t *in_mask,
+                              const int out_size[3], const ResampleMap &map, void *out,
+                              uint8_t *out_mask, cudaStream_t s, bool nearest, int in_dtype,
+                              int out_dtype) {
   ResampleArgs a;
   a.nearest = nearest ? 1 : 0;
   a.in = in; a.inm = in_mask;
@@ -198,16 +239,29 @@ mirorr_status launch_resample(const int in_size[3], const float *in, const uint8
   long long blocks = ((n + 3) / 4 + 255) / 256;
   const long long cap = (long long)sm_count() * 8;
   if (blocks > cap) blocks = cap;
-  if (a.out && a.outm) resample_kernel<true, true><<<(unsigned)blocks, 256, 0, s>>>(a);
-  else if (a.out) resample_kernel<true, false><<<(unsigned)blocks, 256, 0, s>>>(a);
-  else resample_kernel<false, true><<<(unsigned)blocks, 256, 0, s>>>(a);
+  const unsigned nb = (unsigned)blocks;
+  if (!a.out || (in_dtype == MIRORR_DTYPE_F32 && out_dtype == MIRORR_DTYPE_F32)) {
+    launch_rs<float, float>(a, nb, s);
+  } else if (out_dtype == MIRORR_DTYPE_BF16 && in_dtype == MIRORR_DTYPE_F32) {
+    launch_rs<float, __nv_bfloat16>(a, nb, s);
+  } else if (out_dtype == MIRORR_DTYPE_BF16 && in_dtype == MIRORR_DTYPE_BF16) {
+    launch_rs<__nv_bfloat16, __nv_bfloat16>(a, nb, s);
+  } else if (out_dtype == MIRORR_DTYPE_F16 && in_dtype == MIRORR_DTYPE_F32) {
+    launch_rs<float, __half>(a, nb, s);
+  } else if (out_dtype == MIRORR_DTYPE_F16 && in_dtype == MIRORR_DTYPE_F16) {
+    launch_rs<__half, __half>(a, nb, s);
+  } else {
+    set_error("resampler type pair %d -> %d not supported", in_dtype, out_dtype);
+    return MIRORR_EINVAL;
+  }
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
 
 // Separable Gaussian pass: FP64 accumulation in tap order, clamp-to-edge,
-// float output.
-__global__ void smooth_axis_kernel(const float *__restrict__ in, float *__restrict__ out, int nx,
+// float output (the input of the first pass may be 16-bit).
+template <typename TI>
+__global__ void smooth_axis_kernel(const TI *__restrict__ in, float *__restrict__ out, int nx,
                                    int ny, int nz, int axis, const double *__restrict__ w,
                                    int radius) {
   long long n = (long long)nx * ny * nz;
@@ -221,19 +275,50 @@ __global__ void smooth_axis_kernel(const float *__restrict__ in, float *__restri
     for (int t = 0; t <= 2 * radius; ++t) {
       int q = pos + t - radius;
       q = q < 0 ? 0 : (q > len - 1 ? len - 1 : q);
-      acc = __dadd_rn(acc, __dmul_rn(w[t], (double)__ldg(&in[base + q * stride])));
+      acc = __dadd_rn(acc, __dmul_rn(w[t], (double)ld_f(in, base + q * stride)));
     }
     out[o] = __double2float_rn(acc);
   }
 }
 
-mirorr_status launch_smooth_axis(const int size[3], const float *in, float *out, int axis,
-                                 const double *w, int radius, cudaStream_t s) {
+mirorr_status launch_smooth_axis(const int size[3], const void *in, float *out, int axis,
+                                 const double *w, int radius, cudaStream_t s, int in_dtype) {
   long long n = (long long)size[0] * size[1] * size[2];
   long long blocks = (n + 255) / 256;
   if (blocks > (long long)sm_count() * 64) blocks = (long long)sm_count() * 64;
-  smooth_axis_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, out, size[0], size[1], size[2], axis, w,
-                                                      radius);
+  if (in_dtype == MIRORR_DTYPE_BF16)
+    smooth_axis_kernel<<<(unsigned)blocks, 256, 0, s>>>(static_cast<const __nv_bfloat16 *>(in), out,
+                                                        size[0], size[1], size[2], axis, w, radius);
+  else if (in_dtype == MIRORR_DTYPE_F16)
+    smooth_axis_kernel<<<(unsigned)blocks, 256, 0, s>>>(static_cast<const __half *>(in), out,
+                                                        size[0], size[1], size[2], axis, w, radius);
+  else
+    smooth_axis_kernel<<<(unsigned)blocks, 256, 0, s>>>(static_cast<const float *>(in), out,
+                                                        size[0], size[1], size[2], axis, w, radius);
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
+}
+
+// float32 -> 16-bit storage (round to nearest even).
+template <typename TO>
+__global__ void to16_kernel(const float *__restrict__ in, TO *__restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    st_copy(out[i], in[i]);
+}
+
+mirorr_status launch_to16(const float *in, void *out, long long n, int dtype, cudaStream_t s) {
+  if (n <= 0) return MIRORR_OK;
+  long long blocks = (n + 255) / 256;
+  if (blocks > (long long)sm_count() * 16) blocks = (long long)sm_count() * 16;
+  if (dtype == MIRORR_DTYPE_BF16)
+    to16_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, static_cast<__nv_bfloat16 *>(out), n);
+  else if (dtype == MIRORR_DTYPE_F16)
+    to16_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, static_cast<__half *>(out), n);
+  else {
+    set_error("storage type %d is not a 16-bit type", dtype);
+    return MIRORR_EINVAL;
+  }
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }

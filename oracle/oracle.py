@@ -885,9 +885,27 @@ def _grid_image(origin, spacing, direction, size):
                  np.array(origin, np.float64), np.array(direction, np.float64))
 
 
-def _resample_through(src: Image, src_mask, grid: Image, t: Tfm, mask_geom: Image | None):
+def round_storage(a, store):
+    """float32 values as a 16-bit storage type keeps them: round to nearest
+    even into bfloat16 ('bf16') or IEEE half ('f16') and back to float32;
+    None or 'f32' returns the array unchanged."""
+    if store is None or store == "f32":
+        return a
+    a = np.ascontiguousarray(a, np.float32)
+    if store == "f16":
+        return a.astype(np.float16).astype(np.float32)
+    if store == "bf16":
+        u = a.view(np.uint32).astype(np.uint64)
+        r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+        return r.astype(np.uint32).view(np.float32)
+    raise ValueError(f"unknown storage type {store!r}")
+
+
+def _resample_through(src: Image, src_mask, grid: Image, t: Tfm, mask_geom: Image | None,
+                      store=None):
     C, e = resample_map(grid, src, t.M, t.off)
     img, _ = resample(src.data, None, grid.size, C, e)
+    img = round_storage(img, store)
     mg = mask_geom if mask_geom is not None else src
     if src_mask is None:
         src_mask = np.full(mg.data.shape, 255, np.uint8)
@@ -906,6 +924,7 @@ class RegParams:
     iterations: int = 5
     bm: BMParams = field(default_factory=lambda: BMParams(4, 1, 3, 7, 1.0))
     lts_keep: float = 0.5
+    store: str | None = None         # None/'f32' or the 16-bit storage 'bf16' | 'f16'
 
 
 def classic_level(fixed: Image, moving: Image, fmask, mmask, fmask_geom, mmask_geom,
@@ -915,11 +934,11 @@ def classic_level(fixed: Image, moving: Image, fmask, mmask, fmask_geom, mmask_g
     grid_f = _grid_image(origin, spacing, fixed.direction, size)
     grid_m = _grid_image(origin, spacing, moving.direction, size)
     ident = Tfm("affine")
-    mov_img, mov_mask = _resample_through(moving, mmask, grid_m, ident, mmask_geom)
+    mov_img, mov_mask = _resample_through(moving, mmask, grid_m, ident, mmask_geom, rp.store)
     base = geometry_like(grid_m, mov_img)
     last = tfm.params()
     for it in range(abs(rp.iterations)):
-        fix_img, fix_mask = _resample_through(fixed, fmask, grid_f, tfm, fmask_geom)
+        fix_img, fix_mask = _resample_through(fixed, fmask, grid_f, tfm, fmask_geom, rp.store)
         search = geometry_like(grid_f, fix_img)
         bp, mp = get_offsets(base, search, mov_mask, fix_mask, rp.bm, threads)
         lts_classic(tfm, bp, mp, rp.lts_keep)
@@ -956,8 +975,8 @@ def symmetric_level(fixed: Image, moving: Image, fmask, mmask, fmask_geom, mmask
 
     for it in range(abs(rp.iterations)):
         cF, cB = centered()
-        mov_img, mov_mask = _resample_through(moving, mmask, grid_m, cB, mmask_geom)
-        fix_img, fix_mask = _resample_through(fixed, fmask, grid_f, cF, fmask_geom)
+        mov_img, mov_mask = _resample_through(moving, mmask, grid_m, cB, mmask_geom, rp.store)
+        fix_img, fix_mask = _resample_through(fixed, fmask, grid_f, cF, fmask_geom, rp.store)
         base = geometry_like(grid_m, mov_img)
         search = geometry_like(grid_f, fix_img)
         bp1, mp1 = get_offsets(base, search, mov_mask, fix_mask, rp.bm, threads)
@@ -1114,7 +1133,13 @@ def centered_initial_transform(fixed: Image, moving: Image, kind: str) -> Tfm:
 def register(fixed: Image, moving: Image, rp: RegParams, levels: int, fixed_mask=None,
              moving_mask=None, min_length=32, threads=0, init: Tfm | None = None, trace=None):
     """RunMirorr (itkMirorrPyramidImplement.txx:71-158) over the `levels` finest
-    pyramid levels (reference CLI: --pyr-num levels --pyr-end 0)."""
+    pyramid levels (reference CLI: --pyr-num levels --pyr-end 0).  With
+    rp.store set, the input images are taken as stored in that 16-bit type
+    and every middle-space image is rounded to it, as the 16-bit device path
+    stores them (pyramid levels above the finest stay float32)."""
+    if rp.store not in (None, "f32"):
+        fixed = geometry_like(fixed, round_storage(fixed.data, rp.store))
+        moving = geometry_like(moving, round_storage(moving.data, rp.store))
     sm, sf = pyramid_schedule(fixed.size, moving.size, fixed.spacing, moving.spacing, min_length,
                               levels)
     tfm = init.copy() if init is not None else centered_initial_transform(fixed, moving, rp.kind)

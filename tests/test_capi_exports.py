@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol(so):
 
 def test_abi_version(so):
     so.mirorr_abi_version.restype = ctypes.c_int32
-    assert so.mirorr_abi_version() == 1
+    assert so.mirorr_abi_version() == 2
 
 
 def test_no_gpu_fails_loudly(so):

@@ -1,0 +1,123 @@
+"""16-bit storage (BF16 / FP16) path through the C ABI against the FP64 oracle
+run on the same stored values.
+
+The images are stored in 16 bits (round to nearest even from float32); the
+oracle sees exactly those values (oracle.round_storage), so every difference
+left is the arithmetic: the block search sums in FP32 -- the cross term on the
+tensor cores from two 16-bit parts of the centred base block, the rest on the
+CUDA cores -- where the reference sums in FP64.  The bars, per the block
+matcher's own acceptance rule:
+* the searched blocks (variance selection) are identical;
+* best and second-best scores within 1e-4 of the oracle's (FP32 rounding);
+* the argmax equals the oracle's on every block whose oracle best-vs-second
+  gap exceeds 1e-4, and on at least 99.5 % of all searched blocks;
+* registrations: final matrices within 1e-4 of the oracle's registration on
+  the same stored inputs, offsets within 1e-3 mm.
+"""
+import numpy as np
+import pytest
+
+import mirorr_b200 as mb
+from mirorr_b200.phantom import make_phantom, tre
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SCORE_TOL = 1e-4
+GAP = 1e-4
+
+CASES = [
+    dict(id="w7_G3", shape=(52, 44, 30), nw=7, G=3, keep=1.0, mask=None, seed=31),
+    dict(id="w7_G3_search_masked", shape=(52, 44, 30), nw=7, G=3, keep=1.0, mask="search", seed=32),
+    dict(id="w7_G3_both_masked", shape=(48, 40, 28), nw=7, G=3, keep=1.0, mask="both", seed=33),
+    dict(id="w7_G2_keep05", shape=(41, 37, 26), nw=7, G=2, keep=0.5, mask=None, seed=34),
+    dict(id="w5_G1", shape=(30, 28, 22), nw=5, G=1, keep=1.0, mask="search", seed=35),
+    dict(id="w7_G4_x_ragged", shape=(67, 30, 24), nw=7, G=4, keep=1.0, mask=None, seed=36),
+    # window 9: every block through the direct FP32 search
+    dict(id="w9_G3_direct", shape=(40, 36, 28), nw=9, G=3, keep=1.0, mask="search", seed=37),
+]
+
+
+def make_inputs(c, store):
+    ph = make_phantom(c["shape"], n_gauss=12, kind="affine" if c["seed"] % 2 else "rigid",
+                      seed=200 + c["seed"])
+    base = O.round_storage(ph.moving, store)
+    search = O.round_storage(ph.fixed, store)
+    bm = sm = None
+    if c["mask"] in ("search", "both"):
+        sm = np.full(search.shape, 255, np.uint8)
+        sm[:, :, :6] = 0
+        sm[:3] = 0
+        sm[:, 12:14, 9:11] = 0
+    if c["mask"] == "both":
+        bm = np.full(base.shape, 255, np.uint8)
+        bm[:, -7:, :] = 0
+        bm[4:6, :, 11:14] = 0
+    return ph, base, search, bm, sm
+
+
+@pytest.mark.parametrize("store", ["bf16", "f16"])
+@pytest.mark.parametrize("c", CASES, ids=[c["id"] for c in CASES])
+def test_matcher16_matches_oracle(ctx, c, store):
+    ph, base, search, bm, sm = make_inputs(c, store)
+    m = mb.BlockMatcher(ctx)
+    m.SetStorage(store)
+    m.SetBlockWidth(4)
+    m.SetNhoodGap(c["G"])
+    m.SetNhoodWidth(c["nw"])
+    m.SetBlockKeep(c["keep"])
+    m.SetBaseImage(base)
+    m.SetSearchImage(search)
+    if bm is not None:
+        m.SetBaseMask(bm)
+    if sm is not None:
+        m.SetSearchMask(sm)
+    try:
+        bp, mp = m.GetOffsets()
+    except mb.MirorrError as e:
+        assert e.name == "ENOBLOCKS"
+        bp = np.zeros((0, 3))
+    mi, best, second, status = m.BlockResults()
+    diag = m.LastDiagnostics()
+    m.close()
+    p = O.BMParams(4, 1, c["G"], c["nw"], c["keep"])
+    ref = O.match_blocks(base, search, bm, sm, p)
+    np.testing.assert_array_equal((status & 1).astype(np.uint8), ref.status)
+    s = ref.status == 1
+    err = np.abs(best[s].astype(np.float64) - ref.best[s])
+    err2 = np.abs(second[s].astype(np.float64) - ref.second[s])
+    assert err.max() <= SCORE_TOL, f"best score error {err.max():.3g}"
+    assert err2.max() <= SCORE_TOL, f"second score error {err2.max():.3g}"
+    same = np.all(mi == ref.match, axis=1)[s]
+    gap = (ref.best.astype(np.float64) - ref.second)[s]
+    clear = gap > GAP
+    assert np.all(same[clear]), f"{np.sum(~same[clear])} blocks with a clear gap moved"
+    assert same.mean() >= 0.995, f"argmax agreement {same.mean():.4f}"
+    if c["nw"] <= 7:
+        assert diag[4] > 0, "no block took the tensor-core search"
+    print(f"{c['id']} {store}: {s.sum()} blocks, tensor {diag[4]}, direct {diag[5]}, "
+          f"max |d best| {err.max():.2e}, argmax agreement {same.mean():.5f}")
+
+
+@pytest.mark.parametrize("store", ["bf16", "f16"])
+@pytest.mark.parametrize("mode,kind", [("symmetric", "affine"), ("classic", "rigid")])
+def test_register16_matches_oracle(ctx, store, mode, kind):
+    shape = (64, 56, 40)
+    ph = make_phantom(shape, n_gauss=20, kind=kind, seed=41 if kind == "affine" else 42,
+                      max_angle_deg=4.0, max_shift_vox=4.0)
+    rp = O.RegParams(mode, kind, 4, O.BMParams(4, 1, 3, 7, 1.0), 0.5, store)
+    fixed = O.Image(ph.fixed, ph.spacing, ph.origin)
+    moving = O.Image(ph.moving, ph.spacing, ph.origin)
+    to = O.register(fixed, moving, rp, 2)
+    p = mb.reg_params(symmetric=mode == "symmetric", kind=kind, levels=2, iterations=4,
+                      nhood_gap=3, nhood_width=7, storage=store)
+    tg, st = mb.register(ctx, ph.fixed, ph.moving, p)
+    assert st.levels_run == 2 and st.block_ncc_evaluated > 0
+    # the host copies carried 2 bytes per voxel
+    assert st.h2d_bytes >= 2 * 2 * ph.fixed.size
+    dM = np.max(np.abs(tg.M - to.M))
+    err = tre(tg.M, tg.off, ph.true_matrix, ph.true_offset, shape, ph.spacing)
+    err_o = tre(to.M, to.off, ph.true_matrix, ph.true_offset, shape, ph.spacing)
+    print(f"{mode} {kind} {store}: max |dM| {dM:.2e}, TRE gpu {err:.4f} oracle {err_o:.4f}")
+    np.testing.assert_allclose(tg.M, to.M, atol=1e-4, rtol=0)
+    np.testing.assert_allclose(tg.off, to.off, atol=1e-3, rtol=0)
