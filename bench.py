@@ -350,6 +350,10 @@ def run_cuda(args):
         par, cpu = parity_leg(mb, ctx, ph, res_dev, args)
         out["parity"] = par
         out["cpu_baseline"] = cpu
+    if rank == 0 and world == 1 and not args.no_batched:
+        pairs = c2_pairs()
+        out["batched"] = c2_leg(mb, ctx, dev, pairs)
+        out["served"] = c3_leg(mb, ctx, pairs)
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -477,6 +481,164 @@ def parity_leg(mb, ctx, ph, res_dev, args):
     return par, cpu
 
 
+# ---- batched and served configurations ----------------------------------------
+C2_PAIRS = 64
+C2_LEVELS, C2_ITERS, C2_NW, C2_G = 3, 10, 7, 3
+C2_WORKLOAD = ("64 phantom pairs of uneven sizes, per axis U{96..320} x U{96..320} x "
+               "U{48..160}, 40 Gaussians each (per-pair seed), rigid/affine 50/50, classic "
+               "method, 3 pyramid levels, block 4, radius 3 (343 candidates), block spacing 3, "
+               "LTS keep 0.5, 10 iterations/level")
+
+
+def _gen_pair(spec):
+    shape, kind, seed = spec
+    from mirorr_b200.phantom import make_phantom
+    return make_phantom(shape, n_gauss=40, kind=kind, seed=seed, max_angle_deg=5.0,
+                        max_shift_vox=8.0)
+
+
+def c2_pairs(n=C2_PAIRS, seed0=2000):
+    """The batched configuration's pairs, generated on the host cores in a
+    spawn pool (input preparation, outside every timed region)."""
+    import multiprocessing as mp
+    rng = np.random.default_rng(seed0)
+    specs = []
+    for i in range(n):
+        shape = (int(rng.integers(96, 321)), int(rng.integers(96, 321)), int(rng.integers(48, 161)))
+        specs.append((shape, "rigid" if i % 2 == 0 else "affine", seed0 + i))
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        phs = pool.map(_gen_pair, specs)
+    return specs, phs
+
+
+def c2_leg(mb, ctx, dev, pairs, oracle_pairs=2):
+    """Serial per-pair loop (float32 plain path, then the 16-bit path) against
+    the batched form (all pairs in one batch, BF16 and FP16), each through
+    the C ABI from host buffers with the copies inside; registrations/s of
+    each, agreement of the batch with the serial 16-bit loop, and the FP64
+    oracle's registration (same stored inputs) of the smallest pairs."""
+    import torch
+    from oracle import oracle as O
+    specs, phs = pairs
+
+    def params(kind, storage):
+        return mb.reg_params(symmetric=False, kind=kind, levels=C2_LEVELS, iterations=C2_ITERS,
+                             block_width=4, nhood_width=C2_NW, nhood_gap=C2_G, block_keep=1.0,
+                             lts_keep=0.5, storage=storage)
+
+    out = {"workload": C2_WORKLOAD, "pairs": len(phs),
+           "voxels_mean": round(float(np.mean([ph.fixed.size for ph in phs]))), "legs": {}}
+    host16 = {st: [(mb.to_storage(ph.fixed, st), mb.to_storage(ph.moving, st)) for ph in phs]
+              for st in ("bf16", "f16")}
+    res = {}
+    for name, storage in [("serial_f32", "f32"), ("serial_bf16", "bf16")]:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rs = []
+        for (shape, kind, seed), ph in zip(specs, phs):
+            if storage == "f32":
+                r, _ = mb.register(ctx, ph.fixed, ph.moving, params(kind, storage))
+            else:
+                f, m = host16[storage][len(rs)]
+                r, _ = mb.register(ctx, f, m, params(kind, storage))
+            rs.append(r)
+        dt = time.perf_counter() - t0
+        res[name] = rs
+        out["legs"][name] = {"seconds": round(dt, 3), "registrations_per_s": round(len(phs) / dt, 3)}
+    for name, storage in [("batch_bf16", "bf16"), ("batch_f16", "f16")]:
+        b = mb.Batch(ctx, max_slots=len(phs), hbm_budget=150e9)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ids = [b.submit(f, m, params(kind, storage))
+               for (shape, kind, seed), (f, m) in zip(specs, host16[storage])]
+        b.run()
+        rs = [b.result(i)[0] for i in ids]
+        dt = time.perf_counter() - t0
+        info = b.info()
+        b.close()
+        res[name] = rs
+        out["legs"][name] = {"seconds": round(dt, 3), "registrations_per_s": round(len(phs) / dt, 3),
+                             "steps": info["steps"], "graph_replays": info["replays"],
+                             "graph_captures": info["captures"]}
+    f32 = out["legs"]["serial_f32"]["registrations_per_s"]
+    for k in ("serial_bf16", "batch_bf16", "batch_f16"):
+        out["legs"][k]["speedup_vs_serial_f32"] = round(out["legs"][k]["registrations_per_s"] / f32, 3)
+    out["batch_vs_serial_bf16_max_abs_dM"] = float(max(
+        np.max(np.abs(a.M - b.M)) for a, b in zip(res["batch_bf16"], res["serial_bf16"])))
+    # FP64 oracle on the same stored inputs for the smallest pairs
+    order = np.argsort([ph.fixed.size for ph in phs])[:oracle_pairs]
+    checks = []
+    for i in order:
+        (shape, kind, seed), ph = specs[i], phs[i]
+        rp = O.RegParams("classic", kind, C2_ITERS, O.BMParams(4, 1, C2_G, C2_NW, 1.0), 0.5, "bf16")
+        to = O.register(O.Image(ph.fixed, ph.spacing, ph.origin),
+                        O.Image(ph.moving, ph.spacing, ph.origin), rp, C2_LEVELS,
+                        threads=os.cpu_count() or 1)
+        checks.append({"pair": int(i), "shape": list(shape),
+                       "max_abs_dM_batch_bf16_vs_oracle": float(np.max(np.abs(res["batch_bf16"][i].M - to.M))),
+                       "max_abs_dM_serial_f32_vs_oracle_bf16_inputs": float(np.max(np.abs(res["serial_f32"][i].M - to.M)))})
+    out["oracle_checks"] = checks
+    return out
+
+
+def c3_leg(mb, ctx, pairs, rates=(5, 10, 20, 50, 100, 200), per_rate=24, seed=3000):
+    """Served form: Poisson arrivals at each rate, requests drawn from the
+    batched configuration's pairs with 2-4 levels, classic or symmetric and
+    rigid or affine (uniform), admitted into a batch against a 150 GB budget
+    between steps; latency from arrival to result, by the host clock."""
+    specs, phs = pairs
+    rng = np.random.default_rng(seed)
+    host16 = [(mb.to_storage(ph.fixed, "bf16"), mb.to_storage(ph.moving, "bf16")) for ph in phs]
+    table = []
+    for rate in rates:
+        reqs = []
+        t = 0.0
+        for _ in range(per_rate):
+            t += rng.exponential(1.0 / rate)
+            i = int(rng.integers(len(phs)))
+            p = mb.reg_params(symmetric=bool(rng.integers(2)),
+                              kind="rigid" if rng.integers(2) else "affine",
+                              levels=int(rng.integers(2, 5)), iterations=C2_ITERS, block_width=4,
+                              nhood_width=C2_NW, nhood_gap=C2_G, block_keep=1.0, lts_keep=0.5,
+                              storage="bf16")
+            reqs.append((t, i, p))
+        b = mb.Batch(ctx, max_slots=64, hbm_budget=150e9)
+        lat, inflight = [], {}
+        q = 0
+        t0 = time.perf_counter()
+        done_t = []
+        while q < len(reqs) or inflight:
+            now = time.perf_counter() - t0
+            while q < len(reqs) and reqs[q][0] <= now:
+                at, i, p = reqs[q]
+                try:
+                    rid = b.submit(host16[i][0], host16[i][1], p)
+                except mb.MirorrError as e:
+                    if e.name != "EBUSY":
+                        raise
+                    break
+                inflight[rid] = at
+                q += 1
+            if inflight:
+                b.step()
+                for rid in b.poll():
+                    b.result(rid)
+                    end = time.perf_counter() - t0
+                    lat.append(end - inflight.pop(rid))
+                    done_t.append(end)
+            elif q < len(reqs):
+                time.sleep(max(0.0, reqs[q][0] - (time.perf_counter() - t0)))
+        b.close()
+        span = max(done_t) - reqs[0][0]
+        table.append({"rate_per_s": rate, "requests": len(reqs),
+                      "p50_ms": round(1e3 * float(np.percentile(lat, 50)), 2),
+                      "p99_ms": round(1e3 * float(np.percentile(lat, 99)), 2),
+                      "throughput_per_s": round(len(reqs) / span, 3)})
+    return {"workload": "Poisson arrivals, requests drawn from the 64 batched pairs with 2-4 "
+                        "levels, classic or symmetric, rigid or affine (uniform), BF16 storage, "
+                        "150 GB budget, up to 64 in flight", "rates": table}
+
+
 def run_reference(args):
     """Full CPU registrations of the workload by the reference's path restated
     (oracle/), as many as fit REFERENCE_BUDGET_S (at least one, at most
@@ -559,6 +721,37 @@ def run_leg(args):
                    "fast_blocks": d[4], "basemask_blocks": d[5], "blocks": d[3]}
         print(json.dumps(res))
         m.close()
+    elif args.leg == "matcher16":
+        # one matcher call with 16-bit storage (tensor-core search) beside the
+        # same call with float32 storage: block 4, radius --radius, spacing 3
+        res = {}
+        for store in ["f32", args.store]:
+            m = mb.BlockMatcher(ctx)
+            m.SetStorage(store)
+            m.SetBlockWidth(BW)
+            m.SetNhoodWidth(2 * args.radius + 1)
+            m.SetNhoodGap(G)
+            m.SetBaseImage(ph.moving)
+            m.SetSearchImage(ph.fixed)
+            if args.masked:
+                sm = np.zeros(ph.fixed.shape, np.uint8)
+                sm[10:-10, 10:-10, 10:-10] = 255
+                m.SetSearchMask(sm)
+            ts = []
+            for _ in range(args.calls):
+                bp, _ = m.GetOffsets()
+                ts.append([float(v) for v in m.LastTimings()])
+            d = m.LastDiagnostics()
+            res[store] = {"kept": int(bp.shape[0]), "ms_box_stats": ts[-1][0],
+                          "ms_selection": ts[-1][1], "ms_ncc": ts[-1][2],
+                          "ms_postfilter": ts[-1][3], "diag": [int(v) for v in d]}
+            m.close()
+        print(json.dumps(res))
+    elif args.leg == "batched":
+        pairs = c2_pairs(n=args.calls)
+        out = {"batched": c2_leg(mb, ctx, 0, pairs, oracle_pairs=1)}
+        out["served"] = c3_leg(mb, ctx, pairs, per_rate=8)
+        print(json.dumps(out))
     elif args.leg == "resample":
         # final resampling through a small rigid transform with each
         # interpolator, host buffers (upload and read-back included)
@@ -597,7 +790,11 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the FP64 oracle registration (parity and CPU baseline)")
-    ap.add_argument("--leg", choices=["matcher", "resample"], default=None)
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched (64 uneven pairs) and served (Poisson) legs")
+    ap.add_argument("--leg", choices=["matcher", "matcher16", "resample", "batched"], default=None)
+    ap.add_argument("--store", default="bf16")
+    ap.add_argument("--radius", type=int, default=3)
     ap.add_argument("--calls", type=int, default=3)
     ap.add_argument("--shape", default="256,256,128")
     ap.add_argument("--masked", action="store_true")

@@ -43,7 +43,8 @@ typedef enum mirorr_status {
   MIRORR_ECUDA = 4,      /* CUDA runtime / launch error, or no usable B200 */
   MIRORR_ETIMEOUT = 5,   /* a bounded device-side wait gave up */
   MIRORR_ESTATE = 6,     /* call out of order (e.g. GetOffsets before images are set) */
-  MIRORR_ERANGE = 7      /* output buffer too small; *_needed reports the size */
+  MIRORR_ERANGE = 7,     /* output buffer too small, or a request larger than a limit */
+  MIRORR_EBUSY = 8       /* no room now (batch slots or memory budget in use); retry later */
 } mirorr_status;
 
 /* Element type of stored volumes.  F32 is the plain path (the drop-in); BF16
@@ -311,6 +312,56 @@ MIRORR_API mirorr_status mirorr_register_device(mirorr_ctx ctx, const mirorr_geo
                                      const uint8_t *moving_mask, const mirorr_reg_params *p,
                                      const mirorr_transform *init, mirorr_transform *result,
                                      mirorr_reg_stats *stats);
+
+/* ---- batched and served registrations ---------------------------------------
+ * No reference counterpart (the reference runs one registration per process,
+ * mirorr.cxx:93-665).  A batch holds up to max_slots registration requests
+ * (BF16 or F16 storage, block width 4, block gap 1, every block kept) on the
+ * device at once, within hbm_budget bytes of device memory reserved for them.
+ * Each request is one RunMirorr (itkMirorrPyramidImplement.txx:71-158) with
+ * its own size, levels, method and transform kind; its results equal
+ * mirorr_register's on the same inputs and parameters up to the order of the
+ * LTS fit's floating-point sums.  A step advances every running request by
+ * one block-matching iteration with one launch per stage for all of them
+ * (the tensor-core search of every request's blocks in one persistent launch,
+ * every LTS fit in one cooperative launch); while the running set and their
+ * levels stay unchanged, the step replays a captured CUDA graph.  Requests
+ * may be submitted between steps (continuous batching): a new request starts
+ * at its coarsest level while the others continue. */
+typedef struct mirorr_batch_s *mirorr_batch;
+MIRORR_API mirorr_status mirorr_batch_create(mirorr_ctx ctx, int32_t max_slots,
+                                  uint64_t hbm_budget, mirorr_batch *out);
+MIRORR_API mirorr_status mirorr_batch_destroy(mirorr_batch b);
+/* Admits a request: copies its host inputs (elements of p->storage; masks
+ * may be NULL) to the device and reserves its buffers.  MIRORR_EBUSY when no
+ * slot is free or its memory does not fit the budget's remainder (retry after
+ * results are taken); MIRORR_ERANGE when it would not fit the whole budget;
+ * MIRORR_EINVAL for malformed geometry or parameters.  *request_id names it. */
+MIRORR_API mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fixed_geom,
+                                  const void *fixed, const uint8_t *fixed_mask,
+                                  const mirorr_geometry *moving_geom, const void *moving,
+                                  const uint8_t *moving_mask, const mirorr_reg_params *p,
+                                  const mirorr_transform *init, int64_t *request_id);
+/* One iteration of every running request; *running: requests that took part,
+ * *finished: requests that finished (or failed) in this step. */
+MIRORR_API mirorr_status mirorr_batch_step(mirorr_batch b, int32_t *running, int32_t *finished);
+/* Steps until no request is running. */
+MIRORR_API mirorr_status mirorr_batch_run(mirorr_batch b);
+/* Ids of finished or failed requests whose results are not taken yet. */
+MIRORR_API mirorr_status mirorr_batch_poll(mirorr_batch b, int64_t *ids, int32_t capacity,
+                                int32_t *n);
+/* A finished request's transform (moving -> fixed physical points) and
+ * statistics; frees its slot and memory.  A failed request returns its
+ * status (e.g. MIRORR_ENOBLOCKS) and message instead. */
+MIRORR_API mirorr_status mirorr_batch_result(mirorr_batch b, int64_t request_id,
+                                  mirorr_transform *result, mirorr_reg_stats *stats);
+/* Drops a request (running or finished) and frees its slot. */
+MIRORR_API mirorr_status mirorr_batch_cancel(mirorr_batch b, int64_t request_id);
+/* [0] running, [1] finished and not taken, [2] bytes reserved, [3] budget,
+ * [4] steps, [5] steps replayed from a graph, [6] graph captures, [7] 0. */
+MIRORR_API mirorr_status mirorr_batch_info(mirorr_batch b, int64_t info[8]);
+/* Graph replay of unchanged steps on (default) or off. */
+MIRORR_API mirorr_status mirorr_batch_set_graphs(mirorr_batch b, int32_t on);
 
 /* Pyramid schedule (PyramidScheduleTuner::UpdateSymmetric,
  * itkPyramidScheduleTuner.txx:291-414): per level (coarsest first) the

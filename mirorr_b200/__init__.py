@@ -30,7 +30,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmirorr_b200.so")
 
 STATUS = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ENOBLOCKS", 4: "ECUDA", 5: "ETIMEOUT",
-          6: "ESTATE", 7: "ERANGE"}
+          6: "ESTATE", 7: "ERANGE", 8: "EBUSY"}
 RIGID, AFFINE = 0, 1
 
 
@@ -219,6 +219,17 @@ def lib():
         "mirorr_pyramid_schedule": [P(Geometry), P(Geometry), ctypes.c_int32, ctypes.c_int32,
                                     P(ctypes.c_int32), vp, vp],
         "mirorr_pyramid_level": [vp, P(Geometry), vp, vp, P(Geometry), vp, ctypes.c_size_t],
+        "mirorr_batch_create": [vp, ctypes.c_int32, ctypes.c_uint64, P(vp)],
+        "mirorr_batch_destroy": [vp],
+        "mirorr_batch_submit": [vp, P(Geometry), vp, vp, P(Geometry), vp, vp, P(RegParams),
+                                P(Transform), P(ctypes.c_int64)],
+        "mirorr_batch_step": [vp, P(ctypes.c_int32), P(ctypes.c_int32)],
+        "mirorr_batch_run": [vp],
+        "mirorr_batch_poll": [vp, vp, ctypes.c_int32, P(ctypes.c_int32)],
+        "mirorr_batch_result": [vp, ctypes.c_int64, P(Transform), P(RegStats)],
+        "mirorr_batch_cancel": [vp, ctypes.c_int64],
+        "mirorr_batch_info": [vp, vp],
+        "mirorr_batch_set_graphs": [vp, ctypes.c_int32],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -686,3 +697,81 @@ def pyramid_level(ctx: Context, image, factors, geom: Geometry | None = None):
                                       _ptr(out), cap))
     nx, ny, nz = tuple(og.size)
     return out[: nx * ny * nz].reshape(nz, ny, nx), og
+
+
+class Batch:
+    """Many registrations on the device at once (mirorr_batch; no reference
+    counterpart).  submit() admits a request while a slot and the memory
+    budget allow (MirorrError EBUSY otherwise), step() advances every running
+    request by one iteration, result() returns a finished request's transform
+    and frees its slot.  Requests may be submitted between steps."""
+
+    def __init__(self, ctx: Context, max_slots=64, hbm_budget=150e9):
+        self.ctx = ctx
+        self._h = ctypes.c_void_p()
+        _check(lib().mirorr_batch_create(ctx.handle, int(max_slots), int(hbm_budget),
+                                         ctypes.byref(self._h)))
+
+    def submit(self, fixed, moving, params: RegParams, fixed_geom: Geometry | None = None,
+               moving_geom: Geometry | None = None, fixed_mask=None, moving_mask=None,
+               init: Transform | None = None) -> int:
+        f = fixed if np.asarray(fixed).dtype == np.uint16 else to_storage(fixed, params.storage)
+        m = moving if np.asarray(moving).dtype == np.uint16 else to_storage(moving, params.storage)
+        f = np.ascontiguousarray(f)
+        m = np.ascontiguousarray(m)
+        fg = fixed_geom or Geometry.of(f)
+        mg = moving_geom or Geometry.of(m)
+        rid = ctypes.c_int64(0)
+        _check(lib().mirorr_batch_submit(self._h, ctypes.byref(fg), _ptr(f), _ptr(_u8(fixed_mask)),
+                                         ctypes.byref(mg), _ptr(m), _ptr(_u8(moving_mask)),
+                                         ctypes.byref(params), ctypes.byref(init) if init else None,
+                                         ctypes.byref(rid)))
+        return rid.value
+
+    def step(self):
+        """One iteration of every running request: (running, finished)."""
+        r = ctypes.c_int32(0)
+        f = ctypes.c_int32(0)
+        _check(lib().mirorr_batch_step(self._h, ctypes.byref(r), ctypes.byref(f)))
+        return r.value, f.value
+
+    def run(self):
+        _check(lib().mirorr_batch_run(self._h))
+
+    def poll(self):
+        ids = np.zeros(256, np.int64)
+        n = ctypes.c_int32(0)
+        _check(lib().mirorr_batch_poll(self._h, _ptr(ids), 256, ctypes.byref(n)))
+        return [int(v) for v in ids[:min(n.value, 256)]]
+
+    def result(self, request_id: int):
+        res = Transform()
+        st = RegStats()
+        _check(lib().mirorr_batch_result(self._h, int(request_id), ctypes.byref(res),
+                                         ctypes.byref(st)))
+        return res, st
+
+    def cancel(self, request_id: int):
+        _check(lib().mirorr_batch_cancel(self._h, int(request_id)))
+
+    def info(self):
+        v = np.zeros(8, np.int64)
+        _check(lib().mirorr_batch_info(self._h, _ptr(v)))
+        keys = ["running", "finished", "bytes_reserved", "budget", "steps", "replays", "captures"]
+        return dict(zip(keys, [int(x) for x in v[:7]]))
+
+    def set_graphs(self, on: bool):
+        _check(lib().mirorr_batch_set_graphs(self._h, 1 if on else 0))
+
+    def close(self):
+        if self._h:
+            lib().mirorr_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            if not sys.is_finalizing():
+                self.close()
+        except Exception:
+            pass
+

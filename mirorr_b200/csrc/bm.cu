@@ -364,11 +364,12 @@ __device__ inline bool keep_block(const BmOut &o, long long b) {
   return cb > 1e-7 && fabs(cb - c2) > 1e-4;
 }
 
-__global__ void pf_count_kernel(BmOut o, long long n, unsigned int *tile_count) {
+__device__ void pf_count_tile(const BmOut &o, long long n, unsigned int *tile_count, long long tile) {
   __shared__ unsigned int cnt;
+  __syncthreads();
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
-  long long t0 = (long long)blockIdx.x * kTile;
+  long long t0 = tile * kTile;
   unsigned int c = 0;
   for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
     long long b = t0 + i;
@@ -377,10 +378,14 @@ __global__ void pf_count_kernel(BmOut o, long long n, unsigned int *tile_count) 
   c = __reduce_add_sync(0xffffffffu, c);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(&cnt, c);
   __syncthreads();
-  if (threadIdx.x == 0) tile_count[blockIdx.x] = cnt;
+  if (threadIdx.x == 0) tile_count[tile] = cnt;
 }
 
-__global__ void pf_scan_kernel(unsigned int *tile_count, long long ntiles, long long *total) {
+__global__ void pf_count_kernel(BmOut o, long long n, unsigned int *tile_count) {
+  pf_count_tile(o, n, tile_count, blockIdx.x);
+}
+
+__device__ void pf_scan_body(unsigned int *tile_count, long long ntiles, long long *total) {
   // single CTA, 1024 threads: exclusive scan in place (tile counts -> offsets)
   __shared__ unsigned long long carry;
   __shared__ unsigned long long warp_sums[32];
@@ -417,6 +422,10 @@ __global__ void pf_scan_kernel(unsigned int *tile_count, long long ntiles, long 
   if (threadIdx.x == 0) *total = (long long)carry;
 }
 
+__global__ void pf_scan_kernel(unsigned int *tile_count, long long ntiles, long long *total) {
+  pf_scan_body(tile_count, ntiles, total);
+}
+
 __device__ inline void block_point(const PointGeom &pg, int ix, int iy, int iz, double *out) {
   const double idx[3] = {(double)ix, (double)iy, (double)iz};
 #pragma unroll
@@ -428,12 +437,13 @@ __device__ inline void block_point(const PointGeom &pg, int ix, int iy, int iz, 
   }
 }
 
-__global__ void pf_write_kernel(BmOut o, long long n, const unsigned int *tile_off, BmGeom g,
-                                PointGeom pg, double *pts_base, double *pts_match,
-                                const long long *offset_dev) {
+__device__ void pf_write_tile(const BmOut &o, long long n, const unsigned int *tile_off,
+                              const BmGeom &g, const PointGeom &pg, double *pts_base,
+                              double *pts_match, const long long *offset_dev, long long tile) {
   __shared__ unsigned int wsum[8];
+  __syncthreads();
   const int per = kTile / 256;  // 8 consecutive blocks per thread
-  long long t0 = (long long)blockIdx.x * kTile + (long long)threadIdx.x * per;
+  long long t0 = tile * kTile + (long long)threadIdx.x * per;
   unsigned int flags = 0, c = 0;
   for (int k = 0; k < per; ++k) {
     long long b = t0 + k;
@@ -454,7 +464,7 @@ __global__ void pf_write_kernel(BmOut o, long long n, const unsigned int *tile_o
   __syncthreads();
   unsigned int before = 0;
   for (int w = 0; w < wid; ++w) before += wsum[w];
-  unsigned long long pos = (unsigned long long)tile_off[blockIdx.x] + before + x - c;
+  unsigned long long pos = (unsigned long long)tile_off[tile] + before + x - c;
   if (!pts_base) return;
   if (offset_dev) pos += (unsigned long long)*offset_dev;
   for (int k = 0; k < per; ++k) {
@@ -469,6 +479,48 @@ __global__ void pf_write_kernel(BmOut o, long long n, const unsigned int *tile_o
     block_point(pg, mx, my, mz, pts_match + 3 * pos);
     ++pos;
   }
+}
+
+__global__ void pf_write_kernel(BmOut o, long long n, const unsigned int *tile_off, BmGeom g,
+                                PointGeom pg, double *pts_base, double *pts_match,
+                                const long long *offset_dev) {
+  pf_write_tile(o, n, tile_off, g, pg, pts_base, pts_match, offset_dev, blockIdx.x);
+}
+
+// ---- the post-filter of many matcher calls in three launches (grid.y = call)
+__global__ void pf_count_batch_kernel(const PfCall *calls) {
+  const PfCall &c = calls[blockIdx.y];
+  if (!c.active) return;
+  const long long nt = (c.g.nblocks + kTile - 1) / kTile;
+  for (long long t = blockIdx.x; t < nt; t += gridDim.x) pf_count_tile(c.out, c.g.nblocks, c.tiles, t);
+}
+__global__ void pf_scan_batch_kernel(const PfCall *calls) {
+  const PfCall &c = calls[blockIdx.y];
+  if (!c.active) return;
+  pf_scan_body(c.tiles, (c.g.nblocks + kTile - 1) / kTile, c.count);
+}
+__global__ void pf_write_batch_kernel(const PfCall *calls) {
+  const PfCall &c = calls[blockIdx.y];
+  if (!c.active) return;
+  const long long nt = (c.g.nblocks + kTile - 1) / kTile;
+  for (long long t = blockIdx.x; t < nt; t += gridDim.x)
+    pf_write_tile(c.out, c.g.nblocks, c.tiles, c.g, c.pg, c.pts_b, c.pts_m, c.offset, t);
+}
+
+mirorr_status launch_postfilter_batch(const PfCall *dev_calls, int ncalls, long long max_blocks,
+                                      cudaStream_t s) {
+  if (ncalls <= 0) return MIRORR_OK;
+  long long nt = (max_blocks + kTile - 1) / kTile;
+  if (nt < 1) nt = 1;
+  const long long cap = (long long)sm_count() * 4;
+  const unsigned gx = (unsigned)(nt < cap ? nt : cap);
+  pf_count_batch_kernel<<<dim3(gx, ncalls), 256, 0, s>>>(dev_calls);
+  MB2_LAUNCH_CHECK();
+  pf_scan_batch_kernel<<<dim3(1, ncalls), 1024, 0, s>>>(dev_calls);
+  MB2_LAUNCH_CHECK();
+  pf_write_batch_kernel<<<dim3(gx, ncalls), 256, 0, s>>>(dev_calls);
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
 }
 
 mirorr_status launch_postfilter(const BmGeom &g, const BmOut &out, BmWork &w,

@@ -936,7 +936,7 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
                     &c->second, &c->match, &c->status, &c->pts_i, &c->pts_m, &c->up_f,
                     &c->up_m, &c->up_fm, &c->up_mm, &c->bm16.stats, &c->bm16.wand,
                     &c->bm16.prep, &c->bm16.xs, &c->bm16.ctl, &c->bm16.fb_list,
-                    &c->bm16.chunked};
+                    &c->bm16.chunked, &c->bm16.calls};
   for (DevBuf *b : bufs) b->release();
   c->timer.release();
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1718,6 +1718,838 @@ mirorr_status mirorr_pyramid_level(mirorr_ctx c, const mirorr_geometry *ig, cons
   MB2_CUDA_TRY(cudaMemcpyAsync(out, lp, sizeof(float) * vox(g.size), cudaMemcpyDeviceToHost, c->stream));
   MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
   *og = g;
+  return MIRORR_OK;
+}
+
+}  // extern "C"
+
+// ---- batched and served registrations ---------------------------------------
+//
+// A mirorr_batch holds up to max_slots registration requests on the device at
+// once, each with its inputs, pyramid level, middle-space images, matcher
+// buffers, point pairs and fit state.  A round advances every running
+// request by one block-matching iteration with one launch per stage for all
+// of them: the resampling passes, the 16-bit search of every matcher call
+// (box statistics, window-AND, base blocks, the tensor-core search over all
+// calls' tiles in one persistent launch, the direct search), the
+// post-filters and the LTS fits (one cooperative launch, a group of CTAs
+// per request).  The host reads the fit states back once per round and
+// advances each request's iteration, level and convergence as the
+// registration methods do (itkMirorrRegistrationMethod.txx:598-658,
+// itkSymMirorrRegistrationMethod.txx:458-720, itkMirorrPyramidImplement.txx:
+// 107-145).  When the set of requests and their levels is unchanged from the
+// round before, the round's launch sequence is replayed from a CUDA graph
+// captured once (the per-round index maps and fit states come through
+// pinned host buffers the graph's copies read).
+namespace {
+
+constexpr int kLtsCtas = 2;  // CTAs per LTS fit in the batched launch
+
+struct BatchCallBufs {
+  DevBuf stats, wand, prep, xs, chunked, fb, best, second, match, status, tiles;
+};
+
+struct BatchSlot {
+  int state = 0;  // 0 free, 1 running, 2 finished, 3 failed
+  int64_t id = -1;
+  mirorr_status fail = MIRORR_OK;
+  std::string fail_msg;
+  mirorr_reg_params p{};
+  mirorr_geometry fg{}, mg{};
+  DevBuf in_f, in_m, in_fm, in_mm;
+  bool has_fm = false, has_mm = false;
+  int nl = 0, lev = 0, it = 0;
+  int sf[16][3], sm[16][3];
+  double params[12];
+  Tfm tfm, t12f, t12b, fixed_tr, moving_tr;
+  double initial_center[3];
+  double last[12];
+  bool level_ready = false;
+  mirorr_geometry lf{}, lm{}, grid_f{}, grid_m{};
+  DevBuf lvl_f, lvl_m;
+  BmGeom g{};
+  DevBuf img_b, img_s, msk_b, msk_s;
+  BatchCallBufs call[2];
+  DevBuf pts_i, pts_m, lts_scratch;
+  long long cap_blocks = 0;  // blocks the buffers hold (the finest level's)
+  mirorr_reg_stats stats{};
+  std::chrono::steady_clock::time_point t0;
+  size_t bytes = 0;
+};
+
+size_t slot_bytes(const mirorr_geometry &fg, const mirorr_geometry &mg, const mirorr_reg_params &p,
+                  bool fm, bool mm, long long max_vox, long long max_blocks) {
+  const size_t es = elem_size(p.storage);
+  const size_t nf = (size_t)vox(fg.size), nm = (size_t)vox(mg.size);
+  const size_t ncall = p.symmetric ? 2 : 1;
+  const size_t V = (size_t)max_vox, NB = (size_t)max_blocks;
+  size_t b = es * (nf + nm) + (fm ? nf : 0) + (mm ? nm : 0);  // inputs
+  b += 4 * (nf + nm);                                          // float32 levels
+  b += 2 * es * V + 2 * V;                                     // middle-space images, masks
+  b += ncall * (8 * V + 3 * V / 2 + (32 + 256 + 4 + 13) * NB + 2 * V + 64 * 1024);
+  b += 2 * 3 * 8 * ncall * NB;                                 // point pairs
+  b += lts_fit_scratch_bytes((long long)(ncall * NB), kLtsCtas);
+  return b;
+}
+
+}  // namespace
+
+struct mirorr_batch_s {
+  mirorr_ctx c = nullptr;
+  int max_slots = 0;
+  size_t budget = 0, used = 0;
+  std::vector<BatchSlot> slots;
+  int64_t next_id = 1;
+  bool params_set = false;
+  mirorr_bm_params bm{};
+  int storage = MIRORR_DTYPE_BF16;
+  // per-round staging (pinned) and device copies
+  HostBuf h_jobs, h_calls, h_pf, h_states, h_rd;
+  DevBuf d_jobs, d_pf, d_states, d_counts, d_ctl, d_calls, d_lts_args;
+  HostBuf h_lts_args;
+  std::vector<LtsFit> fits;
+  std::vector<int> fit_slot, call_slot;
+  // graph of the last round's launch sequence
+  bool graphs = true;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<long long> gkey;
+  int64_t rounds = 0, replays = 0, captures = 0;
+};
+
+namespace {
+
+// Sets up slot s's current level: the level images (float32), the middle
+// space, the block grid and, for the symmetric method, the half-space
+// transforms (symmetric_level's preamble).
+mirorr_status batch_setup_level(mirorr_batch b, BatchSlot &s) {
+  mirorr_ctx c = b->c;
+  cudaStream_t st = c->stream;
+  const void *pf = nullptr, *pm = nullptr;
+  int tf = 0, tm = 0;
+  MB2_TRY(make_level(c, s.fg, s.in_f.ptr, s.p.storage, s.sf[s.lev], s.lf, s.lvl_f, &pf, &tf));
+  if (tf != MIRORR_DTYPE_F32) {
+    MB2_TRY(s.lvl_f.ensure(sizeof(float) * vox(s.lf.size)));
+    MB2_TRY(launch_from16(pf, s.lvl_f.as<float>(), vox(s.lf.size), tf, st));
+  }
+  MB2_TRY(make_level(c, s.mg, s.in_m.ptr, s.p.storage, s.sm[s.lev], s.lm, s.lvl_m, &pm, &tm));
+  if (tm != MIRORR_DTYPE_F32) {
+    MB2_TRY(s.lvl_m.ensure(sizeof(float) * vox(s.lm.size)));
+    MB2_TRY(launch_from16(pm, s.lvl_m.as<float>(), vox(s.lm.size), tm, st));
+  }
+  double cf[3], cm[3], origin[3], spacing[3];
+  int size[3];
+  center_of(s.lf, cf);
+  center_of(s.lm, cm);
+  for (int d = 0; d < 3; ++d) {
+    origin[d] = s.p.symmetric ? ((s.lf.origin[d] - cf[d]) + (s.lm.origin[d] - cm[d])) / 2.0
+                              : cm[d] + ((s.lf.origin[d] - cf[d]) + (s.lm.origin[d] - cm[d])) / 2.0;
+    spacing[d] = (s.lf.spacing[d] + s.lm.spacing[d]) / 2.0;
+    size[d] = (int)(((double)s.lf.size[d] + (double)s.lm.size[d] + 0.5) / 2.0);
+  }
+  grid_geom(origin, spacing, size, s.lf.direction, s.grid_f);
+  grid_geom(origin, spacing, size, s.lm.direction, s.grid_m);
+  if (!bm_geometry(size, (int)s.p.bm.block_width, (int)s.p.bm.block_gap, (int)s.p.bm.nhood_gap,
+                   (int)s.p.bm.nhood_width, s.g)) {
+    set_error("middle-space image smaller than one block");
+    return MIRORR_EINVAL;
+  }
+  tfm_set_params(s.tfm, s.params);
+  if (s.p.symmetric) {
+    for (int d = 0; d < 3; ++d) s.initial_center[d] = s.tfm.c[d];
+    tfm_center_to_origin(s.tfm);
+    tfm_identity(s.fixed_tr, KIND_RIGID);
+    tfm_identity(s.moving_tr, KIND_RIGID);
+    double pfx[6] = {0, 0, 0, cf[0], cf[1], cf[2]}, pmv[6] = {0, 0, 0, cm[0], cm[1], cm[2]};
+    tfm_set_params(s.fixed_tr, pfx);
+    tfm_set_params(s.moving_tr, pmv);
+    Tfm ifixed;
+    tfm_inverse(s.fixed_tr, ifixed);
+    tfm_compose(s.tfm, ifixed, false);
+    tfm_compose(s.tfm, s.moving_tr, true);
+    half_space(s.tfm, s.t12f, s.t12b);
+  }
+  tfm_params(s.tfm, s.last);
+  s.it = 0;
+  s.level_ready = true;
+  return MIRORR_OK;
+}
+
+void batch_centered(const BatchSlot &s, Tfm &cF, Tfm &cB) {
+  double prm[12];
+  tfm_identity(cF, s.tfm.kind);
+  tfm_identity(cB, s.tfm.kind);
+  tfm_params(s.t12f, prm);
+  tfm_set_params(cF, prm);
+  tfm_compose(cF, s.fixed_tr, false);
+  tfm_params(s.t12b, prm);
+  tfm_set_params(cB, prm);
+  tfm_compose(cB, s.moving_tr, false);
+}
+
+// End of slot s's level: the symmetric method composes the full transform
+// back (symmetric_level's epilogue); the parameters carry to the next level.
+void batch_end_level(BatchSlot &s) {
+  if (s.p.symmetric) {
+    Tfm cF, cB, ib;
+    batch_centered(s, cF, cB);
+    tfm_inverse(cB, ib);
+    tfm_identity(s.tfm, s.tfm.kind);
+    tfm_compose(s.tfm, ib, true);
+    tfm_compose(s.tfm, cF, false);
+    tfm_update_center(s.tfm, s.initial_center);
+  }
+  if (s.lev < 16) s.stats.iterations_run[s.lev] = s.it;
+  tfm_params(s.tfm, s.params);
+  s.level_ready = false;
+  ++s.lev;
+  if (s.lev >= s.nl) {
+    tfm_set_params(s.tfm, s.params);
+    s.stats.levels_run = s.nl;
+    s.stats.seconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - s.t0).count();
+    s.state = 2;
+  }
+}
+
+void batch_fail(mirorr_batch b, BatchSlot &s, mirorr_status st, const char *msg) {
+  s.state = 3;
+  s.fail = st;
+  s.fail_msg = msg;
+  (void)b;
+}
+
+void batch_release(mirorr_batch b, BatchSlot &s) {
+  DevBuf *bufs[] = {&s.in_f, &s.in_m, &s.in_fm, &s.in_mm, &s.lvl_f, &s.lvl_m, &s.img_b, &s.img_s,
+                    &s.msk_b, &s.msk_s, &s.pts_i, &s.pts_m, &s.lts_scratch};
+  for (DevBuf *x : bufs) x->release();
+  for (auto &cb : s.call) {
+    DevBuf *cbs[] = {&cb.stats, &cb.wand, &cb.prep, &cb.xs, &cb.chunked, &cb.fb, &cb.best,
+                     &cb.second, &cb.match, &cb.status, &cb.tiles};
+    for (DevBuf *x : cbs) x->release();
+  }
+  b->used -= s.bytes;
+  s = BatchSlot();
+}
+
+// Host-side check, before any launch, that every buffer a round's
+// descriptors address is large enough for the extent the kernels will touch.
+mirorr_status batch_check_slot(mirorr_ctx c, const BatchSlot &s) {
+  const long long nvox = vox(s.grid_f.size), nb = s.g.nblocks;
+  const size_t es = elem_size(s.p.storage);
+  const int ncall = s.p.symmetric ? 2 : 1;
+  auto need = [&](const DevBuf &x, size_t n, const char *what) -> bool {
+    if (x.bytes >= n && x.ptr) return true;
+    set_error("internal: slot buffer %s holds %zu bytes, the round needs %zu", what, x.bytes, n);
+    return false;
+  };
+  bool ok = need(s.img_b, es * nvox, "img_b") && need(s.img_s, es * nvox, "img_s") &&
+            need(s.msk_b, nvox, "msk_b") && need(s.msk_s, nvox, "msk_s") &&
+            need(s.lvl_f, sizeof(float) * vox(s.lf.size), "lvl_f") &&
+            need(s.lvl_m, sizeof(float) * vox(s.lm.size), "lvl_m") &&
+            need(s.pts_i, sizeof(double) * 3 * ncall * nb, "pts_i") &&
+            need(s.pts_m, sizeof(double) * 3 * ncall * nb, "pts_m") &&
+            need(s.lts_scratch, lts_fit_scratch_bytes(ncall * nb, kLtsCtas), "lts_scratch");
+  if (ok && !s.has_fm) ok = need(c->ones, vox(s.fg.size), "ones (fixed)");
+  if (ok && !s.has_mm) ok = need(c->ones, vox(s.mg.size), "ones (moving)");
+  for (int k = 0; ok && k < ncall; ++k) {
+    Match16Call mc;
+    memset(&mc, 0, sizeof(mc));
+    prepare16(s.g, mc);
+    const BatchCallBufs &cb = s.call[k];
+    ok = need(cb.stats, sizeof(float2) * nvox, "stats") &&
+         need(cb.wand, match16_wand_bytes(mc), "wand") &&
+         need(cb.prep, sizeof(Prep16) * nb, "prep") && need(cb.xs, 256 * (size_t)nb, "xs") &&
+         need(cb.fb, sizeof(int) * nb, "fb") && need(cb.best, sizeof(float) * nb, "best") &&
+         need(cb.second, sizeof(float) * nb, "second") &&
+         need(cb.match, sizeof(int32_t) * nb, "match") && need(cb.status, nb, "status") &&
+         need(cb.tiles, sizeof(unsigned int) * ((nb + 2047) / 2048 + 1), "tiles") &&
+         (!mc.tensor || need(cb.chunked, match16_chunk_bytes(mc), "chunked"));
+  }
+  return ok ? MIRORR_OK : MIRORR_EINVAL;
+}
+
+// The round's launch sequence (also what a graph captures).
+mirorr_status batch_issue(mirorr_batch b, int njobs, long long max_vox, int ncalls, int nfits,
+                          long long max_blocks) {
+  mirorr_ctx c = b->c;
+  cudaStream_t st = c->stream;
+  const int S = b->max_slots;
+  MB2_CUDA_TRY(cudaMemcpyAsync(b->d_jobs.ptr, b->h_jobs.ptr, sizeof(ResampleJob) * njobs,
+                               cudaMemcpyHostToDevice, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(b->d_pf.ptr, b->h_pf.ptr, sizeof(PfCall) * ncalls,
+                               cudaMemcpyHostToDevice, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(b->d_states.ptr, b->h_states.ptr, sizeof(LtsState) * S,
+                               cudaMemcpyHostToDevice, st));
+  MB2_CUDA_TRY(cudaMemsetAsync(b->d_counts.ptr, 0, sizeof(long long) * 4 * S, st));
+  MB2_CUDA_TRY(cudaMemsetAsync(b->d_ctl.ptr, 0, sizeof(unsigned int) * 4 * 2 * S, st));
+  MB2_TRY(launch_resample_batch(b->d_jobs.as<ResampleJob>(), njobs, max_vox, st));
+  MB2_TRY(launch_match16_batch(b->storage, ncalls, b->h_calls.as<Match16Call>(), b->d_calls, st));
+  MB2_TRY(launch_postfilter_batch(b->d_pf.as<PfCall>(), ncalls, max_blocks, st));
+  MB2_TRY(lts_batch_launch(b->fits.data(), nfits, kLtsCtas, c->ltsw.spin_limit, b->d_lts_args,
+                           b->h_lts_args, st));
+  // read back: fit states, point counts, the search's and the fits' give-up flags
+  unsigned char *rd = b->h_rd.as<unsigned char>();
+  MB2_CUDA_TRY(cudaMemcpyAsync(rd, b->d_states.ptr, sizeof(LtsState) * S, cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(rd + sizeof(LtsState) * S, b->d_counts.ptr, sizeof(long long) * 4 * S,
+                               cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(rd + sizeof(LtsState) * S + sizeof(long long) * 4 * S, b->d_ctl.ptr,
+                               sizeof(unsigned int) * 4 * 2 * S, cudaMemcpyDeviceToHost, st));
+  return MIRORR_OK;
+}
+
+// One round over every running request.
+mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
+  mirorr_ctx c = b->c;
+  cudaStream_t st = c->stream;
+  const int S = b->max_slots;
+  int nrun = 0;
+  long long max_in = 0;
+  for (auto &s : b->slots)
+    if (s.state == 1) {
+      ++nrun;
+      max_in = std::max(max_in, (long long)std::max(vox(s.fg.size), vox(s.mg.size)));
+    }
+  if (running) *running = nrun;
+  if (finished) *finished = 0;
+  if (!nrun) return MIRORR_OK;
+  MB2_TRY(ensure_ones(c, max_in));
+  // levels entered this round
+  for (auto &s : b->slots) {
+    if (s.state != 1 || s.level_ready) continue;
+    mirorr_status r = batch_setup_level(b, s);
+    if (r != MIRORR_OK) batch_fail(b, s, r, mirorr_last_error());
+  }
+  ResampleJob *jobs = b->h_jobs.as<ResampleJob>();
+  Match16Call *calls = b->h_calls.as<Match16Call>();
+  PfCall *pf = b->h_pf.as<PfCall>();
+  LtsState *states = b->h_states.as<LtsState>();
+  memset(states, 0, sizeof(LtsState) * S);
+  b->fits.clear();
+  b->fit_slot.clear();
+  b->call_slot.clear();
+  int nj = 0, nc = 0;
+  long long max_vox = 0, max_blocks = 0;
+  std::vector<long long> key;
+  for (int si = 0; si < S; ++si) {
+    BatchSlot &s = b->slots[si];
+    if (s.state != 1) continue;
+    // a slot reused by a later request has other buffers: the request id
+    // (not the slot) keys the graph
+    key.push_back(s.id);
+    key.push_back(s.lev);
+    const long long V = vox(s.grid_f.size);
+    max_vox = std::max(max_vox, V);
+    max_blocks = std::max(max_blocks, s.g.nblocks);
+    // ---- resampling passes of this iteration ------------------------------
+    Tfm tb, tf;
+    if (s.p.symmetric) {
+      batch_centered(s, tf, tb);
+    } else {
+      tfm_identity(tb, KIND_AFFINE);
+      tf = s.tfm;
+    }
+    const uint8_t *fmask = s.has_fm ? s.in_fm.as<uint8_t>() : c->ones.as<uint8_t>();
+    const uint8_t *mmask = s.has_mm ? s.in_mm.as<uint8_t>() : c->ones.as<uint8_t>();
+    struct Src { const float *img; const mirorr_geometry *lg; const uint8_t *mask;
+                 const mirorr_geometry *mgeo; const mirorr_geometry *grid; const Tfm *t;
+                 DevBuf *out; DevBuf *outm; };
+    Src src[2] = {{s.lvl_m.as<float>(), &s.lm, mmask, &s.mg, &s.grid_m, &tb, &s.img_b, &s.msk_b},
+                  {s.lvl_f.as<float>(), &s.lf, fmask, &s.fg, &s.grid_f, &tf, &s.img_s, &s.msk_s}};
+    for (auto &q : src) {
+      ResampleMap mi, mmp;
+      if (!make_map(*q.grid, *q.lg, q.t->M, q.t->off, mi) ||
+          !make_map(*q.grid, *q.mgeo, q.t->M, q.t->off, mmp)) {
+        batch_fail(b, s, MIRORR_EINVAL, "singular image geometry");
+        break;
+      }
+      ResampleJob &ji = jobs[nj++];
+      memset(&ji, 0, sizeof(ji));
+      ji.in = q.img;
+      ji.out = q.out->ptr;
+      for (int d = 0; d < 3; ++d) { ji.in_size[d] = q.lg->size[d]; ji.out_size[d] = q.grid->size[d]; }
+      memcpy(ji.C, mi.C, sizeof(mi.C));
+      memcpy(ji.e, mi.e, sizeof(mi.e));
+      ji.out_dtype = s.p.storage;
+      ji.active = 1;
+      ResampleJob &jm = jobs[nj++];
+      memset(&jm, 0, sizeof(jm));
+      jm.inm = q.mask;
+      jm.outm = q.outm->as<uint8_t>();
+      for (int d = 0; d < 3; ++d) { jm.in_size[d] = q.mgeo->size[d]; jm.out_size[d] = q.grid->size[d]; }
+      memcpy(jm.C, mmp.C, sizeof(mmp.C));
+      memcpy(jm.e, mmp.e, sizeof(mmp.e));
+      jm.active = 1;
+    }
+    if (s.state != 1) continue;
+    // ---- matcher calls: forward, and the swapped one of the symmetric method
+    const int ncall = s.p.symmetric ? 2 : 1;
+    for (int k = 0; k < ncall; ++k) {
+      Match16Call &mc = calls[nc];
+      memset(&mc, 0, sizeof(mc));
+      prepare16(s.g, mc);
+      BatchCallBufs &cb = s.call[k];
+      mc.base = k ? s.img_s.ptr : s.img_b.ptr;
+      mc.bmask = k ? s.msk_s.as<uint8_t>() : s.msk_b.as<uint8_t>();
+      mc.search = k ? s.img_b.ptr : s.img_s.ptr;
+      mc.smask = k ? s.msk_b.as<uint8_t>() : s.msk_s.as<uint8_t>();
+      mc.selected = nullptr;
+      mc.stats = cb.stats.as<float2>();
+      mc.wand = cb.wand.as<uint8_t>();
+      mc.prep = cb.prep.as<Prep16>();
+      mc.xs = cb.xs.as<uint32_t>();
+      mc.chunked = cb.chunked.as<uint4>();
+      mc.best = cb.best.as<float>();
+      mc.second = cb.second.as<float>();
+      mc.match = cb.match.as<int32_t>();
+      mc.status = cb.status.as<uint8_t>();
+      mc.ncc_count = reinterpret_cast<unsigned long long *>(b->d_counts.as<long long>() + 4 * si + 2);
+      mc.ctl = b->d_ctl.as<unsigned int>() + 4 * (2 * si + k);
+      mc.fb_list = cb.fb.as<int>();
+      mc.active = 1;
+      PfCall &pc = pf[nc];
+      memset(&pc, 0, sizeof(pc));
+      pc.out = BmOut{mc.best, mc.second, mc.match, mc.status};
+      pc.g = s.g;
+      const mirorr_geometry &pg_geom = k ? s.grid_f : s.grid_m;
+      point_geom(pg_geom.origin, pg_geom.spacing, pg_geom.direction, (int)s.p.bm.block_width, pc.pg);
+      // the swapped call's lists go in with roles reversed, after the forward ones
+      pc.pts_b = k ? s.pts_m.as<double>() : s.pts_i.as<double>();
+      pc.pts_m = k ? s.pts_i.as<double>() : s.pts_m.as<double>();
+      pc.tiles = cb.tiles.as<unsigned int>();
+      pc.count = b->d_counts.as<long long>() + 4 * si + k;
+      pc.offset = k ? b->d_counts.as<long long>() + 4 * si : nullptr;
+      pc.active = 1;
+      b->call_slot.push_back(si);
+      ++nc;
+    }
+    key.push_back(s.g.nblocks);
+    // ---- the fit --------------------------------------------------------------
+    LtsState &hs = states[si];
+    hs.kind = s.tfm.kind;
+    hs.symmetric = s.p.symmetric;
+    hs.lts_keep = s.p.lts_keep;
+    hs.tfm = s.tfm;
+    if (s.p.symmetric) {
+      hs.t12f = s.t12f;
+      hs.t12b = s.t12b;
+    }
+    lts_begin(hs);
+    LtsFit f;
+    f.state = b->d_states.as<LtsState>() + si;
+    f.init = s.pts_i.as<double>();
+    f.moved = s.pts_m.as<double>();
+    f.n_dev = b->d_counts.as<long long>() + 4 * si;
+    f.scratch = s.lts_scratch.ptr;
+    b->fits.push_back(f);
+    b->fit_slot.push_back(si);
+  }
+  if (nc == 0) return MIRORR_OK;
+  for (int si = 0; si < S; ++si)
+    if (b->slots[si].state == 1) MB2_TRY(batch_check_slot(c, b->slots[si]));
+  // the tile numbering the tensor launch reads from the call descriptors (a
+  // replay copies them from h_calls as written here)
+  match16_number_tiles(calls, nc);
+  // ---- launches (replayed from the graph when the set is unchanged) -------
+  const bool same = b->graphs && b->gexec && key == b->gkey;
+  if (same) {
+    MB2_CUDA_TRY(cudaGraphLaunch(b->gexec, st));
+    ++b->replays;
+  } else if (b->graphs) {
+    if (b->gexec) {
+      cudaGraphExecDestroy(b->gexec);
+      b->gexec = nullptr;
+    }
+    MB2_TRY(b->d_calls.ensure(sizeof(Match16Call) * nc));
+    MB2_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    mirorr_status r = batch_issue(b, nj, max_vox, nc, (int)b->fits.size(), max_blocks);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (r != MIRORR_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return r;
+    }
+    if (e != cudaSuccess) {
+      set_error("capturing the batch round failed: %s", cudaGetErrorString(e));
+      return MIRORR_ECUDA;
+    }
+    e = cudaGraphInstantiate(&b->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      b->gexec = nullptr;
+      set_error("instantiating the batch round failed: %s", cudaGetErrorString(e));
+      return MIRORR_ECUDA;
+    }
+    b->gkey = key;
+    ++b->captures;
+    MB2_CUDA_TRY(cudaGraphLaunch(b->gexec, st));
+  } else {
+    MB2_TRY(batch_issue(b, nj, max_vox, nc, (int)b->fits.size(), max_blocks));
+  }
+  MB2_CUDA_TRY(cudaStreamSynchronize(st));
+  ++b->rounds;
+  // ---- advance every request ----------------------------------------------
+  const unsigned char *rd = b->h_rd.as<unsigned char>();
+  const LtsState *rs = reinterpret_cast<const LtsState *>(rd);
+  const long long *rc = reinterpret_cast<const long long *>(rd + sizeof(LtsState) * S);
+  const unsigned int *rctl =
+      reinterpret_cast<const unsigned int *>(rd + sizeof(LtsState) * S + sizeof(long long) * 4 * S);
+  int nfin = 0;
+  for (size_t fi = 0; fi < b->fit_slot.size(); ++fi) {
+    const int si = b->fit_slot[fi];
+    BatchSlot &s = b->slots[si];
+    if (rctl[4 * (2 * si) + 2] || rctl[4 * (2 * si + 1) + 2]) {
+      batch_fail(b, s, MIRORR_ETIMEOUT, "a bounded wait on a tensor copy of the NCC search gave up");
+      ++nfin;
+      continue;
+    }
+    const long long used = rc[4 * si] + rc[4 * si + 1];
+    s.stats.matcher_calls += s.p.symmetric ? 2 : 1;
+    s.stats.block_ncc_evaluated += rc[4 * si + 2];
+    if (used == 0) {
+      batch_fail(b, s, MIRORR_ENOBLOCKS,
+                 "No block matches occurred. Images probably have zero overlap. "
+                 "Try supplying a better initial transform.");
+      ++nfin;
+      continue;
+    }
+    LtsState hs = rs[si];
+    lts_finish(hs);
+    s.tfm = hs.tfm;
+    if (s.p.symmetric) {
+      s.t12f = hs.t12f;
+      s.t12b = hs.t12b;
+    }
+    double cur[12];
+    tfm_params(s.tfm, cur);
+    const double d = param_delta(s.last, cur, tfm_nparams(s.tfm));
+    for (int i = 0; i < 12; ++i) s.last[i] = cur[i];
+    ++s.it;
+    if (d < 1e-3 || s.it >= std::abs(s.p.iterations)) {
+      batch_end_level(s);
+      if (s.state == 2) ++nfin;
+    }
+  }
+  if (finished) *finished = nfin;
+  return MIRORR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mirorr_status mirorr_batch_create(mirorr_ctx c, int32_t max_slots, uint64_t hbm_budget,
+                                  mirorr_batch *out) {
+  if (!c || !out || max_slots < 1 || max_slots > 64) {
+    set_error("null argument or max_slots outside 1..64");
+    return MIRORR_EINVAL;
+  }
+  *out = nullptr;
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  mirorr_batch b = new (std::nothrow) mirorr_batch_s;
+  if (!b) { set_error("out of host memory"); return MIRORR_ENOMEM; }
+  b->c = c;
+  b->max_slots = max_slots;
+  b->budget = (size_t)hbm_budget;
+  b->slots.resize(max_slots);
+  const int S = max_slots;
+  mirorr_status st = MIRORR_OK;
+  if (st == MIRORR_OK) st = b->h_jobs.ensure(sizeof(ResampleJob) * 4 * S);
+  if (st == MIRORR_OK) st = b->h_calls.ensure(sizeof(Match16Call) * 2 * S);
+  if (st == MIRORR_OK) st = b->h_pf.ensure(sizeof(PfCall) * 2 * S);
+  if (st == MIRORR_OK) st = b->h_states.ensure(sizeof(LtsState) * S);
+  if (st == MIRORR_OK)
+    st = b->h_rd.ensure(sizeof(LtsState) * S + sizeof(long long) * 4 * S + sizeof(unsigned int) * 8 * S);
+  if (st == MIRORR_OK) st = b->d_jobs.ensure(sizeof(ResampleJob) * 4 * S);
+  if (st == MIRORR_OK) st = b->d_pf.ensure(sizeof(PfCall) * 2 * S);
+  if (st == MIRORR_OK) st = b->d_states.ensure(sizeof(LtsState) * S);
+  if (st == MIRORR_OK) st = b->d_counts.ensure(sizeof(long long) * 4 * S);
+  if (st == MIRORR_OK) st = b->d_ctl.ensure(sizeof(unsigned int) * 8 * S);
+  if (st == MIRORR_OK) st = b->d_calls.ensure(sizeof(Match16Call) * 2 * S);
+  if (st == MIRORR_OK) st = b->d_lts_args.ensure(lts_args_bytes() * S);
+  if (st == MIRORR_OK) st = b->h_lts_args.ensure(lts_args_bytes() * S);
+  if (st == MIRORR_OK) st = c->ncc_count.ensure(sizeof(unsigned long long));
+  if (st != MIRORR_OK) {
+    mirorr_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_batch_destroy(mirorr_batch b) {
+  if (!b) return MIRORR_OK;
+  cudaSetDevice(b->c->device);
+  cudaStreamSynchronize(b->c->stream);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  for (auto &s : b->slots)
+    if (s.state) batch_release(b, s);
+  HostBuf *hb[] = {&b->h_jobs, &b->h_calls, &b->h_pf, &b->h_states, &b->h_rd, &b->h_lts_args};
+  for (HostBuf *x : hb) x->release();
+  DevBuf *db[] = {&b->d_jobs, &b->d_pf, &b->d_states, &b->d_counts, &b->d_ctl, &b->d_calls,
+                  &b->d_lts_args};
+  for (DevBuf *x : db) x->release();
+  delete b;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_batch_set_graphs(mirorr_batch b, int32_t on) {
+  if (!b) { set_error("null argument"); return MIRORR_EINVAL; }
+  b->graphs = on != 0;
+  if (!b->graphs && b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, const void *fixed,
+                                  const uint8_t *fmask, const mirorr_geometry *mg,
+                                  const void *moving, const uint8_t *mmask,
+                                  const mirorr_reg_params *p, const mirorr_transform *init,
+                                  int64_t *request_id) {
+  if (!b || !fg || !mg || !fixed || !moving || !p || !request_id) {
+    set_error("null argument");
+    return MIRORR_EINVAL;
+  }
+  mirorr_ctx c = b->c;
+  if (!valid_geom(fg) || !valid_geom(mg)) { set_error("invalid image geometry"); return MIRORR_EINVAL; }
+  if (!is16(p->storage)) {
+    set_error("batched registration stores images in BF16 or F16 (storage %d)", p->storage);
+    return MIRORR_EINVAL;
+  }
+  if (p->kind != KIND_RIGID && p->kind != KIND_AFFINE) {
+    set_error("transform kind must be 0 (rigid) or 1 (affine)");
+    return MIRORR_EINVAL;
+  }
+  MB2_TRY(check_bm_params(p->bm));
+  if (p->bm.block_width != 4 || p->bm.block_gap != 1 || p->bm.nhood_width > 13 ||
+      !(p->bm.block_keep >= 1.0)) {
+    set_error("batched registration needs block width 4, block gap 1, window up to 13 and "
+              "every block kept");
+    return MIRORR_EINVAL;
+  }
+  if (!(p->lts_keep > 0.0 && p->lts_keep <= 1.0)) { set_error("lts_keep must lie in (0, 1]"); return MIRORR_EINVAL; }
+  if (b->params_set && (p->storage != b->storage || p->bm.nhood_width != b->bm.nhood_width ||
+                        p->bm.nhood_gap != b->bm.nhood_gap)) {
+    set_error("the requests of one batch share the storage type, window and block spacing");
+    return MIRORR_EINVAL;
+  }
+  int si = -1;
+  for (int i = 0; i < b->max_slots; ++i)
+    if (b->slots[i].state == 0) { si = i; break; }
+  if (si < 0) { set_error("no free slot"); return MIRORR_EBUSY; }
+  BatchSlot &s = b->slots[si];
+  mirorr_reg_params pp = *p;
+  if (pp.iterations == 0) pp.iterations = 5;
+  if (pp.min_length <= 0) pp.min_length = 32;
+  int sched_m[16][3], sched_f[16][3];
+  int nl = pyramid_schedule(*fg, *mg, pp.min_length, pp.levels, sched_m, sched_f);
+  if (pp.last_level > 0 && pp.last_level < nl) nl = pp.last_level;
+  else if (pp.last_level < 0) nl = std::max(1, nl + pp.last_level);
+  // the largest level's middle space and block grid size the buffers
+  long long max_vox = 0, max_blocks = 0;
+  size_t chunk_b = 0, wand_b = 0;
+  for (int l = 0; l < nl; ++l) {
+    mirorr_geometry lf, lm;
+    level_geometry(*fg, sched_f[l], lf);
+    level_geometry(*mg, sched_m[l], lm);
+    int size[3];
+    for (int d = 0; d < 3; ++d) size[d] = (int)(((double)lf.size[d] + (double)lm.size[d] + 0.5) / 2.0);
+    BmGeom g;
+    if (!bm_geometry(size, (int)pp.bm.block_width, (int)pp.bm.block_gap, (int)pp.bm.nhood_gap,
+                     (int)pp.bm.nhood_width, g)) {
+      set_error("a pyramid level's middle space is smaller than one block");
+      return MIRORR_EINVAL;
+    }
+    Match16Call mc;
+    memset(&mc, 0, sizeof(mc));
+    prepare16(g, mc);
+    max_vox = std::max(max_vox, (long long)size[0] * size[1] * size[2]);
+    max_blocks = std::max(max_blocks, g.nblocks);
+    chunk_b = std::max(chunk_b, match16_chunk_bytes(mc));
+    wand_b = std::max(wand_b, match16_wand_bytes(mc));
+  }
+  const size_t need = slot_bytes(*fg, *mg, pp, fmask != nullptr, mmask != nullptr, max_vox, max_blocks);
+  if (need > b->budget) {
+    set_error("request needs %zu bytes, more than the whole budget of %zu", need, b->budget);
+    return MIRORR_ERANGE;
+  }
+  if (b->used + need > b->budget) {
+    set_error("request needs %zu bytes; %zu of the budget's %zu are in use", need, b->used, b->budget);
+    return MIRORR_EBUSY;
+  }
+  MB2_CUDA_TRY(cudaSetDevice(c->device));
+  s = BatchSlot();
+  s.p = pp;
+  s.fg = *fg;
+  s.mg = *mg;
+  s.nl = nl;
+  memcpy(s.sm, sched_m, sizeof(sched_m));
+  memcpy(s.sf, sched_f, sizeof(sched_f));
+  s.cap_blocks = max_blocks;
+  s.bytes = need;
+  b->used += need;
+  s.state = 1;  // owns buffers from here (released on failure below)
+  const size_t es = elem_size(pp.storage);
+  const int ncall = pp.symmetric ? 2 : 1;
+  mirorr_status st = MIRORR_OK;
+  auto E = [&](DevBuf &x, size_t n) { if (st == MIRORR_OK) st = x.ensure(n); };
+  E(s.in_f, es * vox(fg->size));
+  E(s.in_m, es * vox(mg->size));
+  if (fmask) E(s.in_fm, vox(fg->size));
+  if (mmask) E(s.in_mm, vox(mg->size));
+  E(s.lvl_f, sizeof(float) * vox(fg->size));
+  E(s.lvl_m, sizeof(float) * vox(mg->size));
+  E(s.img_b, es * max_vox);
+  E(s.img_s, es * max_vox);
+  E(s.msk_b, max_vox);
+  E(s.msk_s, max_vox);
+  for (int k = 0; k < ncall; ++k) {
+    BatchCallBufs &cb = s.call[k];
+    E(cb.stats, sizeof(float2) * max_vox);
+    E(cb.wand, wand_b);
+    E(cb.prep, sizeof(Prep16) * max_blocks);
+    E(cb.xs, sizeof(uint32_t) * 64 * max_blocks);
+    E(cb.chunked, chunk_b);
+    E(cb.fb, sizeof(int) * max_blocks);
+    E(cb.best, sizeof(float) * max_blocks);
+    E(cb.second, sizeof(float) * max_blocks);
+    E(cb.match, sizeof(int32_t) * max_blocks);
+    E(cb.status, max_blocks);
+    E(cb.tiles, sizeof(unsigned int) * (max_blocks / 2048 + 2));
+  }
+  E(s.pts_i, sizeof(double) * 3 * ncall * max_blocks);
+  E(s.pts_m, sizeof(double) * 3 * ncall * max_blocks);
+  E(s.lts_scratch, lts_fit_scratch_bytes(ncall * max_blocks, kLtsCtas));
+  if (st == MIRORR_OK) st = upload(c, s.in_f, fixed, es * vox(fg->size));
+  if (st == MIRORR_OK) st = upload(c, s.in_m, moving, es * vox(mg->size));
+  if (st == MIRORR_OK && fmask) st = upload(c, s.in_fm, fmask, vox(fg->size));
+  if (st == MIRORR_OK && mmask) st = upload(c, s.in_mm, mmask, vox(mg->size));
+  s.has_fm = fmask != nullptr;
+  s.has_mm = mmask != nullptr;
+  Tfm t;
+  if (st == MIRORR_OK) {
+    if (init) {
+      if (!from_public(*init, t) || init->kind != pp.kind) {
+        set_error("initial transform kind does not match the requested kind");
+        st = MIRORR_EINVAL;
+      }
+    } else {
+      double cfix[3], cmov[3], tr[3];
+      center_of(*fg, cfix);
+      center_of(*mg, cmov);
+      tfm_identity(t, pp.kind);
+      tfm_set_center(t, cmov);
+      for (int d = 0; d < 3; ++d) tr[d] = cfix[d] - cmov[d];
+      tfm_set_translation(t, tr);
+    }
+  }
+  if (st != MIRORR_OK) {
+    std::string msg = mirorr_last_error();
+    batch_release(b, s);
+    set_error("%s", msg.c_str());
+    return st;
+  }
+  s.tfm = t;
+  tfm_params(t, s.params);
+  s.stats.h2d_bytes = (int64_t)(es * (vox(fg->size) + vox(mg->size)) +
+                                (fmask ? vox(fg->size) : 0) + (mmask ? vox(mg->size) : 0));
+  s.t0 = std::chrono::steady_clock::now();
+  s.id = b->next_id++;
+  if (!b->params_set) {
+    b->params_set = true;
+    b->bm = pp.bm;
+    b->storage = pp.storage;
+  }
+  *request_id = s.id;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_batch_step(mirorr_batch b, int32_t *running, int32_t *finished) {
+  if (!b) { set_error("null argument"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(b->c->device));
+  int r = 0, f = 0;
+  mirorr_status st = batch_round(b, &r, &f);
+  if (running) *running = r;
+  if (finished) *finished = f;
+  return st;
+}
+
+mirorr_status mirorr_batch_run(mirorr_batch b) {
+  if (!b) { set_error("null argument"); return MIRORR_EINVAL; }
+  MB2_CUDA_TRY(cudaSetDevice(b->c->device));
+  for (int guard = 0; guard < 100000; ++guard) {
+    int r = 0, f = 0;
+    MB2_TRY(batch_round(b, &r, &f));
+    if (r == 0) return MIRORR_OK;
+  }
+  set_error("batch did not finish");
+  return MIRORR_ESTATE;
+}
+
+mirorr_status mirorr_batch_poll(mirorr_batch b, int64_t *ids, int32_t capacity, int32_t *n) {
+  if (!b || !n) { set_error("null argument"); return MIRORR_EINVAL; }
+  int k = 0;
+  for (auto &s : b->slots)
+    if (s.state == 2 || s.state == 3) {
+      if (ids && k < capacity) ids[k] = s.id;
+      ++k;
+    }
+  *n = k;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_batch_result(mirorr_batch b, int64_t id, mirorr_transform *result,
+                                  mirorr_reg_stats *stats) {
+  if (!b) { set_error("null argument"); return MIRORR_EINVAL; }
+  for (auto &s : b->slots) {
+    if (s.state == 0 || s.id != id) continue;
+    if (s.state == 1) { set_error("request %lld is still running", (long long)id); return MIRORR_ESTATE; }
+    cudaSetDevice(b->c->device);
+    if (s.state == 3) {
+      const mirorr_status st = s.fail;
+      const std::string msg = s.fail_msg;
+      batch_release(b, s);
+      set_error("%s", msg.c_str());
+      return st;
+    }
+    if (result) to_public(s.tfm, *result);
+    if (stats) *stats = s.stats;
+    batch_release(b, s);
+    return MIRORR_OK;
+  }
+  set_error("no request %lld in the batch", (long long)id);
+  return MIRORR_EINVAL;
+}
+
+mirorr_status mirorr_batch_cancel(mirorr_batch b, int64_t id) {
+  if (!b) { set_error("null argument"); return MIRORR_EINVAL; }
+  for (auto &s : b->slots) {
+    if (s.state == 0 || s.id != id) continue;
+    cudaSetDevice(b->c->device);
+    cudaStreamSynchronize(b->c->stream);
+    batch_release(b, s);
+    return MIRORR_OK;
+  }
+  set_error("no request %lld in the batch", (long long)id);
+  return MIRORR_EINVAL;
+}
+
+mirorr_status mirorr_batch_info(mirorr_batch b, int64_t info[8]) {
+  if (!b || !info) { set_error("null argument"); return MIRORR_EINVAL; }
+  int64_t run = 0, fin = 0;
+  for (auto &s : b->slots) {
+    if (s.state == 1) ++run;
+    if (s.state == 2 || s.state == 3) ++fin;
+  }
+  info[0] = run;
+  info[1] = fin;
+  info[2] = (int64_t)b->used;
+  info[3] = (int64_t)b->budget;
+  info[4] = b->rounds;
+  info[5] = b->replays;
+  info[6] = b->captures;
+  info[7] = 0;
   return MIRORR_OK;
 }
 

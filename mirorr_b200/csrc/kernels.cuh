@@ -82,20 +82,74 @@ mirorr_status launch_postfilter(const BmGeom &g, const BmOut &out, BmWork &w,
                                 long long *count_dev, const long long *offset_dev,
                                 cudaStream_t s);
 
-// Scratch of the 16-bit storage search (tc.cu).
-struct Bm16Work {
-  DevBuf stats;    // float2 per search position: (mean, Syy), Syy sign bit = footprint leaves the mask
-  DevBuf wand;     // window-AND passes and the per-block flags
-  DevBuf prep;     // per-block base statistics
-  DevBuf xs;       // per-block 16-bit parts of the centred base block
-  DevBuf ctl;      // [0] tensor blocks, [1] direct blocks, [2] a bounded wait gave up
-  DevBuf fb_list;  // blocks of the direct search
-  DevBuf chunked;  // x-chunked copy of the search image for the window tensor copies
+// Per-block base statistics of the 16-bit search.
+struct Prep16 {
+  float mu;      // mean of the base block (every voxel)
+  float sxx;     // sum over base-mask voxels of x~^2 (x~ = x - mu)
+  float sxt;     // sum over base-mask voxels of x~
+  float sxt_tc;  // sum over every voxel of the two 16-bit parts of x~
+  int mmode;     // 1: base mask on everywhere, 2: off everywhere, 0: mixed
+  int pad[3];
 };
-// One matcher call on 16-bit images (dtype MIRORR_DTYPE_BF16 or _F16): box
-// statistics, base-block preparation, the tensor-core search and the direct
-// FP32 search of the blocks the tensor form does not take.  Writes `out` for
-// every block (the post-filter follows as for the FP32 path).
+
+// One matcher call of the 16-bit search: inputs, per-call buffers, outputs
+// (filled by the caller) and the geometry and tile layout (prepare16).
+struct Match16Call {
+  const void *base;
+  const uint8_t *bmask;
+  const void *search;
+  const uint8_t *smask;
+  const uint8_t *selected;
+  float2 *stats;          // nvox: (mu_y, Syy), Syy sign bit = footprint leaves the mask
+  uint8_t *wand;          // match16_wand_bytes: window-AND passes and per-block flags
+  Prep16 *prep;           // nblocks
+  uint32_t *xs;           // nblocks x 64 words: the 16-bit parts of the centred base block
+  uint4 *chunked;         // match16_chunk_bytes: x-chunked copy of the search image
+  float *best;
+  float *second;
+  int32_t *match;
+  uint8_t *status;
+  unsigned long long *ncc_count;
+  unsigned int *ctl;      // 4 words, zeroed before the launch: [0] tensor blocks,
+                          // [1] direct blocks, [2] a bounded wait gave up
+  int *fb_list;           // nblocks
+  int nx, ny, nz;
+  int nbx, nby, nbz;
+  int stx, sty, stz;
+  int G, W;
+  int bpt;                // blocks per tensor tile (G bpt a multiple of 8)
+  int tiles_x;
+  int chunk_x0, nxc;      // x of the copy's first 8-wide chunk, chunks per row
+  int tensor;             // the call takes the tensor form
+  int active;             // 0: the launch skips the call
+  long long ntiles;
+  long long tile0;        // first tile of the call in the launch (set by the launcher)
+  long long nblocks;
+};
+// Geometry and tile layout of a call on block grid g.
+void prepare16(const BmGeom &g, Match16Call &c);
+size_t match16_chunk_bytes(const Match16Call &c);
+size_t match16_wand_bytes(const Match16Call &c);
+// Numbers the tensor tiles of calls[0, n) in order (sets each call's tile0)
+// and returns their total.  A replayed graph of launch_match16_batch reads the
+// descriptors from the host array at replay, so the caller numbers them again
+// before every replay.
+long long match16_number_tiles(Match16Call *calls, int n);
+
+// Scratch of the 16-bit storage search of one matcher call (tc.cu).
+struct Bm16Work {
+  DevBuf stats, wand, prep, xs, ctl, fb_list, chunked;
+  DevBuf calls;    // device copy of the call descriptors
+};
+// The 16-bit search of ncalls matcher calls (dtype MIRORR_DTYPE_BF16 or _F16)
+// in one launch per stage: box statistics, window-AND, base-block
+// preparation, the tensor-core search of every call's tensor tiles in one
+// persistent launch, and the direct FP32 search of the blocks the tensor form
+// does not take.  host_calls[i].tile0 is set here (match16_number_tiles);
+// calls_dev receives the descriptors.  Writes every active call's per-block results.
+mirorr_status launch_match16_batch(int dtype, int ncalls, Match16Call *host_calls,
+                                   DevBuf &calls_dev, cudaStream_t s);
+// One matcher call on 16-bit images with the scratch of w.
 mirorr_status launch_match16(int dtype, const BmGeom &g, const void *base, const uint8_t *bmask,
                              const void *search, const uint8_t *smask, const uint8_t *selected,
                              const BmOut &out, Bm16Work &w, unsigned long long *ncc_count,
@@ -105,6 +159,24 @@ mirorr_status match16_take_timeout(Bm16Work &w, cudaStream_t s, bool *timed_out)
 // Blocks of the last 16-bit search taken by [0] the tensor form, [1] the
 // direct search (synchronises).
 mirorr_status match16_counts(Bm16Work &w, cudaStream_t s, unsigned int out[2]);
+
+// One matcher call's post-filter in a batch (launch_postfilter_batch): its
+// per-block results, grid and point geometry, the compaction tiles (one word
+// per 2048 blocks, plus one), the kept-count output and an optional device
+// offset added to the output position (the swapped call of a symmetric
+// iteration appends after the forward one).
+struct PfCall {
+  BmOut out;
+  BmGeom g;
+  PointGeom pg;
+  double *pts_b, *pts_m;
+  unsigned int *tiles;
+  long long *count;
+  const long long *offset;
+  int active;
+};
+mirorr_status launch_postfilter_batch(const PfCall *dev_calls, int ncalls, long long max_blocks,
+                                      cudaStream_t s);
 
 // Linear resampling with an explicit affine index map (see mirorr_b200.h).
 struct ResampleMap {
@@ -118,6 +190,25 @@ mirorr_status launch_resample(const int in_size[3], const void *in, const uint8_
                               const int out_size[3], const ResampleMap &map, void *out,
                               uint8_t *out_mask, cudaStream_t s, bool nearest = false,
                               int in_dtype = MIRORR_DTYPE_F32, int out_dtype = MIRORR_DTYPE_F32);
+// One pass of launch_resample_batch: float32 image (or none) and uint8 mask
+// (or none) on an index map, image output in out_dtype (16-byte aligned),
+// mask output 4-byte aligned; inactive jobs are skipped.
+struct ResampleJob {
+  const float *in;
+  const uint8_t *inm;
+  void *out;
+  uint8_t *outm;
+  int in_size[3];
+  int out_size[3];
+  double C[9];
+  double e[3];
+  int out_dtype;
+  int active;
+};
+mirorr_status launch_resample_batch(const ResampleJob *dev_jobs, int njobs, long long max_voxels,
+                                    cudaStream_t s);
+// BF16 / F16 -> float32 (exact).
+mirorr_status launch_from16(const void *in, float *out, long long n, int dtype, cudaStream_t s);
 // float32 -> BF16 / F16 (round to nearest even).
 mirorr_status launch_to16(const float *in, void *out, long long n, int dtype, cudaStream_t s);
 // Final-resampling interpolators (interp.cu): cubic B-spline (coef: FP64
@@ -160,6 +251,27 @@ mirorr_status launch_window_and(const BmGeom &g, const float2 *stats, DevBuf &bu
                                 const uint8_t **wand, cudaStream_t s);
 // The NCC stage's give-up flag (device word), or nullptr before any search.
 const unsigned int *ncc_timeout_flag(const BmWork &w);
+// One fit of lts_batch_launch: its state (uploaded after lts_begin), point
+// pairs, the two device counters whose sum is the pair count, and scratch of
+// lts_fit_scratch_bytes(n_max, ncta) bytes (256-byte aligned).
+struct LtsFit {
+  LtsState *state;
+  const double *init;
+  const double *moved;
+  const long long *n_dev;
+  void *scratch;
+};
+size_t lts_fit_scratch_bytes(long long n_max, int ncta);
+// Bytes of one fit's launch arguments (lts_batch_launch's staging).
+size_t lts_args_bytes();
+// Runs nfits LTS fits in one cooperative launch, ncta CTAs each (every CTA of
+// the launch resident at once); zeroes each fit's barrier and histograms
+// first.  args_dev / args_host: argument staging reused across calls.
+mirorr_status lts_batch_launch(const LtsFit *fits, int nfits, int ncta, long long spin_limit,
+                               DevBuf &args_dev, HostBuf &args_host, cudaStream_t st);
+// The device word of a fit's scratch that is non-zero when one of its
+// barrier waits gave up.
+const int *lts_fit_error_flag(const void *scratch);
 // lts_run with every scratch buffer in a static device array sized for
 // MIRORR_LTS_NOALLOC_MAX_POINTS pairs: allocates no device memory.  n is the
 // number of pairs (no device counters).  Calls on one device must not overlap.

@@ -55,7 +55,7 @@ struct LtsArgs {
   long long spin_limit;   // polls of a grid-barrier wait before it gives up
 };
 
-__device__ bool grid_sync(LtsCtl *ctl, long long spin_limit) {
+__device__ bool grid_sync(LtsCtl *ctl, long long spin_limit, unsigned int nctas) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -64,7 +64,7 @@ __device__ bool grid_sync(LtsCtl *ctl, long long spin_limit) {
     unsigned int gen = *genp;
     __threadfence();
     unsigned int arrived = atomicAdd(&ctl->bar_count, 1u) + 1u;
-    if (arrived == gridDim.x) {
+    if (arrived == nctas) {
       atomicExch(&ctl->bar_count, 0u);
       __threadfence();
       atomicAdd(&ctl->bar_gen, 1u);
@@ -171,11 +171,12 @@ __device__ inline void block_sums(const double (&v)[N], double *red /* N * 32 */
 // out[q] = sum over the grid's CTAs b of part[b * kPartial + q0 + q], q < nq:
 // warp q % nwarps takes value q, its lanes stride over b, then a shuffle tree
 // (a fixed order).  out in shared memory, valid for every thread on return.
-__device__ inline void grid_partial_sums(const double *part, int q0, int nq, double *out) {
+__device__ inline void grid_partial_sums(const double *part, int q0, int nq, double *out,
+                                         int nctas) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int q = wid; q < nq; q += nw) {
     double x = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(&part[(long long)b * kPartial + q0 + q]);
+    for (int b = lane; b < nctas; b += 32) x += __ldcg(&part[(long long)b * kPartial + q0 + q]);
     for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
     if (lane == 0) out[q] = x;
   }
@@ -198,7 +199,9 @@ __device__ inline double residual(const LtsState &s, const double *x, const doub
   return r;
 }
 
-__global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
+// The LTS loop run by `ncta` CTAs (index `cta` among them) that meet at the
+// bounded grid barrier of a.ctl.
+__device__ void lts_body(const LtsArgs &a, int cta, int ncta) {
   __shared__ __align__(16) LtsState s;
   __shared__ unsigned int h[kBins];
   __shared__ unsigned long long ck[kCandMax];
@@ -207,8 +210,8 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
   __shared__ unsigned long long s_key;
   __shared__ unsigned long long s_pair[2];
   const long long n = __ldcg(&a.n_dev[0]) + __ldcg(&a.n_dev[1]);
-  const long long gstride = (long long)gridDim.x * blockDim.x;
-  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gstride = (long long)ncta * blockDim.x;
+  const long long gtid = (long long)cta * blockDim.x + threadIdx.x;
 
   for (int guard = 0; guard < 200; ++guard) {
     load_cg(&s, a.state, sizeof(LtsState));
@@ -217,7 +220,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
     const bool first = s.fraction > 0.99999;
     // ---- residuals (+ max or first histogram) ----------------------------
     for (int i = threadIdx.x; i < kBins; i += blockDim.x) h[i] = 0;
-    if (blockIdx.x == 0)
+    if (cta == 0)
       for (int i = threadIdx.x; i < kBins; i += blockDim.x) {
         a.hist[kBins + i] = 0;  // next two passes' buffers
       }
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
       for (int i = threadIdx.x; i < kBins; i += blockDim.x)
         if (h[i]) atomicAdd(&a.hist[i], h[i]);
     }
-    if (!grid_sync(a.ctl, a.spin_limit)) return;
+    if (!grid_sync(a.ctl, a.spin_limit, (unsigned)ncta)) return;
     double nth;
     if (first) {
       if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->maxkey);
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         ++pass;
         bits = shift >= 12 ? 12 : shift;
         shift -= bits;
-        if (blockIdx.x == 0) {
+        if (cta == 0) {
           unsigned int *zb = a.hist + ((pass + 1) % 3) * kBins;
           for (int i = threadIdx.x; i < kBins; i += blockDim.x) zb[i] = 0;
         }
@@ -291,7 +294,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
         unsigned int *gh2 = a.hist + (pass % 3) * kBins;
         for (int i = threadIdx.x; i < kBins; i += blockDim.x)
           if (h[i]) atomicAdd(&gh2[i], h[i]);
-        if (!grid_sync(a.ctl, a.spin_limit)) return;
+        if (!grid_sync(a.ctl, a.spin_limit, (unsigned)ncta)) return;
       }
       if (shift == 0) {
         // every bit fixed: the bucket's keys all equal the prefix
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
             if (pos < (unsigned long long)kCandMax) a.cand[pos] = key;
           }
         }
-        if (!grid_sync(a.ctl, a.spin_limit)) return;
+        if (!grid_sync(a.ctl, a.spin_limit, (unsigned)ncta)) return;
         if (threadIdx.x == 0) s_key = __ldcg(&a.ctl->ncand);
         __syncthreads();
         const int nc = (int)(s_key < (unsigned long long)kCandMax ? s_key : kCandMax);
@@ -358,10 +361,10 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
     }
     __shared__ double s_out[28];
     block_sums<28>(acc, red_n, s_out);
-    if (threadIdx.x < 28) a.partial[(long long)blockIdx.x * kPartial + threadIdx.x] = s_out[threadIdx.x];
-    if (!grid_sync(a.ctl, a.spin_limit)) return;
-    if (blockIdx.x == 0) grid_partial_sums(a.partial, 0, 28, s_out);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (threadIdx.x < 28) a.partial[(long long)cta * kPartial + threadIdx.x] = s_out[threadIdx.x];
+    if (!grid_sync(a.ctl, a.spin_limit, (unsigned)ncta)) return;
+    if (cta == 0) grid_partial_sums(a.partial, 0, 28, s_out, ncta);
+    if (cta == 0 && threadIdx.x == 0) {
       LtsMoments mo;
       const double cnt = s_out[0];
       double m[6];
@@ -387,12 +390,23 @@ __global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
       *a.state = s;
       __threadfence();
     }
-    if (blockIdx.x == 0) {
+    if (cta == 0) {
       __syncthreads();
       for (int i = threadIdx.x; i < kBins; i += blockDim.x) a.hist[i] = 0;
     }
-    if (!grid_sync(a.ctl, a.spin_limit)) return;
+    if (!grid_sync(a.ctl, a.spin_limit, (unsigned)ncta)) return;
   }
+}
+
+__global__ void __launch_bounds__(kThreads) lts_kernel(LtsArgs a) {
+  lts_body(a, blockIdx.x, gridDim.x);
+}
+
+// Several independent fits in one cooperative launch: fit f runs on CTAs
+// [f ncta, (f + 1) ncta) with its own arguments and barrier.
+__global__ void __launch_bounds__(kThreads) lts_batch_kernel(const LtsArgs *args, int ncta) {
+  const LtsArgs a = args[blockIdx.x / ncta];
+  lts_body(a, blockIdx.x % ncta, ncta);
 }
 
 }  // namespace
@@ -468,6 +482,74 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
   if (inner_iters) *inner_iters = hs.iter;
   lts_finish(hs);
   return MIRORR_OK;
+}
+
+// ---- many fits in one cooperative launch ----------------------------------------
+//
+// Fit f's CTAs meet at their own barrier (its LtsCtl); each fit has its own
+// state, counters and scratch (LtsFit, all device pointers).  The caller has
+// run lts_begin on every state it uploaded and runs lts_finish on each after
+// reading it back.  A fit whose state is not running returns at once.
+size_t lts_args_bytes() { return sizeof(LtsArgs); }
+
+size_t lts_fit_scratch_bytes(long long n_max, int ncta) {
+  const size_t a = 256;
+  auto up = [&](size_t v) { return (v + a - 1) / a * a; };
+  return up(sizeof(LtsCtl)) + up(sizeof(unsigned int) * 3 * kBins) +
+         up(sizeof(unsigned long long) * kCandMax) + up(sizeof(double) * kPartial * (size_t)ncta) +
+         up(sizeof(double) * (size_t)(n_max > 0 ? n_max : 1));
+}
+
+mirorr_status lts_batch_launch(const LtsFit *fits, int nfits, int ncta, long long spin_limit,
+                               DevBuf &args_dev, HostBuf &args_host, cudaStream_t st) {
+  if (nfits <= 0) return MIRORR_OK;
+  int dev = 0, sms = 0, per = 0;
+  MB2_CUDA_TRY(cudaGetDevice(&dev));
+  MB2_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  MB2_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lts_batch_kernel, kThreads, 0));
+  if ((long long)nfits * ncta > (long long)sms * per) {
+    set_error("%d fits of %d CTAs exceed the %d co-resident CTAs of the LTS kernel", nfits, ncta,
+              sms * per);
+    return MIRORR_EINVAL;
+  }
+  MB2_TRY(args_dev.ensure(sizeof(LtsArgs) * nfits));
+  MB2_TRY(args_host.ensure(sizeof(LtsArgs) * nfits));
+  LtsArgs *ha = args_host.as<LtsArgs>();
+  const size_t al = 256;
+  auto up = [&](size_t v) { return (v + al - 1) / al * al; };
+  for (int f = 0; f < nfits; ++f) {
+    unsigned char *p = static_cast<unsigned char *>(fits[f].scratch);
+    LtsArgs &a = ha[f];
+    a.state = fits[f].state;
+    a.init = fits[f].init;
+    a.moved = fits[f].moved;
+    a.n_dev = fits[f].n_dev;
+    a.ctl = reinterpret_cast<LtsCtl *>(p);
+    p += up(sizeof(LtsCtl));
+    a.hist = reinterpret_cast<unsigned int *>(p);
+    p += up(sizeof(unsigned int) * 3 * kBins);
+    a.cand = reinterpret_cast<unsigned long long *>(p);
+    p += up(sizeof(unsigned long long) * kCandMax);
+    a.partial = reinterpret_cast<double *>(p);
+    p += up(sizeof(double) * kPartial * (size_t)ncta);
+    a.resid = reinterpret_cast<double *>(p);
+    a.spin_limit = spin_limit > 0 ? spin_limit : kDefaultSpinLimit;
+    // zeroed barrier, select control and histograms for this launch
+    MB2_CUDA_TRY(cudaMemsetAsync(fits[f].scratch, 0,
+                                 up(sizeof(LtsCtl)) + up(sizeof(unsigned int) * 3 * kBins), st));
+  }
+  MB2_CUDA_TRY(cudaMemcpyAsync(args_dev.ptr, ha, sizeof(LtsArgs) * nfits, cudaMemcpyHostToDevice, st));
+  const LtsArgs *dargs = args_dev.as<LtsArgs>();
+  void *kargs[] = {(void *)&dargs, (void *)&ncta};
+  MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)lts_batch_kernel, dim3(nfits * ncta),
+                                           dim3(kThreads), kargs, 0, st));
+  ++g_launches;
+  return MIRORR_OK;
+}
+
+// Error flag of fit f's barrier (device word of its scratch).
+const int *lts_fit_error_flag(const void *scratch) {
+  return &static_cast<const LtsCtl *>(scratch)->err;
 }
 
 // ---- allocation-free variant ----------------------------------------------------

@@ -147,12 +147,11 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
 // launcher).  Per voxel the index map is the same FP64 expression as a plain
 // evaluation; only the j and k products are shared along the run.
 template <bool IMG, bool MSK, typename TI, typename TO>
-__global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
+__device__ __forceinline__ void resample_runs(const ResampleArgs &a, long long g0, long long gstride) {
   TO *const out = static_cast<TO *>(a.out);
   const long long n = (long long)a.onx * a.ony * a.onz;
   const long long nrun = (n + 3) >> 2;
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nrun;
-       g += (long long)gridDim.x * blockDim.x) {
+  for (long long g = g0; g < nrun; g += gstride) {
     const long long o0 = g << 2;
     int i, j, k;
     split3(o0, a.onx, a.ony, i, j, k);
@@ -208,6 +207,55 @@ __global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
       }
     }
   }
+}
+
+template <bool IMG, bool MSK, typename TI, typename TO>
+__global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
+  resample_runs<IMG, MSK, TI, TO>(a, blockIdx.x * (long long)blockDim.x + threadIdx.x,
+                                  (long long)gridDim.x * blockDim.x);
+}
+
+// Many resampling passes in one launch (grid.y = job).  A job's image is
+// float32 in and `out_dtype` out (or absent: mask only).
+__global__ void __launch_bounds__(256, 3) resample_batch_kernel(const ResampleJob *jobs) {
+  const ResampleJob &j = jobs[blockIdx.y];
+  if (!j.active) return;
+  ResampleArgs a;
+  a.in = j.in; a.inm = j.inm;
+  a.inx = j.in_size[0]; a.iny = j.in_size[1]; a.inz = j.in_size[2];
+  a.onx = j.out_size[0]; a.ony = j.out_size[1]; a.onz = j.out_size[2];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) a.C[i] = j.C[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) a.e[i] = j.e[i];
+  a.out = j.out; a.outm = j.outm; a.nearest = 0;
+  const long long g0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long gs = (long long)gridDim.x * blockDim.x;
+  if (!a.in || !a.out) {
+    resample_runs<false, true, float, float>(a, g0, gs);
+  } else if (a.inm && a.outm) {
+    if (j.out_dtype == MIRORR_DTYPE_BF16) resample_runs<true, true, float, __nv_bfloat16>(a, g0, gs);
+    else if (j.out_dtype == MIRORR_DTYPE_F16) resample_runs<true, true, float, __half>(a, g0, gs);
+    else resample_runs<true, true, float, float>(a, g0, gs);
+  } else {
+    a.inm = nullptr;
+    a.outm = nullptr;
+    if (j.out_dtype == MIRORR_DTYPE_BF16) resample_runs<true, false, float, __nv_bfloat16>(a, g0, gs);
+    else if (j.out_dtype == MIRORR_DTYPE_F16) resample_runs<true, false, float, __half>(a, g0, gs);
+    else resample_runs<true, false, float, float>(a, g0, gs);
+  }
+}
+
+mirorr_status launch_resample_batch(const ResampleJob *dev_jobs, int njobs, long long max_voxels,
+                                    cudaStream_t s) {
+  if (njobs <= 0) return MIRORR_OK;
+  long long blocks = ((max_voxels + 3) / 4 + 255) / 256;
+  const long long cap = (long long)sm_count() * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  resample_batch_kernel<<<dim3((unsigned)blocks, njobs), 256, 0, s>>>(dev_jobs);
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
 }
 
 template <typename TI, typename TO>
@@ -305,6 +353,30 @@ __global__ void to16_kernel(const float *__restrict__ in, TO *__restrict__ out, 
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     st_copy(out[i], in[i]);
+}
+
+// 16-bit storage -> float32 (exact).
+template <typename TI>
+__global__ void from16_kernel(const TI *__restrict__ in, float *__restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = ld_f(in, i);
+}
+
+mirorr_status launch_from16(const void *in, float *out, long long n, int dtype, cudaStream_t s) {
+  if (n <= 0) return MIRORR_OK;
+  long long blocks = (n + 255) / 256;
+  if (blocks > (long long)sm_count() * 16) blocks = (long long)sm_count() * 16;
+  if (dtype == MIRORR_DTYPE_BF16)
+    from16_kernel<<<(unsigned)blocks, 256, 0, s>>>(static_cast<const __nv_bfloat16 *>(in), out, n);
+  else if (dtype == MIRORR_DTYPE_F16)
+    from16_kernel<<<(unsigned)blocks, 256, 0, s>>>(static_cast<const __half *>(in), out, n);
+  else {
+    set_error("storage type %d is not a 16-bit type", dtype);
+    return MIRORR_EINVAL;
+  }
+  MB2_LAUNCH_CHECK();
+  return MIRORR_OK;
 }
 
 mirorr_status launch_to16(const float *in, void *out, long long n, int dtype, cudaStream_t s) {

@@ -28,13 +28,19 @@
 //   B[(dz, py), k]        = window(k, py + vy, dz + vz)                 (N = 64)
 // so D[(blk, s, split), (dz, py)] = sum over (vz, vy, k) of A B is the split
 // part of the cross term of block blk at candidate (x shift s, y shift py,
-// z shift dz).  A is a banded (Toeplitz) matrix written by the CUDA cores
-// into tensor memory; B is the window itself, brought into shared memory by
-// one TMA tensor copy of the search image in an x-chunked copy
-// ([x / 8][z][y][x % 8], 16-byte rows), so that every (vz, vy, k-step) operand
-// is a plain shared-memory descriptor into that one box (no im2col).  32 MMAs
-// of 128 x 64 x 16 per tile.  The epilogue reads D from tensor memory, adds
-// the two split rows, forms the scores and reduces the top two per block.
+// z shift dz).  A is a banded (Toeplitz) matrix the CUDA cores write into
+// shared memory (each row's band only: the zeros around it are written once
+// per launch and never touched again); B is the window itself, brought into
+// shared memory by one TMA tensor copy of the search image in an x-chunked
+// copy ([x / 8][z][y][x % 8], 16-byte rows), so that every (vz, vy, k-step)
+// operand is a plain shared-memory descriptor into that one box (no im2col).
+// 32 MMAs of 128 x 64 x 16 per tile, accumulating in tensor memory.  The
+// epilogue reads D from tensor memory, adds the two split rows, forms the
+// scores and reduces the top two per block.
+//
+// Every stage takes an array of matcher calls (grid.y or, for the tensor
+// search, a flat tile numbering over the calls), so one launch serves one
+// call or the calls of many image pairs at once.
 //
 // Blocks that do not fit the tensor form -- base block partly or wholly
 // outside its mask, a window candidate whose footprint leaves the search
@@ -75,45 +81,19 @@ constexpr int kPlanes = 11;     // window planes in the box (8 + BW - 1)
 constexpr int kBoxBytes = kXC * kPlanes * kSlots * 16;
 constexpr uint32_t kSBO = kSlots * 16;          // next plane (next 8 rows of N)
 constexpr uint32_t kLBO = kPlanes * kSlots * 16; // next x chunk (next 8 of K)
-constexpr int kTmemCols = 512;  // A: 256 columns, D: 64 columns
-constexpr int kDCol = 256;
+constexpr int kAStepBytes = 128 * 16 * 2;  // one 128 x 16 A operand: [k chunk][row group][8 rows][16 B]
+constexpr int kAChunkSteps = 8;            // the (vy, k-step) operands of one vz
+constexpr int kAChunkBytes = kAChunkSteps * kAStepBytes;
+constexpr int kCtasPerSM = 3;              // resident CTAs per SM (their phases overlap)
+constexpr uint32_t kALBO = 16 * 128;       // next k chunk of A
+constexpr uint32_t kASBO = 128;            // next 8 rows of A
+constexpr int kTmemCols = 64;   // D: 64 columns of FP32
 constexpr int kThreads = 256;
+constexpr int kMaxCalls = 128;  // tensor maps of one launch (kernel parameter space)
 
-struct Prep16 {
-  float mu;      // mean of the base block (every voxel)
-  float sxx;     // sum over base-mask voxels of x~^2
-  float sxt;     // sum over base-mask voxels of x~
-  float sxt_tc;  // sum over every voxel of hi + lo
-  int mmode;     // 1: base mask on everywhere, 2: off everywhere, 0: mixed
-  int pad[3];
-};
 
-struct Args16 {
-  const void *base;
-  const uint8_t *bmask;
-  const void *search;
-  const uint8_t *smask;
-  const float2 *stats;    // (mu_y, Syy) per search position; Syy sign bit: footprint leaves the mask
-  const uint8_t *wand;    // per block: window wholly inside the search mask
-  const uint8_t *selected;
-  const Prep16 *prep;
-  const uint32_t *xs;     // per block [part][vz][vy] 4 values of 16 bits as two 32-bit words
-  int nx, ny, nz;
-  int nbx, nby, nbz;
-  int stx, sty, stz;
-  int G, W;
-  int bpt;          // blocks per tile (G bpt is a multiple of 8: tile windows start on a chunk)
-  int tiles_x;
-  long long ntiles;
-  long long nblocks;
-  float *best;
-  float *second;
-  int32_t *match;
-  uint8_t *status;
-  unsigned long long *ncc_count;
-  unsigned int *ctl;      // [0] tensor blocks, [1] direct blocks, [2] a bounded wait gave up
-  int *fb_list;
-};
+
+using Args16 = Match16Call;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -153,12 +133,6 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
       " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
-}
-
-__device__ __forceinline__ void tmem_st4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(a),
-               "r"(b), "r"(c), "r"(d)
-               : "memory");
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
@@ -234,12 +208,16 @@ __device__ __forceinline__ void cand_range(int o, int S, int W, int &lo, int &hi
 // of the BW^3 footprint (every voxel) and sum (y - mean)^2, FP32 two-pass;
 // the sign bit of Syy is set when a search-mask voxel of the footprint is 0.
 // One thread per 4 consecutive x positions (each footprint row of 7 values
-// serves the 4).
+// serves the 4).  grid.y = call.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) box_stats16_kernel(const T *__restrict__ y,
-                                                          const uint8_t *__restrict__ ms, int nx,
-                                                          int ny, int nz, float2 *__restrict__ out) {
+__global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active) return;
+  const T *__restrict__ y = static_cast<const T *>(a.search);
+  const uint8_t *__restrict__ ms = a.smask;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  float2 *__restrict__ out = a.stats;
   constexpr int PX = 4, RL = PX + kBW - 1;
   const int ngx = (nx + PX - 1) / PX;
   const long long n = (long long)ngx * ny * nz;
@@ -304,21 +282,91 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const T *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// Window-AND per block, separable (x over the rows, then y, then z at block
+// resolution): 1 when every voxel of the block's clipped window box (the
+// union of its candidates' footprints) is inside the search mask.
+// ---------------------------------------------------------------------------
+__global__ void wand_x16_kernel(const Args16 *calls) {
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active) return;
+  const int R = a.W / 2;
+  const long long n = (long long)a.nbx * a.ny * a.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int bx = (int)(i % a.nbx);
+    const long long yz = i / a.nbx;
+    const int ox = a.stx + bx * a.G;
+    int lo = ox - R, hi = ox + R;
+    if (lo < 0) lo = 0;
+    if (hi > a.nx - kBW) hi = a.nx - kBW;
+    unsigned v = 1;
+    const uint8_t *row = a.smask + yz * a.nx;
+    for (int x = lo; x <= hi + kBW - 1; ++x) v &= row[x] != 0 ? 1u : 0u;
+    a.wand[i] = (uint8_t)v;
+  }
+}
+__global__ void wand_y16_kernel(const Args16 *calls) {
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active) return;
+  const int R = a.W / 2;
+  const uint8_t *in = a.wand;
+  uint8_t *out = a.wand + (long long)a.nbx * a.ny * a.nz;
+  const long long n = (long long)a.nbx * a.nby * a.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int bx = (int)(i % a.nbx);
+    const long long r = i / a.nbx;
+    const int by = (int)(r % a.nby), z = (int)(r / a.nby);
+    const int oy = a.sty + by * a.G;
+    int lo = oy - R, hi = oy + R;
+    if (lo < 0) lo = 0;
+    if (hi > a.ny - kBW) hi = a.ny - kBW;
+    unsigned v = 1;
+    for (int y = lo; y <= hi + kBW - 1; ++y) v &= in[((long long)z * a.ny + y) * a.nbx + bx];
+    out[i] = (uint8_t)v;
+  }
+}
+__global__ void wand_z16_kernel(const Args16 *calls) {
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active) return;
+  const int R = a.W / 2;
+  const uint8_t *in = a.wand + (long long)a.nbx * a.ny * a.nz;
+  uint8_t *out = a.wand + (long long)a.nbx * a.ny * a.nz + (long long)a.nbx * a.nby * a.nz;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
+       b += (long long)gridDim.x * blockDim.x) {
+    const long long bxy = b % ((long long)a.nbx * a.nby);
+    const int bz = (int)(b / ((long long)a.nbx * a.nby));
+    const int oz = a.stz + bz * a.G;
+    int lo = oz - R, hi = oz + R;
+    if (lo < 0) lo = 0;
+    if (hi > a.nz - kBW) hi = a.nz - kBW;
+    unsigned v = 1;
+    for (int z = lo; z <= hi + kBW - 1; ++z) v &= in[(long long)z * a.nbx * a.nby + bxy];
+    out[b] = (uint8_t)v;
+  }
+}
+__device__ __forceinline__ const uint8_t *wand_of(const Args16 &a) {
+  return a.wand + (long long)a.nbx * a.ny * a.nz + (long long)a.nbx * a.nby * a.nz;
+}
+
+// ---------------------------------------------------------------------------
 // Base-block preparation, one thread per block: the FP32 mean, the masked
 // sums of x~ and x~^2, the base-mask mode and the two 16-bit parts of x~
-// (packed per (part, vz, vy) as two 32-bit words).
+// (packed per (part, vz, vy) as two 32-bit words).  grid.y = call.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) prep16_kernel(const T *__restrict__ x,
-                                                     const uint8_t *__restrict__ mb, int nx, int ny,
-                                                     int nbx, int nby, long long nblocks, int stx,
-                                                     int sty, int stz, int G, Prep16 *__restrict__ prep,
-                                                     uint32_t *__restrict__ xs) {
-  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nblocks;
+__global__ void __launch_bounds__(256) prep16_kernel(const Args16 *calls) {
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active) return;
+  const T *__restrict__ x = static_cast<const T *>(a.base);
+  const uint8_t *__restrict__ mb = a.bmask;
+  const int nx = a.nx, ny = a.ny;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
        b += (long long)gridDim.x * blockDim.x) {
     int bx, by, bz;
-    split3(b, nbx, nby, bx, by, bz);
-    const long long o = ((long long)(stz + bz * G) * ny + (sty + by * G)) * nx + (stx + bx * G);
+    split3(b, a.nbx, a.nby, bx, by, bz);
+    const long long o =
+        ((long long)(a.stz + bz * a.G) * ny + (a.sty + by * a.G)) * nx + (a.stx + bx * a.G);
     float v[kB];
     uint64_t mbits = 0;
     float sum = 0.f;
@@ -331,6 +379,7 @@ __global__ void __launch_bounds__(256) prep16_kernel(const T *__restrict__ x,
     }
     const float mu = sum * (1.0f / kB);
     float sxx = 0.f, sxt = 0.f, stc = 0.f;
+    uint32_t *xb = a.xs + b * 64;
 #pragma unroll
     for (int r = 0; r < 16; ++r) {  // r = vz * 4 + vy
       uint32_t hw[2] = {0u, 0u}, lw[2] = {0u, 0u};
@@ -348,7 +397,6 @@ __global__ void __launch_bounds__(256) prep16_kernel(const T *__restrict__ x,
         hw[vx >> 1] |= S16<T>::bits(h) << (16 * (vx & 1));
         lw[vx >> 1] |= S16<T>::bits(l) << (16 * (vx & 1));
       }
-      uint32_t *xb = xs + b * 64;
       xb[r * 2] = hw[0];
       xb[r * 2 + 1] = hw[1];
       xb[32 + r * 2] = lw[0];
@@ -361,56 +409,98 @@ __global__ void __launch_bounds__(256) prep16_kernel(const T *__restrict__ x,
     pp.sxt_tc = stc;
     pp.mmode = mbits == ~0ULL ? 1 : (mbits == 0 ? 2 : 0);
     pp.pad[0] = pp.pad[1] = pp.pad[2] = 0;
-    prep[b] = pp;
+    a.prep[b] = pp;
   }
 }
 
 // ---------------------------------------------------------------------------
 // x-chunked copy of the search image for the window tensor copies:
-// out[((xc * nz + z) * ny + y) * 8 + i] = search(x0 + 8 xc + i, y, z), zero
+// out[((xc * nz + z) * ny + y)] = 8 values search(x0 + 8 xc + i, y, z), zero
 // outside the image.  x0 = (block grid x start) - R, so every tile's window
-// starts on a chunk boundary.
+// starts on a chunk boundary.  grid.y = call.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void chunk16_kernel(const T *__restrict__ in, int nx, int ny, int nz, int x0, int nxc,
-                               uint4 *__restrict__ out) {
-  const long long n = (long long)nxc * nz * ny;
+__global__ void chunk16_kernel(const Args16 *calls) {
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active || !a.tensor) return;
+  const T *__restrict__ in = static_cast<const T *>(a.search);
+  const long long n = (long long)a.nxc * a.nz * a.ny;
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
        r += (long long)gridDim.x * blockDim.x) {
-    const int y = (int)(r % ny);
-    const long long t = r / ny;
-    const int z = (int)(t % nz);
-    const int xc = (int)(t / nz);
-    const long long row = ((long long)z * ny + y) * nx;
+    const int y = (int)(r % a.ny);
+    const long long t = r / a.ny;
+    const int z = (int)(t % a.nz);
+    const int xc = (int)(t / a.nz);
+    const long long row = ((long long)z * a.ny + y) * a.nx;
     uint32_t w[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       uint32_t lo = 0u, hi = 0u;
-      const int xa = x0 + 8 * xc + 2 * k, xb2 = xa + 1;
-      if (xa >= 0 && xa < nx) lo = S16<T>::bits(in[row + xa]);
-      if (xb2 >= 0 && xb2 < nx) hi = S16<T>::bits(in[row + xb2]);
+      const int xa = a.chunk_x0 + 8 * xc + 2 * k, xb2 = xa + 1;
+      if (xa >= 0 && xa < a.nx) lo = S16<T>::bits(in[row + xa]);
+      if (xb2 >= 0 && xb2 < a.nx) hi = S16<T>::bits(in[row + xb2]);
       w[k] = lo | (hi << 16);
     }
-    out[r] = make_uint4(w[0], w[1], w[2], w[3]);
+    a.chunked[r] = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
+// Every selected block of a call without the tensor form to the direct
+// search; blocks culled by the variance selection get their culled record.
+__global__ void route_all16_kernel(const Args16 *calls) {
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active || a.tensor) return;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
+       b += (long long)gridDim.x * blockDim.x) {
+    if (a.selected && !a.selected[b]) {
+      int bx, by, bz;
+      split3(b, a.nbx, a.nby, bx, by, bz);
+      const long long orig = ((long long)(a.stz + bz * a.G) * a.ny + (a.sty + by * a.G)) * a.nx +
+                             (a.stx + bx * a.G);
+      write_out(a, b, -3.f, -3.f, orig, 0);
+    } else {
+      const unsigned int k = atomicAdd(&a.ctl[1], 1u);
+      a.fb_list[k] = (int)b;
+    }
+  }
+}
+
+struct TcMaps {
+  CUtensorMap m[kMaxCalls];
+};
+
+// The call of a tile in the launch's flat tile numbering (calls in order).
+__device__ __forceinline__ int call_of_tile(const Args16 *calls, int ncalls, long long tile) {
+  int lo = 0, hi = ncalls - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (calls[mid].tile0 <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // ---------------------------------------------------------------------------
-// The tensor-core search.  Persistent CTAs of 8 warps, one per SM (the
-// 512-column tensor-memory allocation and the shared-memory request keep
-// one CTA per SM).  Warp w owns tensor-memory lanes 32 (w % 4) .. + 31
-// (A rows / D rows (blk, s, part)); warps 0-3 write the A k-step 0 and read
-// D columns 0-31 (dz 0-3), warps 4-7 the k-step 1 and columns 32-63.
+// The tensor-core search.  Persistent CTAs of 8 warps, three per SM (while
+// one waits on memory or on its MMAs the others work).  Row m = 32 (w % 4) +
+// lane of A and D is (blk = m / 16, shift s = (m / 2) % 8, part = m % 2);
+// warps 0-3 write the A band of k-step 0 and read D columns 0-31 (dz 0-3),
+// warps 4-7 k-step 1 and columns 32-63.  A streams through two 32 KB buffers,
+// one vz (8 operands) at a time: the CUDA cores write the next vz's bands
+// while the tensor cores multiply the previous one.
 // ---------------------------------------------------------------------------
 template <typename T, int W>
-__global__ void __launch_bounds__(kThreads, 1)
-    ncc_tc_kernel(Args16 a, const __grid_constant__ CUtensorMap tmap) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSM)
+    ncc_tc_kernel(const Args16 *calls, int ncalls, long long total_tiles,
+                  const __grid_constant__ TcMaps maps) {
   static_assert(W >= 2 && W <= 8, "window of the tensor form");
   constexpr int R = W / 2;
   extern __shared__ __align__(1024) uint8_t dsm[];
-  uint8_t *win = reinterpret_cast<uint8_t *>(
+  uint8_t *const sbase = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(dsm) + 1023) & ~static_cast<uintptr_t>(1023));
-  __shared__ __align__(8) uint64_t s_tma_bar, s_mma_bar;
+  uint8_t *const sa = sbase;                         // A: 2 buffers of one vz's 8 operands
+  uint8_t *const win = sbase + 2 * kAChunkBytes;      // B: the window box
+  __shared__ __align__(8) uint64_t s_tma_bar, s_mma_bar[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_any, s_fail;
   __shared__ long long s_b[kTileBlocks];
@@ -421,12 +511,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int q = warp & 3, half = warp >> 2;
-  const int m = 32 * q + lane;            // tensor-memory lane = A / D row
+  const int m = 32 * q + lane;            // row of A and D (tensor-memory lane)
   const int blk = m >> 4, sft = (m >> 1) & 7, part = m & 1;
 
   if (tid == 0) {
     mbar_init(&s_tma_bar, 1);
-    mbar_init(&s_mma_bar, 1);
+    mbar_init(&s_mma_bar[0], 1);
+    mbar_init(&s_mma_bar[1], 1);
     s_fail = 0;
   }
   if (warp == 0) {
@@ -436,32 +527,34 @@ __global__ void __launch_bounds__(kThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
+  // A starts as zeros; each row later rewrites only the words of its band
+  for (int i = tid; i < 2 * kAChunkBytes / 16; i += kThreads)
+    reinterpret_cast<uint4 *>(sa)[i] = make_uint4(0u, 0u, 0u, 0u);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16);
-  // A starts as zeros: each (vz, vy, k-step) row later rewrites only the four
-  // columns that can hold its band
-  for (int r = 0; r < 16; ++r) {
-    const uint32_t c = (uint32_t)(r * 16 + half * 8);
-    tmem_st4(lane_addr + c, 0u, 0u, 0u, 0u);
-    tmem_st4(lane_addr + c + 4, 0u, 0u, 0u, 0u);
-  }
-  asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+  // this row's band in k-step `half`: element t0 of the step holds x~[0]
+  // (words floor(t0 / 2) ..; an odd t0 straddles the 16-bit halves)
+  int t0 = 0;
+  // byte offset of 32-bit word c of this row in step r: r * 4 KB + row_off + c_off(c)
+  const uint32_t row_off = (uint32_t)(m >> 3) * kASBO + (uint32_t)(m & 7) * 16u;
 
-  // this row's band in k-step `half`: x~[0] of the row sits at k = G blk + s
-  const int t0 = a.G * blk + sft - 16 * half;
-  const bool band = t0 < 16 && t0 + 4 > 0;
-  int c0 = t0 <= 0 ? 0 : (t0 >> 1);
-  if (c0 > 4) c0 = 4;
-  const int dsh = 2 * c0 - t0;  // x offset vx of the first element of the 4-column window
-
-  unsigned tma_phase = 0, mma_phase = 0;
-  for (long long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-    const int bxg = (int)(tile % a.tiles_x);
+  unsigned tma_phase = 0, mma_phase[2] = {0u, 0u};
+  int cur_call = -1;
+  Args16 a;
+  for (long long tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    const int ci = call_of_tile(calls, ncalls, tile);
+    if (ci != cur_call) {
+      a = calls[ci];
+      cur_call = ci;
+      t0 = a.G * blk + sft - 16 * half;
+    }
+    const long long lt = tile - a.tile0;
+    const int bxg = (int)(lt % a.tiles_x);
     const int bx0 = bxg * a.bpt;
-    const long long rest = tile / a.tiles_x;
+    const long long rest = lt / a.tiles_x;
     const int by = (int)(rest % a.nby), bz = (int)(rest / a.nby);
     const int oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
     if (tid < kTileBlocks) {
@@ -476,7 +569,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const Prep16 pp = a.prep[b];
         if (!sel) {
           write_out(a, b, -3.f, -3.f, orig, 0);
-        } else if (pp.mmode == 1 && a.wand[b] && pp.sxx > 0.f) {
+        } else if (pp.mmode == 1 && wand_of(a)[b] && pp.sxx > 0.f) {
           e = 1;
           s_sxx[tid] = pp.sxx;
           s_stc[tid] = pp.sxt_tc;
@@ -502,74 +595,111 @@ __global__ void __launch_bounds__(kThreads, 1)
                        smem_u32(&s_tma_bar)),
                    "r"((unsigned)kBoxBytes)
                    : "memory");
-      tma_load_4d(win, &tmap, 0, oy - R, oz - R, (a.G * bx0) >> 3, &s_tma_bar);
+      tma_load_4d(win, &maps.m[ci], 0, oy - R, oz - R, (a.G * bx0) >> 3, &s_tma_bar);
     }
-    // ---- A: this row's band of the split block, per (vz, vy) --------------
-    // (every lane stores, so the warp-wide tensor-memory stores stay uniform;
-    // rows without a band or block store zeros into zeros)
+    // ---- the block's two 16-bit parts for every (vz, vy), in registers ------
+    const bool band = t0 < 16 && t0 + 4 > 0;
+    const bool live = band && s_elig[blk] != 0;
+    uint2 xw[16];
     {
-      const bool live = band && s_elig[blk] != 0;
       const uint32_t *xr = a.xs + (live ? s_b[blk] : 0) * 64 + part * 32;
-#pragma unroll 4
-      for (int r = 0; r < 16; ++r) {
-        uint64_t u = 0;
-        if (live) {
-          const uint2 w2 = *reinterpret_cast<const uint2 *>(xr + 2 * r);
-          u = (uint64_t)w2.x | ((uint64_t)w2.y << 32);
-        }
-        // the 8 elements of the window hold x~[dsh .. dsh + 7] (zero outside 0..3)
-        unsigned __int128 wv = (unsigned __int128)u;
-        wv = dsh >= 0 ? (wv >> (16 * dsh)) : (wv << (16 * (-dsh)));
-        const uint64_t lo = (uint64_t)wv, hi = (uint64_t)(wv >> 64);
-        tmem_st4(lane_addr + (uint32_t)(r * 16 + half * 8 + c0), (uint32_t)lo,
-                 (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
-      }
-      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+#pragma unroll
+      for (int r = 0; r < 16; ++r)
+        xw[r] = live ? *reinterpret_cast<const uint2 *>(xr + 2 * r) : make_uint2(0u, 0u);
     }
-    tc_fence_before();
-    __syncthreads();
-    // ---- MMAs: one thread issues the 32 k-steps ---------------------------
-    if (tid == 0) {
-      tc_fence_after();
-      const bool landed = mbar_wait(&s_tma_bar, tma_phase, 1 << 22);
-      if (!landed) {
-        s_fail = 1;
-        atomicExch(&a.ctl[2], 1u);
-      } else {
-        constexpr uint32_t idesc = (1u << 4) | (S16<T>::kFmt << 7) | (S16<T>::kFmt << 10) |
-                                   ((uint32_t)(64 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-        const uint32_t wb = smem_u32(win);
+    const int c0 = t0 >= 0 ? (t0 >> 1) : -((1 - t0) >> 1);  // floor(t0 / 2)
+    const bool odd = t0 & 1;
+    constexpr uint32_t idesc = (1u << 4) | (S16<T>::kFmt << 7) | (S16<T>::kFmt << 10) |
+                               ((uint32_t)(64 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    // ---- per vz: write the A operands of buffer vz % 2, multiply --------------
+    for (int vz = 0; vz < 4; ++vz) {
+      const int buf = vz & 1;
+      if (vz >= 2) {
+        // the multiplies of vz - 2 read this buffer: one thread waits for
+        // them, the others at the CTA barrier (no issue slots spent polling)
+        if (tid == 0 && !mbar_wait(&s_mma_bar[buf], mma_phase[buf], 1 << 24)) {
+          atomicExch(&a.ctl[2], 1u);
+          s_fail = 1;
+        }
+        mma_phase[buf] ^= 1u;
+        __syncthreads();
+        if (s_fail) break;
+      }
+      if (band) {
+        uint8_t *const cb = sa + (size_t)buf * kAChunkBytes + row_off;
+#pragma unroll
+        for (int vy = 0; vy < 4; ++vy) {
+          const uint2 w2 = xw[vz * 4 + vy];
+          uint32_t wv[3];
+          if (odd) {
+            wv[0] = w2.x << 16;
+            wv[1] = __byte_perm(w2.x, w2.y, 0x5432);
+            wv[2] = w2.y >> 16;
+          } else {
+            wv[0] = w2.x;
+            wv[1] = w2.y;
+            wv[2] = 0u;
+          }
+          uint8_t *const step = cb + (size_t)(2 * vy + half) * kAStepBytes;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int c = c0 + k;
+            if (c >= 0 && c < 8 && (k < 2 || odd))
+              *reinterpret_cast<uint32_t *>(step + (c >> 2) * kALBO + (c & 3) * 4) = wv[k];
+          }
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0 && !s_fail) {
+        tc_fence_after();
+        if (vz == 0 && !mbar_wait(&s_tma_bar, tma_phase, 1 << 22)) {
+          s_fail = 1;
+          atomicExch(&a.ctl[2], 1u);
+        } else {
+          const uint32_t wb = smem_u32(win), ab = smem_u32(sa) + (uint32_t)buf * kAChunkBytes;
 #pragma unroll 1
-        for (int i = 0; i < 32; ++i) {
-          const int r = i >> 1, ks = i & 1, vz = r >> 2, vy = r & 3;
-          const uint64_t bd = sdesc(wb + (uint32_t)(2 * ks) * kLBO + (uint32_t)vz * kSBO +
-                                        (uint32_t)vy * 16u,
-                                    kLBO, kSBO);
-          const uint32_t at = tmem + (uint32_t)(r * 16 + ks * 8);
+          for (int j = 0; j < kAChunkSteps; ++j) {
+            const int vy = j >> 1, ks = j & 1;
+            const uint64_t ad = sdesc(ab + (uint32_t)j * kAStepBytes, kALBO, kASBO);
+            const uint64_t bd = sdesc(wb + (uint32_t)(2 * ks) * kLBO + (uint32_t)vz * kSBO +
+                                          (uint32_t)vy * 16u,
+                                      kLBO, kSBO);
+            const int acc = (vz | j) != 0;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                : "memory");
+          }
           asm volatile(
-              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-              " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem + kDCol),
-              "r"(at), "l"(bd), "r"(idesc), "r"(i)
+              "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                  smem_u32(&s_mma_bar[buf]))
               : "memory");
         }
-        asm volatile(
-            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                smem_u32(&s_mma_bar))
-            : "memory");
       }
+      __syncthreads();
+      if (s_fail) break;  // every thread sees the same flag
     }
-    __syncthreads();
-    if (s_fail) break;  // every thread sees the same flag; the copy never landed
+    if (s_fail) break;
     tma_phase ^= 1u;
-    // ---- epilogue -----------------------------------------------------------
-    if (!mbar_wait(&s_mma_bar, mma_phase, 1 << 24)) {
-      atomicExch(&a.ctl[2], 1u);
-      s_fail = 1;
+    // ---- epilogue: the last two commits (vz 2 and 3) ------------------------
+    if (tid == 0) {
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+        if (!mbar_wait(&s_mma_bar[bb], mma_phase[bb], 1 << 24)) {
+          atomicExch(&a.ctl[2], 1u);
+          s_fail = 1;
+        }
     }
-    mma_phase ^= 1u;
+    mma_phase[0] ^= 1u;
+    mma_phase[1] ^= 1u;
+    __syncthreads();
+    if (s_fail) break;
     tc_fence_after();
     uint32_t d[32];
-    tmem_ld32(lane_addr + (uint32_t)(kDCol + 32 * half), d);
+    tmem_ld32(lane_addr + (uint32_t)(32 * half), d);
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
     // add the two parts: part 0 keeps columns 0-15 of this half, part 1 16-31
     float v[16];
@@ -640,19 +770,21 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
-// Direct FP32 search for the blocks the tensor form does not take (listed in
-// fb_list): one CTA per block, candidates over the threads, the masked sums
-// of the reference formula per candidate.  A candidate whose footprint lies
-// inside the search mask with the base block inside its mask uses the box
-// statistics for Syy and one product per voxel.
+// Direct FP32 search for the blocks the tensor form does not take (each
+// call's fb_list): one CTA per block, candidates over the threads, the masked
+// sums of the reference formula per candidate.  A candidate whose footprint
+// lies inside the search mask with the base block inside its mask uses the
+// box statistics for Syy and one product per voxel.  grid.y = call.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(128) ncc_fb16_kernel(Args16 a) {
+__global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
   constexpr int NT = 128;
   __shared__ float s_xt[kB], s_mb[kB];
   __shared__ float s_y[16 * 16 * 16];
   __shared__ uint8_t s_m[16 * 16 * 16];
   __shared__ Top2 s_red[NT / 32];
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active) return;
   const int tid = threadIdx.x;
   const T *base = static_cast<const T *>(a.base);
   const T *search = static_cast<const T *>(a.search);
@@ -736,34 +868,9 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(Args16 a) {
   }
 }
 
-// Every block to the direct search (geometries without the tensor form);
-// blocks culled by the variance selection get their culled record.
-__global__ void route_all16_kernel(Args16 a) {
-  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
-       b += (long long)gridDim.x * blockDim.x) {
-    if (a.selected && !a.selected[b]) {
-      int bx, by, bz;
-      split3(b, a.nbx, a.nby, bx, by, bz);
-      const long long orig = ((long long)(a.stz + bz * a.G) * a.ny + (a.sty + by * a.G)) * a.nx +
-                             (a.stx + bx * a.G);
-      write_out(a, b, -3.f, -3.f, orig, 0);
-    } else {
-      const unsigned int k = atomicAdd(&a.ctl[1], 1u);
-      a.fb_list[k] = (int)b;
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-struct MapCache {
-  const void *ptr = nullptr;
-  int dims[4] = {0, 0, 0, 0};
-  int dtype = -1;
-  CUtensorMap map;
-};
-
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -784,132 +891,158 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-template <typename T>
-mirorr_status run16(const BmGeom &g, const void *base, const uint8_t *bmask, const void *search,
-                    const uint8_t *smask, const uint8_t *selected, const BmOut &out, Bm16Work &w,
-                    unsigned long long *ncc_count, cudaStream_t s) {
-  const int nx = g.size[0], ny = g.size[1], nz = g.size[2];
-  const long long nvox = (long long)nx * ny * nz;
-  const int R = g.nw / 2;
-  const int SM = sm_count();
-  MB2_TRY(w.stats.ensure(sizeof(float2) * nvox));
-  MB2_TRY(w.prep.ensure(sizeof(Prep16) * g.nblocks));
-  MB2_TRY(w.xs.ensure(sizeof(uint32_t) * 64 * g.nblocks));
-  MB2_TRY(w.ctl.ensure(4 * sizeof(unsigned int)));
-  MB2_TRY(w.fb_list.ensure(sizeof(int) * g.nblocks));
-  MB2_CUDA_TRY(cudaMemsetAsync(w.ctl.ptr, 0, 4 * sizeof(unsigned int), s));
-  float2 *stats = w.stats.as<float2>();
-  {
-    const long long n = (long long)((nx + 3) / 4) * ny * nz;
-    long long blocks = (n + 255) / 256;
-    if (blocks > (long long)SM * 16) blocks = (long long)SM * 16;
-    box_stats16_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(static_cast<const T *>(search), smask,
-                                                           nx, ny, nz, stats);
-    MB2_LAUNCH_CHECK();
-  }
-  const uint8_t *wand = nullptr;
-  MB2_TRY(launch_window_and(g, stats, w.wand, &wand, s));
-  {
-    long long blocks = (g.nblocks + 255) / 256;
-    if (blocks > (long long)SM * 16) blocks = (long long)SM * 16;
-    prep16_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(
-        static_cast<const T *>(base), bmask, nx, ny, g.nb[0], g.nb[1], g.nblocks, g.st[0], g.st[1],
-        g.st[2], g.ngap, w.prep.as<Prep16>(), w.xs.as<uint32_t>());
-    MB2_LAUNCH_CHECK();
-  }
-  Args16 a;
-  a.base = base;
-  a.bmask = bmask;
-  a.search = search;
-  a.smask = smask;
-  a.stats = stats;
-  a.wand = wand;
-  a.selected = selected;
-  a.prep = w.prep.as<Prep16>();
-  a.xs = w.xs.as<uint32_t>();
-  a.nx = nx; a.ny = ny; a.nz = nz;
-  a.nbx = g.nb[0]; a.nby = g.nb[1]; a.nbz = g.nb[2];
-  a.stx = g.st[0]; a.sty = g.st[1]; a.stz = g.st[2];
-  a.G = g.ngap;
-  a.W = g.nw;
+size_t tc_smem_bytes() { return (size_t)2 * kAChunkBytes + kBoxBytes + 1024; }
+
+}  // namespace
+
+// Derived per-call fields: the tensor form's tile layout and copy geometry.
+void prepare16(const BmGeom &g, Match16Call &c) {
+  c.nx = g.size[0]; c.ny = g.size[1]; c.nz = g.size[2];
+  c.nbx = g.nb[0]; c.nby = g.nb[1]; c.nbz = g.nb[2];
+  c.stx = g.st[0]; c.sty = g.st[1]; c.stz = g.st[2];
+  c.G = g.ngap;
+  c.W = g.nw;
+  c.nblocks = g.nblocks;
   // blocks per tile: the tile's bands fit the 32-wide box, and G bpt is a
   // multiple of 8 so every tile's window starts on a chunk of the copy
-  a.bpt = 0;
+  c.bpt = 0;
   for (int b = kTileBlocks; b >= 1; --b)
     if (g.ngap * (b - 1) + g.nw + kBW - 1 <= 8 * kXC && (g.ngap * b) % 8 == 0) {
-      a.bpt = b;
+      c.bpt = b;
       break;
     }
-  a.tiles_x = a.bpt ? (g.nb[0] + a.bpt - 1) / a.bpt : 0;
-  a.ntiles = (long long)a.tiles_x * g.nb[1] * g.nb[2];
-  a.nblocks = g.nblocks;
-  a.best = out.best;
-  a.second = out.second;
-  a.match = out.match;
-  a.status = out.status;
-  a.ncc_count = ncc_count;
-  a.ctl = w.ctl.as<unsigned int>();
-  a.fb_list = w.fb_list.as<int>();
-  // the tensor form: block width 4, odd window up to 7, block gap 1, blocks of a
-  // tile within the 32-wide window box
-  const bool tensor = g.bw == kBW && g.bgap == 1 && (g.nw & 1) && g.nw <= 7 && g.nw >= 3 &&
-                      a.bpt > 0 && ny >= kSlots && nz >= kPlanes;
-  if (tensor) {
-    // x-chunked copy of the search image whose first chunk starts at stx - R
-    const int x0 = g.st[0] - R;
-    const int nxc = (g.ngap * a.bpt / 8) * (a.tiles_x - 1) + kXC;  // chunks the last box reaches
-    const size_t bytes = sizeof(uint4) * (size_t)nxc * nz * ny;
-    MB2_TRY(w.chunked.ensure(bytes));
-    {
-      const long long n = (long long)nxc * nz * ny;
-      long long blocks = (n + 255) / 256;
-      if (blocks > (long long)SM * 16) blocks = (long long)SM * 16;
-      chunk16_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(static_cast<const T *>(search), nx, ny,
-                                                         nz, x0, nxc, w.chunked.as<uint4>());
-      MB2_LAUNCH_CHECK();
+  c.tensor = g.bw == kBW && g.bgap == 1 && (g.nw & 1) && g.nw <= 7 && g.nw >= 3 && c.bpt > 0 &&
+             c.ny >= kSlots && c.nz >= kPlanes;
+  c.tiles_x = c.tensor ? (g.nb[0] + c.bpt - 1) / c.bpt : 0;
+  c.ntiles = (long long)c.tiles_x * g.nb[1] * g.nb[2];
+  c.chunk_x0 = g.st[0] - g.nw / 2;
+  c.nxc = c.tensor ? (g.ngap * c.bpt / 8) * (c.tiles_x - 1) + kXC : 0;
+}
+
+size_t match16_chunk_bytes(const Match16Call &c) {
+  return c.tensor ? sizeof(uint4) * (size_t)c.nxc * c.nz * c.ny : 0;
+}
+
+long long match16_number_tiles(Match16Call *calls, int n) {
+  long long tiles = 0;
+  for (int i = 0; i < n; ++i) {
+    calls[i].tile0 = tiles;
+    if (calls[i].active && calls[i].tensor) tiles += calls[i].ntiles;
+  }
+  return tiles;
+}
+
+size_t match16_wand_bytes(const Match16Call &c) {
+  return (size_t)c.nbx * c.ny * c.nz + (size_t)c.nbx * c.nby * c.nz + (size_t)c.nblocks;
+}
+
+namespace {
+
+template <typename T>
+mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cudaStream_t s) {
+  const int SM = sm_count();
+  const long long tiles = match16_number_tiles(host_calls, ncalls);
+  long long max_vox = 0, max_blocks = 0, max_chunks = 0;
+  int W = 0, G = 0;
+  bool any_tensor = false;
+  for (int i = 0; i < ncalls; ++i) {
+    const Match16Call &c = host_calls[i];
+    if (c.active && c.tensor) {
+      any_tensor = true;
+      if ((W && W != c.W) || (G && G != c.G)) {
+        set_error("the calls of one launch must share the window and the block spacing");
+        return MIRORR_EINVAL;
+      }
+      W = c.W;
+      G = c.G;
+    }
+    if (!c.active) continue;
+    max_vox = std::max(max_vox, (long long)c.nx * c.ny * c.nz);
+    max_blocks = std::max(max_blocks, c.nblocks);
+    max_chunks = std::max(max_chunks, (long long)c.nxc * c.nz * c.ny);
+  }
+  MB2_TRY(calls_dev.ensure(sizeof(Args16) * ncalls));
+  MB2_CUDA_TRY(cudaMemcpyAsync(calls_dev.ptr, host_calls, sizeof(Args16) * ncalls,
+                               cudaMemcpyHostToDevice, s));
+  const Args16 *dc = calls_dev.as<Args16>();
+  auto grid_for = [&](long long n) {
+    long long b = (n + 255) / 256;
+    if (b > (long long)SM * 4) b = (long long)SM * 4;
+    return dim3((unsigned)(b < 1 ? 1 : b), (unsigned)ncalls);
+  };
+  box_stats16_kernel<T><<<grid_for(max_vox / 4 + 1), 256, 0, s>>>(dc);
+  MB2_LAUNCH_CHECK();
+  wand_x16_kernel<<<grid_for(max_vox / 2 + 1), 256, 0, s>>>(dc);
+  MB2_LAUNCH_CHECK();
+  wand_y16_kernel<<<grid_for(max_vox / 4 + 1), 256, 0, s>>>(dc);
+  MB2_LAUNCH_CHECK();
+  wand_z16_kernel<<<grid_for(max_blocks), 256, 0, s>>>(dc);
+  MB2_LAUNCH_CHECK();
+  prep16_kernel<T><<<grid_for(max_blocks), 256, 0, s>>>(dc);
+  MB2_LAUNCH_CHECK();
+  if (any_tensor) {
+    chunk16_kernel<T><<<grid_for(max_chunks), 256, 0, s>>>(dc);
+    MB2_LAUNCH_CHECK();
+  }
+  route_all16_kernel<<<grid_for(max_blocks), 256, 0, s>>>(dc);
+  MB2_LAUNCH_CHECK();
+  if (any_tensor) {
+    if (ncalls > kMaxCalls) {
+      set_error("more than %d matcher calls in one tensor launch", kMaxCalls);
+      return MIRORR_EINVAL;
     }
     EncodeTiledFn enc = encode_fn();
     if (!enc) {
       set_error("cuTensorMapEncodeTiled is not available from the driver");
       return MIRORR_ECUDA;
     }
-    CUtensorMap map;
-    const cuuint64_t dims[4] = {8, (cuuint64_t)ny, (cuuint64_t)nz, (cuuint64_t)nxc};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)16 * ny, (cuuint64_t)16 * ny * nz};
-    const cuuint32_t box[4] = {8, (cuuint32_t)kSlots, (cuuint32_t)kPlanes, (cuuint32_t)kXC};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(&map,
-                     sizeof(T) == 2 && S16<T>::kFmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
-                     4, w.chunked.ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-      set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
-      return MIRORR_ECUDA;
+    static TcMaps maps;  // the host side of the kernel parameter (large: static)
+    static std::mutex maps_mu;
+    std::lock_guard<std::mutex> lock(maps_mu);
+    memset(&maps, 0, sizeof(maps));
+    for (int i = 0; i < ncalls; ++i) {
+      const Match16Call &c = host_calls[i];
+      if (!c.active || !c.tensor) continue;
+      const cuuint64_t dims[4] = {8, (cuuint64_t)c.ny, (cuuint64_t)c.nz, (cuuint64_t)c.nxc};
+      const cuuint64_t strides[3] = {16, (cuuint64_t)16 * c.ny, (cuuint64_t)16 * c.ny * c.nz};
+      const cuuint32_t box[4] = {8, (cuuint32_t)kSlots, (cuuint32_t)kPlanes, (cuuint32_t)kXC};
+      const cuuint32_t estr[4] = {1, 1, 1, 1};
+      CUresult r = enc(&maps.m[i],
+                       S16<T>::kFmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                       4, c.chunked, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return MIRORR_ECUDA;
+      }
     }
-    const size_t smem = (size_t)kBoxBytes + 1024 + 120 * 1024;  // one CTA per SM
-    auto kern = (g.nw == 7) ? ncc_tc_kernel<T, 7> : (g.nw == 5) ? ncc_tc_kernel<T, 5>
-                                                                : ncc_tc_kernel<T, 3>;
+    const size_t smem = tc_smem_bytes();
+    auto kern = (W == 7) ? ncc_tc_kernel<T, 7> : (W == 5) ? ncc_tc_kernel<T, 5>
+                                                          : ncc_tc_kernel<T, 3>;
     MB2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long long grid = a.ntiles < SM ? a.ntiles : SM;
+    const long long grid = tiles < (long long)SM * kCtasPerSM ? tiles : (long long)SM * kCtasPerSM;
     if (grid > 0) {
-      kern<<<(unsigned)grid, kThreads, smem, s>>>(a, map);
+      kern<<<(unsigned)grid, kThreads, smem, s>>>(dc, ncalls, tiles, maps);
       MB2_LAUNCH_CHECK();
     }
-  } else {
-    // every block through the direct search
-    route_all16_kernel<<<(unsigned)((g.nblocks + 255) / 256 < SM * 8 ? (g.nblocks + 255) / 256
-                                                                       : SM * 8),
-                         256, 0, s>>>(a);
-    MB2_LAUNCH_CHECK();
   }
-  ncc_fb16_kernel<T><<<(unsigned)SM * 8, 128, 0, s>>>(a);
+  ncc_fb16_kernel<T><<<dim3((unsigned)SM * 4, (unsigned)ncalls), 128, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
 
 }  // namespace
+
+mirorr_status launch_match16_batch(int dtype, int ncalls, Match16Call *host_calls,
+                                   DevBuf &calls_dev, cudaStream_t s) {
+  if (ncalls <= 0) return MIRORR_OK;
+  if (dtype == MIRORR_DTYPE_BF16) return run16<__nv_bfloat16>(ncalls, host_calls, calls_dev, s);
+  if (dtype == MIRORR_DTYPE_F16) return run16<__half>(ncalls, host_calls, calls_dev, s);
+  set_error("storage type %d is not a 16-bit type", dtype);
+  return MIRORR_EINVAL;
+}
 
 mirorr_status launch_match16(int dtype, const BmGeom &g, const void *base, const uint8_t *bmask,
                              const void *search, const uint8_t *smask, const uint8_t *selected,
@@ -927,13 +1060,40 @@ mirorr_status launch_match16(int dtype, const BmGeom &g, const void *base, const
     set_error("the 16-bit search supports windows up to 13 (got %d)", g.nw);
     return MIRORR_EINVAL;
   }
-  if (dtype == MIRORR_DTYPE_BF16)
-    return run16<__nv_bfloat16>(g, base, bmask, search, smask, selected, out, w, ncc_count, s);
-  if (dtype == MIRORR_DTYPE_F16)
-    return run16<__half>(g, base, bmask, search, smask, selected, out, w, ncc_count, s);
-  set_error("storage type %d is not a 16-bit type", dtype);
-  return MIRORR_EINVAL;
+  Match16Call c;
+  memset(&c, 0, sizeof(c));
+  prepare16(g, c);
+  const long long nvox = (long long)g.size[0] * g.size[1] * g.size[2];
+  MB2_TRY(w.stats.ensure(sizeof(float2) * nvox));
+  MB2_TRY(w.wand.ensure(match16_wand_bytes(c)));
+  MB2_TRY(w.prep.ensure(sizeof(Prep16) * g.nblocks));
+  MB2_TRY(w.xs.ensure(sizeof(uint32_t) * 64 * g.nblocks));
+  MB2_TRY(w.ctl.ensure(4 * sizeof(unsigned int)));
+  MB2_TRY(w.fb_list.ensure(sizeof(int) * g.nblocks));
+  if (c.tensor) MB2_TRY(w.chunked.ensure(match16_chunk_bytes(c)));
+  MB2_CUDA_TRY(cudaMemsetAsync(w.ctl.ptr, 0, 4 * sizeof(unsigned int), s));
+  c.base = base;
+  c.bmask = bmask;
+  c.search = search;
+  c.smask = smask;
+  c.selected = selected;
+  c.stats = w.stats.as<float2>();
+  c.wand = w.wand.as<uint8_t>();
+  c.prep = w.prep.as<Prep16>();
+  c.xs = w.xs.as<uint32_t>();
+  c.chunked = w.chunked.as<uint4>();
+  c.best = out.best;
+  c.second = out.second;
+  c.match = out.match;
+  c.status = out.status;
+  c.ncc_count = ncc_count;
+  c.ctl = w.ctl.as<unsigned int>();
+  c.fb_list = w.fb_list.as<int>();
+  c.active = 1;
+  return launch_match16_batch(dtype, 1, &c, w.calls, s);
 }
+
+size_t match16_prep_bytes() { return sizeof(Prep16); }
 
 mirorr_status match16_take_timeout(Bm16Work &w, cudaStream_t s, bool *timed_out) {
   *timed_out = false;

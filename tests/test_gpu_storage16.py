@@ -102,7 +102,7 @@ def test_matcher16_matches_oracle(ctx, c, store):
 @pytest.mark.parametrize("store", ["bf16", "f16"])
 @pytest.mark.parametrize("mode,kind", [("symmetric", "affine"), ("classic", "rigid")])
 def test_register16_matches_oracle(ctx, store, mode, kind):
-    shape = (64, 56, 40)
+    shape = (72, 64, 48)
     ph = make_phantom(shape, n_gauss=20, kind=kind, seed=41 if kind == "affine" else 42,
                       max_angle_deg=4.0, max_shift_vox=4.0)
     rp = O.RegParams(mode, kind, 4, O.BMParams(4, 1, 3, 7, 1.0), 0.5, store)
