@@ -555,11 +555,14 @@ def c2_leg(mb, ctx, dev, pairs, oracle_pairs=2):
         rs = [b.result(i)[0] for i in ids]
         dt = time.perf_counter() - t0
         info = b.info()
+        tm = b.times()
         b.close()
         res[name] = rs
         out["legs"][name] = {"seconds": round(dt, 3), "registrations_per_s": round(len(phs) / dt, 3),
                              "steps": info["steps"], "graph_replays": info["replays"],
-                             "graph_captures": info["captures"]}
+                             "graph_instantiations": info["captures"],
+                             "graph_updates": info["updates"],
+                             "host_seconds": {k: round(v, 4) for k, v in tm.items()}}
     f32 = out["legs"]["serial_f32"]["registrations_per_s"]
     for k in ("serial_bf16", "batch_bf16", "batch_f16"):
         out["legs"][k]["speedup_vs_serial_f32"] = round(out["legs"][k]["registrations_per_s"] / f32, 3)

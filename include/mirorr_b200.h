@@ -358,8 +358,13 @@ MIRORR_API mirorr_status mirorr_batch_result(mirorr_batch b, int64_t request_id,
 /* Drops a request (running or finished) and frees its slot. */
 MIRORR_API mirorr_status mirorr_batch_cancel(mirorr_batch b, int64_t request_id);
 /* [0] running, [1] finished and not taken, [2] bytes reserved, [3] budget,
- * [4] steps, [5] steps replayed from a graph, [6] graph captures, [7] 0. */
+ * [4] steps, [5] steps replayed from a graph, [6] graph instantiations,
+ * [7] graph updates in place (a step whose set of requests or levels changed). */
 MIRORR_API mirorr_status mirorr_batch_info(mirorr_batch b, int64_t info[8]);
+/* Host-clock seconds the batch's steps spent so far: [0] setting up pyramid
+ * levels, [1] building the step's descriptors and graph, [2] from launch to
+ * the end of the step's device work, [3] advancing the requests. */
+MIRORR_API mirorr_status mirorr_batch_times(mirorr_batch b, double seconds[4]);
 /* Graph replay of unchanged steps on (default) or off. */
 MIRORR_API mirorr_status mirorr_batch_set_graphs(mirorr_batch b, int32_t on);
 

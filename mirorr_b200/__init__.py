@@ -230,6 +230,7 @@ def lib():
         "mirorr_batch_cancel": [vp, ctypes.c_int64],
         "mirorr_batch_info": [vp, vp],
         "mirorr_batch_set_graphs": [vp, ctypes.c_int32],
+        "mirorr_batch_times": [vp, vp],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -757,8 +758,16 @@ class Batch:
     def info(self):
         v = np.zeros(8, np.int64)
         _check(lib().mirorr_batch_info(self._h, _ptr(v)))
-        keys = ["running", "finished", "bytes_reserved", "budget", "steps", "replays", "captures"]
-        return dict(zip(keys, [int(x) for x in v[:7]]))
+        keys = ["running", "finished", "bytes_reserved", "budget", "steps", "replays", "captures",
+                "updates"]
+        return dict(zip(keys, [int(x) for x in v]))
+
+    def times(self):
+        """Host-clock seconds spent by the steps so far: level setup, descriptor
+        and graph building, launch to end of device work, request advance."""
+        v = np.zeros(4, np.float64)
+        _check(lib().mirorr_batch_times(self._h, _ptr(v)))
+        return dict(zip(["setup", "issue", "device", "advance"], [float(x) for x in v]))
 
     def set_graphs(self, on: bool):
         _check(lib().mirorr_batch_set_graphs(self._h, 1 if on else 0))

@@ -1813,7 +1813,10 @@ struct mirorr_batch_s {
   bool graphs = true;
   cudaGraphExec_t gexec = nullptr;
   std::vector<long long> gkey;
-  int64_t rounds = 0, replays = 0, captures = 0;
+  int64_t rounds = 0, replays = 0, captures = 0, updates = 0;
+  // host-clock seconds: level setup, descriptors and graph work, launch to
+  // synchronisation, advancing the requests
+  double t_setup = 0, t_issue = 0, t_device = 0, t_advance = 0;
 };
 
 namespace {
@@ -1983,7 +1986,8 @@ mirorr_status batch_issue(mirorr_batch b, int njobs, long long max_vox, int ncal
   MB2_CUDA_TRY(cudaMemsetAsync(b->d_counts.ptr, 0, sizeof(long long) * 4 * S, st));
   MB2_CUDA_TRY(cudaMemsetAsync(b->d_ctl.ptr, 0, sizeof(unsigned int) * 4 * 2 * S, st));
   MB2_TRY(launch_resample_batch(b->d_jobs.as<ResampleJob>(), njobs, max_vox, st));
-  MB2_TRY(launch_match16_batch(b->storage, ncalls, b->h_calls.as<Match16Call>(), b->d_calls, st));
+  MB2_TRY(launch_match16_batch(b->storage, ncalls, b->h_calls.as<Match16Call>(), b->d_calls, st,
+                               true));
   MB2_TRY(launch_postfilter_batch(b->d_pf.as<PfCall>(), ncalls, max_blocks, st));
   MB2_TRY(lts_batch_launch(b->fits.data(), nfits, kLtsCtas, c->ltsw.spin_limit, b->d_lts_args,
                            b->h_lts_args, st));
@@ -2012,6 +2016,11 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
   if (running) *running = nrun;
   if (finished) *finished = 0;
   if (!nrun) return MIRORR_OK;
+  using clk = std::chrono::steady_clock;
+  auto secs = [](clk::time_point a, clk::time_point z) {
+    return std::chrono::duration<double>(z - a).count();
+  };
+  const clk::time_point t0 = clk::now();
   MB2_TRY(ensure_ones(c, max_in));
   // levels entered this round
   for (auto &s : b->slots) {
@@ -2019,6 +2028,8 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
     mirorr_status r = batch_setup_level(b, s);
     if (r != MIRORR_OK) batch_fail(b, s, r, mirorr_last_error());
   }
+  const clk::time_point t1 = clk::now();
+  b->t_setup += secs(t0, t1);
   ResampleJob *jobs = b->h_jobs.as<ResampleJob>();
   Match16Call *calls = b->h_calls.as<Match16Call>();
   PfCall *pf = b->h_pf.as<PfCall>();
@@ -2149,16 +2160,19 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
   // the tile numbering the tensor launch reads from the call descriptors (a
   // replay copies them from h_calls as written here)
   match16_number_tiles(calls, nc);
-  // ---- launches (replayed from the graph when the set is unchanged) -------
+  // ---- launches ---------------------------------------------------------------
+  // Replayed from the graph when the set of requests and levels is unchanged.
+  // Otherwise the round is captured again; as every round launches the same
+  // sequence of nodes (only sizes, grids and arguments differ), the existing
+  // executable graph is updated in place, and instantiated anew only when the
+  // update is refused.
   const bool same = b->graphs && b->gexec && key == b->gkey;
   if (same) {
+    const clk::time_point t2 = clk::now();
+    b->t_issue += secs(t1, t2);
     MB2_CUDA_TRY(cudaGraphLaunch(b->gexec, st));
     ++b->replays;
   } else if (b->graphs) {
-    if (b->gexec) {
-      cudaGraphExecDestroy(b->gexec);
-      b->gexec = nullptr;
-    }
     MB2_TRY(b->d_calls.ensure(sizeof(Match16Call) * nc));
     MB2_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     mirorr_status r = batch_issue(b, nj, max_vox, nc, (int)b->fits.size(), max_blocks);
@@ -2172,20 +2186,42 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
       set_error("capturing the batch round failed: %s", cudaGetErrorString(e));
       return MIRORR_ECUDA;
     }
-    e = cudaGraphInstantiate(&b->gexec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      b->gexec = nullptr;
-      set_error("instantiating the batch round failed: %s", cudaGetErrorString(e));
-      return MIRORR_ECUDA;
+    bool updated = false;
+    if (b->gexec) {
+      cudaGraphExecUpdateResultInfo ui;
+      if (cudaGraphExecUpdate(b->gexec, graph, &ui) == cudaSuccess) {
+        updated = true;
+        ++b->updates;
+      } else {
+        cudaGetLastError();
+        cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+      }
     }
+    if (!updated) {
+      e = cudaGraphInstantiate(&b->gexec, graph, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        b->gexec = nullptr;
+        set_error("instantiating the batch round failed: %s", cudaGetErrorString(e));
+        return MIRORR_ECUDA;
+      }
+      ++b->captures;
+    }
+    cudaGraphDestroy(graph);
     b->gkey = key;
-    ++b->captures;
+    const clk::time_point t2 = clk::now();
+    b->t_issue += secs(t1, t2);
     MB2_CUDA_TRY(cudaGraphLaunch(b->gexec, st));
   } else {
+    const clk::time_point t2 = clk::now();
+    b->t_issue += secs(t1, t2);
     MB2_TRY(batch_issue(b, nj, max_vox, nc, (int)b->fits.size(), max_blocks));
   }
+  const clk::time_point t3 = clk::now();
   MB2_CUDA_TRY(cudaStreamSynchronize(st));
+  const clk::time_point t4 = clk::now();
+  b->t_device += secs(t3, t4);
   ++b->rounds;
   // ---- advance every request ----------------------------------------------
   const unsigned char *rd = b->h_rd.as<unsigned char>();
@@ -2230,6 +2266,7 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
     }
   }
   if (finished) *finished = nfin;
+  b->t_advance += secs(t4, clk::now());
   return MIRORR_OK;
 }
 
@@ -2549,7 +2586,16 @@ mirorr_status mirorr_batch_info(mirorr_batch b, int64_t info[8]) {
   info[4] = b->rounds;
   info[5] = b->replays;
   info[6] = b->captures;
-  info[7] = 0;
+  info[7] = b->updates;
+  return MIRORR_OK;
+}
+
+mirorr_status mirorr_batch_times(mirorr_batch b, double seconds[4]) {
+  if (!b || !seconds) { set_error("null argument"); return MIRORR_EINVAL; }
+  seconds[0] = b->t_setup;
+  seconds[1] = b->t_issue;
+  seconds[2] = b->t_device;
+  seconds[3] = b->t_advance;
   return MIRORR_OK;
 }
 

@@ -147,8 +147,10 @@ struct Bm16Work {
 // persistent launch, and the direct FP32 search of the blocks the tensor form
 // does not take.  host_calls[i].tile0 is set here (match16_number_tiles);
 // calls_dev receives the descriptors.  Writes every active call's per-block results.
+// every_stage: launch every stage even when no call has tensor tiles (the
+// same launch sequence for any set of calls, as a graph update needs).
 mirorr_status launch_match16_batch(int dtype, int ncalls, Match16Call *host_calls,
-                                   DevBuf &calls_dev, cudaStream_t s);
+                                   DevBuf &calls_dev, cudaStream_t s, bool every_stage = false);
 // One matcher call on 16-bit images with the scratch of w.
 mirorr_status launch_match16(int dtype, const BmGeom &g, const void *base, const uint8_t *bmask,
                              const void *search, const uint8_t *smask, const uint8_t *selected,

@@ -409,6 +409,13 @@ __global__ void __launch_bounds__(kThreads) lts_batch_kernel(const LtsArgs *args
   lts_body(a, blockIdx.x % ncta, ncta);
 }
 
+// Zeroes each fit's barrier, select control and histograms (CTA f: fit f) so
+// a batch's launch sequence has the same nodes whatever the number of fits.
+__global__ void lts_batch_zero_kernel(const LtsArgs *args, unsigned long long words) {
+  uint4 *p = reinterpret_cast<uint4 *>(args[blockIdx.x].ctl);
+  for (unsigned long long i = threadIdx.x; i < words; i += blockDim.x) p[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 }  // namespace
 
 mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const double *moved_dev,
@@ -534,12 +541,15 @@ mirorr_status lts_batch_launch(const LtsFit *fits, int nfits, int ncta, long lon
     p += up(sizeof(double) * kPartial * (size_t)ncta);
     a.resid = reinterpret_cast<double *>(p);
     a.spin_limit = spin_limit > 0 ? spin_limit : kDefaultSpinLimit;
-    // zeroed barrier, select control and histograms for this launch
-    MB2_CUDA_TRY(cudaMemsetAsync(fits[f].scratch, 0,
-                                 up(sizeof(LtsCtl)) + up(sizeof(unsigned int) * 3 * kBins), st));
   }
   MB2_CUDA_TRY(cudaMemcpyAsync(args_dev.ptr, ha, sizeof(LtsArgs) * nfits, cudaMemcpyHostToDevice, st));
   const LtsArgs *dargs = args_dev.as<LtsArgs>();
+  // zeroed barrier, select control and histograms of every fit (the scratch
+  // starts 256-byte aligned: the region is whole 16-byte words)
+  const size_t zbytes = up(sizeof(LtsCtl)) + up(sizeof(unsigned int) * 3 * kBins);
+  lts_batch_zero_kernel<<<nfits, 256, 0, st>>>(dargs, (unsigned long long)(zbytes / 16));
+  MB2_LAUNCH_CHECK();
+  ++g_launches;
   void *kargs[] = {(void *)&dargs, (void *)&ncta};
   MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)lts_batch_kernel, dim3(nfits * ncta),
                                            dim3(kThreads), kargs, 0, st));

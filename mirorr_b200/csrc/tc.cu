@@ -1,7 +1,7 @@
 // tc.cu -- the 16-bit storage search (BF16 or FP16 volumes) for sm_100a: the
 // block-vs-window cross term of the NCC search on the tensor cores
 // (tcgen05.mma, FP32 accumulation in tensor memory), the rest on the CUDA
-// cores in FP32.  No FP64 anywhere in this file.
+// cores in FP32 (the box statistics from exact FP64 sums).
 //
 // Semantics are those of the reference matcher (itkBlockMatcher.txx:46-101,
 // 631-848; see ncc.cu): for each block and each candidate of its clipped
@@ -18,8 +18,9 @@
 // lo = T(x~ - hi); the window values y are the stored 16-bit values
 // themselves, exact in the operands.  The tensor cores sum x~' y
 // (x~' = hi + lo) in FP32; Sxy = sum x~' y - mu_y sum x~' removes the window
-// mean afterwards (sum x~' is about 0, so nothing large cancels).  Sxx and the
-// box statistics (mu_y, Syy) are FP32 two-pass sums.
+// mean afterwards (sum x~' is about 0, so nothing large cancels).  Sxx is an
+// FP32 two-pass sum; the box statistics (mu_y, Syy) come from exact FP64 sums
+// of the 16-bit window values.
 //
 // Tensor formulation (block width 4, window W <= 8, block gap 1).  A tile is
 // up to 8 consecutive blocks of one row of the block grid (same by, bz).  With
@@ -50,6 +51,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <cfloat>
 #include <mutex>
 
 #include "kernels.cuh"
@@ -84,11 +86,9 @@ constexpr uint32_t kLBO = kPlanes * kSlots * 16; // next x chunk (next 8 of K)
 constexpr int kAStepBytes = 128 * 16 * 2;  // one 128 x 16 A operand: [k chunk][row group][8 rows][16 B]
 constexpr int kAChunkSteps = 8;            // the (vy, k-step) operands of one vz
 constexpr int kAChunkBytes = kAChunkSteps * kAStepBytes;
-constexpr int kCtasPerSM = 3;              // resident CTAs per SM (their phases overlap)
 constexpr uint32_t kALBO = 16 * 128;       // next k chunk of A
 constexpr uint32_t kASBO = 128;            // next 8 rows of A
-constexpr int kTmemCols = 64;   // D: 64 columns of FP32
-constexpr int kThreads = 256;
+constexpr int kTmemCols = 128;  // D: two accumulators of 64 FP32 columns (tiles alternate)
 constexpr int kMaxCalls = 128;  // tensor maps of one launch (kernel parameter space)
 
 
@@ -112,14 +112,20 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int limit) {
+// Waits for the phase of parity `parity` of the barrier to complete.  Each
+// try_wait suspends the thread until the phase completes or about 20 us pass
+// (no polling loop spends issue slots); after `limit` such waits (about
+// limit x 20 us) the wait gives up and returns false.
+constexpr int kWaitSuspendNs = 20000;
+constexpr int kWaitLimit = 50000;  // about one second
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int limit = kWaitLimit) {
   for (int i = 0; i < limit; ++i) {
     unsigned done;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
         " selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kWaitSuspendNs)
         : "memory");
     if (done) return true;
   }
@@ -135,15 +141,13 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+      " [%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
-        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
-        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[14]), "=r"(r[15])
       : "r"(addr));
 }
 
@@ -205,78 +209,105 @@ __device__ __forceinline__ void cand_range(int o, int S, int W, int &lo, int &hi
 
 // ---------------------------------------------------------------------------
 // Box statistics of the 16-bit search image: per candidate origin p, the mean
-// of the BW^3 footprint (every voxel) and sum (y - mean)^2, FP32 two-pass;
-// the sign bit of Syy is set when a search-mask voxel of the footprint is 0.
-// One thread per 4 consecutive x positions (each footprint row of 7 values
-// serves the 4).  grid.y = call.
+// of the BW^3 footprint (every voxel) and Syy = sum (y - mean)^2, from the
+// footprint's sum and sum of squares in FP64.  Both sums of 16-bit values are
+// exact in FP64 (a square has at most 22 significant bits), and so is
+// Syy = sum y^2 - (sum y)^2 / 64 up to its final rounding: the two terms are
+// exact and their difference is exact (Sterbenz), so Syy is correctly
+// rounded to FP32 and 0 exactly when the footprint is constant.  The sign
+// bit of Syy is set when a search-mask voxel of the footprint is 0.
+//
+// Separable: a CTA of 32 x 8 threads owns 32 x 8 output columns and walks
+// 16 output planes; per input plane it stages the 35 x 11 halo (values and
+// mask) in shared memory, sums each row's 4-wide runs along x (FP64), then
+// each thread sums 4 of those along y and keeps the last four planes' sums in
+// registers for the z sum.  grid.y = call; grid.x strides over the tiles.
 // ---------------------------------------------------------------------------
+constexpr int kStX = 32, kStY = 8, kStZ = 16;
+__device__ __forceinline__ long long stats_tiles(const Args16 &a, int &tx, int &ty) {
+  const int vx = a.nx - kBW + 1, vy = a.ny - kBW + 1, vz = a.nz - kBW + 1;
+  if (vx <= 0 || vy <= 0 || vz <= 0) return 0;
+  tx = (vx + kStX - 1) / kStX;
+  ty = (vy + kStY - 1) / kStY;
+  return (long long)tx * ty * ((vz + kStZ - 1) / kStZ);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
+  constexpr int HX = kStX + kBW - 1, HY = kStY + kBW - 1;  // 35 x 11 halo
+  __shared__ float s_v[HY][HX + 1];
+  __shared__ uint8_t s_m[HY][HX + 1];
+  __shared__ double s_sx[HY][kStX], s_sq[HY][kStX];
+  __shared__ uint8_t s_mx[HY][kStX];
   const Args16 &a = calls[blockIdx.y];
   if (!a.active) return;
+  int ntx = 0, nty = 0;
+  const long long ntiles = stats_tiles(a, ntx, nty);
   const T *__restrict__ y = static_cast<const T *>(a.search);
   const uint8_t *__restrict__ ms = a.smask;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  float2 *__restrict__ out = a.stats;
-  constexpr int PX = 4, RL = PX + kBW - 1;
-  const int ngx = (nx + PX - 1) / PX;
-  const long long n = (long long)ngx * ny * nz;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
-       p += (long long)gridDim.x * blockDim.x) {
-    int gx, yy, z;
-    split3(p, ngx, ny, gx, yy, z);
-    const int x0 = gx * PX;
-    const long long o = ((long long)z * ny + yy) * nx + x0;
-    const bool rowok = yy <= ny - kBW && z <= nz - kBW;
-    float sum[PX], ss[PX];
-    unsigned allm = ~0u;
-#pragma unroll
-    for (int j = 0; j < PX; ++j) sum[j] = ss[j] = 0.f;
-    if (rowok && x0 <= nx - kBW) {
-#pragma unroll
-      for (int vz = 0; vz < kBW; ++vz)
-#pragma unroll
-        for (int vy = 0; vy < kBW; ++vy) {
-          const long long q = o + ((long long)vz * ny + vy) * nx;
-          float v[RL];
-          unsigned mb = 0u;
-#pragma unroll
-          for (int i = 0; i < RL; ++i) {
-            const bool in = x0 + i < nx;
-            v[i] = in ? S16<T>::f(y[q + i]) : 0.f;
-            mb |= ((in && ms[q + i] != 0) ? 1u : 0u) << i;
-          }
-          allm &= mb;
-#pragma unroll
-          for (int vx = 0; vx < kBW; ++vx)
-#pragma unroll
-            for (int j = 0; j < PX; ++j) sum[j] += v[j + vx];
+  const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int x0 = (int)(t % ntx) * kStX;
+    const long long r = t / ntx;
+    const int y0 = (int)(r % nty) * kStY, z0 = (int)(r / nty) * kStZ;
+    double s0 = 0, s1 = 0, s2 = 0, q0 = 0, q1 = 0, q2 = 0;
+    unsigned m0 = 0, m1 = 0, m2 = 0;
+    const int zend = min(z0 + kStZ + kBW - 1, nz);
+    for (int zi = z0; zi < zend; ++zi) {
+      __syncthreads();  // the previous plane's x sums are read
+      const long long plane = (long long)zi * ny;
+      for (int i = tid; i < HY * HX; i += 256) {
+        const int hy = i / HX, hx = i - hy * HX;
+        const int gx = x0 + hx, gy = y0 + hy;
+        float v = 0.f;
+        uint8_t m = 0;
+        if (gx < nx && gy < ny) {
+          const long long q = (plane + gy) * nx + gx;
+          v = S16<T>::f(y[q]);
+          m = ms[q] != 0 ? 1 : 0;
         }
-      float mu[PX];
-#pragma unroll
-      for (int j = 0; j < PX; ++j) mu[j] = sum[j] * (1.0f / kB);
-#pragma unroll
-      for (int vz = 0; vz < kBW; ++vz)
-#pragma unroll
-        for (int vy = 0; vy < kBW; ++vy) {
-          const long long q = o + ((long long)vz * ny + vy) * nx;
-          float v[RL];
-#pragma unroll
-          for (int i = 0; i < RL; ++i) v[i] = (x0 + i < nx) ? S16<T>::f(y[q + i]) : 0.f;
-#pragma unroll
-          for (int vx = 0; vx < kBW; ++vx)
-#pragma unroll
-            for (int j = 0; j < PX; ++j) {
-              const float d = v[j + vx] - mu[j];
-              ss[j] = fmaf(d, d, ss[j]);
-            }
-        }
-#pragma unroll
-      for (int j = 0; j < PX; ++j) {
-        if (x0 + j > nx - kBW) continue;
-        const bool inm = ((allm >> j) & 0xFu) == 0xFu;
-        out[o + j] = make_float2(mu[j], inm ? ss[j] : -ss[j] - 0.0f);
+        s_v[hy][hx] = v;
+        s_m[hy][hx] = m;
       }
+      __syncthreads();
+      for (int i = tid; i < HY * kStX; i += 256) {
+        const int hy = i >> 5, hx = i & 31;
+        double sx = 0.0, sq = 0.0;
+        unsigned mk = 1;
+#pragma unroll
+        for (int k = 0; k < kBW; ++k) {
+          const double v = (double)s_v[hy][hx + k];
+          sx += v;
+          sq = fma(v, v, sq);
+          mk &= s_m[hy][hx + k];
+        }
+        s_sx[hy][hx] = sx;
+        s_sq[hy][hx] = sq;
+        s_mx[hy][hx] = (uint8_t)mk;
+      }
+      __syncthreads();
+      double sy = 0.0, qy = 0.0;
+      unsigned my = 1;
+#pragma unroll
+      for (int k = 0; k < kBW; ++k) {
+        sy += s_sx[ly + k][lx];
+        qy += s_sq[ly + k][lx];
+        my &= s_mx[ly + k][lx];
+      }
+      const int oz = zi - (kBW - 1);
+      const int ox = x0 + lx, oy = y0 + ly;
+      if (oz >= z0 && ox <= nx - kBW && oy <= ny - kBW) {
+        const double S = ((s0 + s1) + s2) + sy, Q = ((q0 + q1) + q2) + qy;
+        const bool inm = (m0 & m1 & m2 & my) != 0;
+        const double syy = Q - S * S * (1.0 / kB);
+        const float f = (float)syy;
+        a.stats[((long long)oz * ny + oy) * nx + ox] =
+            make_float2((float)(S * (1.0 / kB)), inm ? f : -f - 0.0f);
+      }
+      s0 = s1; s1 = s2; s2 = sy;
+      q0 = q1; q1 = q2; q2 = qy;
+      m0 = m1; m1 = m2; m2 = my;
     }
   }
 }
@@ -350,10 +381,17 @@ __device__ __forceinline__ const uint8_t *wand_of(const Args16 &a) {
 }
 
 // ---------------------------------------------------------------------------
-// Base-block preparation, one thread per block: the FP32 mean, the masked
-// sums of x~ and x~^2, the base-mask mode and the two 16-bit parts of x~
-// (packed per (part, vz, vy) as two 32-bit words).  grid.y = call.
+// Base-block preparation, 16 lanes per block (lane r = vz * 4 + vy holds base
+// row r): the FP32 mean, the masked sums of x~ and x~^2, the base-mask mode
+// and the two 16-bit parts of x~ (packed per (part, vz, vy) as two 32-bit
+// words).  Sums over the block are half-warp shuffle trees.  grid.y = call.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float half_sum(float v) {
+#pragma unroll
+  for (int o = 8; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) prep16_kernel(const Args16 *calls) {
   const Args16 &a = calls[blockIdx.y];
@@ -361,55 +399,64 @@ __global__ void __launch_bounds__(256) prep16_kernel(const Args16 *calls) {
   const T *__restrict__ x = static_cast<const T *>(a.base);
   const uint8_t *__restrict__ mb = a.bmask;
   const int nx = a.nx, ny = a.ny;
-  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
-       b += (long long)gridDim.x * blockDim.x) {
-    int bx, by, bz;
-    split3(b, a.nbx, a.nby, bx, by, bz);
-    const long long o =
-        ((long long)(a.stz + bz * a.G) * ny + (a.sty + by * a.G)) * nx + (a.stx + bx * a.G);
-    float v[kB];
-    uint64_t mbits = 0;
-    float sum = 0.f;
+  const int r = threadIdx.x & 15;
+  const unsigned half_mask = (threadIdx.x & 16) ? 0xFFFF0000u : 0x0000FFFFu;
+  // every lane of a warp runs the same number of iterations (the half-warp
+  // shuffles need both halves), blocks past the end idle
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  const long long niter = (a.nblocks * 16 + nthreads - 1) / nthreads;
+  for (long long it = 0; it < niter; ++it) {
+    const long long b = (it * nthreads + blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4;
+    const bool live = b < a.nblocks;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    unsigned mbits = 0;
+    if (live) {
+      int bx, by, bz;
+      split3(b, a.nbx, a.nby, bx, by, bz);
+      const long long q = ((long long)(a.stz + bz * a.G + (r >> 2)) * ny + (a.sty + by * a.G + (r & 3))) * nx +
+                          (a.stx + bx * a.G);
 #pragma unroll
-    for (int i = 0; i < kB; ++i) {
-      const long long q = o + ((long long)(i >> 4) * ny + ((i >> 2) & 3)) * nx + (i & 3);
-      v[i] = S16<T>::f(x[q]);
-      mbits |= (uint64_t)(mb[q] != 0 ? 1u : 0u) << i;
-      sum += v[i];
-    }
-    const float mu = sum * (1.0f / kB);
-    float sxx = 0.f, sxt = 0.f, stc = 0.f;
-    uint32_t *xb = a.xs + b * 64;
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {  // r = vz * 4 + vy
-      uint32_t hw[2] = {0u, 0u}, lw[2] = {0u, 0u};
-#pragma unroll
-      for (int vx = 0; vx < 4; ++vx) {
-        const int i = r * 4 + vx;
-        const float d = v[i] - mu;
-        if ((mbits >> i) & 1u) {
-          sxx = fmaf(d, d, sxx);
-          sxt += d;
-        }
-        const T h = S16<T>::t(d);
-        const T l = S16<T>::t(d - S16<T>::f(h));
-        stc += S16<T>::f(h) + S16<T>::f(l);
-        hw[vx >> 1] |= S16<T>::bits(h) << (16 * (vx & 1));
-        lw[vx >> 1] |= S16<T>::bits(l) << (16 * (vx & 1));
+      for (int i = 0; i < 4; ++i) {
+        v[i] = S16<T>::f(x[q + i]);
+        mbits |= (mb[q + i] != 0 ? 1u : 0u) << i;
       }
-      xb[r * 2] = hw[0];
-      xb[r * 2 + 1] = hw[1];
-      xb[32 + r * 2] = lw[0];
-      xb[32 + r * 2 + 1] = lw[1];
     }
-    Prep16 pp;
-    pp.mu = mu;
-    pp.sxx = sxx;
-    pp.sxt = sxt;
-    pp.sxt_tc = stc;
-    pp.mmode = mbits == ~0ULL ? 1 : (mbits == 0 ? 2 : 0);
-    pp.pad[0] = pp.pad[1] = pp.pad[2] = 0;
-    a.prep[b] = pp;
+    const float mu = half_sum((v[0] + v[1]) + (v[2] + v[3])) * (1.0f / kB);
+    float sxx = 0.f, sxt = 0.f, stc = 0.f;
+    uint32_t hw[2] = {0u, 0u}, lw[2] = {0u, 0u};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float d = v[i] - mu;
+      if ((mbits >> i) & 1u) {
+        sxx = fmaf(d, d, sxx);
+        sxt += d;
+      }
+      const T h = S16<T>::t(d);
+      const T l = S16<T>::t(d - S16<T>::f(h));
+      stc += S16<T>::f(h) + S16<T>::f(l);
+      hw[i >> 1] |= S16<T>::bits(h) << (16 * (i & 1));
+      lw[i >> 1] |= S16<T>::bits(l) << (16 * (i & 1));
+    }
+    sxx = half_sum(sxx);
+    sxt = half_sum(sxt);
+    stc = half_sum(stc);
+    const unsigned full = __ballot_sync(0xffffffffu, mbits == 0xFu) & half_mask;
+    const unsigned none = __ballot_sync(0xffffffffu, mbits == 0u) & half_mask;
+    if (live) {
+      uint32_t *xb = a.xs + b * 64;
+      *reinterpret_cast<uint2 *>(xb + r * 2) = make_uint2(hw[0], hw[1]);
+      *reinterpret_cast<uint2 *>(xb + 32 + r * 2) = make_uint2(lw[0], lw[1]);
+      if (r == 0) {
+        Prep16 pp;
+        pp.mu = mu;
+        pp.sxx = sxx;
+        pp.sxt = sxt;
+        pp.sxt_tc = stc;
+        pp.mmode = full == half_mask ? 1 : (none == half_mask ? 2 : 0);
+        pp.pad[0] = pp.pad[1] = pp.pad[2] = 0;
+        a.prep[b] = pp;
+      }
+    }
   }
 }
 
@@ -480,44 +527,136 @@ __device__ __forceinline__ int call_of_tile(const Args16 *calls, int ncalls, lon
   return lo;
 }
 
+// Where tile `tile` lies: its call, first block column and block row.
+struct TilePos {
+  int ci, bx0, by, bz;
+};
+__device__ __forceinline__ TilePos tile_pos(const Args16 *calls, int ncalls, long long tile) {
+  TilePos p;
+  p.ci = call_of_tile(calls, ncalls, tile);
+  const Args16 &a = calls[p.ci];
+  const int lt = (int)(tile - a.tile0);  // tiles of one call < 2^31
+  const int tx = a.tiles_x, nby = a.nby;
+  const int r = lt / tx;
+  p.bx0 = (lt - r * tx) * a.bpt;
+  p.bz = r / nby;
+  p.by = r - p.bz * nby;
+  return p;
+}
+
+// Top two over a thread's or a block's candidates with a 32-bit raster key
+// (tile-local: (dz * 8 + py) * 8 + x shift; raster order of the candidates
+// of one block), same rule as Top2.
+struct Top2k {
+  float b1, b2;
+  int k1;
+};
+__device__ __forceinline__ void top2k_merge(Top2k &t, const Top2k &u) {
+  if (u.b1 > t.b1 || (u.b1 == t.b1 && u.k1 < t.k1)) {
+    t.b2 = fmaxf(t.b1, fmaxf(t.b2, u.b2));
+    t.b1 = u.b1;
+    t.k1 = u.k1;
+  } else {
+    t.b2 = fmaxf(t.b2, fmaxf(u.b1, u.b2));
+  }
+}
+__device__ __forceinline__ Top2k top2k_shfl_xor(const Top2k &t, int m) {
+  Top2k u;
+  u.b1 = __shfl_xor_sync(0xffffffffu, t.b1, m);
+  u.b2 = __shfl_xor_sync(0xffffffffu, t.b2, m);
+  u.k1 = __shfl_xor_sync(0xffffffffu, t.k1, m);
+  return u;
+}
+
 // ---------------------------------------------------------------------------
-// The tensor-core search.  Persistent CTAs of 8 warps, three per SM (while
-// one waits on memory or on its MMAs the others work).  Row m = 32 (w % 4) +
-// lane of A and D is (blk = m / 16, shift s = (m / 2) % 8, part = m % 2);
-// warps 0-3 write the A band of k-step 0 and read D columns 0-31 (dz 0-3),
-// warps 4-7 k-step 1 and columns 32-63.  A streams through two 32 KB buffers,
-// one vz (8 operands) at a time: the CUDA cores write the next vz's bands
-// while the tensor cores multiply the previous one.
+// The tensor-core search: a warp-specialised persistent kernel, one CTA of 16
+// warps per SM, the CTA's tiles taken round-robin (tile = CTA + k x grid).
+//
+//   warp 1, one thread (control): requests each tile's window box (TMA, a
+//     ring of kBoxSlots) and issues the tile's 32 MMAs into one of two
+//     accumulators in tensor memory (64 FP32 columns each);
+//   warps 4-7 (producers): thread m writes row m of A -- the bands of both
+//     k-steps -- into a ring of kASlots buffers of one vz each (8 operands);
+//   warps 8-15 (epilogue): warp 8 + 4 h + q reads lanes 32q.. and columns
+//     32h.. of a finished accumulator, scores the candidates and reduces the
+//     top two per block; one thread per block writes the block's record.
+//
+// Row m = (blk = m / 16, x shift s = (m / 2) % 8, part = m % 2) of A and D;
+// column n = (dz = n / 8, py = n % 8).  Every hand-off is an mbarrier:
+//   a_full[s]  producers (128 arrivals) -> control       A slot s written
+//   a_empty[s] control (tcgen05.commit) -> producers     its multiplies done
+//   b_full[s]  TMA (transaction bytes)  -> control       box s landed
+//   b_empty[s] control (commit)         -> control       box s read
+//   d_full[d]  control (commit)         -> epilogue      accumulator d done
+//   d_empty[d] epilogue (256 arrivals)  -> control       accumulator d read
+// A role derives what it needs from the tile index (the call, block
+// coordinates, the blocks' records), so nothing else passes between roles.
+// Every wait is bounded; a wait that gives up sets the call's flag and the
+// CTA's, each role leaves its loop, and the control thread lets its copies
+// and multiplies land (bounded) before tensor memory is released.
 // ---------------------------------------------------------------------------
+constexpr int kASlots = 4;     // A ring: one vz (8 operands, 32 KB) per slot
+constexpr int kBoxSlots = 3;   // window-box ring
+constexpr int kWsThreads = 512;
+
+struct TcBars {
+  uint64_t a_full[kASlots], a_empty[kASlots];
+  uint64_t b_full[kBoxSlots], b_empty[kBoxSlots];
+  uint64_t d_full[2], d_empty[2];
+};
+
+size_t tc_ws_smem_bytes() {
+  return (size_t)kASlots * kAChunkBytes + (size_t)kBoxSlots * ((kBoxBytes + 1023) / 1024 * 1024) + 1024;
+}
+
+// phase-parity wait on a use count: the k-th completion of a barrier (k = 0,
+// 1, ...) has parity k & 1
+__device__ __forceinline__ bool wait_use(uint64_t *bar, long long k) {
+  return mbar_wait(bar, (unsigned)(k & 1));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
 template <typename T, int W>
-__global__ void __launch_bounds__(kThreads, kCtasPerSM)
+__global__ void __launch_bounds__(kWsThreads, 1)
     ncc_tc_kernel(const Args16 *calls, int ncalls, long long total_tiles,
                   const __grid_constant__ TcMaps maps) {
   static_assert(W >= 2 && W <= 8, "window of the tensor form");
   constexpr int R = W / 2;
+  constexpr uint32_t kBoxStride = (kBoxBytes + 1023) / 1024 * 1024;
   extern __shared__ __align__(1024) uint8_t dsm[];
   uint8_t *const sbase = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(dsm) + 1023) & ~static_cast<uintptr_t>(1023));
-  uint8_t *const sa = sbase;                         // A: 2 buffers of one vz's 8 operands
-  uint8_t *const win = sbase + 2 * kAChunkBytes;      // B: the window box
-  __shared__ __align__(8) uint64_t s_tma_bar, s_mma_bar[2];
+  uint8_t *const sa = sbase;                              // A ring
+  uint8_t *const sbox = sbase + kASlots * kAChunkBytes;   // box ring
+  __shared__ __align__(8) TcBars bars;
   __shared__ uint32_t s_tmem;
-  __shared__ int s_any, s_fail;
-  __shared__ long long s_b[kTileBlocks];
-  __shared__ int s_elig[kTileBlocks];
-  __shared__ float s_sxx[kTileBlocks], s_stc[kTileBlocks];
-  __shared__ Top2 s_part[kTileBlocks];
-  __shared__ unsigned int s_cnt[kTileBlocks];
+  __shared__ volatile int s_fail;
+  __shared__ int s_ep_ok;
+  __shared__ Top2k s_part[2][kTileBlocks];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int q = warp & 3, half = warp >> 2;
-  const int m = 32 * q + lane;            // row of A and D (tensor-memory lane)
-  const int blk = m >> 4, sft = (m >> 1) & 7, part = m & 1;
-
   if (tid == 0) {
-    mbar_init(&s_tma_bar, 1);
-    mbar_init(&s_mma_bar[0], 1);
-    mbar_init(&s_mma_bar[1], 1);
+    for (int i = 0; i < kASlots; ++i) {
+      mbar_init(&bars.a_full[i], 128);
+      mbar_init(&bars.a_empty[i], 1);
+    }
+    for (int i = 0; i < kBoxSlots; ++i) {
+      mbar_init(&bars.b_full[i], 1);
+      mbar_init(&bars.b_empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&bars.d_full[i], 1);
+      mbar_init(&bars.d_empty[i], 256);
+    }
     s_fail = 0;
   }
   if (warp == 0) {
@@ -528,105 +667,152 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
   // A starts as zeros; each row later rewrites only the words of its band
-  for (int i = tid; i < 2 * kAChunkBytes / 16; i += kThreads)
+  for (int i = tid; i < kASlots * kAChunkBytes / 16; i += kWsThreads)
     reinterpret_cast<uint4 *>(sa)[i] = make_uint4(0u, 0u, 0u, 0u);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16);
-  // this row's band in k-step `half`: element t0 of the step holds x~[0]
-  // (words floor(t0 / 2) ..; an odd t0 straddles the 16-bit halves)
-  int t0 = 0;
-  // byte offset of 32-bit word c of this row in step r: r * 4 KB + row_off + c_off(c)
-  const uint32_t row_off = (uint32_t)(m >> 3) * kASBO + (uint32_t)(m & 7) * 16u;
+  const long long first = blockIdx.x, step = gridDim.x;
+  const long long ntile = first < total_tiles ? (total_tiles - first + step - 1) / step : 0;
 
-  unsigned tma_phase = 0, mma_phase[2] = {0u, 0u};
-  int cur_call = -1;
-  Args16 a;
-  for (long long tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-    const int ci = call_of_tile(calls, ncalls, tile);
-    if (ci != cur_call) {
-      a = calls[ci];
-      cur_call = ci;
-      t0 = a.G * blk + sft - 16 * half;
-    }
-    const long long lt = tile - a.tile0;
-    const int bxg = (int)(lt % a.tiles_x);
-    const int bx0 = bxg * a.bpt;
-    const long long rest = lt / a.tiles_x;
-    const int by = (int)(rest % a.nby), bz = (int)(rest / a.nby);
-    const int oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
-    if (tid < kTileBlocks) {
-      const int bx = bx0 + tid;
-      int e = 0;
-      long long b = -1;
-      if (tid < a.bpt && bx < a.nbx) {
-        b = ((long long)bz * a.nby + by) * a.nbx + bx;
-        const int ox = a.stx + bx * a.G;
-        const long long orig = ((long long)oz * a.ny + oy) * a.nx + ox;
-        const bool sel = !a.selected || a.selected[b];
-        const Prep16 pp = a.prep[b];
-        if (!sel) {
-          write_out(a, b, -3.f, -3.f, orig, 0);
-        } else if (pp.mmode == 1 && wand_of(a)[b] && pp.sxx > 0.f) {
-          e = 1;
-          s_sxx[tid] = pp.sxx;
-          s_stc[tid] = pp.sxt_tc;
-        } else {
-          const unsigned int k = atomicAdd(&a.ctl[1], 1u);
-          a.fb_list[k] = (int)b;
-        }
-      }
-      s_b[tid] = b;
-      s_elig[tid] = e;
-      s_cnt[tid] = 0u;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      int any = 0;
-      for (int j = 0; j < kTileBlocks; ++j) any |= s_elig[j];
-      s_any = any;
-    }
-    __syncthreads();
-    if (!s_any) continue;
-    if (tid == 0) {
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
-                       smem_u32(&s_tma_bar)),
-                   "r"((unsigned)kBoxBytes)
-                   : "memory");
-      tma_load_4d(win, &maps.m[ci], 0, oy - R, oz - R, (a.G * bx0) >> 3, &s_tma_bar);
-    }
-    // ---- the block's two 16-bit parts for every (vz, vy), in registers ------
-    const bool band = t0 < 16 && t0 + 4 > 0;
-    const bool live = band && s_elig[blk] != 0;
-    uint2 xw[16];
-    {
-      const uint32_t *xr = a.xs + (live ? s_b[blk] : 0) * 64 + part * 32;
-#pragma unroll
-      for (int r = 0; r < 16; ++r)
-        xw[r] = live ? *reinterpret_cast<const uint2 *>(xr + 2 * r) : make_uint2(0u, 0u);
-    }
-    const int c0 = t0 >= 0 ? (t0 >> 1) : -((1 - t0) >> 1);  // floor(t0 / 2)
-    const bool odd = t0 & 1;
+  if (warp == 1) {
+   if (lane == 0) {
+    // ======================= control: boxes and multiplies ===================
     constexpr uint32_t idesc = (1u << 4) | (S16<T>::kFmt << 7) | (S16<T>::kFmt << 10) |
                                ((uint32_t)(64 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-    // ---- per vz: write the A operands of buffer vz % 2, multiply --------------
-    for (int vz = 0; vz < 4; ++vz) {
-      const int buf = vz & 1;
-      if (vz >= 2) {
-        // the multiplies of vz - 2 read this buffer: one thread waits for
-        // them, the others at the CTA barrier (no issue slots spent polling)
-        if (tid == 0 && !mbar_wait(&s_mma_bar[buf], mma_phase[buf], 1 << 24)) {
-          atomicExch(&a.ctl[2], 1u);
-          s_fail = 1;
+    long long requested = 0;  // boxes requested (tiles 0 .. requested-1 of this CTA)
+    auto request = [&](long long j) {
+      const long long tile = first + j * step;
+      const TilePos p = tile_pos(calls, ncalls, tile);
+      const Args16 &c = calls[p.ci];
+      const int s = (int)(j % kBoxSlots);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                       smem_u32(&bars.b_full[s])),
+                   "r"((unsigned)kBoxBytes)
+                   : "memory");
+      tma_load_4d(sbox + s * kBoxStride, &maps.m[p.ci], 0, c.sty + p.by * c.G - R,
+                  c.stz + p.bz * c.G - R, (c.G * p.bx0) >> 3, &bars.b_full[s]);
+    };
+    long long j = 0;
+    int fail_ci = 0;
+    bool ok = true;
+    if (ntile > 0) {
+      request(0);
+      requested = 1;
+    }
+    for (; j < ntile && ok; ++j) {
+      const long long tile = first + j * step;
+      fail_ci = call_of_tile(calls, ncalls, tile);
+      // the next tile's box: its slot was last read by tile j + 1 - kBoxSlots
+      if (j + 1 < ntile) {
+        const long long jp = j + 1 - kBoxSlots;
+        if (jp >= 0 && !wait_use(&bars.b_empty[(j + 1) % kBoxSlots], jp / kBoxSlots)) {
+          ok = false;
+          break;
         }
-        mma_phase[buf] ^= 1u;
-        __syncthreads();
-        if (s_fail) break;
+        request(j + 1);
+        requested = j + 2;
       }
-      if (band) {
-        uint8_t *const cb = sa + (size_t)buf * kAChunkBytes + row_off;
+      const int bs = (int)(j % kBoxSlots), dacc = (int)(j & 1);
+      if (!wait_use(&bars.b_full[bs], j / kBoxSlots)) { ok = false; break; }
+      if (j >= 2 && !wait_use(&bars.d_empty[dacc], (j - 2) / 2)) { ok = false; break; }
+      tc_fence_after();
+      const uint32_t wb = smem_u32(sbox + bs * kBoxStride);
+      const uint32_t dst = tmem + (uint32_t)dacc * 64u;
+      for (int vz = 0; vz < 4 && ok; ++vz) {
+        const long long g = j * 4 + vz;
+        const int as = (int)(g % kASlots);
+        if (!wait_use(&bars.a_full[as], g / kASlots)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t ab = smem_u32(sa) + (uint32_t)as * kAChunkBytes;
+#pragma unroll
+        for (int jj = 0; jj < kAChunkSteps; ++jj) {
+          const int vy = jj >> 1, ks = jj & 1;
+          const uint64_t ad = sdesc(ab + (uint32_t)jj * kAStepBytes, kALBO, kASBO);
+          const uint64_t bd =
+              sdesc(wb + (uint32_t)(2 * ks) * kLBO + (uint32_t)vz * kSBO + (uint32_t)vy * 16u, kLBO, kSBO);
+          const int acc = (vz | jj) != 0;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dst),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
+        tc_commit(&bars.a_empty[as]);
+      }
+      if (!ok) break;
+      tc_commit(&bars.b_empty[bs]);
+      tc_commit(&bars.d_full[dacc]);
+    }
+    if (!ok) {
+      atomicExch(&calls[fail_ci].ctl[2], 1u);
+      s_fail = 1;
+      // let requested boxes land (bounded) ...
+      for (long long k = j; k < requested; ++k) wait_use(&bars.b_full[k % kBoxSlots], k / kBoxSlots);
+      // ... and every issued multiply finish: a commit on tile j's
+      // accumulator barrier tracks all of them (the epilogue sees s_fail)
+      if (j < ntile) {
+        tc_commit(&bars.d_full[j & 1]);
+        wait_use(&bars.d_full[j & 1], j / 2);
+      }
+    } else if (j > 0) {
+      wait_use(&bars.d_full[(j - 1) & 1], (j - 1) / 2);
+    }
+   }
+    __syncwarp();  // the warp leaves the role converged
+  } else if (warp >= 4 && warp < 8) {
+    // ======================= producers: the A bands ==========================
+    const int m = tid - 128;  // row of A
+    const int blk = m >> 4, sft = (m >> 1) & 7, part = m & 1;
+    const uint32_t row_off = (uint32_t)(m >> 3) * kASBO + (uint32_t)(m & 7) * 16u;
+    int band_call = -1;
+    uint32_t off[2][3] = {{0u, 0u, 0u}, {0u, 0u, 0u}};
+    unsigned msk[2] = {0u, 0u};
+    bool odd = false;
+    for (long long j = 0; j < ntile; ++j) {
+      if (s_fail) break;
+      const long long tile = first + j * step;
+      const TilePos p = tile_pos(calls, ncalls, tile);
+      const Args16 &a = calls[p.ci];
+      if (p.ci != band_call) {
+        band_call = p.ci;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int t0 = a.G * blk + sft - 16 * h;
+          const bool band = t0 < 16 && t0 + 4 > 0;
+          odd = t0 & 1;  // the same for both halves
+          const int c0 = t0 >= 0 ? (t0 >> 1) : -((1 - t0) >> 1);  // floor(t0 / 2)
+          msk[h] = 0u;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int c = c0 + k;
+            const bool on = band && c >= 0 && c < 8 && (k < 2 || odd);
+            off[h][k] = on ? (uint32_t)(h * kAStepBytes + (c >> 2) * kALBO + (c & 3) * 4) : 0u;
+            msk[h] |= (on ? 1u : 0u) << k;
+          }
+        }
+      }
+      const int bx = p.bx0 + blk;
+      const bool live = blk < a.bpt && bx < a.nbx;
+      uint2 xw[16];
+      {
+        const long long b = live ? ((long long)p.bz * a.nby + p.by) * a.nbx + bx : 0;
+        const uint32_t *xr = a.xs + b * 64 + part * 32;
+#pragma unroll
+        for (int r = 0; r < 16; ++r)
+          xw[r] = live ? *reinterpret_cast<const uint2 *>(xr + 2 * r) : make_uint2(0u, 0u);
+      }
+      bool ok = true;
+#pragma unroll
+      for (int vz = 0; vz < 4; ++vz) {
+        const long long g = j * 4 + vz;
+        const int as = (int)(g % kASlots);
+        if (g >= kASlots && !wait_use(&bars.a_empty[as], g / kASlots - 1)) {
+          ok = false;
+          break;
+        }
+        uint8_t *const cb = sa + (size_t)as * kAChunkBytes + row_off;
 #pragma unroll
         for (int vy = 0; vy < 4; ++vy) {
           const uint2 w2 = xw[vz * 4 + vy];
@@ -640,125 +826,170 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSM)
             wv[1] = w2.y;
             wv[2] = 0u;
           }
-          uint8_t *const step = cb + (size_t)(2 * vy + half) * kAStepBytes;
+          uint8_t *const stp = cb + (size_t)(2 * vy) * kAStepBytes;
 #pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const int c = c0 + k;
-            if (c >= 0 && c < 8 && (k < 2 || odd))
-              *reinterpret_cast<uint32_t *>(step + (c >> 2) * kALBO + (c & 3) * 4) = wv[k];
-          }
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+              if ((msk[h] >> k) & 1u) *reinterpret_cast<uint32_t *>(stp + off[h][k]) = wv[k];
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_arrive(&bars.a_full[as]);
+      }
+      if (!ok) {
+        s_fail = 1;
+        break;
+      }
+    }
+    __syncwarp();
+  } else if (warp >= 8) {
+    // ======================= epilogue: scores and top two ====================
+    const int et = tid - 256;  // 0..255
+    const int q = warp & 3, half = (warp - 8) >> 2;
+    const int m = 32 * q + lane;
+    const int blk = m >> 4, sft = (m >> 1) & 7, part = m & 1;
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16);
+    const bool finisher = half == 0 && (lane & 15) == 0;
+    int cnt_call = -1;
+    unsigned int cnt_blocks = 0;
+    unsigned long long cnt_cands = 0;
+    for (long long j = 0; j < ntile; ++j) {
+      const long long tile = first + j * step;
+      const TilePos p = tile_pos(calls, ncalls, tile);
+      const Args16 &a = calls[p.ci];
+      const int oy = a.sty + p.by * a.G, oz = a.stz + p.bz * a.G;
+      const int bx = p.bx0 + blk;
+      const int ox = a.stx + bx * a.G;
+      // this row's block: its record, read before the accumulator is ready
+      long long b = -1;
+      int elig = 0, sel = 0;
+      float sxx = 0.f, stc = 0.f;
+      if (blk < a.bpt && bx < a.nbx) {
+        b = ((long long)p.bz * a.nby + p.by) * a.nbx + bx;
+        sel = !a.selected || a.selected[b];
+        const Prep16 pp = a.prep[b];
+        elig = sel && pp.mmode == 1 && wand_of(a)[b] && pp.sxx > 0.f;
+        sxx = pp.sxx;
+        stc = pp.sxt_tc;
+      }
+      // the accumulator: one thread waits, the epilogue warps agree
+      const int dacc = (int)(j & 1);
+      if (et == 0) s_ep_ok = wait_use(&bars.d_full[dacc], j / 2) && !s_fail;
+      __syncwarp();
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      if (!s_ep_ok) {
+        if (et == 0) s_fail = 1;
+        break;
+      }
+      tc_fence_after();
+      float v[16];
+      const uint32_t dcol = lane_addr + (uint32_t)dacc * 64u + (uint32_t)(32 * half);
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        uint32_t d[16];
+        tmem_ld16(dcol + 16u * hh, d);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          const float o = __shfl_xor_sync(0xffffffffu, __uint_as_float(d[jj]), 1);
+          if (part == hh) v[jj] = __uint_as_float(d[jj]) + o;
         }
       }
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       tc_fence_before();
-      __syncthreads();
-      if (tid == 0 && !s_fail) {
-        tc_fence_after();
-        if (vz == 0 && !mbar_wait(&s_tma_bar, tma_phase, 1 << 22)) {
-          s_fail = 1;
-          atomicExch(&a.ctl[2], 1u);
+      mbar_arrive(&bars.d_empty[dacc]);
+      // this thread's candidates: x shift sft, planes dz0 (jj < 8) and dz0 + 1
+      // (jj >= 8), rows py = jj % 8; jj order is their raster order
+      Top2k t2;
+      t2.b1 = -3.f;
+      t2.b2 = -3.f;
+      t2.k1 = 0x7fffffff;
+      const int nx = a.nx, ny = a.ny, nz = a.nz;
+      const int dz0 = 4 * half + 2 * part;
+      if (elig && sft < W) {
+        int xlo, xhi, ylo, yhi, zlo, zhi;
+        cand_range(ox, nx, W, xlo, xhi);
+        cand_range(oy, ny, W, ylo, yhi);
+        cand_range(oz, nz, W, zlo, zhi);
+        const int cx = ox - R + sft;
+        if (cx >= xlo && cx <= xhi) {
+          // valid rows py in [pylo, pyhi] (never empty: the block's own row is
+          // one), planes dz0 + h valid when zok[h]; an invalid candidate
+          // loads a valid position's statistics (clamped row and plane) and
+          // is scored -FLT_MAX, so the loop has no branches
+          const int pylo = max(ylo - (oy - R), 0), pyhi = min(yhi - (oy - R), W - 1);
+          const int cz0 = oz - R + dz0;
+          const bool zok0 = dz0 < W && cz0 >= zlo && cz0 <= zhi;
+          const bool zok1 = dz0 + 1 < W && cz0 + 1 >= zlo && cz0 + 1 <= zhi;
+          const unsigned rows = ((2u << pyhi) - 1u) & ~((1u << pylo) - 1u);
+          const unsigned vmask = (zok0 ? rows : 0u) | (zok1 ? rows << 8 : 0u);
+          const long long row0 = (long long)(oy - R) * nx + cx;
+          const long long i0 = (long long)(zok0 ? cz0 : zlo) * ((long long)nx * ny) + row0;
+          const long long i1 = (long long)(zok1 ? cz0 + 1 : zlo) * ((long long)nx * ny) + row0;
+          int offr[8];
+#pragma unroll
+          for (int py = 0; py < 8; ++py) offr[py] = min(max(py, pylo), pyhi) * nx;
+          int kbest = -1;
+          float b1 = -3.f, b2 = -3.f;
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) {
+            const float2 st = __ldg(a.stats + ((jj < 8 ? i0 : i1) + offr[jj & 7]));
+            const float sxy = fmaf(-st.x, stc, v[jj]);
+            float sc = st.y > 0.f ? __fdividef(sxy * sxy, sxx * st.y) : -2.f;
+            sc = ((vmask >> jj) & 1u) ? sc : -FLT_MAX;
+            const bool gt = sc > b1;
+            b2 = gt ? b1 : fmaxf(b2, sc);
+            b1 = gt ? sc : b1;
+            kbest = gt ? jj : kbest;
+          }
+          if (kbest >= 0) {
+            t2.b1 = b1;
+            t2.b2 = b2;
+            t2.k1 = ((dz0 + (kbest >> 3)) * 8 + (kbest & 7)) * 8 + sft;
+          }
+        }
+      }
+      // reduce over the 16 lanes of the block (8 shifts x 2 parts) ...
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) top2k_merge(t2, top2k_shfl_xor(t2, o));
+      // ... then over the two halves of the candidate planes
+      if (half == 1 && (lane & 15) == 0) s_part[j & 1][blk] = t2;
+      __syncwarp();
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      if (finisher && b >= 0) {
+        if (!sel) {
+          write_out(a, b, -3.f, -3.f, ((long long)oz * ny + oy) * nx + ox, 0);
+        } else if (!elig) {
+          const unsigned int k = atomicAdd(&a.ctl[1], 1u);
+          a.fb_list[k] = (int)b;
         } else {
-          const uint32_t wb = smem_u32(win), ab = smem_u32(sa) + (uint32_t)buf * kAChunkBytes;
-#pragma unroll 1
-          for (int j = 0; j < kAChunkSteps; ++j) {
-            const int vy = j >> 1, ks = j & 1;
-            const uint64_t ad = sdesc(ab + (uint32_t)j * kAStepBytes, kALBO, kASBO);
-            const uint64_t bd = sdesc(wb + (uint32_t)(2 * ks) * kLBO + (uint32_t)vz * kSBO +
-                                          (uint32_t)vy * 16u,
-                                      kLBO, kSBO);
-            const int acc = (vz | j) != 0;
-            asm volatile(
-                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                : "memory");
+          top2k_merge(t2, s_part[j & 1][blk]);
+          const int k = t2.k1;
+          const long long idx =
+              ((long long)(oz - R + (k >> 6)) * ny + (oy - R + ((k >> 3) & 7))) * nx + (ox - R + (k & 7));
+          write_out(a, b, t2.b1, t2.b2, idx, 1);
+          if (p.ci != cnt_call) {
+            if (cnt_call >= 0) {
+              atomicAdd(&calls[cnt_call].ctl[0], cnt_blocks);
+              if (calls[cnt_call].ncc_count) atomicAdd(calls[cnt_call].ncc_count, cnt_cands);
+            }
+            cnt_call = p.ci;
+            cnt_blocks = 0;
+            cnt_cands = 0;
           }
-          asm volatile(
-              "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                  smem_u32(&s_mma_bar[buf]))
-              : "memory");
-        }
-      }
-      __syncthreads();
-      if (s_fail) break;  // every thread sees the same flag
-    }
-    if (s_fail) break;
-    tma_phase ^= 1u;
-    // ---- epilogue: the last two commits (vz 2 and 3) ------------------------
-    if (tid == 0) {
-#pragma unroll
-      for (int bb = 0; bb < 2; ++bb)
-        if (!mbar_wait(&s_mma_bar[bb], mma_phase[bb], 1 << 24)) {
-          atomicExch(&a.ctl[2], 1u);
-          s_fail = 1;
-        }
-    }
-    mma_phase[0] ^= 1u;
-    mma_phase[1] ^= 1u;
-    __syncthreads();
-    if (s_fail) break;
-    tc_fence_after();
-    uint32_t d[32];
-    tmem_ld32(lane_addr + (uint32_t)(32 * half), d);
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    // add the two parts: part 0 keeps columns 0-15 of this half, part 1 16-31
-    float v[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const float mine = __uint_as_float(part ? d[16 + j] : d[j]);
-      const float send = __uint_as_float(part ? d[j] : d[16 + j]);
-      v[j] = mine + __shfl_xor_sync(0xffffffffu, send, 1);
-    }
-    Top2 tp;
-    tp.b1 = -3.f;
-    tp.b2 = -3.f;
-    tp.i1 = 0x7fffffffffffffffLL;
-    unsigned int cnt = 0;
-    if (s_elig[blk] && sft < W) {
-      const int ox = a.stx + (bx0 + blk) * a.G;
-      const int cx = ox - R + sft;
-      int xlo, xhi, ylo, yhi, zlo, zhi;
-      cand_range(ox, a.nx, W, xlo, xhi);
-      cand_range(oy, a.ny, W, ylo, yhi);
-      cand_range(oz, a.nz, W, zlo, zhi);
-      const float sxx = s_sxx[blk], stc = s_stc[blk];
-      if (cx >= xlo && cx <= xhi) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int dz = 4 * half + 2 * part + (j >> 3), py = j & 7;
-          const int cy = oy - R + py, cz = oz - R + dz;
-          if (py < W && dz < W && cy >= ylo && cy <= yhi && cz >= zlo && cz <= zhi) {
-            const long long idx = ((long long)cz * a.ny + cy) * a.nx + cx;
-            const float2 st = __ldg(a.stats + idx);
-            const float sxy = v[j] - st.x * stc;
-            const float syy = st.y;
-            const float sc = syy > 0.f ? __fdividef(sxy * sxy, sxx * syy) : -2.f;
-            top2_add(tp, sc, idx);
-            ++cnt;
-          }
+          int xlo, xhi, ylo, yhi, zlo, zhi;
+          cand_range(ox, nx, W, xlo, xhi);
+          cand_range(oy, ny, W, ylo, yhi);
+          cand_range(oz, nz, W, zlo, zhi);
+          ++cnt_blocks;
+          cnt_cands += (unsigned long long)(xhi - xlo + 1) * (yhi - ylo + 1) * (zhi - zlo + 1);
         }
       }
     }
-    // reduce over the 16 lanes of the block (8 shifts x 2 parts) ...
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) top2_merge(tp, top2_shfl_xor(tp, o));
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    // ... then over the two halves of the candidate planes
-    if (half == 1 && (lane & 15) == 0) {
-      s_part[blk] = tp;
-      s_cnt[blk] = cnt;
+    if (finisher && cnt_call >= 0 && cnt_blocks) {
+      atomicAdd(&calls[cnt_call].ctl[0], cnt_blocks);
+      if (calls[cnt_call].ncc_count) atomicAdd(calls[cnt_call].ncc_count, cnt_cands);
     }
-    tc_fence_before();
-    __syncthreads();
-    if (half == 0 && (lane & 15) == 0 && s_elig[blk]) {
-      top2_merge(tp, s_part[blk]);
-      cnt += s_cnt[blk];
-      write_out(a, s_b[blk], tp.b1, tp.b2, tp.i1, 1);
-      atomicAdd(&a.ctl[0], 1u);
-      if (a.ncc_count) atomicAdd(a.ncc_count, (unsigned long long)cnt);
-    }
-    if (s_fail) break;
+    __syncwarp();
   }
   tc_fence_before();
   __syncthreads();
@@ -891,7 +1122,6 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-size_t tc_smem_bytes() { return (size_t)2 * kAChunkBytes + kBoxBytes + 1024; }
 
 }  // namespace
 
@@ -939,7 +1169,8 @@ size_t match16_wand_bytes(const Match16Call &c) {
 namespace {
 
 template <typename T>
-mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cudaStream_t s) {
+mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cudaStream_t s,
+                    bool every_stage) {
   const int SM = sm_count();
   const long long tiles = match16_number_tiles(host_calls, ncalls);
   long long max_vox = 0, max_blocks = 0, max_chunks = 0;
@@ -970,7 +1201,20 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
     if (b > (long long)SM * 4) b = (long long)SM * 4;
     return dim3((unsigned)(b < 1 ? 1 : b), (unsigned)ncalls);
   };
-  box_stats16_kernel<T><<<grid_for(max_vox / 4 + 1), 256, 0, s>>>(dc);
+  {
+    long long st_tiles = 0;
+    for (int i = 0; i < ncalls; ++i) {
+      const Match16Call &c = host_calls[i];
+      if (!c.active) continue;
+      const long long vx = c.nx - kBW + 1, vy = c.ny - kBW + 1, vz = c.nz - kBW + 1;
+      if (vx > 0 && vy > 0 && vz > 0)
+        st_tiles = std::max(st_tiles, ((vx + kStX - 1) / kStX) * ((vy + kStY - 1) / kStY) *
+                                          ((vz + kStZ - 1) / kStZ));
+    }
+    long long gx = std::min(st_tiles, (long long)SM * 8);
+    if (gx < 1) gx = 1;
+    box_stats16_kernel<T><<<dim3((unsigned)gx, (unsigned)ncalls), 256, 0, s>>>(dc);
+  }
   MB2_LAUNCH_CHECK();
   wand_x16_kernel<<<grid_for(max_vox / 2 + 1), 256, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
@@ -978,15 +1222,15 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
   MB2_LAUNCH_CHECK();
   wand_z16_kernel<<<grid_for(max_blocks), 256, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
-  prep16_kernel<T><<<grid_for(max_blocks), 256, 0, s>>>(dc);
+  prep16_kernel<T><<<grid_for(max_blocks * 16), 256, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
-  if (any_tensor) {
+  if (any_tensor || every_stage) {
     chunk16_kernel<T><<<grid_for(max_chunks), 256, 0, s>>>(dc);
     MB2_LAUNCH_CHECK();
   }
   route_all16_kernel<<<grid_for(max_blocks), 256, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
-  if (any_tensor) {
+  if (any_tensor || every_stage) {
     if (ncalls > kMaxCalls) {
       set_error("more than %d matcher calls in one tensor launch", kMaxCalls);
       return MIRORR_EINVAL;
@@ -1018,13 +1262,16 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
         return MIRORR_ECUDA;
       }
     }
-    const size_t smem = tc_smem_bytes();
+    const size_t smem = tc_ws_smem_bytes();
     auto kern = (W == 7) ? ncc_tc_kernel<T, 7> : (W == 5) ? ncc_tc_kernel<T, 5>
                                                           : ncc_tc_kernel<T, 3>;
     MB2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long long grid = tiles < (long long)SM * kCtasPerSM ? tiles : (long long)SM * kCtasPerSM;
+    long long grid = tiles < (long long)SM ? tiles : (long long)SM;
+    // with every stage launched (a graph of fixed shape), a launch without
+    // tensor tiles is one CTA that finds no tile
+    if (grid < 1 && every_stage) grid = 1;
     if (grid > 0) {
-      kern<<<(unsigned)grid, kThreads, smem, s>>>(dc, ncalls, tiles, maps);
+      kern<<<(unsigned)grid, kWsThreads, smem, s>>>(dc, ncalls, tiles, maps);
       MB2_LAUNCH_CHECK();
     }
   }
@@ -1036,10 +1283,11 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
 }  // namespace
 
 mirorr_status launch_match16_batch(int dtype, int ncalls, Match16Call *host_calls,
-                                   DevBuf &calls_dev, cudaStream_t s) {
+                                   DevBuf &calls_dev, cudaStream_t s, bool every_stage) {
   if (ncalls <= 0) return MIRORR_OK;
-  if (dtype == MIRORR_DTYPE_BF16) return run16<__nv_bfloat16>(ncalls, host_calls, calls_dev, s);
-  if (dtype == MIRORR_DTYPE_F16) return run16<__half>(ncalls, host_calls, calls_dev, s);
+  if (dtype == MIRORR_DTYPE_BF16)
+    return run16<__nv_bfloat16>(ncalls, host_calls, calls_dev, s, every_stage);
+  if (dtype == MIRORR_DTYPE_F16) return run16<__half>(ncalls, host_calls, calls_dev, s, every_stage);
   set_error("storage type %d is not a 16-bit type", dtype);
   return MIRORR_EINVAL;
 }
