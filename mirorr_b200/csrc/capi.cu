@@ -1786,7 +1786,9 @@ size_t slot_bytes(const mirorr_geometry &fg, const mirorr_geometry &mg, const mi
   size_t b = es * (nf + nm) + (fm ? nf : 0) + (mm ? nm : 0);  // inputs
   b += 4 * (nf + nm);                                          // float32 levels
   b += 2 * es * V + 2 * V;                                     // middle-space images, masks
-  b += ncall * (8 * V + 3 * V / 2 + (32 + 256 + 4 + 13) * NB + 2 * V + 64 * 1024);
+  // statistics with even-pitch rows (<= 8 V (1 + 1 / nx), nx >= 4), window-AND,
+  // x-chunked copy, per-block records
+  b += ncall * (10 * V + 3 * V / 2 + (32 + 256 + 4 + 13) * NB + 2 * V + 64 * 1024);
   b += 2 * 3 * 8 * ncall * NB;                                 // point pairs
   b += lts_fit_scratch_bytes((long long)(ncall * NB), kLtsCtas);
   return b;
@@ -1959,7 +1961,7 @@ mirorr_status batch_check_slot(mirorr_ctx c, const BatchSlot &s) {
     memset(&mc, 0, sizeof(mc));
     prepare16(s.g, mc);
     const BatchCallBufs &cb = s.call[k];
-    ok = need(cb.stats, sizeof(float2) * nvox, "stats") &&
+    ok = need(cb.stats, match16_stats_bytes(mc), "stats") &&
          need(cb.wand, match16_wand_bytes(mc), "wand") &&
          need(cb.prep, sizeof(Prep16) * nb, "prep") && need(cb.xs, 256 * (size_t)nb, "xs") &&
          need(cb.fb, sizeof(int) * nb, "fb") && need(cb.best, sizeof(float) * nb, "best") &&
@@ -2157,9 +2159,10 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
   if (nc == 0) return MIRORR_OK;
   for (int si = 0; si < S; ++si)
     if (b->slots[si].state == 1) MB2_TRY(batch_check_slot(c, b->slots[si]));
-  // the tile numbering the tensor launch reads from the call descriptors (a
-  // replay copies them from h_calls as written here)
+  // the tile numbering and copy descriptors the tensor launch reads from the
+  // call descriptors (a replay copies them from h_calls as written here)
   match16_number_tiles(calls, nc);
+  MB2_TRY(match16_prepare_copies(b->storage, calls, nc));
   // ---- launches ---------------------------------------------------------------
   // Replayed from the graph when the set of requests and levels is unchanged.
   // Otherwise the round is captured again; as every round launches the same
@@ -2385,7 +2388,7 @@ mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, con
   else if (pp.last_level < 0) nl = std::max(1, nl + pp.last_level);
   // the largest level's middle space and block grid size the buffers
   long long max_vox = 0, max_blocks = 0;
-  size_t chunk_b = 0, wand_b = 0;
+  size_t chunk_b = 0, wand_b = 0, stats_b = 0;
   for (int l = 0; l < nl; ++l) {
     mirorr_geometry lf, lm;
     level_geometry(*fg, sched_f[l], lf);
@@ -2405,6 +2408,7 @@ mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, con
     max_blocks = std::max(max_blocks, g.nblocks);
     chunk_b = std::max(chunk_b, match16_chunk_bytes(mc));
     wand_b = std::max(wand_b, match16_wand_bytes(mc));
+    stats_b = std::max(stats_b, match16_stats_bytes(mc));
   }
   const size_t need = slot_bytes(*fg, *mg, pp, fmask != nullptr, mmask != nullptr, max_vox, max_blocks);
   if (need > b->budget) {
@@ -2443,7 +2447,7 @@ mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, con
   E(s.msk_s, max_vox);
   for (int k = 0; k < ncall; ++k) {
     BatchCallBufs &cb = s.call[k];
-    E(cb.stats, sizeof(float2) * max_vox);
+    E(cb.stats, stats_b);
     E(cb.wand, wand_b);
     E(cb.prep, sizeof(Prep16) * max_blocks);
     E(cb.xs, sizeof(uint32_t) * 64 * max_blocks);

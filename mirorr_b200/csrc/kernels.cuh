@@ -89,18 +89,25 @@ struct Prep16 {
   float sxt;     // sum over base-mask voxels of x~
   float sxt_tc;  // sum over every voxel of the two 16-bit parts of x~
   int mmode;     // 1: base mask on everywhere, 2: off everywhere, 0: mixed
-  int pad[3];
+  int route;     // 1: the tensor-core search takes the block (else the direct
+                 // search's list holds it, or the selection culled it)
+  int pad[2];
 };
 
 // One matcher call of the 16-bit search: inputs, per-call buffers, outputs
-// (filled by the caller) and the geometry and tile layout (prepare16).
-struct Match16Call {
+// (filled by the caller) and the geometry and tile layout (prepare16); the
+// two tensor-copy descriptors are written by match16_prepare_copies.
+struct alignas(64) Match16Call {
+  // tensor-copy descriptors (CUtensorMap, 128 bytes each): [0] the window box
+  // from the x-chunked copy, [1] the box of the search statistics
+  alignas(64) unsigned char tmap[2][128];
   const void *base;
   const uint8_t *bmask;
   const void *search;
   const uint8_t *smask;
   const uint8_t *selected;
-  float2 *stats;          // nvox: (mu_y, Syy), Syy sign bit = footprint leaves the mask
+  float2 *stats;          // match16_stats_bytes, rows of pitch sp: (mu_y, Syy), Syy sign
+                          // bit = footprint leaves the mask
   uint8_t *wand;          // match16_wand_bytes: window-AND passes and per-block flags
   Prep16 *prep;           // nblocks
   uint32_t *xs;           // nblocks x 64 words: the 16-bit parts of the centred base block
@@ -114,6 +121,7 @@ struct Match16Call {
                           // [1] direct blocks, [2] a bounded wait gave up
   int *fb_list;           // nblocks
   int nx, ny, nz;
+  int sp;                 // row pitch of stats (nx rounded up to even: 16-byte rows)
   int nbx, nby, nbz;
   int stx, sty, stz;
   int G, W;
@@ -130,6 +138,12 @@ struct Match16Call {
 void prepare16(const BmGeom &g, Match16Call &c);
 size_t match16_chunk_bytes(const Match16Call &c);
 size_t match16_wand_bytes(const Match16Call &c);
+size_t match16_stats_bytes(const Match16Call &c);
+// Writes the tensor-copy descriptors of calls[0, n) (dtype: the storage
+// type) from their buffers and geometry.  A replayed graph reads the
+// descriptors from the host array at replay, so the caller writes them again
+// before every replay (with the tile numbering).
+mirorr_status match16_prepare_copies(int dtype, Match16Call *calls, int n);
 // Numbers the tensor tiles of calls[0, n) in order (sets each call's tile0)
 // and returns their total.  A replayed graph of launch_match16_batch reads the
 // descriptors from the host array at replay, so the caller numbers them again

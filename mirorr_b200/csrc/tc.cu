@@ -89,7 +89,6 @@ constexpr int kAChunkBytes = kAChunkSteps * kAStepBytes;
 constexpr uint32_t kALBO = 16 * 128;       // next k chunk of A
 constexpr uint32_t kASBO = 128;            // next 8 rows of A
 constexpr int kTmemCols = 128;  // D: two accumulators of 64 FP32 columns (tiles alternate)
-constexpr int kMaxCalls = 128;  // tensor maps of one launch (kernel parameter space)
 
 
 
@@ -132,7 +131,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int li
   return false;
 }
 
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *map, int c0, int c1, int c2,
                                             int c3, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
@@ -223,22 +222,22 @@ __device__ __forceinline__ void cand_range(int o, int S, int W, int &lo, int &hi
 // each thread sums 4 of those along y and keeps the last four planes' sums in
 // registers for the z sum.  grid.y = call; grid.x strides over the tiles.
 // ---------------------------------------------------------------------------
-constexpr int kStX = 32, kStY = 8, kStZ = 16;
+constexpr int kBsX = 32, kBsY = 8, kBsZ = 16;
 __device__ __forceinline__ long long stats_tiles(const Args16 &a, int &tx, int &ty) {
   const int vx = a.nx - kBW + 1, vy = a.ny - kBW + 1, vz = a.nz - kBW + 1;
   if (vx <= 0 || vy <= 0 || vz <= 0) return 0;
-  tx = (vx + kStX - 1) / kStX;
-  ty = (vy + kStY - 1) / kStY;
-  return (long long)tx * ty * ((vz + kStZ - 1) / kStZ);
+  tx = (vx + kBsX - 1) / kBsX;
+  ty = (vy + kBsY - 1) / kBsY;
+  return (long long)tx * ty * ((vz + kBsZ - 1) / kBsZ);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
-  constexpr int HX = kStX + kBW - 1, HY = kStY + kBW - 1;  // 35 x 11 halo
+  constexpr int HX = kBsX + kBW - 1, HY = kBsY + kBW - 1;  // 35 x 11 halo
   __shared__ float s_v[HY][HX + 1];
   __shared__ uint8_t s_m[HY][HX + 1];
-  __shared__ double s_sx[HY][kStX], s_sq[HY][kStX];
-  __shared__ uint8_t s_mx[HY][kStX];
+  __shared__ double s_sx[HY][kBsX], s_sq[HY][kBsX];
+  __shared__ uint8_t s_mx[HY][kBsX];
   const Args16 &a = calls[blockIdx.y];
   if (!a.active) return;
   int ntx = 0, nty = 0;
@@ -248,12 +247,12 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int x0 = (int)(t % ntx) * kStX;
+    const int x0 = (int)(t % ntx) * kBsX;
     const long long r = t / ntx;
-    const int y0 = (int)(r % nty) * kStY, z0 = (int)(r / nty) * kStZ;
+    const int y0 = (int)(r % nty) * kBsY, z0 = (int)(r / nty) * kBsZ;
     double s0 = 0, s1 = 0, s2 = 0, q0 = 0, q1 = 0, q2 = 0;
     unsigned m0 = 0, m1 = 0, m2 = 0;
-    const int zend = min(z0 + kStZ + kBW - 1, nz);
+    const int zend = min(z0 + kBsZ + kBW - 1, nz);
     for (int zi = z0; zi < zend; ++zi) {
       __syncthreads();  // the previous plane's x sums are read
       const long long plane = (long long)zi * ny;
@@ -271,7 +270,7 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
         s_m[hy][hx] = m;
       }
       __syncthreads();
-      for (int i = tid; i < HY * kStX; i += 256) {
+      for (int i = tid; i < HY * kBsX; i += 256) {
         const int hy = i >> 5, hx = i & 31;
         double sx = 0.0, sq = 0.0;
         unsigned mk = 1;
@@ -302,7 +301,7 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
         const bool inm = (m0 & m1 & m2 & my) != 0;
         const double syy = Q - S * S * (1.0 / kB);
         const float f = (float)syy;
-        a.stats[((long long)oz * ny + oy) * nx + ox] =
+        a.stats[((long long)oz * ny + oy) * a.sp + ox] =
             make_float2((float)(S * (1.0 / kB)), inm ? f : -f - 0.0f);
       }
       s0 = s1; s1 = s2; s2 = sy;
@@ -453,7 +452,22 @@ __global__ void __launch_bounds__(256) prep16_kernel(const Args16 *calls) {
         pp.sxt = sxt;
         pp.sxt_tc = stc;
         pp.mmode = full == half_mask ? 1 : (none == half_mask ? 2 : 0);
-        pp.pad[0] = pp.pad[1] = pp.pad[2] = 0;
+        // the block's route: culled by the selection (its record written
+        // here), the tensor-core search (base block and every candidate
+        // footprint inside the masks, Sxx > 0), else the direct search's list
+        pp.route = 0;
+        pp.pad[0] = pp.pad[1] = 0;
+        if (a.selected && !a.selected[b]) {
+          int bx, by, bz;
+          split3(b, a.nbx, a.nby, bx, by, bz);
+          write_out(a, b, -3.f, -3.f,
+                    ((long long)(a.stz + bz * a.G) * ny + (a.sty + by * a.G)) * nx + (a.stx + bx * a.G), 0);
+        } else if (a.tensor && pp.mmode == 1 && wand_of(a)[b] && sxx > 0.f) {
+          pp.route = 1;
+        } else {
+          const unsigned int k = atomicAdd(&a.ctl[1], 1u);
+          a.fb_list[k] = (int)b;
+        }
         a.prep[b] = pp;
       }
     }
@@ -491,30 +505,6 @@ __global__ void chunk16_kernel(const Args16 *calls) {
     a.chunked[r] = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
-
-// Every selected block of a call without the tensor form to the direct
-// search; blocks culled by the variance selection get their culled record.
-__global__ void route_all16_kernel(const Args16 *calls) {
-  const Args16 &a = calls[blockIdx.y];
-  if (!a.active || a.tensor) return;
-  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
-       b += (long long)gridDim.x * blockDim.x) {
-    if (a.selected && !a.selected[b]) {
-      int bx, by, bz;
-      split3(b, a.nbx, a.nby, bx, by, bz);
-      const long long orig = ((long long)(a.stz + bz * a.G) * a.ny + (a.sty + by * a.G)) * a.nx +
-                             (a.stx + bx * a.G);
-      write_out(a, b, -3.f, -3.f, orig, 0);
-    } else {
-      const unsigned int k = atomicAdd(&a.ctl[1], 1u);
-      a.fb_list[k] = (int)b;
-    }
-  }
-}
-
-struct TcMaps {
-  CUtensorMap m[kMaxCalls];
-};
 
 // The call of a tile in the launch's flat tile numbering (calls in order).
 __device__ __forceinline__ int call_of_tile(const Args16 *calls, int ncalls, long long tile) {
@@ -572,41 +562,63 @@ __device__ __forceinline__ Top2k top2k_shfl_xor(const Top2k &t, int m) {
 // The tensor-core search: a warp-specialised persistent kernel, one CTA of 16
 // warps per SM, the CTA's tiles taken round-robin (tile = CTA + k x grid).
 //
-//   warp 1, one thread (control): requests each tile's window box (TMA, a
-//     ring of kBoxSlots) and issues the tile's 32 MMAs into one of two
+//   warp 2 (loader): lanes 0-7 make the tile's block records (which blocks
+//     take the tensor form; blocks that do not are listed for the direct
+//     search, unselected ones written out); lane 0 brings into a ring of
+//     kLdSlots the tile's window box and the box of the search statistics
+//     (TMA tensor copies) and its blocks' 16-bit parts (one bulk copy);
+//   warp 1, one thread (control): issues the tile's 32 MMAs into one of two
 //     accumulators in tensor memory (64 FP32 columns each);
 //   warps 4-7 (producers): thread m writes row m of A -- the bands of both
 //     k-steps -- into a ring of kASlots buffers of one vz each (8 operands);
 //   warps 8-15 (epilogue): warp 8 + 4 h + q reads lanes 32q.. and columns
-//     32h.. of a finished accumulator, scores the candidates and reduces the
-//     top two per block; one thread per block writes the block's record.
+//     32h.. of a finished accumulator, scores the candidates against the
+//     staged statistics and reduces the top two per block; one thread per
+//     block writes the block's record.
 //
 // Row m = (blk = m / 16, x shift s = (m / 2) % 8, part = m % 2) of A and D;
 // column n = (dz = n / 8, py = n % 8).  Every hand-off is an mbarrier:
-//   a_full[s]  producers (128 arrivals) -> control       A slot s written
-//   a_empty[s] control (tcgen05.commit) -> producers     its multiplies done
-//   b_full[s]  TMA (transaction bytes)  -> control       box s landed
-//   b_empty[s] control (commit)         -> control       box s read
-//   d_full[d]  control (commit)         -> epilogue      accumulator d done
-//   d_empty[d] epilogue (256 arrivals)  -> control       accumulator d read
-// A role derives what it needs from the tile index (the call, block
-// coordinates, the blocks' records), so nothing else passes between roles.
+//   l_full[s]  loader (records + copies)     -> everyone    slot s ready
+//   l_empty[s] control commit, producers,
+//              epilogue (1 + 128 + 256)      -> loader      slot s read
+//   a_full[s]  producers (128 arrivals)      -> control     A slot s written
+//   a_empty[s] control (tcgen05.commit)      -> producers   its multiplies done
+//   d_full[d]  control (commit)              -> epilogue    accumulator d done
+//   d_empty[d] epilogue (256 arrivals)       -> control     accumulator d read
 // Every wait is bounded; a wait that gives up sets the call's flag and the
-// CTA's, each role leaves its loop, and the control thread lets its copies
-// and multiplies land (bounded) before tensor memory is released.
+// CTA's, each role leaves its loop, and the loader and the control thread let
+// their copies and multiplies land (bounded) before tensor memory is
+// released.
 // ---------------------------------------------------------------------------
 constexpr int kASlots = 4;     // A ring: one vz (8 operands, 32 KB) per slot
-constexpr int kBoxSlots = 3;   // window-box ring
+constexpr int kLdSlots = 3;    // load ring
 constexpr int kWsThreads = 512;
+constexpr int kStX = 32, kStY = 8, kStZ = 8;                 // statistics box (float2)
+constexpr uint32_t kLdBox = 0;                                // window box (kBoxBytes)
+constexpr uint32_t kLdStats = 8192;                           // statistics box
+constexpr uint32_t kStatsBytes = kStX * kStY * kStZ * 8;      // 16 KB
+constexpr uint32_t kLdXs = kLdStats + kStatsBytes;            // blocks' 16-bit parts
+constexpr uint32_t kLdPrep = kLdXs + kTileBlocks * 256;       // blocks' records (Prep16)
+constexpr uint32_t kLdSlotBytes = 27 * 1024;
+static_assert(kLdPrep + kTileBlocks * sizeof(Prep16) <= kLdSlotBytes, "load slot layout");
+static_assert(kBoxBytes <= kLdStats, "window box fits its place in the slot");
 
 struct TcBars {
+  uint64_t l_full[kLdSlots], l_empty[kLdSlots];
   uint64_t a_full[kASlots], a_empty[kASlots];
-  uint64_t b_full[kBoxSlots], b_empty[kBoxSlots];
   uint64_t d_full[2], d_empty[2];
 };
 
+// Where one tile lies (shared memory, one per load slot); its blocks'
+// records (Prep16) and 16-bit parts are copied into the slot.
+struct TileRec {
+  long long b0;                    // index of the tile's first block
+  int nblk;                        // blocks of the tile in the grid
+  int ci, bx0, oy, oz, xs0;        // call, first block column, window origin, statistics box x
+};
+
 size_t tc_ws_smem_bytes() {
-  return (size_t)kASlots * kAChunkBytes + (size_t)kBoxSlots * ((kBoxBytes + 1023) / 1024 * 1024) + 1024;
+  return (size_t)kASlots * kAChunkBytes + (size_t)kLdSlots * kLdSlotBytes + 1024;
 }
 
 // phase-parity wait on a use count: the k-th completion of a barrier (k = 0,
@@ -625,33 +637,49 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
                : "memory");
 }
 
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 template <typename T, int W>
 __global__ void __launch_bounds__(kWsThreads, 1)
-    ncc_tc_kernel(const Args16 *calls, int ncalls, long long total_tiles,
-                  const __grid_constant__ TcMaps maps) {
+    ncc_tc_kernel(const Args16 *calls, int ncalls, long long total_tiles) {
   static_assert(W >= 2 && W <= 8, "window of the tensor form");
   constexpr int R = W / 2;
-  constexpr uint32_t kBoxStride = (kBoxBytes + 1023) / 1024 * 1024;
   extern __shared__ __align__(1024) uint8_t dsm[];
   uint8_t *const sbase = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(dsm) + 1023) & ~static_cast<uintptr_t>(1023));
   uint8_t *const sa = sbase;                              // A ring
-  uint8_t *const sbox = sbase + kASlots * kAChunkBytes;   // box ring
+  uint8_t *const sld = sbase + kASlots * kAChunkBytes;    // load ring
   __shared__ __align__(8) TcBars bars;
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_fail;
   __shared__ int s_ep_ok;
+  __shared__ TileRec s_rec[kLdSlots];
   __shared__ Top2k s_part[2][kTileBlocks];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
+    for (int i = 0; i < kLdSlots; ++i) {
+      mbar_init(&bars.l_full[i], 1);
+      mbar_init(&bars.l_empty[i], 1 + 128 + 256);
+    }
     for (int i = 0; i < kASlots; ++i) {
       mbar_init(&bars.a_full[i], 128);
       mbar_init(&bars.a_empty[i], 1);
-    }
-    for (int i = 0; i < kBoxSlots; ++i) {
-      mbar_init(&bars.b_full[i], 1);
-      mbar_init(&bars.b_empty[i], 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&bars.d_full[i], 1);
@@ -676,90 +704,133 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   const long long first = blockIdx.x, step = gridDim.x;
   const long long ntile = first < total_tiles ? (total_tiles - first + step - 1) / step : 0;
 
-  if (warp == 1) {
-   if (lane == 0) {
-    // ======================= control: boxes and multiplies ===================
-    constexpr uint32_t idesc = (1u << 4) | (S16<T>::kFmt << 7) | (S16<T>::kFmt << 10) |
-                               ((uint32_t)(64 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-    long long requested = 0;  // boxes requested (tiles 0 .. requested-1 of this CTA)
-    auto request = [&](long long j) {
-      const long long tile = first + j * step;
-      const TilePos p = tile_pos(calls, ncalls, tile);
-      const Args16 &c = calls[p.ci];
-      const int s = (int)(j % kBoxSlots);
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
-                       smem_u32(&bars.b_full[s])),
-                   "r"((unsigned)kBoxBytes)
-                   : "memory");
-      tma_load_4d(sbox + s * kBoxStride, &maps.m[p.ci], 0, c.sty + p.by * c.G - R,
-                  c.stz + p.bz * c.G - R, (c.G * p.bx0) >> 3, &bars.b_full[s]);
-    };
+  if (warp == 2) {
+    // ======================= loader: records and copies ======================
     long long j = 0;
-    int fail_ci = 0;
+    int fail_ci = 0, map_call = -1, cur = -1;
+    long long call_t0 = 0, call_end = -1;
     bool ok = true;
-    if (ntile > 0) {
-      request(0);
-      requested = 1;
-    }
-    for (; j < ntile && ok; ++j) {
+    for (; j < ntile; ++j) {
+      const int ls = (int)(j % kLdSlots);
+      int wok = 1;
+      if (lane == 0 && j >= kLdSlots) wok = wait_use(&bars.l_empty[ls], j / kLdSlots - 1) && !s_fail;
+      wok = __shfl_sync(0xffffffffu, wok, 0);
+      if (!wok) {
+        ok = false;
+        break;
+      }
       const long long tile = first + j * step;
-      fail_ci = call_of_tile(calls, ncalls, tile);
-      // the next tile's box: its slot was last read by tile j + 1 - kBoxSlots
-      if (j + 1 < ntile) {
-        const long long jp = j + 1 - kBoxSlots;
-        if (jp >= 0 && !wait_use(&bars.b_empty[(j + 1) % kBoxSlots], jp / kBoxSlots)) {
-          ok = false;
-          break;
+      if (lane == 0) {
+        // the tile's call and place, from the cached call when it is the same
+        if (tile >= call_end) {
+          cur = tile_pos(calls, ncalls, tile).ci;
+          const Args16 &c = calls[cur];
+          call_t0 = c.tile0;
+          call_end = c.tile0 + c.ntiles;
         }
-        request(j + 1);
-        requested = j + 2;
-      }
-      const int bs = (int)(j % kBoxSlots), dacc = (int)(j & 1);
-      if (!wait_use(&bars.b_full[bs], j / kBoxSlots)) { ok = false; break; }
-      if (j >= 2 && !wait_use(&bars.d_empty[dacc], (j - 2) / 2)) { ok = false; break; }
-      tc_fence_after();
-      const uint32_t wb = smem_u32(sbox + bs * kBoxStride);
-      const uint32_t dst = tmem + (uint32_t)dacc * 64u;
-      for (int vz = 0; vz < 4 && ok; ++vz) {
-        const long long g = j * 4 + vz;
-        const int as = (int)(g % kASlots);
-        if (!wait_use(&bars.a_full[as], g / kASlots)) { ok = false; break; }
-        tc_fence_after();
-        const uint32_t ab = smem_u32(sa) + (uint32_t)as * kAChunkBytes;
-#pragma unroll
-        for (int jj = 0; jj < kAChunkSteps; ++jj) {
-          const int vy = jj >> 1, ks = jj & 1;
-          const uint64_t ad = sdesc(ab + (uint32_t)jj * kAStepBytes, kALBO, kASBO);
-          const uint64_t bd =
-              sdesc(wb + (uint32_t)(2 * ks) * kLBO + (uint32_t)vz * kSBO + (uint32_t)vy * 16u, kLBO, kSBO);
-          const int acc = (vz | jj) != 0;
-          asm volatile(
-              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dst),
-              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-              : "memory");
+        const Args16 &a = calls[cur];
+        fail_ci = cur;
+        const int lt = (int)(tile - call_t0);
+        const int tx = a.tiles_x, nby = a.nby;
+        const int rr = lt / tx;
+        const int bx0 = (lt - rr * tx) * a.bpt, bz = rr / nby, by = rr - bz * nby;
+        TileRec &r = s_rec[ls];
+        const int oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
+        const int x0 = a.stx + bx0 * a.G - R;  // the tile's first candidate x
+        r.b0 = ((long long)bz * nby + by) * a.nbx + bx0;
+        r.nblk = min(a.bpt, a.nbx - bx0);
+        r.ci = cur;
+        r.bx0 = bx0;
+        r.oy = oy;
+        r.oz = oz;
+        r.xs0 = (x0 & 1) ? x0 - 1 : x0;  // even (16-byte aligned copy), <= x0
+        if (cur != map_call) {
+          // the call's copy descriptors were written by the host before the
+          // launch; order the tensor-map proxy after them
+          map_call = cur;
+          asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(
+                           reinterpret_cast<uint64_t>(a.tmap[0]))
+                       : "memory");
+          asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(
+                           reinterpret_cast<uint64_t>(a.tmap[1]))
+                       : "memory");
         }
-        tc_commit(&bars.a_empty[as]);
+        uint8_t *const slot = sld + (size_t)ls * kLdSlotBytes;
+        const unsigned nb = (unsigned)r.nblk;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                         smem_u32(&bars.l_full[ls])),
+                     "r"((unsigned)kBoxBytes + kStatsBytes + nb * 256u + nb * (unsigned)sizeof(Prep16))
+                     : "memory");
+        tma_load_4d(slot + kLdBox, a.tmap[0], 0, oy - R, oz - R, (a.G * bx0) >> 3, &bars.l_full[ls]);
+        tma_load_3d(slot + kLdStats, a.tmap[1], 2 * r.xs0, oy - R, oz - R, &bars.l_full[ls]);
+        bulk_load(slot + kLdXs, a.xs + r.b0 * 64, nb * 256u, &bars.l_full[ls]);
+        bulk_load(slot + kLdPrep, a.prep + r.b0, nb * (unsigned)sizeof(Prep16), &bars.l_full[ls]);
       }
-      if (!ok) break;
-      tc_commit(&bars.b_empty[bs]);
-      tc_commit(&bars.d_full[dacc]);
+      __syncwarp();
     }
-    if (!ok) {
+    if (!ok && lane == 0) {
       atomicExch(&calls[fail_ci].ctl[2], 1u);
       s_fail = 1;
-      // let requested boxes land (bounded) ...
-      for (long long k = j; k < requested; ++k) wait_use(&bars.b_full[k % kBoxSlots], k / kBoxSlots);
-      // ... and every issued multiply finish: a commit on tile j's
-      // accumulator barrier tracks all of them (the epilogue sees s_fail)
-      if (j < ntile) {
-        tc_commit(&bars.d_full[j & 1]);
-        wait_use(&bars.d_full[j & 1], j / 2);
-      }
-    } else if (j > 0) {
-      wait_use(&bars.d_full[(j - 1) & 1], (j - 1) / 2);
     }
-   }
+    // copies still in flight land before the CTA ends (bounded): the last
+    // request of each slot
+    if (lane == 0)
+      for (long long k = max(j - kLdSlots, 0LL); k < j; ++k) wait_use(&bars.l_full[k % kLdSlots], k / kLdSlots);
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ===================== control: the multiplies ===========================
+      constexpr uint32_t idesc = (1u << 4) | (S16<T>::kFmt << 7) | (S16<T>::kFmt << 10) |
+                                 ((uint32_t)(64 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+      long long j = 0;
+      bool ok = true;
+      for (; j < ntile && ok; ++j) {
+        const int ls = (int)(j % kLdSlots), dacc = (int)(j & 1);
+        if (!wait_use(&bars.l_full[ls], j / kLdSlots) || s_fail) { ok = false; break; }
+        if (j >= 2 && !wait_use(&bars.d_empty[dacc], (j - 2) / 2)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t wb = smem_u32(sld + (size_t)ls * kLdSlotBytes + kLdBox);
+        const uint32_t dst = tmem + (uint32_t)dacc * 64u;
+        for (int vz = 0; vz < 4 && ok; ++vz) {
+          const long long g = j * 4 + vz;
+          const int as = (int)(g % kASlots);
+          if (!wait_use(&bars.a_full[as], g / kASlots)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t ab = smem_u32(sa) + (uint32_t)as * kAChunkBytes;
+#pragma unroll
+          for (int jj = 0; jj < kAChunkSteps; ++jj) {
+            const int vy = jj >> 1, ks = jj & 1;
+            const uint64_t ad = sdesc(ab + (uint32_t)jj * kAStepBytes, kALBO, kASBO);
+            const uint64_t bd = sdesc(wb + (uint32_t)(2 * ks) * kLBO + (uint32_t)vz * kSBO +
+                                          (uint32_t)vy * 16u,
+                                      kLBO, kSBO);
+            const int acc = (vz | jj) != 0;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dst),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                : "memory");
+          }
+          tc_commit(&bars.a_empty[as]);
+        }
+        if (!ok) break;
+        tc_commit(&bars.l_empty[ls]);
+        tc_commit(&bars.d_full[dacc]);
+      }
+      if (!ok) {
+        const long long tile = first + (j < ntile ? j : ntile - 1) * step;
+        atomicExch(&calls[call_of_tile(calls, ncalls, tile)].ctl[2], 1u);
+        s_fail = 1;
+        // every issued multiply finishes: a commit on tile j's accumulator
+        // barrier tracks all of them (the epilogue sees s_fail)
+        if (j < ntile) {
+          tc_commit(&bars.d_full[j & 1]);
+          wait_use(&bars.d_full[j & 1], j / 2);
+        }
+      } else if (j > 0) {
+        wait_use(&bars.d_full[(j - 1) & 1], (j - 1) / 2);
+      }
+    }
     __syncwarp();  // the warp leaves the role converged
   } else if (warp >= 4 && warp < 8) {
     // ======================= producers: the A bands ==========================
@@ -771,15 +842,18 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     unsigned msk[2] = {0u, 0u};
     bool odd = false;
     for (long long j = 0; j < ntile; ++j) {
-      if (s_fail) break;
-      const long long tile = first + j * step;
-      const TilePos p = tile_pos(calls, ncalls, tile);
-      const Args16 &a = calls[p.ci];
-      if (p.ci != band_call) {
-        band_call = p.ci;
+      const int ls = (int)(j % kLdSlots);
+      if (s_fail || !wait_use(&bars.l_full[ls], j / kLdSlots)) {
+        s_fail = 1;
+        break;
+      }
+      const TileRec &r = s_rec[ls];
+      if (r.ci != band_call) {
+        band_call = r.ci;
+        const int G = calls[r.ci].G;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const int t0 = a.G * blk + sft - 16 * h;
+          const int t0 = G * blk + sft - 16 * h;
           const bool band = t0 < 16 && t0 + 4 > 0;
           odd = t0 & 1;  // the same for both halves
           const int c0 = t0 >= 0 ? (t0 >> 1) : -((1 - t0) >> 1);  // floor(t0 / 2)
@@ -793,16 +867,15 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           }
         }
       }
-      const int bx = p.bx0 + blk;
-      const bool live = blk < a.bpt && bx < a.nbx;
+      const bool live = blk < r.nblk;
       uint2 xw[16];
       {
-        const long long b = live ? ((long long)p.bz * a.nby + p.by) * a.nbx + bx : 0;
-        const uint32_t *xr = a.xs + b * 64 + part * 32;
+        const uint2 *xr = reinterpret_cast<const uint2 *>(sld + (size_t)ls * kLdSlotBytes + kLdXs +
+                                                          blk * 256 + part * 128);
 #pragma unroll
-        for (int r = 0; r < 16; ++r)
-          xw[r] = live ? *reinterpret_cast<const uint2 *>(xr + 2 * r) : make_uint2(0u, 0u);
+        for (int q2 = 0; q2 < 16; ++q2) xw[q2] = live ? xr[q2] : make_uint2(0u, 0u);
       }
+      mbar_arrive(&bars.l_empty[ls]);  // the slot's parts are in registers
       bool ok = true;
 #pragma unroll
       for (int vz = 0; vz < 4; ++vz) {
@@ -850,31 +923,16 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     const int blk = m >> 4, sft = (m >> 1) & 7, part = m & 1;
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16);
     const bool finisher = half == 0 && (lane & 15) == 0;
+    const int dz0 = 4 * half + 2 * part;
     int cnt_call = -1;
     unsigned int cnt_blocks = 0;
     unsigned long long cnt_cands = 0;
     for (long long j = 0; j < ntile; ++j) {
-      const long long tile = first + j * step;
-      const TilePos p = tile_pos(calls, ncalls, tile);
-      const Args16 &a = calls[p.ci];
-      const int oy = a.sty + p.by * a.G, oz = a.stz + p.bz * a.G;
-      const int bx = p.bx0 + blk;
-      const int ox = a.stx + bx * a.G;
-      // this row's block: its record, read before the accumulator is ready
-      long long b = -1;
-      int elig = 0, sel = 0;
-      float sxx = 0.f, stc = 0.f;
-      if (blk < a.bpt && bx < a.nbx) {
-        b = ((long long)p.bz * a.nby + p.by) * a.nbx + bx;
-        sel = !a.selected || a.selected[b];
-        const Prep16 pp = a.prep[b];
-        elig = sel && pp.mmode == 1 && wand_of(a)[b] && pp.sxx > 0.f;
-        sxx = pp.sxx;
-        stc = pp.sxt_tc;
-      }
-      // the accumulator: one thread waits, the epilogue warps agree
-      const int dacc = (int)(j & 1);
-      if (et == 0) s_ep_ok = wait_use(&bars.d_full[dacc], j / 2) && !s_fail;
+      const int ls = (int)(j % kLdSlots), dacc = (int)(j & 1);
+      // the slot and the accumulator: one thread waits, the epilogue warps agree
+      if (et == 0)
+        s_ep_ok = wait_use(&bars.l_full[ls], j / kLdSlots) && wait_use(&bars.d_full[dacc], j / 2) &&
+                  !s_fail;
       __syncwarp();
       asm volatile("bar.sync 1, 256;\n" ::: "memory");
       if (!s_ep_ok) {
@@ -897,55 +955,54 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       }
       tc_fence_before();
       mbar_arrive(&bars.d_empty[dacc]);
+      const TileRec &r = s_rec[ls];
+      const Prep16 *const pr = reinterpret_cast<const Prep16 *>(sld + (size_t)ls * kLdSlotBytes + kLdPrep);
+      const Args16 &a = calls[r.ci];
+      const int nx = a.nx, ny = a.ny, nz = a.nz;
+      const int oy = r.oy, oz = r.oz;
+      const int ox = a.stx + (r.bx0 + blk) * a.G;
+      const bool elig = blk < r.nblk && pr[blk].route == 1;
       // this thread's candidates: x shift sft, planes dz0 (jj < 8) and dz0 + 1
       // (jj >= 8), rows py = jj % 8; jj order is their raster order
       Top2k t2;
       t2.b1 = -3.f;
       t2.b2 = -3.f;
       t2.k1 = 0x7fffffff;
-      const int nx = a.nx, ny = a.ny, nz = a.nz;
-      const int dz0 = 4 * half + 2 * part;
-      if (elig && sft < W) {
-        int xlo, xhi, ylo, yhi, zlo, zhi;
-        cand_range(ox, nx, W, xlo, xhi);
-        cand_range(oy, ny, W, ylo, yhi);
-        cand_range(oz, nz, W, zlo, zhi);
-        const int cx = ox - R + sft;
-        if (cx >= xlo && cx <= xhi) {
-          // valid rows py in [pylo, pyhi] (never empty: the block's own row is
-          // one), planes dz0 + h valid when zok[h]; an invalid candidate
-          // loads a valid position's statistics (clamped row and plane) and
-          // is scored -FLT_MAX, so the loop has no branches
-          const int pylo = max(ylo - (oy - R), 0), pyhi = min(yhi - (oy - R), W - 1);
-          const int cz0 = oz - R + dz0;
-          const bool zok0 = dz0 < W && cz0 >= zlo && cz0 <= zhi;
-          const bool zok1 = dz0 + 1 < W && cz0 + 1 >= zlo && cz0 + 1 <= zhi;
-          const unsigned rows = ((2u << pyhi) - 1u) & ~((1u << pylo) - 1u);
-          const unsigned vmask = (zok0 ? rows : 0u) | (zok1 ? rows << 8 : 0u);
-          const long long row0 = (long long)(oy - R) * nx + cx;
-          const long long i0 = (long long)(zok0 ? cz0 : zlo) * ((long long)nx * ny) + row0;
-          const long long i1 = (long long)(zok1 ? cz0 + 1 : zlo) * ((long long)nx * ny) + row0;
-          int offr[8];
+      int xlo, xhi, ylo, yhi, zlo, zhi;
+      cand_range(ox, nx, W, xlo, xhi);
+      cand_range(oy, ny, W, ylo, yhi);
+      cand_range(oz, nz, W, zlo, zhi);
+      const int cx = ox - R + sft;
+      if (elig && sft < W && cx >= xlo && cx <= xhi) {
+        // valid rows py in [pylo, pyhi], planes dz0 + h valid when zok[h];
+        // the statistics box holds every candidate of the tile (zeros where
+        // it leaves the volume), invalid ones are scored -FLT_MAX
+        const int pylo = max(ylo - (oy - R), 0), pyhi = min(yhi - (oy - R), W - 1);
+        const int cz0 = oz - R + dz0;
+        const bool zok0 = dz0 < W && cz0 >= zlo && cz0 <= zhi;
+        const bool zok1 = dz0 + 1 < W && cz0 + 1 >= zlo && cz0 + 1 <= zhi;
+        const unsigned rows = ((2u << pyhi) - 1u) & ~((1u << pylo) - 1u);
+        const unsigned vmask = (zok0 ? rows : 0u) | (zok1 ? rows << 8 : 0u);
+        const float2 *sst = reinterpret_cast<const float2 *>(sld + (size_t)ls * kLdSlotBytes + kLdStats) +
+                            (dz0 * kStY) * kStX + (cx - r.xs0);
+        const float sxx = pr[blk].sxx, stc = pr[blk].sxt_tc;
+        int kbest = -1;
+        float b1 = -3.f, b2 = -3.f;
 #pragma unroll
-          for (int py = 0; py < 8; ++py) offr[py] = min(max(py, pylo), pyhi) * nx;
-          int kbest = -1;
-          float b1 = -3.f, b2 = -3.f;
-#pragma unroll
-          for (int jj = 0; jj < 16; ++jj) {
-            const float2 st = __ldg(a.stats + ((jj < 8 ? i0 : i1) + offr[jj & 7]));
-            const float sxy = fmaf(-st.x, stc, v[jj]);
-            float sc = st.y > 0.f ? __fdividef(sxy * sxy, sxx * st.y) : -2.f;
-            sc = ((vmask >> jj) & 1u) ? sc : -FLT_MAX;
-            const bool gt = sc > b1;
-            b2 = gt ? b1 : fmaxf(b2, sc);
-            b1 = gt ? sc : b1;
-            kbest = gt ? jj : kbest;
-          }
-          if (kbest >= 0) {
-            t2.b1 = b1;
-            t2.b2 = b2;
-            t2.k1 = ((dz0 + (kbest >> 3)) * 8 + (kbest & 7)) * 8 + sft;
-          }
+        for (int jj = 0; jj < 16; ++jj) {
+          const float2 st = sst[((jj >> 3) * kStY + (jj & 7)) * kStX];
+          const float sxy = fmaf(-st.x, stc, v[jj]);
+          float sc = st.y > 0.f ? __fdividef(sxy * sxy, sxx * st.y) : -2.f;
+          sc = ((vmask >> jj) & 1u) ? sc : -FLT_MAX;
+          const bool gt = sc > b1;
+          b2 = gt ? b1 : fmaxf(b2, sc);
+          b1 = gt ? sc : b1;
+          kbest = gt ? jj : kbest;
+        }
+        if (kbest >= 0) {
+          t2.b1 = b1;
+          t2.b2 = b2;
+          t2.k1 = ((dz0 + (kbest >> 3)) * 8 + (kbest & 7)) * 8 + sft;
         }
       }
       // reduce over the 16 lanes of the block (8 shifts x 2 parts) ...
@@ -955,35 +1012,26 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       if (half == 1 && (lane & 15) == 0) s_part[j & 1][blk] = t2;
       __syncwarp();
       asm volatile("bar.sync 1, 256;\n" ::: "memory");
-      if (finisher && b >= 0) {
-        if (!sel) {
-          write_out(a, b, -3.f, -3.f, ((long long)oz * ny + oy) * nx + ox, 0);
-        } else if (!elig) {
-          const unsigned int k = atomicAdd(&a.ctl[1], 1u);
-          a.fb_list[k] = (int)b;
-        } else {
-          top2k_merge(t2, s_part[j & 1][blk]);
-          const int k = t2.k1;
-          const long long idx =
-              ((long long)(oz - R + (k >> 6)) * ny + (oy - R + ((k >> 3) & 7))) * nx + (ox - R + (k & 7));
-          write_out(a, b, t2.b1, t2.b2, idx, 1);
-          if (p.ci != cnt_call) {
-            if (cnt_call >= 0) {
-              atomicAdd(&calls[cnt_call].ctl[0], cnt_blocks);
-              if (calls[cnt_call].ncc_count) atomicAdd(calls[cnt_call].ncc_count, cnt_cands);
-            }
-            cnt_call = p.ci;
-            cnt_blocks = 0;
-            cnt_cands = 0;
+      if (finisher && elig) {
+        top2k_merge(t2, s_part[j & 1][blk]);
+        const int k = t2.k1;
+        const long long idx =
+            ((long long)(oz - R + (k >> 6)) * ny + (oy - R + ((k >> 3) & 7))) * nx + (ox - R + (k & 7));
+        write_out(a, r.b0 + blk, t2.b1, t2.b2, idx, 1);
+        if (r.ci != cnt_call) {
+          if (cnt_call >= 0) {
+            atomicAdd(&calls[cnt_call].ctl[0], cnt_blocks);
+            if (calls[cnt_call].ncc_count) atomicAdd(calls[cnt_call].ncc_count, cnt_cands);
           }
-          int xlo, xhi, ylo, yhi, zlo, zhi;
-          cand_range(ox, nx, W, xlo, xhi);
-          cand_range(oy, ny, W, ylo, yhi);
-          cand_range(oz, nz, W, zlo, zhi);
-          ++cnt_blocks;
-          cnt_cands += (unsigned long long)(xhi - xlo + 1) * (yhi - ylo + 1) * (zhi - zlo + 1);
+          cnt_call = r.ci;
+          cnt_blocks = 0;
+          cnt_cands = 0;
         }
+        ++cnt_blocks;
+        cnt_cands += (unsigned long long)(xhi - xlo + 1) * (yhi - ylo + 1) * (zhi - zlo + 1);
       }
+      __syncwarp();
+      mbar_arrive(&bars.l_empty[ls]);  // the slot's records and statistics are read
     }
     if (finisher && cnt_call >= 0 && cnt_blocks) {
       atomicAdd(&calls[cnt_call].ctl[0], cnt_blocks);
@@ -1056,7 +1104,7 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
       const int px = c % ncx, py = (c / ncx) % ncy, pz = c / (ncx * ncy);
       const int cx = xlo + px, cy = ylo + py, cz = zlo + pz;
       const long long idx = ((long long)cz * a.ny + cy) * a.nx + cx;
-      const float2 st = __ldg(a.stats + idx);
+      const float2 st = __ldg(a.stats + ((long long)cz * a.ny + cy) * a.sp + cx);
       const float muy = st.x;
       float sxy = 0.f, sxx = 0.f, syy = 0.f;
       if (pp.mmode == 1 && !signbit(st.y)) {
@@ -1128,6 +1176,7 @@ EncodeTiledFn encode_fn() {
 // Derived per-call fields: the tensor form's tile layout and copy geometry.
 void prepare16(const BmGeom &g, Match16Call &c) {
   c.nx = g.size[0]; c.ny = g.size[1]; c.nz = g.size[2];
+  c.sp = (c.nx + 1) & ~1;
   c.nbx = g.nb[0]; c.nby = g.nb[1]; c.nbz = g.nb[2];
   c.stx = g.st[0]; c.sty = g.st[1]; c.stz = g.st[2];
   c.G = g.ngap;
@@ -1162,6 +1211,60 @@ long long match16_number_tiles(Match16Call *calls, int n) {
   return tiles;
 }
 
+mirorr_status match16_prepare_copies(int dtype, Match16Call *calls, int n) {
+  EncodeTiledFn enc = nullptr;
+  for (int i = 0; i < n; ++i) {
+    Match16Call &c = calls[i];
+    memset(c.tmap, 0, sizeof(c.tmap));
+    if (!c.active || !c.tensor) continue;
+    if (!enc) {
+      enc = encode_fn();
+      if (!enc) {
+        set_error("cuTensorMapEncodeTiled is not available from the driver");
+        return MIRORR_ECUDA;
+      }
+    }
+    CUtensorMap *m = reinterpret_cast<CUtensorMap *>(c.tmap[0]);
+    {
+      // the window box: [x / 8][z][y][x % 8] 16-bit values, box 8 x 11 x 11 x 4
+      const cuuint64_t dims[4] = {8, (cuuint64_t)c.ny, (cuuint64_t)c.nz, (cuuint64_t)c.nxc};
+      const cuuint64_t strides[3] = {16, (cuuint64_t)16 * c.ny, (cuuint64_t)16 * c.ny * c.nz};
+      const cuuint32_t box[4] = {8, (cuuint32_t)kSlots, (cuuint32_t)kPlanes, (cuuint32_t)kXC};
+      const cuuint32_t estr[4] = {1, 1, 1, 1};
+      const CUresult r = enc(&m[0],
+                             dtype == MIRORR_DTYPE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                        : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                             4, c.chunked, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (window box) failed (%d)", (int)r);
+        return MIRORR_ECUDA;
+      }
+    }
+    {
+      // the statistics box: float2 rows of pitch sp seen as pairs of float32,
+      // box 32 positions x 8 rows x 8 planes
+      const cuuint64_t dims[3] = {(cuuint64_t)2 * c.sp, (cuuint64_t)c.ny, (cuuint64_t)c.nz};
+      const cuuint64_t strides[2] = {(cuuint64_t)8 * c.sp, (cuuint64_t)8 * c.sp * c.ny};
+      const cuuint32_t box[3] = {(cuuint32_t)(2 * kStX), (cuuint32_t)kStY, (cuuint32_t)kStZ};
+      const cuuint32_t estr[3] = {1, 1, 1};
+      const CUresult r = enc(&m[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, c.stats, dims, strides, box,
+                             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (statistics box) failed (%d)", (int)r);
+        return MIRORR_ECUDA;
+      }
+    }
+  }
+  return MIRORR_OK;
+}
+
+size_t match16_stats_bytes(const Match16Call &c) {
+  return sizeof(float2) * (size_t)c.sp * c.ny * c.nz;
+}
+
 size_t match16_wand_bytes(const Match16Call &c) {
   return (size_t)c.nbx * c.ny * c.nz + (size_t)c.nbx * c.nby * c.nz + (size_t)c.nblocks;
 }
@@ -1173,6 +1276,8 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
                     bool every_stage) {
   const int SM = sm_count();
   const long long tiles = match16_number_tiles(host_calls, ncalls);
+  MB2_TRY(match16_prepare_copies(S16<T>::kFmt == 1 ? MIRORR_DTYPE_BF16 : MIRORR_DTYPE_F16, host_calls,
+                                 ncalls));
   long long max_vox = 0, max_blocks = 0, max_chunks = 0;
   int W = 0, G = 0;
   bool any_tensor = false;
@@ -1208,8 +1313,8 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
       if (!c.active) continue;
       const long long vx = c.nx - kBW + 1, vy = c.ny - kBW + 1, vz = c.nz - kBW + 1;
       if (vx > 0 && vy > 0 && vz > 0)
-        st_tiles = std::max(st_tiles, ((vx + kStX - 1) / kStX) * ((vy + kStY - 1) / kStY) *
-                                          ((vz + kStZ - 1) / kStZ));
+        st_tiles = std::max(st_tiles, ((vx + kBsX - 1) / kBsX) * ((vy + kBsY - 1) / kBsY) *
+                                          ((vz + kBsZ - 1) / kBsZ));
     }
     long long gx = std::min(st_tiles, (long long)SM * 8);
     if (gx < 1) gx = 1;
@@ -1228,40 +1333,7 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
     chunk16_kernel<T><<<grid_for(max_chunks), 256, 0, s>>>(dc);
     MB2_LAUNCH_CHECK();
   }
-  route_all16_kernel<<<grid_for(max_blocks), 256, 0, s>>>(dc);
-  MB2_LAUNCH_CHECK();
   if (any_tensor || every_stage) {
-    if (ncalls > kMaxCalls) {
-      set_error("more than %d matcher calls in one tensor launch", kMaxCalls);
-      return MIRORR_EINVAL;
-    }
-    EncodeTiledFn enc = encode_fn();
-    if (!enc) {
-      set_error("cuTensorMapEncodeTiled is not available from the driver");
-      return MIRORR_ECUDA;
-    }
-    static TcMaps maps;  // the host side of the kernel parameter (large: static)
-    static std::mutex maps_mu;
-    std::lock_guard<std::mutex> lock(maps_mu);
-    memset(&maps, 0, sizeof(maps));
-    for (int i = 0; i < ncalls; ++i) {
-      const Match16Call &c = host_calls[i];
-      if (!c.active || !c.tensor) continue;
-      const cuuint64_t dims[4] = {8, (cuuint64_t)c.ny, (cuuint64_t)c.nz, (cuuint64_t)c.nxc};
-      const cuuint64_t strides[3] = {16, (cuuint64_t)16 * c.ny, (cuuint64_t)16 * c.ny * c.nz};
-      const cuuint32_t box[4] = {8, (cuuint32_t)kSlots, (cuuint32_t)kPlanes, (cuuint32_t)kXC};
-      const cuuint32_t estr[4] = {1, 1, 1, 1};
-      CUresult r = enc(&maps.m[i],
-                       S16<T>::kFmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
-                       4, c.chunked, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS) {
-        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
-        return MIRORR_ECUDA;
-      }
-    }
     const size_t smem = tc_ws_smem_bytes();
     auto kern = (W == 7) ? ncc_tc_kernel<T, 7> : (W == 5) ? ncc_tc_kernel<T, 5>
                                                           : ncc_tc_kernel<T, 3>;
@@ -1271,7 +1343,7 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
     // tensor tiles is one CTA that finds no tile
     if (grid < 1 && every_stage) grid = 1;
     if (grid > 0) {
-      kern<<<(unsigned)grid, kWsThreads, smem, s>>>(dc, ncalls, tiles, maps);
+      kern<<<(unsigned)grid, kWsThreads, smem, s>>>(dc, ncalls, tiles);
       MB2_LAUNCH_CHECK();
     }
   }
@@ -1311,8 +1383,7 @@ mirorr_status launch_match16(int dtype, const BmGeom &g, const void *base, const
   Match16Call c;
   memset(&c, 0, sizeof(c));
   prepare16(g, c);
-  const long long nvox = (long long)g.size[0] * g.size[1] * g.size[2];
-  MB2_TRY(w.stats.ensure(sizeof(float2) * nvox));
+  MB2_TRY(w.stats.ensure(match16_stats_bytes(c)));
   MB2_TRY(w.wand.ensure(match16_wand_bytes(c)));
   MB2_TRY(w.prep.ensure(sizeof(Prep16) * g.nblocks));
   MB2_TRY(w.xs.ensure(sizeof(uint32_t) * 64 * g.nblocks));
