@@ -270,6 +270,14 @@ __global__ void select_hist_kernel(const unsigned long long *__restrict__ key, l
     if (h[i]) atomicAdd(&hist[i], h[i]);
 }
 
+// The select's initial state (a kernel rather than a host copy, so the
+// sequence can be captured into a graph).
+__global__ void select_init_kernel(SelectCtl *ctl, unsigned long long k, unsigned long long n,
+                                   unsigned int *hist) {
+  if (threadIdx.x == 0) *ctl = SelectCtl{0ULL, 0ULL, k, n};
+  hist[threadIdx.x] = 0u;
+}
+
 __global__ void select_scan_kernel(SelectCtl *ctl, int shift, unsigned int *hist) {
   __shared__ unsigned int h[256];
   int t = threadIdx.x;
@@ -335,10 +343,9 @@ mirorr_status launch_variance_selection(const BmGeom &g, const void *base, doubl
   // cut-off index (unsigned)((1 - keep) * N); index >= N -> the maximum
   unsigned long long idx = (unsigned long long)(unsigned int)((1.0 - keep) * (double)n);
   if (idx >= (unsigned long long)n) idx = n - 1;
-  SelectCtl c0{0ULL, 0ULL, idx, (unsigned long long)n};
-  MB2_CUDA_TRY(cudaMemcpyAsync(w.select_state.ptr, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
-  MB2_CUDA_TRY(cudaMemsetAsync(w.hist.ptr, 0, 256 * sizeof(unsigned int), s));
   SelectCtl *ctl = w.select_state.as<SelectCtl>();
+  select_init_kernel<<<1, 256, 0, s>>>(ctl, idx, (unsigned long long)n, w.hist.as<unsigned int>());
+  MB2_LAUNCH_CHECK();
   for (int pass = 0; pass < 8; ++pass) {
     int shift = 56 - 8 * pass;
     select_hist_kernel<<<(unsigned)blocks, threads, 0, s>>>(key, n, ctl, shift,

@@ -9,6 +9,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <iterator>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -1747,6 +1749,7 @@ constexpr int kLtsCtas = 2;  // CTAs per LTS fit in the batched launch
 
 struct BatchCallBufs {
   DevBuf stats, wand, prep, xs, chunked, fb, best, second, match, status, tiles;
+  BmWork sel;  // variance selection (var, selected, select_state, hist) when keep < 1
 };
 
 struct BatchSlot {
@@ -1775,6 +1778,9 @@ struct BatchSlot {
   mirorr_reg_stats stats{};
   std::chrono::steady_clock::time_point t0;
   size_t bytes = 0;
+  // one device allocation holds every buffer above (they are views into it)
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
 };
 
 size_t slot_bytes(const mirorr_geometry &fg, const mirorr_geometry &mg, const mirorr_reg_params &p,
@@ -1789,6 +1795,7 @@ size_t slot_bytes(const mirorr_geometry &fg, const mirorr_geometry &mg, const mi
   // statistics with even-pitch rows (<= 8 V (1 + 1 / nx), nx >= 4), window-AND,
   // x-chunked copy, per-block records
   b += ncall * (10 * V + 3 * V / 2 + (32 + 256 + 4 + 13) * NB + 2 * V + 64 * 1024);
+  if (p.bm.block_keep < 1.0) b += ncall * (17 * NB + 2048);  // variance selection
   b += 2 * 3 * 8 * ncall * NB;                                 // point pairs
   b += lts_fit_scratch_bytes((long long)(ncall * NB), kLtsCtas);
   return b;
@@ -1816,6 +1823,10 @@ struct mirorr_batch_s {
   cudaGraphExec_t gexec = nullptr;
   std::vector<long long> gkey;
   int64_t rounds = 0, replays = 0, captures = 0, updates = 0;
+  // arenas of finished requests, kept for the next ones (by size); their
+  // bytes plus the live requests' stay within the budget
+  std::multimap<size_t, void *> pool;
+  size_t pool_bytes = 0;
   // host-clock seconds: level setup, descriptors and graph work, launch to
   // synchronisation, advancing the requests
   double t_setup = 0, t_issue = 0, t_device = 0, t_advance = 0;
@@ -1923,17 +1934,67 @@ void batch_fail(mirorr_batch b, BatchSlot &s, mirorr_status st, const char *msg)
   (void)b;
 }
 
+// Frees cached arenas, largest first, while the live requests and the cache
+// together exceed the budget.
+void pool_trim(mirorr_batch b, size_t extra) {
+  while (!b->pool.empty() && b->used + b->pool_bytes + extra > b->budget) {
+    auto last = std::prev(b->pool.end());
+    cudaFree(last->second);
+    b->pool_bytes -= last->first;
+    b->pool.erase(last);
+  }
+}
+
+// The slot's buffers (each of `list`'s sizes, 256-byte aligned) as views into
+// one arena: the smallest cached arena that holds them, else a new one.
+mirorr_status slot_carve(mirorr_batch b, BatchSlot &s,
+                         const std::vector<std::pair<DevBuf *, size_t>> &list) {
+  auto up = [](size_t v) { return (std::max<size_t>(v, 1) + 255) / 256 * 256; };
+  size_t total = 0;
+  for (auto &e : list) total += up(e.second);
+  void *p = nullptr;
+  size_t pb = 0;
+  auto it = b->pool.lower_bound(total);
+  if (it != b->pool.end()) {
+    p = it->second;
+    pb = it->first;
+    b->pool_bytes -= pb;
+    b->pool.erase(it);
+  } else {
+    pool_trim(b, 0);
+    cudaError_t e = cudaMalloc(&p, total);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      pool_trim(b, b->budget);  // everything cached
+      e = cudaMalloc(&p, total);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaMalloc(%zu) for a batch request failed: %s", total, cudaGetErrorString(e));
+        return MIRORR_ENOMEM;
+      }
+    }
+    pb = total;
+  }
+  s.arena = p;
+  s.arena_bytes = pb;
+  size_t off = 0;
+  for (auto &e : list) {
+    e.first->ptr = static_cast<char *>(p) + off;
+    e.first->bytes = up(e.second);
+    off += up(e.second);
+  }
+  return MIRORR_OK;
+}
+
+// The slot's arena goes back to the cache; its buffers were views into it.
 void batch_release(mirorr_batch b, BatchSlot &s) {
-  DevBuf *bufs[] = {&s.in_f, &s.in_m, &s.in_fm, &s.in_mm, &s.lvl_f, &s.lvl_m, &s.img_b, &s.img_s,
-                    &s.msk_b, &s.msk_s, &s.pts_i, &s.pts_m, &s.lts_scratch};
-  for (DevBuf *x : bufs) x->release();
-  for (auto &cb : s.call) {
-    DevBuf *cbs[] = {&cb.stats, &cb.wand, &cb.prep, &cb.xs, &cb.chunked, &cb.fb, &cb.best,
-                     &cb.second, &cb.match, &cb.status, &cb.tiles};
-    for (DevBuf *x : cbs) x->release();
+  if (s.arena) {
+    b->pool.insert({s.arena_bytes, s.arena});
+    b->pool_bytes += s.arena_bytes;
   }
   b->used -= s.bytes;
   s = BatchSlot();
+  pool_trim(b, 0);
 }
 
 // Host-side check, before any launch, that every buffer a round's
@@ -1968,7 +2029,10 @@ mirorr_status batch_check_slot(mirorr_ctx c, const BatchSlot &s) {
          need(cb.second, sizeof(float) * nb, "second") &&
          need(cb.match, sizeof(int32_t) * nb, "match") && need(cb.status, nb, "status") &&
          need(cb.tiles, sizeof(unsigned int) * ((nb + 2047) / 2048 + 1), "tiles") &&
-         (!mc.tensor || need(cb.chunked, match16_chunk_bytes(mc), "chunked"));
+         (!mc.tensor || need(cb.chunked, match16_chunk_bytes(mc), "chunked")) &&
+         (!(s.p.bm.block_keep < 1.0) ||
+          (need(cb.sel.var, 16 * (size_t)nb, "selection keys") &&
+           need(cb.sel.selected, (size_t)nb, "selection flags")));
   }
   return ok ? MIRORR_OK : MIRORR_EINVAL;
 }
@@ -1988,6 +2052,22 @@ mirorr_status batch_issue(mirorr_batch b, int njobs, long long max_vox, int ncal
   MB2_CUDA_TRY(cudaMemsetAsync(b->d_counts.ptr, 0, sizeof(long long) * 4 * S, st));
   MB2_CUDA_TRY(cudaMemsetAsync(b->d_ctl.ptr, 0, sizeof(unsigned int) * 4 * 2 * S, st));
   MB2_TRY(launch_resample_batch(b->d_jobs.as<ResampleJob>(), njobs, max_vox, st));
+  // the variance selection of the calls of requests that keep a fraction of
+  // their blocks (on this iteration's resampled base images)
+  {
+    const Match16Call *calls = b->h_calls.as<Match16Call>();
+    int prev = -1;
+    for (int ci = 0; ci < ncalls; ++ci) {
+      const int si = b->call_slot[ci];
+      const int k = si == prev ? 1 : 0;
+      prev = si;
+      BatchSlot &s = b->slots[si];
+      if (!(s.p.bm.block_keep < 1.0)) continue;
+      const uint8_t *sel = nullptr;
+      MB2_TRY(launch_variance_selection(s.g, calls[ci].base, s.p.bm.block_keep, s.call[k].sel, &sel, st,
+                                        b->storage));
+    }
+  }
   MB2_TRY(launch_match16_batch(b->storage, ncalls, b->h_calls.as<Match16Call>(), b->d_calls, st,
                                true));
   MB2_TRY(launch_postfilter_batch(b->d_pf.as<PfCall>(), ncalls, max_blocks, st));
@@ -2105,7 +2185,7 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
       mc.bmask = k ? s.msk_s.as<uint8_t>() : s.msk_b.as<uint8_t>();
       mc.search = k ? s.img_b.ptr : s.img_s.ptr;
       mc.smask = k ? s.msk_b.as<uint8_t>() : s.msk_s.as<uint8_t>();
-      mc.selected = nullptr;
+      mc.selected = s.p.bm.block_keep < 1.0 ? cb.sel.selected.as<uint8_t>() : nullptr;
       mc.stats = cb.stats.as<float2>();
       mc.wand = cb.wand.as<uint8_t>();
       mc.prep = cb.prep.as<Prep16>();
@@ -2323,6 +2403,9 @@ mirorr_status mirorr_batch_destroy(mirorr_batch b) {
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
   for (auto &s : b->slots)
     if (s.state) batch_release(b, s);
+  for (auto &e : b->pool) cudaFree(e.second);
+  b->pool.clear();
+  b->pool_bytes = 0;
   HostBuf *hb[] = {&b->h_jobs, &b->h_calls, &b->h_pf, &b->h_states, &b->h_rd, &b->h_lts_args};
   for (HostBuf *x : hb) x->release();
   DevBuf *db[] = {&b->d_jobs, &b->d_pf, &b->d_states, &b->d_counts, &b->d_ctl, &b->d_calls,
@@ -2362,16 +2445,18 @@ mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, con
     return MIRORR_EINVAL;
   }
   MB2_TRY(check_bm_params(p->bm));
-  if (p->bm.block_width != 4 || p->bm.block_gap != 1 || p->bm.nhood_width > 13 ||
-      !(p->bm.block_keep >= 1.0)) {
-    set_error("batched registration needs block width 4, block gap 1, window up to 13 and "
-              "every block kept");
+  if ((p->bm.block_width != 4 && p->bm.block_width != 5) || p->bm.block_gap != 1 ||
+      p->bm.nhood_width + p->bm.block_width - 1 > 16) {
+    set_error("batched registration needs block width 4 or 5, block gap 1 and a window up to "
+              "17 - block width");
     return MIRORR_EINVAL;
   }
   if (!(p->lts_keep > 0.0 && p->lts_keep <= 1.0)) { set_error("lts_keep must lie in (0, 1]"); return MIRORR_EINVAL; }
   if (b->params_set && (p->storage != b->storage || p->bm.nhood_width != b->bm.nhood_width ||
-                        p->bm.nhood_gap != b->bm.nhood_gap)) {
-    set_error("the requests of one batch share the storage type, window and block spacing");
+                        p->bm.nhood_gap != b->bm.nhood_gap ||
+                        p->bm.block_width != b->bm.block_width)) {
+    set_error("the requests of one batch share the storage type, block width, window and block "
+              "spacing");
     return MIRORR_EINVAL;
   }
   int si = -1;
@@ -2434,7 +2519,8 @@ mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, con
   const size_t es = elem_size(pp.storage);
   const int ncall = pp.symmetric ? 2 : 1;
   mirorr_status st = MIRORR_OK;
-  auto E = [&](DevBuf &x, size_t n) { if (st == MIRORR_OK) st = x.ensure(n); };
+  std::vector<std::pair<DevBuf *, size_t>> bufs;
+  auto E = [&](DevBuf &x, size_t n) { bufs.push_back({&x, n}); };
   E(s.in_f, es * vox(fg->size));
   E(s.in_m, es * vox(mg->size));
   if (fmask) E(s.in_fm, vox(fg->size));
@@ -2458,10 +2544,17 @@ mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, con
     E(cb.match, sizeof(int32_t) * max_blocks);
     E(cb.status, max_blocks);
     E(cb.tiles, sizeof(unsigned int) * (max_blocks / 2048 + 2));
+    if (pp.bm.block_keep < 1.0) {
+      E(cb.sel.var, (sizeof(double) + sizeof(unsigned long long)) * max_blocks);
+      E(cb.sel.selected, max_blocks);
+      E(cb.sel.select_state, 64);
+      E(cb.sel.hist, 256 * sizeof(unsigned int));
+    }
   }
   E(s.pts_i, sizeof(double) * 3 * ncall * max_blocks);
   E(s.pts_m, sizeof(double) * 3 * ncall * max_blocks);
   E(s.lts_scratch, lts_fit_scratch_bytes(ncall * max_blocks, kLtsCtas));
+  st = slot_carve(b, s, bufs);
   if (st == MIRORR_OK) st = upload(c, s.in_f, fixed, es * vox(fg->size));
   if (st == MIRORR_OK) st = upload(c, s.in_m, moving, es * vox(mg->size));
   if (st == MIRORR_OK && fmask) st = upload(c, s.in_fm, fmask, vox(fg->size));

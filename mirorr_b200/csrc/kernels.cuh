@@ -125,6 +125,7 @@ struct alignas(64) Match16Call {
   int nbx, nby, nbz;
   int stx, sty, stz;
   int G, W;
+  int bw;                 // block width (4: tensor form possible; 5: direct search only)
   int bpt;                // blocks per tensor tile (G bpt a multiple of 8)
   int tiles_x;
   int chunk_x0, nxc;      // x of the copy's first 8-wide chunk, chunks per row

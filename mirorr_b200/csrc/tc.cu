@@ -199,11 +199,11 @@ __device__ __forceinline__ void write_out(const Args16 &a, long long b, float be
 }
 
 // Clipped candidate range of one axis for block gap 1 (itkBlockMatcher.txx:744-756).
-__device__ __forceinline__ void cand_range(int o, int S, int W, int &lo, int &hi) {
+__device__ __forceinline__ void cand_range(int o, int S, int W, int BW, int &lo, int &hi) {
   lo = o - W / 2;
   hi = lo + W - 1;
   if (lo < 0) lo = 0;
-  if (hi > S - kBW) hi = S - kBW;
+  if (hi > S - BW) hi = S - BW;
 }
 
 // ---------------------------------------------------------------------------
@@ -211,29 +211,30 @@ __device__ __forceinline__ void cand_range(int o, int S, int W, int &lo, int &hi
 // of the BW^3 footprint (every voxel) and Syy = sum (y - mean)^2, from the
 // footprint's sum and sum of squares in FP64.  Both sums of 16-bit values are
 // exact in FP64 (a square has at most 22 significant bits), and so is
-// Syy = sum y^2 - (sum y)^2 / 64 up to its final rounding: the two terms are
-// exact and their difference is exact (Sterbenz), so Syy is correctly
-// rounded to FP32 and 0 exactly when the footprint is constant.  The sign
-// bit of Syy is set when a search-mask voxel of the footprint is 0.
+// B^3 sum y^2 - (sum y)^2 (B^3 = BW^3 voxels): Syy is that over B^3, rounded
+// once, and 0 exactly when the footprint is constant.  The sign bit of Syy
+// is set when a search-mask voxel of the footprint is 0.
 //
 // Separable: a CTA of 32 x 8 threads owns 32 x 8 output columns and walks
-// 16 output planes; per input plane it stages the 35 x 11 halo (values and
-// mask) in shared memory, sums each row's 4-wide runs along x (FP64), then
-// each thread sums 4 of those along y and keeps the last four planes' sums in
-// registers for the z sum.  grid.y = call; grid.x strides over the tiles.
+// 16 output planes; per input plane it stages the (32 + BW - 1) x (8 + BW - 1)
+// halo (values and mask) in shared memory, sums each row's BW-wide runs
+// along x (FP64), then each thread sums BW of those along y and keeps the
+// last BW planes' sums in registers for the z sum.  grid.y = call; grid.x
+// strides over the tiles.
 // ---------------------------------------------------------------------------
 constexpr int kBsX = 32, kBsY = 8, kBsZ = 16;
-__device__ __forceinline__ long long stats_tiles(const Args16 &a, int &tx, int &ty) {
-  const int vx = a.nx - kBW + 1, vy = a.ny - kBW + 1, vz = a.nz - kBW + 1;
+__device__ __forceinline__ long long stats_tiles(const Args16 &a, int BW, int &tx, int &ty) {
+  const int vx = a.nx - BW + 1, vy = a.ny - BW + 1, vz = a.nz - BW + 1;
   if (vx <= 0 || vy <= 0 || vz <= 0) return 0;
   tx = (vx + kBsX - 1) / kBsX;
   ty = (vy + kBsY - 1) / kBsY;
   return (long long)tx * ty * ((vz + kBsZ - 1) / kBsZ);
 }
 
-template <typename T>
+template <typename T, int BW>
 __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
-  constexpr int HX = kBsX + kBW - 1, HY = kBsY + kBW - 1;  // 35 x 11 halo
+  constexpr int HX = kBsX + BW - 1, HY = kBsY + BW - 1;  // halo (35 x 11 for BW 4)
+  constexpr int NB = BW * BW * BW;
   __shared__ float s_v[HY][HX + 1];
   __shared__ uint8_t s_m[HY][HX + 1];
   __shared__ double s_sx[HY][kBsX], s_sq[HY][kBsX];
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
   const Args16 &a = calls[blockIdx.y];
   if (!a.active) return;
   int ntx = 0, nty = 0;
-  const long long ntiles = stats_tiles(a, ntx, nty);
+  const long long ntiles = stats_tiles(a, BW, ntx, nty);
   const T *__restrict__ y = static_cast<const T *>(a.search);
   const uint8_t *__restrict__ ms = a.smask;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
@@ -250,9 +251,15 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
     const int x0 = (int)(t % ntx) * kBsX;
     const long long r = t / ntx;
     const int y0 = (int)(r % nty) * kBsY, z0 = (int)(r / nty) * kBsZ;
-    double s0 = 0, s1 = 0, s2 = 0, q0 = 0, q1 = 0, q2 = 0;
-    unsigned m0 = 0, m1 = 0, m2 = 0;
-    const int zend = min(z0 + kBsZ + kBW - 1, nz);
+    // the previous BW - 1 planes' sums (sum, sum of squares, mask-AND)
+    double zs[BW - 1], zq[BW - 1];
+    unsigned zm[BW - 1];
+#pragma unroll
+    for (int k = 0; k < BW - 1; ++k) {
+      zs[k] = zq[k] = 0.0;
+      zm[k] = 0u;
+    }
+    const int zend = min(z0 + kBsZ + BW - 1, nz);
     for (int zi = z0; zi < zend; ++zi) {
       __syncthreads();  // the previous plane's x sums are read
       const long long plane = (long long)zi * ny;
@@ -275,7 +282,7 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
         double sx = 0.0, sq = 0.0;
         unsigned mk = 1;
 #pragma unroll
-        for (int k = 0; k < kBW; ++k) {
+        for (int k = 0; k < BW; ++k) {
           const double v = (double)s_v[hy][hx + k];
           sx += v;
           sq = fma(v, v, sq);
@@ -289,24 +296,37 @@ __global__ void __launch_bounds__(256) box_stats16_kernel(const Args16 *calls) {
       double sy = 0.0, qy = 0.0;
       unsigned my = 1;
 #pragma unroll
-      for (int k = 0; k < kBW; ++k) {
+      for (int k = 0; k < BW; ++k) {
         sy += s_sx[ly + k][lx];
         qy += s_sq[ly + k][lx];
         my &= s_mx[ly + k][lx];
       }
-      const int oz = zi - (kBW - 1);
+      const int oz = zi - (BW - 1);
       const int ox = x0 + lx, oy = y0 + ly;
-      if (oz >= z0 && ox <= nx - kBW && oy <= ny - kBW) {
-        const double S = ((s0 + s1) + s2) + sy, Q = ((q0 + q1) + q2) + qy;
-        const bool inm = (m0 & m1 & m2 & my) != 0;
-        const double syy = Q - S * S * (1.0 / kB);
+      if (oz >= z0 && ox <= nx - BW && oy <= ny - BW) {
+        double S = sy, Q = qy;
+        unsigned inm = my;
+#pragma unroll
+        for (int k = 0; k < BW - 1; ++k) {
+          S += zs[k];
+          Q += zq[k];
+          inm &= zm[k];
+        }
+        // NB Q - S^2 is exact (both terms are), so Syy is rounded once
+        const double syy = ((double)NB * Q - S * S) / (double)NB;
         const float f = (float)syy;
         a.stats[((long long)oz * ny + oy) * a.sp + ox] =
-            make_float2((float)(S * (1.0 / kB)), inm ? f : -f - 0.0f);
+            make_float2((float)(S / (double)NB), inm ? f : -f - 0.0f);
       }
-      s0 = s1; s1 = s2; s2 = sy;
-      q0 = q1; q1 = q2; q2 = qy;
-      m0 = m1; m1 = m2; m2 = my;
+#pragma unroll
+      for (int k = 0; k < BW - 2; ++k) {
+        zs[k] = zs[k + 1];
+        zq[k] = zq[k + 1];
+        zm[k] = zm[k + 1];
+      }
+      zs[BW - 2] = sy;
+      zq[BW - 2] = qy;
+      zm[BW - 2] = my;
     }
   }
 }
@@ -328,10 +348,10 @@ __global__ void wand_x16_kernel(const Args16 *calls) {
     const int ox = a.stx + bx * a.G;
     int lo = ox - R, hi = ox + R;
     if (lo < 0) lo = 0;
-    if (hi > a.nx - kBW) hi = a.nx - kBW;
+    if (hi > a.nx - a.bw) hi = a.nx - a.bw;
     unsigned v = 1;
     const uint8_t *row = a.smask + yz * a.nx;
-    for (int x = lo; x <= hi + kBW - 1; ++x) v &= row[x] != 0 ? 1u : 0u;
+    for (int x = lo; x <= hi + a.bw - 1; ++x) v &= row[x] != 0 ? 1u : 0u;
     a.wand[i] = (uint8_t)v;
   }
 }
@@ -350,9 +370,9 @@ __global__ void wand_y16_kernel(const Args16 *calls) {
     const int oy = a.sty + by * a.G;
     int lo = oy - R, hi = oy + R;
     if (lo < 0) lo = 0;
-    if (hi > a.ny - kBW) hi = a.ny - kBW;
+    if (hi > a.ny - a.bw) hi = a.ny - a.bw;
     unsigned v = 1;
-    for (int y = lo; y <= hi + kBW - 1; ++y) v &= in[((long long)z * a.ny + y) * a.nbx + bx];
+    for (int y = lo; y <= hi + a.bw - 1; ++y) v &= in[((long long)z * a.ny + y) * a.nbx + bx];
     out[i] = (uint8_t)v;
   }
 }
@@ -369,9 +389,9 @@ __global__ void wand_z16_kernel(const Args16 *calls) {
     const int oz = a.stz + bz * a.G;
     int lo = oz - R, hi = oz + R;
     if (lo < 0) lo = 0;
-    if (hi > a.nz - kBW) hi = a.nz - kBW;
+    if (hi > a.nz - a.bw) hi = a.nz - a.bw;
     unsigned v = 1;
-    for (int z = lo; z <= hi + kBW - 1; ++z) v &= in[(long long)z * a.nbx * a.nby + bxy];
+    for (int z = lo; z <= hi + a.bw - 1; ++z) v &= in[(long long)z * a.nbx * a.nby + bxy];
     out[b] = (uint8_t)v;
   }
 }
@@ -470,6 +490,81 @@ __global__ void __launch_bounds__(256) prep16_kernel(const Args16 *calls) {
         }
         a.prep[b] = pp;
       }
+    }
+  }
+}
+
+// Base-block preparation for other block widths (no tensor form): one warp
+// per block, lane l < BW^2 holds base row (vz, vy) = (l / BW, l % BW); the
+// FP32 mean, the masked sums of x~ and x~^2, the base-mask mode and the
+// block's route (culled, or the direct search's list).  grid.y = call.
+template <typename T, int BW>
+__global__ void __launch_bounds__(256) prep16w_kernel(const Args16 *calls) {
+  static_assert(BW * BW <= 32, "one warp per block");
+  constexpr int NB = BW * BW * BW;
+  const Args16 &a = calls[blockIdx.y];
+  if (!a.active) return;
+  const T *__restrict__ x = static_cast<const T *>(a.base);
+  const uint8_t *__restrict__ mb = a.bmask;
+  const int nx = a.nx, ny = a.ny;
+  const int lane = threadIdx.x & 31;
+  const bool row = lane < BW * BW;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long b = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); b < a.nblocks;
+       b += nwarps) {
+    int bx, by, bz;
+    split3(b, a.nbx, a.nby, bx, by, bz);
+    const int ox = a.stx + bx * a.G, oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
+    float v[BW];
+    unsigned mbits = 0;
+    float sum = 0.f;
+    if (row) {
+      const long long q = ((long long)(oz + lane / BW) * ny + (oy + lane % BW)) * nx + ox;
+#pragma unroll
+      for (int i = 0; i < BW; ++i) {
+        v[i] = S16<T>::f(x[q + i]);
+        mbits |= (mb[q + i] != 0 ? 1u : 0u) << i;
+        sum += v[i];
+      }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    const float mu = sum * (1.0f / NB);
+    float sxx = 0.f, sxt = 0.f;
+    if (row) {
+#pragma unroll
+      for (int i = 0; i < BW; ++i) {
+        const float d = v[i] - mu;
+        if ((mbits >> i) & 1u) {
+          sxx = fmaf(d, d, sxx);
+          sxt += d;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      sxx += __shfl_xor_sync(0xffffffffu, sxx, o);
+      sxt += __shfl_xor_sync(0xffffffffu, sxt, o);
+    }
+    constexpr unsigned rows_mask = (BW * BW == 32) ? 0xffffffffu : ((1u << (BW * BW)) - 1u);
+    const unsigned full = __ballot_sync(0xffffffffu, row && mbits == (1u << BW) - 1u) & rows_mask;
+    const unsigned none = __ballot_sync(0xffffffffu, row && mbits == 0u) & rows_mask;
+    if (lane == 0) {
+      Prep16 pp;
+      pp.mu = mu;
+      pp.sxx = sxx;
+      pp.sxt = sxt;
+      pp.sxt_tc = 0.f;
+      pp.mmode = full == rows_mask ? 1 : (none == rows_mask ? 2 : 0);
+      pp.route = 0;
+      pp.pad[0] = pp.pad[1] = 0;
+      if (a.selected && !a.selected[b]) {
+        write_out(a, b, -3.f, -3.f, ((long long)oz * ny + oy) * nx + ox, 0);
+      } else {
+        const unsigned int k = atomicAdd(&a.ctl[1], 1u);
+        a.fb_list[k] = (int)b;
+      }
+      a.prep[b] = pp;
     }
   }
 }
@@ -969,9 +1064,9 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       t2.b2 = -3.f;
       t2.k1 = 0x7fffffff;
       int xlo, xhi, ylo, yhi, zlo, zhi;
-      cand_range(ox, nx, W, xlo, xhi);
-      cand_range(oy, ny, W, ylo, yhi);
-      cand_range(oz, nz, W, zlo, zhi);
+      cand_range(ox, nx, W, kBW, xlo, xhi);
+      cand_range(oy, ny, W, kBW, ylo, yhi);
+      cand_range(oz, nz, W, kBW, zlo, zhi);
       const int cx = ox - R + sft;
       if (elig && sft < W && cx >= xlo && cx <= xhi) {
         // valid rows py in [pylo, pyhi], planes dz0 + h valid when zok[h];
@@ -1055,10 +1150,11 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 // lies inside the search mask with the base block inside its mask uses the
 // box statistics for Syy and one product per voxel.  grid.y = call.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int BW>
 __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
   constexpr int NT = 128;
-  __shared__ float s_xt[kB], s_mb[kB];
+  constexpr int NB = BW * BW * BW;
+  __shared__ float s_xt[NB], s_mb[NB];
   __shared__ float s_y[16 * 16 * 16];
   __shared__ uint8_t s_m[16 * 16 * 16];
   __shared__ Top2 s_red[NT / 32];
@@ -1074,19 +1170,19 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
     split3(b, a.nbx, a.nby, bx, by, bz);
     const int ox = a.stx + bx * a.G, oy = a.sty + by * a.G, oz = a.stz + bz * a.G;
     int xlo, xhi, ylo, yhi, zlo, zhi;
-    cand_range(ox, a.nx, a.W, xlo, xhi);
-    cand_range(oy, a.ny, a.W, ylo, yhi);
-    cand_range(oz, a.nz, a.W, zlo, zhi);
+    cand_range(ox, a.nx, a.W, BW, xlo, xhi);
+    cand_range(oy, a.ny, a.W, BW, ylo, yhi);
+    cand_range(oz, a.nz, a.W, BW, zlo, zhi);
     const int ncx = xhi - xlo + 1, ncy = yhi - ylo + 1, ncz = zhi - zlo + 1;
-    const int ex = ncx + kBW - 1, ey = ncy + kBW - 1, ez = ncz + kBW - 1;
+    const int ex = ncx + BW - 1, ey = ncy + BW - 1, ez = ncz + BW - 1;
     const Prep16 pp = a.prep[b];
     __syncthreads();
-    if (tid < kB) {
-      const int vx = tid & 3, vy = (tid >> 2) & 3, vz = tid >> 4;
+    for (int t = tid; t < NB; t += NT) {
+      const int vx = t % BW, vy = (t / BW) % BW, vz = t / (BW * BW);
       const long long qq = ((long long)(oz + vz) * a.ny + (oy + vy)) * a.nx + (ox + vx);
       const float mv = a.bmask[qq] != 0 ? 1.f : 0.f;
-      s_xt[tid] = S16<T>::f(base[qq]) - pp.mu;
-      s_mb[tid] = mv;
+      s_xt[t] = S16<T>::f(base[qq]) - pp.mu;
+      s_mb[t] = mv;
     }
     for (int i = tid; i < ex * ey * ez; i += NT) {
       const int wx = i % ex, wy = (i / ex) % ey, wz = i / (ex * ey);
@@ -1109,18 +1205,18 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
       float sxy = 0.f, sxx = 0.f, syy = 0.f;
       if (pp.mmode == 1 && !signbit(st.y)) {
         // footprint and base block wholly inside their masks
-#pragma unroll 8
-        for (int i = 0; i < kB; ++i) {
-          const int vx = i & 3, vy = (i >> 2) & 3, vz = i >> 4;
+#pragma unroll 5
+        for (int i = 0; i < NB; ++i) {
+          const int vx = i % BW, vy = (i / BW) % BW, vz = i / (BW * BW);
           sxy = fmaf(s_xt[i], s_y[((pz + vz) * 16 + py + vy) * 16 + px + vx], sxy);
         }
         sxy -= muy * pp.sxt;
         sxx = pp.sxx;
         syy = st.y;
       } else {
-#pragma unroll 8
-        for (int i = 0; i < kB; ++i) {
-          const int vx = i & 3, vy = (i >> 2) & 3, vz = i >> 4;
+#pragma unroll 5
+        for (int i = 0; i < NB; ++i) {
+          const int vx = i % BW, vy = (i / BW) % BW, vz = i / (BW * BW);
           const int w = ((pz + vz) * 16 + py + vy) * 16 + px + vx;
           const float mk = s_mb[i] * (float)s_m[w];
           const float dy = s_y[w] - muy;
@@ -1181,6 +1277,7 @@ void prepare16(const BmGeom &g, Match16Call &c) {
   c.stx = g.st[0]; c.sty = g.st[1]; c.stz = g.st[2];
   c.G = g.ngap;
   c.W = g.nw;
+  c.bw = g.bw;
   c.nblocks = g.nblocks;
   // blocks per tile: the tile's bands fit the 32-wide box, and G bpt is a
   // multiple of 8 so every tile's window starts on a chunk of the copy
@@ -1279,10 +1376,17 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
   MB2_TRY(match16_prepare_copies(S16<T>::kFmt == 1 ? MIRORR_DTYPE_BF16 : MIRORR_DTYPE_F16, host_calls,
                                  ncalls));
   long long max_vox = 0, max_blocks = 0, max_chunks = 0;
-  int W = 0, G = 0;
+  int W = 0, G = 0, BWc = 0;
   bool any_tensor = false;
   for (int i = 0; i < ncalls; ++i) {
     const Match16Call &c = host_calls[i];
+    if (c.active) {
+      if (BWc && BWc != c.bw) {
+        set_error("the calls of one launch must share the block width");
+        return MIRORR_EINVAL;
+      }
+      BWc = c.bw;
+    }
     if (c.active && c.tensor) {
       any_tensor = true;
       if ((W && W != c.W) || (G && G != c.G)) {
@@ -1311,14 +1415,15 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
     for (int i = 0; i < ncalls; ++i) {
       const Match16Call &c = host_calls[i];
       if (!c.active) continue;
-      const long long vx = c.nx - kBW + 1, vy = c.ny - kBW + 1, vz = c.nz - kBW + 1;
+      const long long vx = c.nx - c.bw + 1, vy = c.ny - c.bw + 1, vz = c.nz - c.bw + 1;
       if (vx > 0 && vy > 0 && vz > 0)
         st_tiles = std::max(st_tiles, ((vx + kBsX - 1) / kBsX) * ((vy + kBsY - 1) / kBsY) *
                                           ((vz + kBsZ - 1) / kBsZ));
     }
     long long gx = std::min(st_tiles, (long long)SM * 8);
     if (gx < 1) gx = 1;
-    box_stats16_kernel<T><<<dim3((unsigned)gx, (unsigned)ncalls), 256, 0, s>>>(dc);
+    if (BWc == 5) box_stats16_kernel<T, 5><<<dim3((unsigned)gx, (unsigned)ncalls), 256, 0, s>>>(dc);
+    else box_stats16_kernel<T, 4><<<dim3((unsigned)gx, (unsigned)ncalls), 256, 0, s>>>(dc);
   }
   MB2_LAUNCH_CHECK();
   wand_x16_kernel<<<grid_for(max_vox / 2 + 1), 256, 0, s>>>(dc);
@@ -1327,7 +1432,8 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
   MB2_LAUNCH_CHECK();
   wand_z16_kernel<<<grid_for(max_blocks), 256, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
-  prep16_kernel<T><<<grid_for(max_blocks * 16), 256, 0, s>>>(dc);
+  if (BWc == 5) prep16w_kernel<T, 5><<<grid_for(max_blocks * 32), 256, 0, s>>>(dc);
+  else prep16_kernel<T><<<grid_for(max_blocks * 16), 256, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
   if (any_tensor || every_stage) {
     chunk16_kernel<T><<<grid_for(max_chunks), 256, 0, s>>>(dc);
@@ -1347,7 +1453,8 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
       MB2_LAUNCH_CHECK();
     }
   }
-  ncc_fb16_kernel<T><<<dim3((unsigned)SM * 4, (unsigned)ncalls), 128, 0, s>>>(dc);
+  if (BWc == 5) ncc_fb16_kernel<T, 5><<<dim3((unsigned)SM * 4, (unsigned)ncalls), 128, 0, s>>>(dc);
+  else ncc_fb16_kernel<T, 4><<<dim3((unsigned)SM * 4, (unsigned)ncalls), 128, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }
@@ -1368,16 +1475,17 @@ mirorr_status launch_match16(int dtype, const BmGeom &g, const void *base, const
                              const void *search, const uint8_t *smask, const uint8_t *selected,
                              const BmOut &out, Bm16Work &w, unsigned long long *ncc_count,
                              cudaStream_t s) {
-  if (g.bw != kBW) {
-    set_error("the 16-bit search supports block width 4 (got %d)", g.bw);
+  if (g.bw != 4 && g.bw != 5) {
+    set_error("the 16-bit search supports block widths 4 and 5 (got %d)", g.bw);
     return MIRORR_EINVAL;
   }
   if (g.bgap != 1) {
     set_error("the 16-bit search supports block gap 1 (got %d)", g.bgap);
     return MIRORR_EINVAL;
   }
-  if (g.nw > 13) {
-    set_error("the 16-bit search supports windows up to 13 (got %d)", g.nw);
+  if (g.nw + g.bw - 1 > 16) {
+    set_error("the 16-bit search supports windows up to %d for block width %d (got %d)",
+              17 - g.bw, g.bw, g.nw);
     return MIRORR_EINVAL;
   }
   Match16Call c;

@@ -58,6 +58,33 @@ def test_batch_equals_single_requests(ctx, graphs):
     b.close()
 
 
+def test_batch_block_width5_keep_fraction(ctx):
+    """Block width 5, window 11, 30 % of the blocks kept (the large stress
+    configuration's search at small size): the batch runs the variance
+    selection of every call on its resampled base image; each request's
+    result equals the single-request path's."""
+    reqs = [dict(shape=(72, 64, 48), mode="symmetric", kind="affine", seed=61, levels=2),
+            dict(shape=(64, 80, 40), mode="classic", kind="rigid", seed=62, levels=2)]
+    singles, subs = [], []
+    for r in reqs:
+        ph = make_phantom(r["shape"], n_gauss=16, kind=r["kind"], seed=r["seed"], max_angle_deg=4.0,
+                          max_shift_vox=4.0)
+        p = mb.reg_params(symmetric=r["mode"] == "symmetric", kind=r["kind"], levels=r["levels"],
+                          iterations=4, block_width=5, nhood_gap=3, nhood_width=11, block_keep=0.3,
+                          storage="f16")
+        singles.append(mb.register(ctx, ph.fixed, ph.moving, p)[0])
+        subs.append((ph, p))
+    b = mb.Batch(ctx, max_slots=4, hbm_budget=8e9)
+    ids = [b.submit(ph.fixed, ph.moving, p) for ph, p in subs]
+    b.run()
+    for rid, t1 in zip(ids, singles):
+        t, st = b.result(rid)
+        np.testing.assert_allclose(t.M, t1.M, atol=1e-9, rtol=0)
+        np.testing.assert_allclose(t.off, t1.off, atol=1e-7, rtol=0)
+        assert st.block_ncc_evaluated > 0
+    b.close()
+
+
 def test_batch_alone_equals_in_the_mix(ctx):
     """Continuous batching: request 0 runs alone; then again while others are
     admitted between its steps.  Its result must not change."""

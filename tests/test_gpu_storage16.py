@@ -35,6 +35,10 @@ CASES = [
     dict(id="w7_G4_x_ragged", shape=(67, 30, 24), nw=7, G=4, keep=1.0, mask=None, seed=36),
     # window 9: every block through the direct FP32 search
     dict(id="w9_G3_direct", shape=(40, 36, 28), nw=9, G=3, keep=1.0, mask="search", seed=37),
+    # block width 5 (direct search), the large stress configuration's
+    # geometry at small size: window 11, spacing 3, 30 % of the blocks kept
+    dict(id="bw5_w11_G3_keep03", shape=(44, 40, 30), nw=11, G=3, keep=0.3, mask=None, seed=38, bw=5),
+    dict(id="bw5_w7_G2_masked", shape=(36, 34, 26), nw=7, G=2, keep=1.0, mask="both", seed=39, bw=5),
 ]
 
 
@@ -62,7 +66,8 @@ def test_matcher16_matches_oracle(ctx, c, store):
     ph, base, search, bm, sm = make_inputs(c, store)
     m = mb.BlockMatcher(ctx)
     m.SetStorage(store)
-    m.SetBlockWidth(4)
+    bw = c.get("bw", 4)
+    m.SetBlockWidth(bw)
     m.SetNhoodGap(c["G"])
     m.SetNhoodWidth(c["nw"])
     m.SetBlockKeep(c["keep"])
@@ -80,7 +85,7 @@ def test_matcher16_matches_oracle(ctx, c, store):
     mi, best, second, status = m.BlockResults()
     diag = m.LastDiagnostics()
     m.close()
-    p = O.BMParams(4, 1, c["G"], c["nw"], c["keep"])
+    p = O.BMParams(bw, 1, c["G"], c["nw"], c["keep"])
     ref = O.match_blocks(base, search, bm, sm, p)
     np.testing.assert_array_equal((status & 1).astype(np.uint8), ref.status)
     s = ref.status == 1
@@ -93,26 +98,31 @@ def test_matcher16_matches_oracle(ctx, c, store):
     clear = gap > GAP
     assert np.all(same[clear]), f"{np.sum(~same[clear])} blocks with a clear gap moved"
     assert same.mean() >= 0.995, f"argmax agreement {same.mean():.4f}"
-    if c["nw"] <= 7:
+    if c["nw"] <= 7 and bw == 4:
         assert diag[4] > 0, "no block took the tensor-core search"
     print(f"{c['id']} {store}: {s.sum()} blocks, tensor {diag[4]}, direct {diag[5]}, "
           f"max |d best| {err.max():.2e}, argmax agreement {same.mean():.5f}")
 
 
 @pytest.mark.parametrize("store", ["bf16", "f16"])
-@pytest.mark.parametrize("mode,kind", [("symmetric", "affine"), ("classic", "rigid")])
-def test_register16_matches_oracle(ctx, store, mode, kind):
-    shape = (72, 64, 48)
+@pytest.mark.parametrize("mode,kind,bw,nw,keep,shape,levels", [
+    ("symmetric", "affine", 4, 7, 1.0, (72, 64, 48), 2),
+    ("classic", "rigid", 4, 7, 1.0, (72, 64, 48), 2),
+    # block width 5, window 11, 30 % kept (the large stress configuration's
+    # search), one level of a volume where the registration converges
+    ("symmetric", "affine", 5, 11, 0.3, (96, 88, 64), 1)])
+def test_register16_matches_oracle(ctx, store, mode, kind, bw, nw, keep, shape, levels):
     ph = make_phantom(shape, n_gauss=20, kind=kind, seed=41 if kind == "affine" else 42,
                       max_angle_deg=4.0, max_shift_vox=4.0)
-    rp = O.RegParams(mode, kind, 4, O.BMParams(4, 1, 3, 7, 1.0), 0.5, store)
+    rp = O.RegParams(mode, kind, 4, O.BMParams(bw, 1, 3, nw, keep), 0.5, store)
     fixed = O.Image(ph.fixed, ph.spacing, ph.origin)
     moving = O.Image(ph.moving, ph.spacing, ph.origin)
-    to = O.register(fixed, moving, rp, 2)
-    p = mb.reg_params(symmetric=mode == "symmetric", kind=kind, levels=2, iterations=4,
-                      nhood_gap=3, nhood_width=7, storage=store)
+    to = O.register(fixed, moving, rp, levels)
+    p = mb.reg_params(symmetric=mode == "symmetric", kind=kind, levels=levels, iterations=4,
+                      block_width=bw, nhood_gap=3, nhood_width=nw, block_keep=keep,
+                      storage=store)
     tg, st = mb.register(ctx, ph.fixed, ph.moving, p)
-    assert st.levels_run == 2 and st.block_ncc_evaluated > 0
+    assert st.levels_run == levels and st.block_ncc_evaluated > 0
     # the host copies carried 2 bytes per voxel
     assert st.h2d_bytes >= 2 * 2 * ph.fixed.size
     dM = np.max(np.abs(tg.M - to.M))
