@@ -316,18 +316,23 @@ MIRORR_API mirorr_status mirorr_register_device(mirorr_ctx ctx, const mirorr_geo
 /* ---- batched and served registrations ---------------------------------------
  * No reference counterpart (the reference runs one registration per process,
  * mirorr.cxx:93-665).  A batch holds up to max_slots registration requests
- * (BF16 or F16 storage, block width 4, block gap 1, every block kept) on the
- * device at once, within hbm_budget bytes of device memory reserved for them.
- * Each request is one RunMirorr (itkMirorrPyramidImplement.txx:71-158) with
- * its own size, levels, method and transform kind; its results equal
- * mirorr_register's on the same inputs and parameters up to the order of the
- * LTS fit's floating-point sums.  A step advances every running request by
- * one block-matching iteration with one launch per stage for all of them
- * (the tensor-core search of every request's blocks in one persistent launch,
- * every LTS fit in one cooperative launch); while the running set and their
- * levels stay unchanged, the step replays a captured CUDA graph.  Requests
- * may be submitted between steps (continuous batching): a new request starts
- * at its coarsest level while the others continue. */
+ * (BF16 or F16 storage, block width 4 or 5, block gap 1, any block keep; the
+ * requests of one batch share the storage type, block width, window and block
+ * spacing) on the device at once, within hbm_budget bytes of device memory
+ * reserved for them.  Each request is one RunMirorr
+ * (itkMirorrPyramidImplement.txx:71-158) with its own size, levels, method and
+ * transform kind; its results equal mirorr_register's on the same inputs and
+ * parameters up to the order of the LTS fit's floating-point sums.  A step
+ * advances every running request by one block-matching iteration with one
+ * launch per stage for all of them (the variance selections, the tensor-core
+ * search of every request's blocks in one persistent launch, every LTS fit in
+ * one cooperative launch).  The step's launches run from a CUDA graph: replayed
+ * while the running set and their levels stay unchanged, otherwise updated in
+ * place.  Requests may be submitted between steps (continuous batching): a new
+ * request starts at its coarsest level while the others continue.  Each
+ * request's device buffers live in one allocation; a finished request's
+ * allocation is kept for later ones (within the budget), so a running service
+ * does not allocate or free device memory per request. */
 typedef struct mirorr_batch_s *mirorr_batch;
 MIRORR_API mirorr_status mirorr_batch_create(mirorr_ctx ctx, int32_t max_slots,
                                   uint64_t hbm_budget, mirorr_batch *out);
