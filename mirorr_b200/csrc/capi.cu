@@ -551,16 +551,19 @@ mirorr_status resample_into(mirorr_ctx c, const RegImage &src, const uint8_t *ma
   if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], c->stream));
   const bool same_grid = src.g.size[0] == mask_g.size[0] && src.g.size[1] == mask_g.size[1] &&
                          src.g.size[2] == mask_g.size[2] && memcmp(&mi, &mm, sizeof(mi)) == 0;
+  // the default mask (no mask given) is 255 everywhere and is not read
+  const bool ones = c->ones.ptr && mask == c->ones.as<uint8_t>();
   if (same_grid) {
     // image and mask on one input grid (the finest level): one pass computes
     // each voxel's index map once for both
     MB2_TRY(launch_resample(src.g.size, src.img, mask, grid.size, mi, img.ptr, msk.as<uint8_t>(),
-                            c->stream, false, src.dtype, out_dtype));
+                            c->stream, false, src.dtype, out_dtype, ones));
   } else {
     MB2_TRY(launch_resample(src.g.size, src.img, nullptr, grid.size, mi, img.ptr, nullptr,
                             c->stream, false, src.dtype, out_dtype));
     MB2_TRY(launch_resample(mask_g.size, nullptr, mask, grid.size, mm, nullptr,
-                            msk.as<uint8_t>(), c->stream));
+                            msk.as<uint8_t>(), c->stream, false, MIRORR_DTYPE_F32, MIRORR_DTYPE_F32,
+                            ones));
   }
   if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], c->stream));
   return MIRORR_OK;
@@ -2168,6 +2171,7 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
       memset(&jm, 0, sizeof(jm));
       jm.inm = q.mask;
       jm.outm = q.outm->as<uint8_t>();
+      jm.mask_ones = q.mask == c->ones.as<uint8_t>() ? 1 : 0;
       for (int d = 0; d < 3; ++d) { jm.in_size[d] = q.mgeo->size[d]; jm.out_size[d] = q.grid->size[d]; }
       memcpy(jm.C, mmp.C, sizeof(mmp.C));
       memcpy(jm.e, mmp.e, sizeof(mmp.e));

@@ -203,10 +203,13 @@ struct ResampleMap {
 // in / out: float32, or 16-bit per in_dtype / out_dtype (MIRORR_DTYPE_*):
 // F32 -> F32, F32 -> BF16/F16, and BF16 -> BF16 / F16 -> F16.  A 16-bit output
 // is the float result rounded to the storage type.
+// mask_ones: in_mask is 255 everywhere (not read; the output mask is 255
+// inside the input grid and 0 outside, as its interpolation gives).
 mirorr_status launch_resample(const int in_size[3], const void *in, const uint8_t *in_mask,
                               const int out_size[3], const ResampleMap &map, void *out,
                               uint8_t *out_mask, cudaStream_t s, bool nearest = false,
-                              int in_dtype = MIRORR_DTYPE_F32, int out_dtype = MIRORR_DTYPE_F32);
+                              int in_dtype = MIRORR_DTYPE_F32, int out_dtype = MIRORR_DTYPE_F32,
+                              bool mask_ones = false);
 // One pass of launch_resample_batch: float32 image (or none) and uint8 mask
 // (or none) on an index map, image output in out_dtype (16-byte aligned),
 // mask output 4-byte aligned; inactive jobs are skipped.
@@ -221,6 +224,7 @@ struct ResampleJob {
   double e[3];
   int out_dtype;
   int active;
+  int mask_ones;  // inm is 255 everywhere (not read)
 };
 mirorr_status launch_resample_batch(const ResampleJob *dev_jobs, int njobs, long long max_voxels,
                                     cudaStream_t s);

@@ -32,7 +32,10 @@ struct ResampleArgs {
   double e[3];
   void *out;       // float32, or 16-bit
   uint8_t *outm;
-  int nearest;  // nearest-neighbour instead of linear interpolation
+  int nearest;    // nearest-neighbour instead of linear interpolation
+  int mask_ones;  // the input mask is 255 everywhere: the output mask is 255
+                  // inside the input and 0 outside (every interpolation of
+                  // 255s is 255), so the mask is not read
 };
 
 __device__ __forceinline__ float ld_f(const float *p, long long i) { return __ldg(p + i); }
@@ -79,6 +82,9 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
     if (MSK) *m = 0;
     return;
   }
+  const bool mread = MSK && !a.mask_ones;
+  if (MSK && a.mask_ones) *m = 255;
+  if (!IMG && !mread) return;
   if (a.nearest) {
     // NearestNeighborInterpolateImageFunction: index = floor(c + 0.5)
     long long q = 0, stride = 1;
@@ -91,7 +97,7 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
       stride *= nn[r];
     }
     if (IMG) st_copy(*v, ld_f(in, q));
-    if (MSK) *m = __ldg(a.inm + q);
+    if (mread) *m = __ldg(a.inm + q);
     return;
   }
   int i0[3], i1[3];
@@ -119,7 +125,7 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
     const double x11 = dlerp((double)ld_f(in, q011), (double)ld_f(in, q111), t[0]);
     st_v(*v, dlerp(dlerp(x00, x10, t[1]), dlerp(x01, x11, t[1]), t[2]));
   }
-  if (MSK) {
+  if (mread) {
     const uint8_t *p = a.inm;
     const uint8_t m000 = __ldg(p + q000), m100 = __ldg(p + q100), m010 = __ldg(p + q010),
                   m110 = __ldg(p + q110), m001 = __ldg(p + q001), m101 = __ldg(p + q101),
@@ -228,7 +234,7 @@ __global__ void __launch_bounds__(256, 3) resample_batch_kernel(const ResampleJo
   for (int i = 0; i < 9; ++i) a.C[i] = j.C[i];
 #pragma unroll
   for (int i = 0; i < 3; ++i) a.e[i] = j.e[i];
-  a.out = j.out; a.outm = j.outm; a.nearest = 0;
+  a.out = j.out; a.outm = j.outm; a.nearest = 0; a.mask_ones = j.mask_ones;
   const long long g0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long gs = (long long)gridDim.x * blockDim.x;
   if (!a.in || !a.out) {
@@ -268,9 +274,10 @@ void launch_rs(const ResampleArgs &a, unsigned blocks, cudaStream_t s) {
 mirorr_status launch_resample(const int in_size[3], const void *in, const uint8_t *in_mask,
                               const int out_size[3], const ResampleMap &map, void *out,
                               uint8_t *out_mask, cudaStream_t s, bool nearest, int in_dtype,
-                              int out_dtype) {
+                              int out_dtype, bool mask_ones) {
   ResampleArgs a;
   a.nearest = nearest ? 1 : 0;
+  a.mask_ones = mask_ones ? 1 : 0;
   a.in = in; a.inm = in_mask;
   a.inx = in_size[0]; a.iny = in_size[1]; a.inz = in_size[2];
   a.onx = out_size[0]; a.ony = out_size[1]; a.onz = out_size[2];
