@@ -409,6 +409,13 @@ MIRORR_API int64_t mirorr_ctx_kernel_launches(mirorr_ctx ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events against the library's. */
 MIRORR_API void *mirorr_ctx_stream(mirorr_ctx ctx);
+/* Iteration graphs of float32 registrations on (default) or off: the first
+ * iteration of each pyramid level runs its launches directly, the others
+ * replay one CUDA graph of them captured for the level (the same kernels and
+ * arithmetic; the transforms and the fit state travel through pinned
+ * staging).  Off: every iteration launches directly.  Profiling
+ * (mirorr_ctx_set_profiling) and verbosity >= 2 run directly regardless. */
+MIRORR_API mirorr_status mirorr_ctx_set_graphs(mirorr_ctx ctx, int32_t on);
 /* Per-stage timing of the matcher calls made by registrations: when enabled,
  * CUDA events bracket each stage; mirorr_ctx_stage_times returns the
  * accumulated milliseconds of [box statistics, variance selection, NCC

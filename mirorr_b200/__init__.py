@@ -231,6 +231,7 @@ def lib():
         "mirorr_batch_info": [vp, vp],
         "mirorr_batch_set_graphs": [vp, ctypes.c_int32],
         "mirorr_batch_times": [vp, vp],
+        "mirorr_ctx_set_graphs": [vp, ctypes.c_int32],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -298,6 +299,10 @@ class Context:
 
     def set_profiling(self, on: bool):
         _check(lib().mirorr_ctx_set_profiling(self._h, 1 if on else 0))
+
+    def set_graphs(self, on: bool):
+        """Iteration graphs of float32 registrations on (default) or off."""
+        _check(lib().mirorr_ctx_set_graphs(self._h, 1 if on else 0))
 
     def stage_times(self):
         """(ms[box_stats, selection, ncc, postfilter], matcher calls) since the last read."""

@@ -155,6 +155,18 @@ struct mirorr_ctx_s {
   DevBuf best, second, match, status;
   DevBuf pts_i, pts_m;
   DevBuf up_f, up_m, up_fm, up_mm;
+  // iteration graphs of the float32 registration: the resampling jobs and the
+  // fit's state travel through pinned staging; one executable graph per
+  // pyramid level, kept for the next registration while its key (geometry,
+  // parameters, every buffer its launches address) is unchanged
+  HostBuf it_jobs, it_lts_in, it_lts_out;
+  DevBuf it_jobs_d;
+  bool graphs = true;
+  struct LevelGraph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+  };
+  LevelGraph lgraph[16];
 };
 
 struct Vol {
@@ -569,6 +581,147 @@ mirorr_status resample_into(mirorr_ctx c, const RegImage &src, const uint8_t *ma
   return MIRORR_OK;
 }
 
+// The resampling jobs resample_into launches for (src, mask) onto grid through
+// t, appended to jobs[nj..]: one image + mask job on a shared input grid,
+// else an image job and a mask job (float32 images only).
+mirorr_status make_jobs(mirorr_ctx c, const RegImage &src, const uint8_t *mask,
+                        const mirorr_geometry &mask_g, const mirorr_geometry &grid, const Tfm &t,
+                        DevBuf &img, DevBuf &msk, int out_dtype, ResampleJob *jobs, int &nj) {
+  ResampleMap mi, mm;
+  if (!make_map(grid, src.g, t.M, t.off, mi) || !make_map(grid, mask_g, t.M, t.off, mm)) {
+    set_error("singular image geometry");
+    return MIRORR_EINVAL;
+  }
+  const bool same_grid = src.g.size[0] == mask_g.size[0] && src.g.size[1] == mask_g.size[1] &&
+                         src.g.size[2] == mask_g.size[2] && memcmp(&mi, &mm, sizeof(mi)) == 0;
+  const int ones = c->ones.ptr && mask == c->ones.as<uint8_t>() ? 1 : 0;
+  ResampleJob &j = jobs[nj++];
+  memset(&j, 0, sizeof(j));
+  j.in = static_cast<const float *>(src.img);
+  j.out = img.ptr;
+  for (int d = 0; d < 3; ++d) { j.in_size[d] = src.g.size[d]; j.out_size[d] = grid.size[d]; }
+  memcpy(j.C, mi.C, sizeof(mi.C));
+  memcpy(j.e, mi.e, sizeof(mi.e));
+  j.out_dtype = out_dtype;
+  j.active = 1;
+  if (same_grid) {
+    j.inm = mask;
+    j.outm = msk.as<uint8_t>();
+    j.mask_ones = ones;
+    return MIRORR_OK;
+  }
+  ResampleJob &k = jobs[nj++];
+  memset(&k, 0, sizeof(k));
+  k.inm = mask;
+  k.outm = msk.as<uint8_t>();
+  for (int d = 0; d < 3; ++d) { k.in_size[d] = mask_g.size[d]; k.out_size[d] = grid.size[d]; }
+  memcpy(k.C, mm.C, sizeof(mm.C));
+  memcpy(k.e, mm.e, sizeof(mm.e));
+  k.active = 1;
+  k.mask_ones = ones;
+  return MIRORR_OK;
+}
+
+// An iteration's launches captured once per pyramid level and replayed for
+// its later iterations, and for the same level of later registrations while
+// the key is unchanged (float32 storage, no profiling, no per-call printing).
+// The key: the level, the middle space and block grid, the parameters baked
+// into the launches, and the address and size of every buffer they touch.
+std::vector<uint64_t> level_key(mirorr_ctx c, const RegRun &r, const mirorr_geometry &grid,
+                                const BmGeom &g, int nj) {
+  std::vector<uint64_t> k;
+  auto add = [&](uint64_t v) { k.push_back(v); };
+  auto buf = [&](const DevBuf &b) {
+    add(reinterpret_cast<uint64_t>(b.ptr));
+    add(b.bytes);
+  };
+  add((uint64_t)r.level);
+  add((uint64_t)r.p->symmetric);
+  add((uint64_t)nj);
+  for (int d = 0; d < 3; ++d) add((uint64_t)grid.size[d]);
+  uint64_t gb[sizeof(BmGeom) / 8 + 1] = {0};
+  memcpy(gb, &g, sizeof(BmGeom));
+  for (uint64_t v : gb) add(v);
+  uint64_t pb[sizeof(mirorr_bm_params) / 8 + 1] = {0};
+  memcpy(pb, &r.p->bm, sizeof(mirorr_bm_params));
+  for (uint64_t v : pb) add(v);
+  const DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
+                          &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl,
+                          &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->bmw.ncc_pad, &c->bmw.ncc_wand,
+                          &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best, &c->second,
+                          &c->match, &c->status, &c->pts_i, &c->pts_m, &c->counts, &c->ncc_count,
+                          &c->xl_count, &c->ltsw.state, &c->ltsw.resid, &c->ltsw.partial,
+                          &c->ltsw.hist, &c->ltsw.ctrl, &c->ltsw.cand, &c->it_jobs_d};
+  for (const DevBuf *b : bufs) buf(*b);
+  add(reinterpret_cast<uint64_t>(c->it_jobs.ptr));
+  add(reinterpret_cast<uint64_t>(c->it_lts_in.ptr));
+  add(reinterpret_cast<uint64_t>(c->it_lts_out.ptr));
+  add((uint64_t)c->ltsw.max_ctas);
+  add((uint64_t)c->ltsw.spin_limit);
+  return k;
+}
+
+bool iteration_graphs(const RegRun &r) {
+  return r.c->graphs && r.p->storage == MIRORR_DTYPE_F32 && !r.c->timer.on && r.p->verbosity < 2;
+}
+
+// Captures issue() on the context's stream into the level's graph, replacing
+// the one kept there (the capture always ends).
+template <class F>
+mirorr_status capture_iteration(mirorr_ctx c, int level, std::vector<uint64_t> key, F issue) {
+  auto &g = c->lgraph[level];
+  if (g.exec) {
+    cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+  }
+  g.key.clear();
+  MB2_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const mirorr_status rs = issue();
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  if (rs != MIRORR_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rs;
+  }
+  if (e != cudaSuccess) {
+    set_error("capturing a registration iteration failed: %s", cudaGetErrorString(e));
+    return MIRORR_ECUDA;
+  }
+  e = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g.exec = nullptr;
+    set_error("instantiating a registration iteration failed: %s", cudaGetErrorString(e));
+    return MIRORR_ECUDA;
+  }
+  g.key = std::move(key);
+  return MIRORR_OK;
+}
+
+// After a replayed iteration: the fit's results, as run_lts reports them.
+mirorr_status collect_lts(RegRun &r, LtsState &hs, long long *n_used) {
+  mirorr_ctx c = r.c;
+  unsigned int gave_up = 0;
+  int inner = 0;
+  MB2_TRY(lts_collect(c->ltsw, c->it_lts_out.ptr, hs, &inner, n_used, &gave_up));
+  if (gave_up) {
+    bool to = false;
+    MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
+    set_error("a bounded wait on a tensor copy of the NCC search gave up");
+    return MIRORR_ETIMEOUT;
+  }
+  if (r.stats) {
+    r.stats->h2d_bytes += (int64_t)sizeof(LtsState);
+    r.stats->d2h_bytes += (int64_t)(sizeof(LtsState) + 2 * sizeof(long long) + 32);
+  }
+  if (*n_used == 0) {
+    set_error("No block matches occurred. Images probably have zero overlap. "
+              "Try supplying a better initial transform.");
+    return MIRORR_ENOBLOCKS;
+  }
+  return MIRORR_OK;
+}
+
 mirorr_status run_lts(RegRun &r, LtsState &hs, long long nmax, long long *n_used) {
   int inner = 0;
   mirorr_ctx c = r.c;
@@ -680,12 +833,8 @@ mirorr_status classic_level(RegRun &r, const RegImage &fl, const RegImage &ml, T
   tfm_params(tfm, last);
   int np = tfm_nparams(tfm);
   int it = 0;
+  const bool graphs = iteration_graphs(r) && r.level < 16;
   for (; it < std::abs(p.iterations); ++it) {
-    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, tfm, c->img_s, c->msk_s, p.storage));
-    MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
-    MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
-                       c->msk_s.as<uint8_t>(), grid_m, c->pts_i.as<double>(),
-                       c->pts_m.as<double>(), 0, nullptr));
     LtsState hs;
     memset(&hs, 0, sizeof(hs));
     hs.kind = tfm.kind;
@@ -693,7 +842,49 @@ mirorr_status classic_level(RegRun &r, const RegImage &fl, const RegImage &ml, T
     hs.lts_keep = p.lts_keep;
     hs.tfm = tfm;
     long long used = 0;
-    MB2_TRY(run_lts(r, hs, g.nblocks, &used));
+    // the level's graph: kept from an earlier iteration or registration when
+    // its key matches; else captured at the second iteration (the first one
+    // runs directly and sizes every buffer)
+    int nj = 0;
+    std::vector<uint64_t> key;
+    bool use_graph = false;
+    if (graphs) {
+      ResampleJob *jobs = c->it_jobs.as<ResampleJob>();
+      MB2_TRY(make_jobs(c, fl, r.fmask, r.fmask_g, grid_f, tfm, c->img_s, c->msk_s, p.storage, jobs, nj));
+      key = level_key(c, r, grid_f, g, nj);
+      use_graph = (c->lgraph[r.level].exec && c->lgraph[r.level].key == key) || it > 0;
+    }
+    if (use_graph) {
+      lts_begin(hs);
+      memcpy(c->it_lts_in.ptr, &hs, sizeof(hs));
+      if (!c->lgraph[r.level].exec || c->lgraph[r.level].key != key) {
+        const int64_t calls0 = r.stats ? r.stats->matcher_calls : 0;
+        MB2_TRY(capture_iteration(c, r.level, key, [&]() -> mirorr_status {
+          MB2_CUDA_TRY(cudaMemcpyAsync(c->it_jobs_d.ptr, c->it_jobs.ptr, sizeof(ResampleJob) * nj,
+                                       cudaMemcpyHostToDevice, c->stream));
+          MB2_TRY(launch_resample_batch(c->it_jobs_d.as<ResampleJob>(), nj, vox(grid_f.size), c->stream));
+          MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
+          MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
+                             c->msk_s.as<uint8_t>(), grid_m, c->pts_i.as<double>(),
+                             c->pts_m.as<double>(), 0, nullptr));
+          return lts_issue(c->ltsw, c->it_lts_in.as<LtsState>(), c->pts_i.as<double>(),
+                           c->pts_m.as<double>(), c->counts.as<long long>(), g.nblocks, c->stream,
+                           c->it_lts_out.ptr, ncc_timeout_flag(c->bmw));
+        }));
+        if (r.stats) r.stats->matcher_calls = calls0;
+      }
+      MB2_CUDA_TRY(cudaGraphLaunch(c->lgraph[r.level].exec, c->stream));
+      MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      if (r.stats) r.stats->matcher_calls += 1;
+      MB2_TRY(collect_lts(r, hs, &used));
+    } else {
+      MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, tfm, c->img_s, c->msk_s, p.storage));
+      MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
+      MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
+                         c->msk_s.as<uint8_t>(), grid_m, c->pts_i.as<double>(),
+                         c->pts_m.as<double>(), 0, nullptr));
+      MB2_TRY(run_lts(r, hs, g.nblocks, &used));
+    }
     tfm = hs.tfm;
     tfm_params(tfm, cur);
     double d = param_delta(last, cur, np);
@@ -755,20 +946,11 @@ mirorr_status symmetric_level(RegRun &r, const RegImage &fl, const RegImage &ml,
     tfm_compose(cB, moving_tr, false);
   };
   int it = 0;
+  const bool graphs = iteration_graphs(r) && r.level < 16;
   for (; it < std::abs(p.iterations); ++it) {
     Tfm cF, cB;
     centered(cF, cB);
-    MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, cB, c->img_b, c->msk_b, p.storage));
-    MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, cF, c->img_s, c->msk_s, p.storage));
-    MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
     double *pi = c->pts_i.as<double>(), *pmv = c->pts_m.as<double>();
-    // forward: base = moving, search = fixed
-    MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
-                       c->msk_s.as<uint8_t>(), grid_m, pi, pmv, 0, nullptr));
-    // swapped: base = fixed, search = moving; its lists are appended with
-    // roles reversed (itkSymMirorrRegistrationMethod.txx:595-602)
-    MB2_TRY(match_into(r, c->img_s.ptr, c->msk_s.as<uint8_t>(), c->img_b.ptr,
-                       c->msk_b.as<uint8_t>(), grid_f, pmv, pi, 1, c->counts.as<long long>()));
     LtsState hs;
     memset(&hs, 0, sizeof(hs));
     hs.kind = tfm.kind;
@@ -778,7 +960,55 @@ mirorr_status symmetric_level(RegRun &r, const RegImage &fl, const RegImage &ml,
     hs.t12f = t12f;
     hs.t12b = t12b;
     long long used = 0;
-    MB2_TRY(run_lts(r, hs, 2 * g.nblocks, &used));
+    // the level's graph: kept from an earlier iteration or registration when
+    // its key matches; else captured at the second iteration (the first one
+    // runs directly and sizes every buffer)
+    int nj = 0;
+    std::vector<uint64_t> key;
+    bool use_graph = false;
+    if (graphs) {
+      ResampleJob *jobs = c->it_jobs.as<ResampleJob>();
+      MB2_TRY(make_jobs(c, ml, r.mmask, r.mmask_g, grid_m, cB, c->img_b, c->msk_b, p.storage, jobs, nj));
+      MB2_TRY(make_jobs(c, fl, r.fmask, r.fmask_g, grid_f, cF, c->img_s, c->msk_s, p.storage, jobs, nj));
+      key = level_key(c, r, grid_f, g, nj);
+      use_graph = (c->lgraph[r.level].exec && c->lgraph[r.level].key == key) || it > 0;
+    }
+    if (use_graph) {
+      lts_begin(hs);
+      memcpy(c->it_lts_in.ptr, &hs, sizeof(hs));
+      if (!c->lgraph[r.level].exec || c->lgraph[r.level].key != key) {
+        const int64_t calls0 = r.stats ? r.stats->matcher_calls : 0;
+        MB2_TRY(capture_iteration(c, r.level, key, [&]() -> mirorr_status {
+          MB2_CUDA_TRY(cudaMemcpyAsync(c->it_jobs_d.ptr, c->it_jobs.ptr, sizeof(ResampleJob) * nj,
+                                       cudaMemcpyHostToDevice, c->stream));
+          MB2_TRY(launch_resample_batch(c->it_jobs_d.as<ResampleJob>(), nj, vox(grid_f.size), c->stream));
+          MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
+          MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
+                             c->msk_s.as<uint8_t>(), grid_m, pi, pmv, 0, nullptr));
+          MB2_TRY(match_into(r, c->img_s.ptr, c->msk_s.as<uint8_t>(), c->img_b.ptr,
+                             c->msk_b.as<uint8_t>(), grid_f, pmv, pi, 1, c->counts.as<long long>()));
+          return lts_issue(c->ltsw, c->it_lts_in.as<LtsState>(), pi, pmv, c->counts.as<long long>(),
+                           2 * g.nblocks, c->stream, c->it_lts_out.ptr, ncc_timeout_flag(c->bmw));
+        }));
+        if (r.stats) r.stats->matcher_calls = calls0;
+      }
+      MB2_CUDA_TRY(cudaGraphLaunch(c->lgraph[r.level].exec, c->stream));
+      MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      if (r.stats) r.stats->matcher_calls += 2;
+      MB2_TRY(collect_lts(r, hs, &used));
+    } else {
+      MB2_TRY(resample_into(c, ml, r.mmask, r.mmask_g, grid_m, cB, c->img_b, c->msk_b, p.storage));
+      MB2_TRY(resample_into(c, fl, r.fmask, r.fmask_g, grid_f, cF, c->img_s, c->msk_s, p.storage));
+      MB2_CUDA_TRY(cudaMemsetAsync(c->counts.ptr, 0, 4 * sizeof(long long), c->stream));
+      // forward: base = moving, search = fixed
+      MB2_TRY(match_into(r, c->img_b.ptr, c->msk_b.as<uint8_t>(), c->img_s.ptr,
+                         c->msk_s.as<uint8_t>(), grid_m, pi, pmv, 0, nullptr));
+      // swapped: base = fixed, search = moving; its lists are appended with
+      // roles reversed (itkSymMirorrRegistrationMethod.txx:595-602)
+      MB2_TRY(match_into(r, c->img_s.ptr, c->msk_s.as<uint8_t>(), c->img_b.ptr,
+                         c->msk_b.as<uint8_t>(), grid_f, pmv, pi, 1, c->counts.as<long long>()));
+      MB2_TRY(run_lts(r, hs, 2 * g.nblocks, &used));
+    }
     tfm = hs.tfm;
     t12f = hs.t12f;
     t12b = hs.t12b;
@@ -832,6 +1062,10 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const void 
   if (pp.min_length <= 0) pp.min_length = 32;
   MB2_TRY(c->counts.ensure(4 * sizeof(long long)));
   MB2_TRY(c->ncc_count.ensure(sizeof(unsigned long long)));
+  MB2_TRY(c->it_jobs.ensure(sizeof(ResampleJob) * 4));
+  MB2_TRY(c->it_jobs_d.ensure(sizeof(ResampleJob) * 4));
+  MB2_TRY(c->it_lts_in.ensure(sizeof(LtsState)));
+  MB2_TRY(c->it_lts_out.ensure(lts_out_bytes()));
   MB2_CUDA_TRY(cudaMemsetAsync(c->ncc_count.ptr, 0, sizeof(unsigned long long), c->stream));
   if (stats) memset(stats, 0, sizeof(*stats));
   long long nmax = std::max(vox(fg->size), vox(mg->size));
@@ -941,8 +1175,12 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
                     &c->second, &c->match, &c->status, &c->pts_i, &c->pts_m, &c->up_f,
                     &c->up_m, &c->up_fm, &c->up_mm, &c->bm16.stats, &c->bm16.wand,
                     &c->bm16.prep, &c->bm16.xs, &c->bm16.ctl, &c->bm16.fb_list,
-                    &c->bm16.chunked, &c->bm16.calls};
+                    &c->bm16.chunked, &c->bm16.calls, &c->it_jobs_d};
   for (DevBuf *b : bufs) b->release();
+  HostBuf *hbufs[] = {&c->it_jobs, &c->it_lts_in, &c->it_lts_out, &c->ltsw.out};
+  for (HostBuf *b : hbufs) b->release();
+  for (auto &lg : c->lgraph)
+    if (lg.exec) cudaGraphExecDestroy(lg.exec);
   c->timer.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -952,6 +1190,12 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
 int64_t mirorr_ctx_kernel_launches(mirorr_ctx c) { return c ? g_launches - c->launches0 : g_launches; }
 
 void *mirorr_ctx_stream(mirorr_ctx c) { return c ? (void *)c->stream : nullptr; }
+
+mirorr_status mirorr_ctx_set_graphs(mirorr_ctx c, int32_t on) {
+  if (!c) { set_error("null argument"); return MIRORR_EINVAL; }
+  c->graphs = on != 0;
+  return MIRORR_OK;
+}
 
 mirorr_status mirorr_ctx_set_profiling(mirorr_ctx c, int32_t on) {
   if (!c) { set_error("null argument"); return MIRORR_EINVAL; }

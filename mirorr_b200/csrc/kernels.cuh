@@ -255,7 +255,20 @@ struct LtsWork {
   DevBuf cand;      // candidate keys
   int max_ctas = 0;
   long long spin_limit = 0;  // grid-barrier polls before giving up (0: the default)
+  HostBuf out;               // pinned read-back of an uncaptured fit (lts_out_bytes)
 };
+// A fit in two halves, so that a captured sequence can hold the first: lts_issue
+// enqueues the upload of *state_in (after lts_begin), the cooperative launch
+// and the read-back of the state, the barrier control and the point counts
+// (and *watch_dev when given) into out_host (lts_out_bytes() bytes of host
+// memory, pinned when captured; null: the work area's own); lts_collect, after
+// the stream has synchronised, takes them into hs (lts_finish applied).
+size_t lts_out_bytes();
+mirorr_status lts_issue(LtsWork &w, const LtsState *state_in, const double *init_dev,
+                        const double *moved_dev, const long long *n_dev, long long n,
+                        cudaStream_t st, void *out_host, const unsigned int *watch_dev);
+mirorr_status lts_collect(LtsWork &w, const void *out_host, LtsState &hs, int *inner_iters,
+                          long long *n_used, unsigned int *watch_host);
 // n_dev: two device counters whose sum is the number of point pairs; n_max is
 // an upper bound used for sizing.  Runs lts_begin / the inner loop /
 // lts_finish on host_state.  watch_dev (optional): a device word read back in

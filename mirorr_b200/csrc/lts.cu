@@ -430,6 +430,25 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
     if (n_used) *n_used = 0;
     return MIRORR_OK;
   }
+  MB2_TRY(lts_issue(w, &hs, init_dev, moved_dev, n_dev, n, st, nullptr, watch_dev));
+  MB2_CUDA_TRY(cudaStreamSynchronize(st));
+  return lts_collect(w, nullptr, hs, inner_iters, n_used, watch_host);
+}
+
+// What lts_issue reads back, in host memory (pinned staging for a captured
+// sequence, or the work area's own copy).
+struct LtsOut {
+  LtsState state;
+  LtsCtl ctl;
+  long long n[2];
+  unsigned int watch;
+};
+
+size_t lts_out_bytes() { return sizeof(LtsOut); }
+
+mirorr_status lts_issue(LtsWork &w, const LtsState *state_in, const double *init_dev,
+                        const double *moved_dev, const long long *n_dev, long long n,
+                        cudaStream_t st, void *out_host, const unsigned int *watch_dev) {
   int dev = 0;
   MB2_CUDA_TRY(cudaGetDevice(&dev));
   if (w.max_ctas == 0) {
@@ -455,7 +474,12 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
   MB2_TRY(w.hist.ensure(sizeof(unsigned int) * 3 * kBins));
   MB2_TRY(w.ctrl.ensure(sizeof(LtsCtl)));
   MB2_TRY(w.cand.ensure(sizeof(unsigned long long) * kCandMax));
-  MB2_CUDA_TRY(cudaMemcpyAsync(w.state.ptr, &hs, sizeof(LtsState), cudaMemcpyHostToDevice, st));
+  if (!out_host) {
+    MB2_TRY(w.out.ensure(sizeof(LtsOut)));
+    out_host = w.out.ptr;
+  }
+  LtsOut *o = static_cast<LtsOut *>(out_host);
+  MB2_CUDA_TRY(cudaMemcpyAsync(w.state.ptr, state_in, sizeof(LtsState), cudaMemcpyHostToDevice, st));
   MB2_CUDA_TRY(cudaMemsetAsync(w.hist.ptr, 0, sizeof(unsigned int) * 3 * kBins, st));
   MB2_CUDA_TRY(cudaMemsetAsync(w.ctrl.ptr, 0, sizeof(LtsCtl), st));
   LtsArgs a;
@@ -472,17 +496,23 @@ mirorr_status lts_run(LtsWork &w, LtsState &hs, const double *init_dev, const do
   void *args[] = {&a};
   MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)lts_kernel, dim3(grid), dim3(kThreads), args, 0, st));
   ++g_launches;
-  LtsCtl ctl;
-  long long nn[2] = {0, 0};
-  MB2_CUDA_TRY(cudaMemcpyAsync(&hs, w.state.ptr, sizeof(LtsState), cudaMemcpyDeviceToHost, st));
-  MB2_CUDA_TRY(cudaMemcpyAsync(&ctl, w.ctrl.ptr, sizeof(LtsCtl), cudaMemcpyDeviceToHost, st));
-  MB2_CUDA_TRY(cudaMemcpyAsync(nn, n_dev, sizeof(nn), cudaMemcpyDeviceToHost, st));
-  if (watch_dev && watch_host)
-    MB2_CUDA_TRY(cudaMemcpyAsync(watch_host, watch_dev, sizeof(unsigned int),
-                                 cudaMemcpyDeviceToHost, st));
-  MB2_CUDA_TRY(cudaStreamSynchronize(st));
-  if (n_used) *n_used = nn[0] + nn[1];
-  if (ctl.err) {
+  MB2_CUDA_TRY(cudaMemcpyAsync(&o->state, w.state.ptr, sizeof(LtsState), cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(&o->ctl, w.ctrl.ptr, sizeof(LtsCtl), cudaMemcpyDeviceToHost, st));
+  MB2_CUDA_TRY(cudaMemcpyAsync(o->n, n_dev, sizeof(o->n), cudaMemcpyDeviceToHost, st));
+  if (watch_dev)
+    MB2_CUDA_TRY(cudaMemcpyAsync(&o->watch, watch_dev, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+  else
+    o->watch = 0;
+  return MIRORR_OK;
+}
+
+mirorr_status lts_collect(LtsWork &w, const void *out_host, LtsState &hs, int *inner_iters,
+                          long long *n_used, unsigned int *watch_host) {
+  const LtsOut *o = static_cast<const LtsOut *>(out_host ? out_host : w.out.ptr);
+  hs = o->state;
+  if (watch_host) *watch_host = o->watch;
+  if (n_used) *n_used = o->n[0] + o->n[1];
+  if (o->ctl.err) {
     set_error("LTS grid barrier timed out");
     return MIRORR_ETIMEOUT;
   }
