@@ -24,8 +24,14 @@ Arms:
                 resampler and loop) running full registrations of the same pair
                 on all host cores, as many as fit a time budget.
 
-Profiling legs (`--leg matcher|resample`): one finest-level matcher call or
-the final-resampling interpolators on the same pair, for ncu captures.
+Profiling legs (`--leg ...`), for ncu captures on one GPU:
+  matcher        one finest-level matcher call (--masked, --base-masked add
+                 field-of-view masks);
+  matcher16      the same call with 16-bit storage beside float32;
+  selector       the variance selection stage (block keep 0.5);
+  resample-pass  one finest-level image + mask resampling pass;
+  resample       the final-resampling interpolators through host buffers;
+  batched, large the batched/served and large-configuration legs alone.
 
 Multi-GPU: registrations are independent, so N ranks run N replicas, each its
 own pair (weak scaling, no collective on the data path).
@@ -387,7 +393,7 @@ def selector_leg(mb, ctx, ph, hbm_peak, peak_src, calls=5):
     ms = statistics.median(ts)
     nbytes = 4 * ph.moving.size + 8 * nb
     gbs = nbytes / (ms / 1e3) / 1e9
-    return {"kernel": "variance selection (block_variance_kernel + radix select passes)",
+    return {"kernel": "variance selection (select_kernel: variances, radix select and flags in one cooperative launch)",
             "bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(gbs / hbm_peak, 4), "ms_per_call": round(ms, 4), "blocks": nb,
             "algorithmic_bytes": int(nbytes), "block_keep": 0.5,
@@ -833,6 +839,17 @@ def run_leg(args):
                           "ms_postfilter": ts[-1][3], "diag": [int(v) for v in d]}
             m.close()
         print(json.dumps(res))
+    elif args.leg in ("selector", "resample-pass"):
+        # the variance selection stage (keep 0.5) or one finest-level image +
+        # mask resampling pass, with their HBM rooflines
+        import torch
+        peaks, peak_src = load_peaks()
+        hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+        if args.leg == "selector":
+            print(json.dumps(selector_leg(mb, ctx, ph, hbm_peak, peak_src, calls=args.calls)))
+        else:
+            print(json.dumps(resample_finest_leg(mb, ctx, ph, torch.cuda.current_device(),
+                                                 hbm_peak, peak_src, reps=args.calls)))
     elif args.leg == "batched":
         pairs = c2_pairs(n=args.calls)
         out = {"batched": c2_leg(mb, ctx, 0, pairs, oracle_pairs=1)}
@@ -880,7 +897,8 @@ def main():
                     help="skip the FP64 oracle registration (parity and CPU baseline)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched (64 uneven pairs) and served (Poisson) legs")
-    ap.add_argument("--leg", choices=["matcher", "matcher16", "resample", "batched", "large"],
+    ap.add_argument("--leg", choices=["matcher", "matcher16", "resample", "resample-pass",
+                                      "selector", "batched", "large"],
                     default=None)
     ap.add_argument("--store", default="bf16")
     ap.add_argument("--radius", type=int, default=3)

@@ -15,8 +15,10 @@
 //                   deterministic raster-order compaction and block -> mm points
 //                   (itkAbstractBlockMatcher.h:271-287).
 #include <cuda_bf16.h>
+#include <type_traits>
 #include <cuda_fp16.h>
 
+#include "gridsel.cuh"
 #include "kernels.cuh"
 
 namespace mb2 {
@@ -52,20 +54,22 @@ void point_geom(const double origin[3], const double spacing[3], const double di
 // ---------------------------------------------------------------------------
 // 1. box statistics
 // ---------------------------------------------------------------------------
-// Each thread computes PX consecutive x positions of one row: every footprint
-// row of PX + BW - 1 floats is loaded once and serves all PX positions.  Per
-// position the statistics are the two-pass ones of normalizedCorrelation
-// (mean over all voxels, then the masked sum of squares,
-// itkBlockMatcher.txx:57-95).  The mean is an FP64 sum (exact for float
-// inputs of ordinary range, so a flat footprint's mean is its value); the
-// sum of squares is taken in FP32 about the FP32 mean.  They feed the FP32
-// search only, where the one decision that must be exact is Syy = 0.  When
-// the FP64 mean is a float, a masked voxel differs from it in FP32 exactly
-// when it does in FP64; otherwise an FP32 sum of at least 1e-30 implies a
-// non-zero FP64 one, and below that the position is recomputed with the FP64
-// two-pass sum, zero exactly when every masked voxel equals the mean, as in
-// the reference.
-constexpr int kBoxPX = 4;
+// Each thread computes PZ consecutive z positions of one (x, y) column, and
+// the lanes of a warp take consecutive x: every footprint row load is a
+// coalesced warp-wide read, and each of the PZ + BW - 1 window planes' rows is
+// loaded once for all PZ positions.  Per position the statistics are the
+// two-pass ones of normalizedCorrelation (mean over all voxels, then the
+// masked sum of squares, itkBlockMatcher.txx:57-95), both accumulated in the
+// reference's raster order (vz, vy, vx) whatever the interleaving across
+// positions.  The mean is an FP64 sum (exact for float inputs of ordinary
+// range, so a flat footprint's mean is its value); the sum of squares is
+// taken in FP32 about the FP32 mean.  They feed the FP32 search only, where
+// the one decision that must be exact is Syy = 0.  When the FP64 mean is a
+// float, a masked voxel differs from it in FP32 exactly when it does in FP64;
+// otherwise an FP32 sum of at least 1e-30 implies a non-zero FP64 one, and
+// below that the position is recomputed with the FP64 two-pass sum, zero
+// exactly when every masked voxel equals the mean, as in the reference.
+constexpr int kBoxPZ = 8;
 
 // FP64 masked sum of squares about mean of the footprint at linear index o
 // (raster order, fused multiply-adds); the footprint lies inside the volume.
@@ -90,107 +94,109 @@ template <int BW>
 __global__ void __launch_bounds__(256) box_stats_kernel(const float *__restrict__ y,
                                                         const uint8_t *__restrict__ ms, int nx,
                                                         int ny, int nz, float2 *__restrict__ out) {
-  constexpr int PX = kBoxPX, RL = PX + BW - 1;
-  const int ngx = (nx + PX - 1) / PX;
-  const long long n = (long long)ngx * ny * nz;
+  constexpr int PZ = kBoxPZ, NP = PZ + BW - 1;
+  const int ngz = (nz + PZ - 1) / PZ;
+  const long long n = (long long)nx * ny * ngz;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
        p += (long long)gridDim.x * blockDim.x) {
-    int gx, yy, z;
-    split3(p, ngx, ny, gx, yy, z);
-    const int x0 = gx * PX;
-    const long long o = ((long long)z * ny + yy) * nx + x0;
-    const bool rowok = yy <= ny - BW && z <= nz - BW;
-    double sum[PX], mean[PX], ss[PX];
-    bool all_in[PX], ok[PX];
+    int x, yy, gz;
+    split3(p, nx, ny, x, yy, gz);
+    const int z0 = gz * PZ;
+    const long long o = ((long long)z0 * ny + yy) * nx + x;
+    const long long plane = (long long)nx * ny;
+    const bool colok = x <= nx - BW && yy <= ny - BW;
+    // planes z0 .. zend - 1 are read; positions z0 + j <= nz - BW are valid
+    const int zend = min(z0 + NP, nz);
+    double sum[PZ], mean[PZ];
+    float s32[PZ];
+    bool all_in[PZ], any_in[PZ], ok[PZ];
 #pragma unroll
-    for (int j = 0; j < PX; ++j) {
+    for (int j = 0; j < PZ; ++j) {
       sum[j] = 0.0;
-      ss[j] = 0.0;
+      s32[j] = 0.f;
       all_in[j] = true;
-      ok[j] = rowok && x0 + j <= nx - BW;
+      any_in[j] = false;
+      ok[j] = colok && z0 + j <= nz - BW;
     }
-    if (rowok && x0 <= nx - BW) {
+    if (ok[0]) {
 #pragma unroll
-      for (int vz = 0; vz < BW; ++vz)
-#pragma unroll
-        for (int vy = 0; vy < BW; ++vy) {
-          const float *r = y + o + ((long long)vz * ny + vy) * nx;
-          float v[RL];
-#pragma unroll
-          for (int i = 0; i < RL; ++i) v[i] = (x0 + i < nx) ? __ldg(r + i) : 0.f;
-#pragma unroll
-          for (int vx = 0; vx < BW; ++vx)
-#pragma unroll
-            for (int j = 0; j < PX; ++j) sum[j] = __dadd_rn(sum[j], (double)v[j + vx]);
-        }
-      constexpr int B = BW * BW * BW;
-#pragma unroll
-      for (int j = 0; j < PX; ++j)
-        mean[j] = (B & (B - 1)) == 0 ? sum[j] * (1.0 / B) : __ddiv_rn(sum[j], (double)B);
-      float mu[PX], s32[PX];
-#pragma unroll
-      for (int j = 0; j < PX; ++j) { mu[j] = (float)mean[j]; s32[j] = 0.f; }
-      // mask columns of the PX + BW - 1 wide footprint rows: in the mask in
-      // every row (allb) and in some row (anyb)
-      unsigned int allb = ~0u, anyb = 0u;
-#pragma unroll
-      for (int vz = 0; vz < BW; ++vz)
+      for (int wz = 0; wz < NP; ++wz) {
+        if (z0 + wz >= zend) break;
 #pragma unroll
         for (int vy = 0; vy < BW; ++vy) {
-          const long long q = o + ((long long)vz * ny + vy) * nx;
-          float v[RL];
-          bool m[RL];
-          unsigned int mb = 0u;
+          const float *r = y + o + wz * plane + (long long)vy * nx;
+          float v[BW];
 #pragma unroll
-          for (int i = 0; i < RL; ++i) {
-            const bool in = x0 + i < nx;
-            v[i] = in ? __ldg(y + q + i) : 0.f;
-            m[i] = in && __ldg(ms + q + i) != 0;
-            mb |= (m[i] ? 1u : 0u) << i;
+          for (int vx = 0; vx < BW; ++vx) v[vx] = __ldg(r + vx);
+#pragma unroll
+          for (int j = 0; j < PZ; ++j) {
+            const int vz = wz - j;
+            if (vz < 0 || vz >= BW) continue;
+#pragma unroll
+            for (int vx = 0; vx < BW; ++vx) sum[j] = __dadd_rn(sum[j], (double)v[vx]);
           }
-          allb &= mb;
-          anyb |= mb;
-#pragma unroll
-          for (int vx = 0; vx < BW; ++vx)
-#pragma unroll
-            for (int j = 0; j < PX; ++j) {
-              const float d = m[j + vx] ? v[j + vx] - mu[j] : 0.f;
-              s32[j] = fmaf(d, d, s32[j]);
-            }
         }
-      constexpr unsigned int kRow = (1u << BW) - 1u;
-      bool any_in[PX];
+      }
+      constexpr int B = BW * BW * BW;
+      float mu[PZ];
 #pragma unroll
-      for (int j = 0; j < PX; ++j) {
-        all_in[j] = ((allb >> j) & kRow) == kRow;
-        any_in[j] = ((anyb >> j) & kRow) != 0u;
+      for (int j = 0; j < PZ; ++j) {
+        mean[j] = (B & (B - 1)) == 0 ? sum[j] * (1.0 / B) : __ddiv_rn(sum[j], (double)B);
+        mu[j] = (float)mean[j];
       }
 #pragma unroll
-      for (int j = 0; j < PX; ++j) {
-        ss[j] = (double)s32[j];
+      for (int wz = 0; wz < NP; ++wz) {
+        if (z0 + wz >= zend) break;
+#pragma unroll
+        for (int vy = 0; vy < BW; ++vy) {
+          const long long q = o + wz * plane + (long long)vy * nx;
+          float v[BW];
+          bool m[BW];
+          bool rall = true, rany = false;
+#pragma unroll
+          for (int vx = 0; vx < BW; ++vx) {
+            v[vx] = __ldg(y + q + vx);
+            m[vx] = __ldg(ms + q + vx) != 0;
+            rall = rall && m[vx];
+            rany = rany || m[vx];
+          }
+#pragma unroll
+          for (int j = 0; j < PZ; ++j) {
+            const int vz = wz - j;
+            if (vz < 0 || vz >= BW) continue;
+            all_in[j] = all_in[j] && rall;
+            any_in[j] = any_in[j] || rany;
+#pragma unroll
+            for (int vx = 0; vx < BW; ++vx) {
+              const float d = m[vx] ? v[vx] - mu[j] : 0.f;
+              s32[j] = fmaf(d, d, s32[j]);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < PZ; ++j) {
+      if (z0 + j >= nz) break;
+      float2 r = make_float2(0.f, 0.f);
+      if (ok[j]) {
+        double ss = (double)s32[j];
         // no masked voxel: zero; with a mean that is a float, v - mean is zero
         // in FP32 exactly when it is in FP64; otherwise a tiny FP32 sum is
         // recomputed in FP64
-        if (ok[j] && any_in[j] && s32[j] < 1e-30f && (double)mu[j] != mean[j])
-          ss[j] = box_ss64<BW>(y, ms, o + j, nx, ny, mean[j]);
+        if (any_in[j] && s32[j] < 1e-30f && (double)(float)mean[j] != mean[j])
+          ss = box_ss64<BW>(y, ms, o + j * plane, nx, ny, mean[j]);
+        const float fs = (float)ss;
+        r = make_float2((float)mean[j], all_in[j] ? fs : -fs);
       }
-    }
-#pragma unroll
-    for (int j = 0; j < PX; ++j) {
-      if (x0 + j >= nx) break;
-      if (!ok[j]) {
-        out[o + j] = make_float2(0.f, 0.f);
-      } else {
-        const float fs = (float)ss[j];
-        out[o + j] = make_float2((float)mean[j], all_in[j] ? fs : -fs);
-      }
+      out[o + j * plane] = r;
     }
   }
 }
 
 mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8_t *smask,
                                float2 *stats, cudaStream_t s) {
-  long long n = (long long)((g.size[0] + kBoxPX - 1) / kBoxPX) * g.size[1] * g.size[2];
+  long long n = (long long)g.size[0] * g.size[1] * ((g.size[2] + kBoxPZ - 1) / kBoxPZ);
   int threads = 256;
   long long blocks = (n + threads - 1) / threads;
   if (blocks > (long long)sm_count() * 64) blocks = (long long)sm_count() * 64;
@@ -219,143 +225,244 @@ __device__ __forceinline__ float to_float(float v) { return v; }
 __device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
 
-template <typename T>
-__global__ void block_variance_kernel(const T *__restrict__ img, int nx, int ny, int nbx,
-                                      int nby, int nbz, int stx, int sty, int stz, int G, int bw,
-                                      double *__restrict__ var, unsigned long long *__restrict__ key) {
-  long long nb = (long long)nbx * nby * nbz;
-  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
-       b += (long long)gridDim.x * blockDim.x) {
-    int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((long long)nbx * nby));
-    long long o = ((long long)(stz + bz * G) * ny + (sty + by * G)) * nx + (stx + bx * G);
-    double cnt = 0.0, sum = 0.0, ssq = 0.0;
-    for (int z = 0; z < bw; ++z)
-      for (int y = 0; y < bw; ++y)
-        for (int x = 0; x < bw; ++x) {
-          float v = to_float(img[o + ((long long)z * ny + y) * nx + x]);
-          cnt = __dadd_rn(cnt, 1.0);
-          sum = __dadd_rn(sum, (double)v);
-          float sq = __fmul_rn(v, v);  // float * float in the reference
-          ssq = __dadd_rn(ssq, (double)sq);
-        }
-    double mean = __ddiv_rn(sum, cnt);
-    double v = __dsub_rn(__ddiv_rn(ssq, cnt), __dmul_rn(mean, mean));
-    var[b] = v;
-    key[b] = order_key(v);
-  }
-}
+// The whole selection in one cooperative launch (CTAs meet at a grid barrier
+// whose wait is bounded):
+//   1. per block (one thread each) the variance as the reference computes it
+//      (itkBlockMatcher.txx:664-719: FP64 count, sum and sum of float
+//      squares in raster order, var = ssq / cnt - mean^2), its order key, and
+//      a histogram of the keys' top 12 bits;
+//   2. an MSD radix select of the key of rank idx: while more than one CTA's
+//      worth of keys share the prefix, the next 12 bits are histogrammed;
+//      then those keys are gathered and ranked by counting;
+//   3. selected[b] = var[b] > the selected value.
+constexpr int kSelThreads = 256;
+constexpr int kSelBins = 4096;
+constexpr int kSelCand = kSelThreads;
 
-// Radix select control block (device memory).
+// Device control block of one selection, followed in memory by 3 * kSelBins
+// histogram words; the launcher zeroes both.
 struct SelectCtl {
-  unsigned long long prefix;
-  unsigned long long mask;
-  unsigned long long k;      // rank still to find within the prefix bucket
-  unsigned long long n;
+  unsigned int bar_count;
+  unsigned int bar_gen;
+  int err;
+  int pad;
+  unsigned long long ncand;
 };
 
-__global__ void select_hist_kernel(const unsigned long long *__restrict__ key, long long n,
-                                   const SelectCtl *__restrict__ ctl, int shift,
-                                   unsigned int *__restrict__ hist) {
-  __shared__ unsigned int h[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+struct SelectArgs {
+  const void *img;
+  int nx, ny, nbx, nby, nbz, stx, sty, stz, G, bw;
+  long long n;
+  unsigned long long idx;  // rank of the cut-off value (ascending)
+  double *var;
+  unsigned long long *key;
+  unsigned long long *cand;  // kSelCand
+  SelectCtl *ctl;
+  unsigned int *hist;        // 3 * kSelBins
+  uint8_t *selected;
+  unsigned int *give_up;     // set when a barrier wait gives up (may be null)
+  long long spin_limit;
+};
+
+// BW > 0: the block width known at compile time (the 64 or 125 loads of a
+// block are all issued before the sums); BW = 0: a.bw at run time.
+template <typename T, int BW>
+__device__ inline double block_variance(const T *__restrict__ img, const SelectArgs &a,
+                                        long long b) {
+  const int bw = BW > 0 ? BW : a.bw;
+  const int bx = (int)(b % a.nbx), by = (int)((b / a.nbx) % a.nby);
+  const int bz = (int)(b / ((long long)a.nbx * a.nby));
+  const long long o =
+      ((long long)(a.stz + bz * a.G) * a.ny + (a.sty + by * a.G)) * a.nx + (a.stx + bx * a.G);
+  double cnt = 0.0, sum = 0.0, ssq = 0.0;
+#pragma unroll
+  for (int z = 0; z < bw; ++z)
+#pragma unroll
+    for (int y = 0; y < bw; ++y)
+#pragma unroll
+      for (int x = 0; x < bw; ++x) {
+        const float v = to_float(img[o + ((long long)z * a.ny + y) * a.nx + x]);
+        cnt = __dadd_rn(cnt, 1.0);
+        sum = __dadd_rn(sum, (double)v);
+        const float sq = __fmul_rn(v, v);  // float * float in the reference
+        ssq = __dadd_rn(ssq, (double)sq);
+      }
+  const double mean = __ddiv_rn(sum, cnt);
+  return __dsub_rn(__ddiv_rn(ssq, cnt), __dmul_rn(mean, mean));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSelThreads) select_kernel(SelectArgs a) {
+  __shared__ unsigned int h[kSelBins];
+  __shared__ unsigned long long ck[kSelCand];
+  __shared__ unsigned long long s_pair[2];
+  __shared__ unsigned long long s_cut;
+  __shared__ unsigned long long s_nc;
+  const T *img = static_cast<const T *>(a.img);
+  const long long n = a.n;
+  const long long gstride = (long long)gridDim.x * blockDim.x;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned int nctas = gridDim.x;
+  SelectCtl *ctl = a.ctl;
+  // ---- 1. variances, keys, histogram of the top 12 bits --------------------
+  for (int i = threadIdx.x; i < kSelBins; i += blockDim.x) h[i] = 0;
   __syncthreads();
-  unsigned long long prefix = ctl->prefix, mask = ctl->mask;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    unsigned long long k = key[i];
-    if ((k & mask) == prefix) atomicAdd(&h[(k >> shift) & 0xFF], 1u);
+  for (long long b = gtid; b < n; b += gstride) {
+    const double v = a.bw == 4   ? block_variance<T, 4>(img, a, b)
+                     : a.bw == 5 ? block_variance<T, 5>(img, a, b)
+                                 : block_variance<T, 0>(img, a, b);
+    const unsigned long long k = order_key(v);
+    a.var[b] = v;
+    a.key[b] = k;
+    hist_add(h, (unsigned)(k >> 52));
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 256; i += blockDim.x)
-    if (h[i]) atomicAdd(&hist[i], h[i]);
-}
-
-// The select's initial state (a kernel rather than a host copy, so the
-// sequence can be captured into a graph).
-__global__ void select_init_kernel(SelectCtl *ctl, unsigned long long k, unsigned long long n,
-                                   unsigned int *hist) {
-  if (threadIdx.x == 0) *ctl = SelectCtl{0ULL, 0ULL, k, n};
-  hist[threadIdx.x] = 0u;
-}
-
-__global__ void select_scan_kernel(SelectCtl *ctl, int shift, unsigned int *hist) {
-  __shared__ unsigned int h[256];
-  int t = threadIdx.x;
-  h[t] = hist[t];
-  __syncthreads();
-  if (t == 0) {
-    unsigned long long k = ctl->k, cum = 0;
+  for (int i = threadIdx.x; i < kSelBins; i += blockDim.x)
+    if (h[i]) atomicAdd(&a.hist[i], h[i]);
+  bool ok = grid_barrier(&ctl->bar_count, &ctl->bar_gen, &ctl->err, a.spin_limit, nctas);
+  // ---- 2. radix select of rank idx -----------------------------------------
+  unsigned long long k = a.idx, prefix = 0, mask = 0;
+  int shift = 52, bits = 12, pass = 0;
+  while (ok) {
+    // every CTA scans the global histogram of this pass identically
+    const unsigned int *gh = a.hist + (pass % 3) * kSelBins;
+    for (int i = threadIdx.x; i < kSelBins; i += blockDim.x) h[i] = __ldcg(&gh[i]);
+    __syncthreads();
     int d = 0;
-    for (; d < 256; ++d) {
-      if (cum + h[d] > k) break;
-      cum += h[d];
+    unsigned long long cum = 0;
+    find_bucket<kSelBins, kSelThreads>(h, k, 1 << bits, s_pair, &d, &cum);
+    const unsigned long long bucket = h[d];
+    k -= cum;
+    prefix |= (unsigned long long)d << shift;
+    mask |= ((1ULL << bits) - 1ULL) << shift;
+    __syncthreads();
+    if (bucket <= (unsigned long long)kSelCand || shift == 0) break;
+    // more than one CTA's worth of keys share the prefix: the next bits
+    ++pass;
+    bits = shift >= 12 ? 12 : shift;
+    shift -= bits;
+    if (blockIdx.x == 0) {
+      unsigned int *zb = a.hist + ((pass + 1) % 3) * kSelBins;
+      for (int i = threadIdx.x; i < kSelBins; i += blockDim.x) zb[i] = 0;
     }
-    if (d == 256) d = 255;  // cannot happen for k < count
-    ctl->k = k - cum;
-    ctl->prefix |= ((unsigned long long)d) << shift;
-    ctl->mask |= 0xFFULL << shift;
+    for (int i = threadIdx.x; i < kSelBins; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (long long i = gtid; i < n; i += gstride) {
+      const unsigned long long key = a.key[i];
+      if ((key & mask) == prefix) hist_add(h, (unsigned)(key >> shift) & ((1u << bits) - 1u));
+    }
+    __syncthreads();
+    unsigned int *gh2 = a.hist + (pass % 3) * kSelBins;
+    for (int i = threadIdx.x; i < kSelBins; i += blockDim.x)
+      if (h[i]) atomicAdd(&gh2[i], h[i]);
+    ok = grid_barrier(&ctl->bar_count, &ctl->bar_gen, &ctl->err, a.spin_limit, nctas);
   }
-  __syncthreads();
-  hist[t] = 0;
+  if (ok && shift != 0) {
+    // the bucket's keys (at most one per thread of a CTA), ranked by counting
+    for (long long i = gtid; i < n; i += gstride) {
+      const unsigned long long key = a.key[i];
+      if ((key & mask) == prefix) {
+        const unsigned long long pos = atomicAdd(&ctl->ncand, 1ULL);
+        if (pos < (unsigned long long)kSelCand) a.cand[pos] = key;
+      }
+    }
+    ok = grid_barrier(&ctl->bar_count, &ctl->bar_gen, &ctl->err, a.spin_limit, nctas);
+    if (ok) {
+      if (threadIdx.x == 0) {
+        s_nc = __ldcg(&ctl->ncand);
+        s_cut = prefix;
+      }
+      __syncthreads();
+      const int nc = (int)(s_nc < (unsigned long long)kSelCand ? s_nc : kSelCand);
+      const unsigned long long kk = k < (unsigned long long)nc ? k : (nc > 0 ? nc - 1 : 0);
+      for (int i = threadIdx.x; i < nc; i += blockDim.x) ck[i] = __ldcg(&a.cand[i]);
+      __syncthreads();
+      if (threadIdx.x < nc) {
+        const unsigned long long v = ck[threadIdx.x];
+        int lo = 0, eq = 0;
+        for (int j = 0; j < nc; ++j) {
+          lo += ck[j] < v;
+          eq += ck[j] == v;
+        }
+        if ((unsigned long long)lo <= kk && kk < (unsigned long long)(lo + eq)) s_cut = v;
+      }
+      __syncthreads();
+      prefix = s_cut;
+    }
+  }
+  if (!ok) {
+    if (threadIdx.x == 0 && a.give_up) atomicExch(a.give_up, 1u);
+    return;
+  }
+  // ---- 3. flags --------------------------------------------------------------
+  const unsigned long long u =
+      (prefix & 0x8000000000000000ULL) ? (prefix & 0x7FFFFFFFFFFFFFFFULL) : ~prefix;
+  const double cutoff = __longlong_as_double((long long)u);
+  for (long long b = gtid; b < n; b += gstride) a.selected[b] = a.var[b] > cutoff ? 1 : 0;
 }
 
-__global__ void select_flags_kernel(const double *__restrict__ var, long long n,
-                                    const SelectCtl *__restrict__ ctl,
-                                    uint8_t *__restrict__ selected) {
-  unsigned long long p = ctl->prefix;
-  unsigned long long u = (p & 0x8000000000000000ULL) ? (p & 0x7FFFFFFFFFFFFFFFULL) : ~p;
-  double cutoff = __longlong_as_double((long long)u);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    selected[i] = var[i] > cutoff ? 1 : 0;
+template <typename T>
+mirorr_status launch_select(SelectArgs &a, cudaStream_t s) {
+  static int per_sm[3] = {0, 0, 0};
+  const int slot = std::is_same<T, float>::value ? 0 : (std::is_same<T, __half>::value ? 2 : 1);
+  if (per_sm[slot] == 0) {
+    int per = 0;
+    MB2_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, select_kernel<T>, kSelThreads, 0));
+    per_sm[slot] = per > 0 ? per : 1;
+  }
+  long long want = (a.n + 4 * kSelThreads - 1) / (4 * kSelThreads);
+  const long long cap = (long long)sm_count() * per_sm[slot];
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  void *args[] = {&a};
+  MB2_CUDA_TRY(cudaLaunchCooperativeKernel((void *)select_kernel<T>, dim3((unsigned)want),
+                                           dim3(kSelThreads), args, 0, s));
+  ++g_launches;
+  return MIRORR_OK;
 }
+
+size_t selection_var_bytes(long long nblocks) {
+  return sizeof(double) * nblocks + sizeof(unsigned long long) * (nblocks + kSelCand);
+}
+
+size_t selection_state_bytes() { return sizeof(SelectCtl) + sizeof(unsigned int) * 3 * kSelBins; }
 
 mirorr_status launch_variance_selection(const BmGeom &g, const void *base, double keep,
                                         BmWork &w, const uint8_t **selected_out,
-                                        cudaStream_t s, int dtype) {
+                                        cudaStream_t s, int dtype, unsigned int *give_up) {
   *selected_out = nullptr;
   if (!(keep < 1.0)) return MIRORR_OK;
   long long n = g.nblocks;
-  MB2_TRY(w.var.ensure(sizeof(double) * n + sizeof(unsigned long long) * n));
+  MB2_TRY(w.var.ensure(selection_var_bytes(n)));
   MB2_TRY(w.selected.ensure(n));
-  MB2_TRY(w.select_state.ensure(sizeof(SelectCtl)));
-  MB2_TRY(w.hist.ensure(256 * sizeof(unsigned int)));
-  double *var = w.var.as<double>();
-  unsigned long long *key = reinterpret_cast<unsigned long long *>(var + n);
-  int threads = 256;
-  long long blocks = (n + threads - 1) / threads;
-  if (blocks > (long long)sm_count() * 32) blocks = (long long)sm_count() * 32;
-  // the reference's FP64 variance (exact k-th value, so the selected blocks
-  // are the reference's for any storage type)
-  if (dtype == MIRORR_DTYPE_BF16)
-    block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
-        static_cast<const __nv_bfloat16 *>(base), g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2],
-        g.st[0], g.st[1], g.st[2], g.ngap, g.bw, var, key);
-  else if (dtype == MIRORR_DTYPE_F16)
-    block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
-        static_cast<const __half *>(base), g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2],
-        g.st[0], g.st[1], g.st[2], g.ngap, g.bw, var, key);
-  else
-    block_variance_kernel<<<(unsigned)blocks, threads, 0, s>>>(
-        static_cast<const float *>(base), g.size[0], g.size[1], g.nb[0], g.nb[1], g.nb[2],
-        g.st[0], g.st[1], g.st[2], g.ngap, g.bw, var, key);
-  MB2_LAUNCH_CHECK();
+  const size_t ctl_bytes = selection_state_bytes();
+  MB2_TRY(w.select_state.ensure(ctl_bytes));
+  SelectArgs a;
+  a.img = base;
+  a.nx = g.size[0]; a.ny = g.size[1];
+  a.nbx = g.nb[0]; a.nby = g.nb[1]; a.nbz = g.nb[2];
+  a.stx = g.st[0]; a.sty = g.st[1]; a.stz = g.st[2];
+  a.G = g.ngap; a.bw = g.bw;
+  a.n = n;
   // cut-off index (unsigned)((1 - keep) * N); index >= N -> the maximum
   unsigned long long idx = (unsigned long long)(unsigned int)((1.0 - keep) * (double)n);
   if (idx >= (unsigned long long)n) idx = n - 1;
-  SelectCtl *ctl = w.select_state.as<SelectCtl>();
-  select_init_kernel<<<1, 256, 0, s>>>(ctl, idx, (unsigned long long)n, w.hist.as<unsigned int>());
-  MB2_LAUNCH_CHECK();
-  for (int pass = 0; pass < 8; ++pass) {
-    int shift = 56 - 8 * pass;
-    select_hist_kernel<<<(unsigned)blocks, threads, 0, s>>>(key, n, ctl, shift,
-                                                            w.hist.as<unsigned int>());
-    MB2_LAUNCH_CHECK();
-    select_scan_kernel<<<1, 256, 0, s>>>(ctl, shift, w.hist.as<unsigned int>());
-    MB2_LAUNCH_CHECK();
-  }
-  select_flags_kernel<<<(unsigned)blocks, threads, 0, s>>>(var, n, ctl, w.selected.as<uint8_t>());
-  MB2_LAUNCH_CHECK();
+  a.idx = idx;
+  a.var = w.var.as<double>();
+  a.key = reinterpret_cast<unsigned long long *>(a.var + n);
+  a.cand = a.key + n;
+  a.ctl = w.select_state.as<SelectCtl>();
+  a.hist = reinterpret_cast<unsigned int *>(a.ctl + 1);
+  a.selected = w.selected.as<uint8_t>();
+  a.give_up = give_up;
+  a.spin_limit = 1LL << 23;  // about 0.84 s of polling
+  // a memset, not a host copy, so the sequence can be captured into a graph
+  MB2_CUDA_TRY(cudaMemsetAsync(w.select_state.ptr, 0, ctl_bytes, s));
+  // the reference's FP64 variance (exact k-th value, so the selected blocks
+  // are the reference's for any storage type)
+  if (dtype == MIRORR_DTYPE_BF16) MB2_TRY(launch_select<__nv_bfloat16>(a, s));
+  else if (dtype == MIRORR_DTYPE_F16) MB2_TRY(launch_select<__half>(a, s));
+  else MB2_TRY(launch_select<float>(a, s));
   *selected_out = w.selected.as<uint8_t>();
   return MIRORR_OK;
 }

@@ -224,6 +224,8 @@ bool valid_geom(const mirorr_geometry *g) {
   if (!g) return false;
   for (int d = 0; d < 3; ++d)
     if (g->size[d] <= 0 || !(g->spacing[d] > 0.0)) return false;
+  // the resampler addresses within a slice with 32-bit offsets
+  if ((long long)g->size[0] * g->size[1] >= (1LL << 31)) return false;
   double A[9], Ai[9];
   for (int r = 0; r < 3; ++r)
     for (int c = 0; c < 3; ++c) A[3 * r + c] = g->direction[3 * r + c] * g->spacing[c];
@@ -342,7 +344,10 @@ mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall
     if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[0], s));
     if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], s));
     const uint8_t *sel = nullptr;
-    MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s, mc.dtype));
+    unsigned int *give_up = nullptr;
+    if (p.block_keep < 1.0) MB2_TRY(ncc_give_up_flag(c->bmw, s, &give_up));
+    MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s, mc.dtype,
+                                      give_up));
     if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
     MB2_TRY(launch_match16(mc.dtype, g, mc.base, mc.bmask, mc.search, mc.smask, sel, out, c->bm16,
                            c->ncc_count.as<unsigned long long>(), s));
@@ -354,7 +359,10 @@ mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall
                              c->bmw.stats.as<float2>(), s));
     if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[1], s));
     const uint8_t *sel = nullptr;
-    MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s));
+    unsigned int *give_up = nullptr;
+    if (p.block_keep < 1.0) MB2_TRY(ncc_give_up_flag(c->bmw, s, &give_up));
+    MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s,
+                                      MIRORR_DTYPE_F32, give_up));
     if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
     MB2_TRY(launch_ncc(g, static_cast<const float *>(mc.base), mc.bmask,
                        static_cast<const float *>(mc.search), mc.smask, c->bmw.stats.as<float2>(),
@@ -646,7 +654,7 @@ std::vector<uint64_t> level_key(mirorr_ctx c, const RegRun &r, const mirorr_geom
   memcpy(pb, &r.p->bm, sizeof(mirorr_bm_params));
   for (uint64_t v : pb) add(v);
   const DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
-                          &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl,
+                          &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl,
                           &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->bmw.ncc_pad, &c->bmw.ncc_wand,
                           &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best, &c->second,
                           &c->match, &c->status, &c->pts_i, &c->pts_m, &c->counts, &c->ncc_count,
@@ -707,7 +715,7 @@ mirorr_status collect_lts(RegRun &r, LtsState &hs, long long *n_used) {
   if (gave_up) {
     bool to = false;
     MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
-    set_error("a bounded wait on a tensor copy of the NCC search gave up");
+    set_error("a bounded wait of the block search (a tensor copy or a grid barrier) gave up");
     return MIRORR_ETIMEOUT;
   }
   if (r.stats) {
@@ -737,7 +745,7 @@ mirorr_status run_lts(RegRun &r, LtsState &hs, long long nmax, long long *n_used
     bool to = false;
     if (is16(r.p->storage)) MB2_CUDA_TRY(cudaMemsetAsync(c->bm16.ctl.ptr, 0, 16, c->stream));
     else MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
-    set_error("a bounded wait on a tensor copy of the NCC search gave up");
+    set_error("a bounded wait of the block search (a tensor copy or a grid barrier) gave up");
     return MIRORR_ETIMEOUT;
   }
   if (r.stats) {
@@ -1109,7 +1117,7 @@ mirorr_status register_impl(mirorr_ctx c, const mirorr_geometry *fg, const void 
     MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
     MB2_TRY(match16_take_timeout(c->bm16, c->stream, &to16));
     if (to || to16) {
-      set_error("a bounded wait on a tensor copy of the NCC search gave up");
+      set_error("a bounded wait of the block search (a tensor copy or a grid barrier) gave up");
       return MIRORR_ETIMEOUT;
     }
   }
@@ -1168,7 +1176,7 @@ mirorr_status mirorr_ctx_destroy(mirorr_ctx c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf *bufs[] = {&c->bmw.stats, &c->bmw.var, &c->bmw.selected, &c->bmw.select_state,
-                    &c->bmw.hist, &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->bmw.ncc_pad, &c->bmw.ncc_wand, &c->ltsw.state, &c->ltsw.resid, &c->xl_count,
+                    &c->bmw.tiles, &c->bmw.ncc_lists, &c->bmw.ncc_ctl, &c->bmw.ncc_rec, &c->bmw.ncc_bstat, &c->bmw.ncc_pad, &c->bmw.ncc_wand, &c->ltsw.state, &c->ltsw.resid, &c->xl_count,
                     &c->ltsw.partial, &c->ltsw.hist, &c->ltsw.ctrl, &c->ltsw.cand, &c->counts,
                     &c->ncc_count, &c->ones, &c->lvl_f, &c->lvl_m, &c->tmp_a, &c->tmp_b,
                     &c->weights, &c->img_b, &c->img_s, &c->msk_b, &c->msk_s, &c->best,
@@ -1497,11 +1505,12 @@ mirorr_status mirorr_bm_get_offsets(mirorr_matcher m, size_t capacity, double *b
   MB2_CUDA_TRY(cudaStreamSynchronize(c->stream));
   for (int s = 0; s < 4; ++s) cudaEventElapsedTime(&m->timings[s], m->ev[s], m->ev[s + 1]);
   {
-    bool to = false;
+    bool to = false, to_sel = false;
+    // the variance selection reports through the FP32 search's flag
     if (is16(m->storage)) MB2_TRY(match16_take_timeout(c->bm16, c->stream, &to));
-    else MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to));
-    if (to) {
-      set_error("a bounded wait on a tensor copy of the NCC search gave up");
+    MB2_TRY(ncc_take_timeout(c->bmw, c->stream, &to_sel));
+    if (to || to_sel) {
+      set_error("a bounded wait of the block search (a tensor copy or a grid barrier) gave up");
       return MIRORR_ETIMEOUT;
     }
   }
@@ -2278,8 +2287,9 @@ mirorr_status batch_check_slot(mirorr_ctx c, const BatchSlot &s) {
          need(cb.tiles, sizeof(unsigned int) * ((nb + 2047) / 2048 + 1), "tiles") &&
          (!mc.tensor || need(cb.chunked, match16_chunk_bytes(mc), "chunked")) &&
          (!(s.p.bm.block_keep < 1.0) ||
-          (need(cb.sel.var, 16 * (size_t)nb, "selection keys") &&
-           need(cb.sel.selected, (size_t)nb, "selection flags")));
+          (need(cb.sel.var, selection_var_bytes(nb), "selection keys") &&
+           need(cb.sel.selected, (size_t)nb, "selection flags") &&
+           need(cb.sel.select_state, selection_state_bytes(), "selection state")));
   }
   return ok ? MIRORR_OK : MIRORR_EINVAL;
 }
@@ -2312,7 +2322,7 @@ mirorr_status batch_issue(mirorr_batch b, int njobs, long long max_vox, int ncal
       if (!(s.p.bm.block_keep < 1.0)) continue;
       const uint8_t *sel = nullptr;
       MB2_TRY(launch_variance_selection(s.g, calls[ci].base, s.p.bm.block_keep, s.call[k].sel, &sel, st,
-                                        b->storage));
+                                        b->storage, calls[ci].ctl + 2));
     }
   }
   MB2_TRY(launch_match16_batch(b->storage, ncalls, b->h_calls.as<Match16Call>(), b->d_calls, st,
@@ -2565,7 +2575,7 @@ mirorr_status batch_round(mirorr_batch b, int *running, int *finished) {
     const int si = b->fit_slot[fi];
     BatchSlot &s = b->slots[si];
     if (rctl[4 * (2 * si) + 2] || rctl[4 * (2 * si + 1) + 2]) {
-      batch_fail(b, s, MIRORR_ETIMEOUT, "a bounded wait on a tensor copy of the NCC search gave up");
+      batch_fail(b, s, MIRORR_ETIMEOUT, "a bounded wait of the block search (a tensor copy or a grid barrier) gave up");
       ++nfin;
       continue;
     }
@@ -2793,10 +2803,9 @@ mirorr_status mirorr_batch_submit(mirorr_batch b, const mirorr_geometry *fg, con
     E(cb.status, max_blocks);
     E(cb.tiles, sizeof(unsigned int) * (max_blocks / 2048 + 2));
     if (pp.bm.block_keep < 1.0) {
-      E(cb.sel.var, (sizeof(double) + sizeof(unsigned long long)) * max_blocks);
+      E(cb.sel.var, selection_var_bytes(max_blocks));
       E(cb.sel.selected, max_blocks);
-      E(cb.sel.select_state, 64);
-      E(cb.sel.hist, 256 * sizeof(unsigned int));
+      E(cb.sel.select_state, selection_state_bytes());
     }
   }
   E(s.pts_i, sizeof(double) * 3 * ncall * max_blocks);

@@ -23,8 +23,7 @@ struct BmWork {
   DevBuf stats;     // float2 per voxel of the search image: (mean, masked SS)
   DevBuf var;       // double per block (variance selection)
   DevBuf selected;  // uint8 per block
-  DevBuf select_state;
-  DevBuf hist;
+  DevBuf select_state;  // selection control block and radix histograms
   DevBuf tiles;     // compaction tile counts/offsets
   DevBuf ncc_lists; // block lists of the NCC stages (general path, fallback)
   DevBuf ncc_ctl;   // NCC counters: [0] general-path blocks, [1] fallback blocks,
@@ -55,9 +54,15 @@ void point_geom(const double origin[3], const double spacing[3], const double di
 mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8_t *smask,
                                float2 *stats, cudaStream_t s);
 // base: float32, or 16-bit when dtype is MIRORR_DTYPE_BF16 / _F16.
+// Work-area sizes of one selection: BmWork::var and BmWork::select_state.
+size_t selection_var_bytes(long long nblocks);
+size_t selection_state_bytes();
+// give_up: a device flag the selection sets when one of its grid-barrier waits
+// gives up (the call's result is then invalid), or null.
 mirorr_status launch_variance_selection(const BmGeom &g, const void *base, double keep,
                                         BmWork &w, const uint8_t **selected_out,
-                                        cudaStream_t s, int dtype = MIRORR_DTYPE_F32);
+                                        cudaStream_t s, int dtype = MIRORR_DTYPE_F32,
+                                        unsigned int *give_up = nullptr);
 // ncc_count (optional): device counter incremented by the number of candidate
 // scores evaluated.  Profiling (optional): kev[0], kev[1] are recorded around
 // the per-x-lane search kernel's launch and xl_count adds up the candidates it
@@ -285,6 +290,9 @@ mirorr_status launch_window_and(const BmGeom &g, const float2 *stats, DevBuf &bu
                                 const uint8_t **wand, cudaStream_t s);
 // The NCC stage's give-up flag (device word), or nullptr before any search.
 const unsigned int *ncc_timeout_flag(const BmWork &w);
+// The give-up flag ncc_take_timeout reads, allocated (and zeroed) if the
+// search has not run yet, for the stages before it.
+mirorr_status ncc_give_up_flag(BmWork &w, cudaStream_t s, unsigned int **flag);
 // One fit of lts_batch_launch: its state (uploaded after lts_begin), point
 // pairs, the two device counters whose sum is the pair count, and scratch of
 // lts_fit_scratch_bytes(n_max, ncta) bytes (256-byte aligned).

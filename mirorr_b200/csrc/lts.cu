@@ -19,6 +19,7 @@
 
 #include <mutex>
 
+#include "gridsel.cuh"
 #include "kernels.cuh"
 
 namespace mb2 {
@@ -55,96 +56,14 @@ struct LtsArgs {
   long long spin_limit;   // polls of a grid-barrier wait before it gives up
 };
 
-__device__ bool grid_sync(LtsCtl *ctl, long long spin_limit, unsigned int nctas) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned int *genp = &ctl->bar_gen;
-    volatile int *errp = &ctl->err;
-    unsigned int gen = *genp;
-    __threadfence();
-    unsigned int arrived = atomicAdd(&ctl->bar_count, 1u) + 1u;
-    if (arrived == nctas) {
-      atomicExch(&ctl->bar_count, 0u);
-      __threadfence();
-      atomicAdd(&ctl->bar_gen, 1u);
-    } else {
-      long long spins = 0;
-      while (*genp == gen && *errp == 0) {
-        if (spins > 256) __nanosleep(100);
-        if (++spins > spin_limit) {
-          atomicExch(&ctl->err, 1);
-          break;
-        }
-      }
-    }
-    __threadfence();
-    s_ok = (*errp == 0);
-  }
-  __syncthreads();
-  return s_ok != 0;
+__device__ inline bool grid_sync(LtsCtl *ctl, long long spin_limit, unsigned int nctas) {
+  return grid_barrier(&ctl->bar_count, &ctl->bar_gen, &ctl->err, spin_limit, nctas);
 }
 
 __device__ inline void load_cg(void *dst, const void *src, int bytes) {
   const unsigned long long *s = static_cast<const unsigned long long *>(src);
   unsigned long long *d = static_cast<unsigned long long *>(dst);
   for (int i = threadIdx.x; i < bytes / 8; i += blockDim.x) d[i] = __ldcg(s + i);
-}
-
-// Adds 1 to bin of a shared histogram, one atomic per group of lanes of the
-// warp that hit the same bin.
-__device__ inline void hist_add(unsigned int *h, unsigned int bin) {
-  const unsigned active = __activemask();
-  const unsigned same = __match_any_sync(active, bin);
-  if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicAdd(&h[bin], (unsigned)__popc(same));
-}
-
-// Bucket of rank k in the shared histogram h[0, kBins): the bin d with
-// cum(d) <= k < cum(d) + h[d] (cum = sum of the bins below d), found with a
-// block-wide scan.  Returns d in *d_out and cum(d) in *cum_out (every thread).
-__device__ inline void find_bucket(const unsigned int *h, unsigned long long k, int nb,
-                                   unsigned long long *s_pair, int *d_out,
-                                   unsigned long long *cum_out) {
-  constexpr int kPer = kBins / kThreads;  // bins per thread
-  __shared__ unsigned long long s_wsum[kThreads / 32];
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  unsigned long long local = 0;
-#pragma unroll
-  for (int i = 0; i < kPer; ++i) local += h[t * kPer + i];
-  unsigned long long inc = local;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    unsigned long long o = __shfl_up_sync(0xffffffffu, inc, off);
-    if (lane >= off) inc += o;
-  }
-  if (lane == 31) s_wsum[wid] = inc;
-  if (t == 0) { s_pair[0] = ~0ULL; s_pair[1] = 0; }
-  __syncthreads();
-  unsigned long long wbase = 0;
-  for (int w = 0; w < wid; ++w) wbase += s_wsum[w];
-  const unsigned long long base = wbase + inc - local;
-  if (local > 0 && base <= k && k < base + local) {
-    unsigned long long cum = base;
-    int d = t * kPer;
-    for (int i = 0; i < kPer; ++i, ++d) {
-      if (cum + h[d] > k) break;
-      cum += h[d];
-    }
-    s_pair[0] = (unsigned long long)d;
-    s_pair[1] = cum;
-  }
-  __syncthreads();
-  if (s_pair[0] == ~0ULL) {
-    // k beyond the histogram's count: the last bin, cum = total
-    unsigned long long total = 0;
-    for (int w = 0; w < kThreads / 32; ++w) total += s_wsum[w];
-    *d_out = nb - 1;
-    *cum_out = total;
-  } else {
-    *d_out = (int)s_pair[0];
-    *cum_out = s_pair[1];
-  }
-  __syncthreads();
 }
 
 // Sums each of v[0, N) over the CTA (per value: shuffle tree within each
@@ -268,7 +187,7 @@ __device__ void lts_body(const LtsArgs &a, int cta, int ncta) {
         __syncthreads();
         int d = 0;
         unsigned long long cum = 0;
-        find_bucket(h, k, 1 << bits, s_pair, &d, &cum);
+        find_bucket<kBins, kThreads>(h, k, 1 << bits, s_pair, &d, &cum);
         bucket = h[d];
         k -= cum;
         prefix |= (unsigned long long)d << shift;
@@ -364,31 +283,44 @@ __device__ void lts_body(const LtsArgs &a, int cta, int ncta) {
     if (threadIdx.x < 28) a.partial[(long long)cta * kPartial + threadIdx.x] = s_out[threadIdx.x];
     if (!grid_sync(a.ctl, a.spin_limit, (unsigned)ncta)) return;
     if (cta == 0) grid_partial_sums(a.partial, 0, 28, s_out, ncta);
-    if (cta == 0 && threadIdx.x == 0) {
-      LtsMoments mo;
-      const double cnt = s_out[0];
-      double m[6];
-      for (int r = 0; r < 6; ++r) m[r] = s_out[1 + r] / cnt;
-      mo.n = cnt;
-      for (int c = 0; c < 3; ++c) { mo.mean_i[c] = z0[c] + m[c]; mo.mean_m[c] = z0[3 + c] + m[3 + c]; }
-      int q = 7;
-      for (int r = 0; r < 6; ++r)
-        for (int c = r; c < 6; ++c) {
-          const double zz = s_out[q++] - cnt * m[r] * m[c];
-          mo.Z[6 * r + c] = zz;
-          mo.Z[6 * c + r] = zz;
-        }
-      if (s.symmetric) lts_symmetric_step(s, mo);
-      else lts_classic_step(s, mo);
-      s.fraction = s.lts_keep;
-      s.iter += 1;
-      s.running = lts_continue(s) ? 1 : 0;
-      if (s.iter > 101) s.running = 0;
-      // reset select scratch for the next iteration
-      a.ctl->maxkey = 0;
-      a.ctl->ncand = 0;
-      *a.state = s;
-      __threadfence();
+    // the solve: warp 0 of CTA 0; the symmetric fit's two square roots run
+    // on lanes 0 and 1 at once
+    __shared__ SymHalf s_half;
+    __shared__ double s_root[2][16];
+    if (cta == 0 && threadIdx.x < 32) {
+      if (threadIdx.x == 0) {
+        LtsMoments mo;
+        const double cnt = s_out[0];
+        double m[6];
+        for (int r = 0; r < 6; ++r) m[r] = s_out[1 + r] / cnt;
+        mo.n = cnt;
+        for (int c = 0; c < 3; ++c) { mo.mean_i[c] = z0[c] + m[c]; mo.mean_m[c] = z0[3 + c] + m[3 + c]; }
+        int q = 7;
+        for (int r = 0; r < 6; ++r)
+          for (int c = r; c < 6; ++c) {
+            const double zz = s_out[q++] - cnt * m[r] * m[c];
+            mo.Z[6 * r + c] = zz;
+            mo.Z[6 * c + r] = zz;
+          }
+        if (s.symmetric) lts_symmetric_pre(s, mo, s_half);
+        else lts_classic_step(s, mo);
+      }
+      __syncwarp();
+      if (s.symmetric && threadIdx.x < 2)
+        half_step(s_half.K[threadIdx.x], s_half.t[threadIdx.x], s_root[threadIdx.x]);
+      __syncwarp();
+      if (threadIdx.x == 0) {
+        if (s.symmetric) lts_symmetric_post(s, s_half, s_root[0], s_root[1]);
+        s.fraction = s.lts_keep;
+        s.iter += 1;
+        s.running = lts_continue(s) ? 1 : 0;
+        if (s.iter > 101) s.running = 0;
+        // reset select scratch for the next iteration
+        a.ctl->maxkey = 0;
+        a.ctl->ncand = 0;
+        *a.state = s;
+        __threadfence();
+      }
     }
     if (cta == 0) {
       __syncthreads();

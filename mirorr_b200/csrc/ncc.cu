@@ -2077,6 +2077,15 @@ const unsigned int *ncc_timeout_flag(const BmWork &w) {
   return w.ncc_ctl.ptr ? w.ncc_ctl.as<unsigned int>() + 5 : nullptr;
 }
 
+mirorr_status ncc_give_up_flag(BmWork &w, cudaStream_t s, unsigned int **flag) {
+  const void *before = w.ncc_ctl.ptr;
+  MB2_TRY(w.ncc_ctl.ensure(sizeof(unsigned int) * 8));
+  if (w.ncc_ctl.ptr != before)
+    MB2_CUDA_TRY(cudaMemsetAsync(w.ncc_ctl.ptr, 0, sizeof(unsigned int) * 8, s));
+  *flag = w.ncc_ctl.as<unsigned int>() + 5;
+  return MIRORR_OK;
+}
+
 mirorr_status ncc_take_timeout(BmWork &w, cudaStream_t s, bool *timed_out) {
   *timed_out = false;
   if (!w.ncc_ctl.ptr) return MIRORR_OK;

@@ -77,15 +77,14 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
 #pragma unroll
   for (int r = 0; r < 3; ++r)
     if (!(c[r] >= -0.5 && c[r] < (double)nn[r] - 0.5)) inside = false;
-  if (!inside) {
-    if (IMG) st_copy(*v, 0.0f);
-    if (MSK) *m = 0;
-    return;
-  }
   const bool mread = MSK && !a.mask_ones;
-  if (MSK && a.mask_ones) *m = 255;
-  if (!IMG && !mread) return;
   if (a.nearest) {
+    if (!inside) {
+      if (IMG) st_copy(*v, 0.0f);
+      if (MSK) *m = 0;
+      return;
+    }
+    if (MSK && a.mask_ones) *m = 255;
     // NearestNeighborInterpolateImageFunction: index = floor(c + 0.5)
     long long q = 0, stride = 1;
 #pragma unroll
@@ -100,38 +99,51 @@ __device__ __forceinline__ void resample_voxel(const ResampleArgs &a, int i, con
     if (mread) *m = __ldg(a.inm + q);
     return;
   }
+  if (!IMG && !mread) {
+    if (MSK) *m = inside ? 255 : 0;
+    return;
+  }
+  // Linear: every voxel is evaluated, with its neighbours clamped into the
+  // image (straight-line code, so the voxels of a run overlap), and the
+  // inside test selects the result.  Inside the image the clamps change
+  // nothing: floor(c) lies in [-1, n - 1].
   int i0[3], i1[3];
   double t[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    int b = (int)floor(c[r]);
-    if (b < 0) b = 0;
+    const double cc = fmin(fmax(c[r], -1.0), (double)nn[r]);  // NaN -> -1
+    int b = (int)floor(cc);
+    b = b < 0 ? 0 : (b > nn[r] - 1 ? nn[r] - 1 : b);
     double d = __dsub_rn(c[r], (double)b);
     if (d <= 0.0) d = 0.0;
     i0[r] = b;
     i1[r] = (b + 1 > nn[r] - 1) ? b : b + 1;
     t[r] = d;
   }
-  const long long sy = a.inx, sz = (long long)a.inx * a.iny;
-  const long long z0 = i0[2] * sz, z1 = i1[2] * sz, y0 = i0[1] * sy, y1 = i1[1] * sy;
-  const long long q000 = z0 + y0 + i0[0], q100 = z0 + y0 + i1[0];
-  const long long q010 = z0 + y1 + i0[0], q110 = z0 + y1 + i1[0];
-  const long long q001 = z1 + y0 + i0[0], q101 = z1 + y0 + i1[0];
-  const long long q011 = z1 + y1 + i0[0], q111 = z1 + y1 + i1[0];
+  // the eight neighbours: a base pointer and 32-bit deltas (a slice holds
+  // fewer than 2^31 voxels, checked by the launcher)
+  const int sy = a.inx, sz = a.inx * a.iny;
+  const long long q000 = (long long)i0[2] * sz + (long long)(i0[1] * sy + i0[0]);
+  const int dx = i1[0] - i0[0], dy = (i1[1] - i0[1]) * sy, dz = (i1[2] - i0[2]) * sz;
   if (IMG) {
-    const double x00 = dlerp((double)ld_f(in, q000), (double)ld_f(in, q100), t[0]);
-    const double x10 = dlerp((double)ld_f(in, q010), (double)ld_f(in, q110), t[0]);
-    const double x01 = dlerp((double)ld_f(in, q001), (double)ld_f(in, q101), t[0]);
-    const double x11 = dlerp((double)ld_f(in, q011), (double)ld_f(in, q111), t[0]);
-    st_v(*v, dlerp(dlerp(x00, x10, t[1]), dlerp(x01, x11, t[1]), t[2]));
+    const TI *p = in + q000;
+    const double x00 = dlerp((double)ld_f(p, 0), (double)ld_f(p, dx), t[0]);
+    const double x10 = dlerp((double)ld_f(p, dy), (double)ld_f(p, dy + dx), t[0]);
+    const double x01 = dlerp((double)ld_f(p, dz), (double)ld_f(p, dz + dx), t[0]);
+    const double x11 = dlerp((double)ld_f(p, dz + dy), (double)ld_f(p, dz + dy + dx), t[0]);
+    const double val = dlerp(dlerp(x00, x10, t[1]), dlerp(x01, x11, t[1]), t[2]);
+    st_v(*v, inside ? val : 0.0);
   }
+  if (MSK && !mread) *m = inside ? 255 : 0;
   if (mread) {
-    const uint8_t *p = a.inm;
-    const uint8_t m000 = __ldg(p + q000), m100 = __ldg(p + q100), m010 = __ldg(p + q010),
-                  m110 = __ldg(p + q110), m001 = __ldg(p + q001), m101 = __ldg(p + q101),
-                  m011 = __ldg(p + q011), m111 = __ldg(p + q111);
-    if (m000 == m100 && m000 == m010 && m000 == m110 && m000 == m001 && m000 == m101 &&
-        m000 == m011 && m000 == m111) {
+    const uint8_t *p = a.inm + q000;
+    const uint8_t m000 = __ldg(p), m100 = __ldg(p + dx), m010 = __ldg(p + dy),
+                  m110 = __ldg(p + dy + dx), m001 = __ldg(p + dz), m101 = __ldg(p + dz + dx),
+                  m011 = __ldg(p + dz + dy), m111 = __ldg(p + dz + dy + dx);
+    if (!inside) {
+      *m = 0;
+    } else if (m000 == m100 && m000 == m010 && m000 == m110 && m000 == m001 && m000 == m101 &&
+               m000 == m011 && m000 == m111) {
       // every lerp of equal values returns that value exactly
       *m = m000;
     } else {
@@ -157,10 +169,21 @@ __device__ __forceinline__ void resample_runs(const ResampleArgs &a, long long g
   TO *const out = static_cast<TO *>(a.out);
   const long long n = (long long)a.onx * a.ony * a.onz;
   const long long nrun = (n + 3) >> 2;
+  const bool narrow = n < (1LL << 31);
+  const bool row_runs = (a.onx & 3) == 0;  // then no run crosses a row
   for (long long g = g0; g < nrun; g += gstride) {
     const long long o0 = g << 2;
     int i, j, k;
-    split3(o0, a.onx, a.ony, i, j, k);
+    if (narrow) {
+      // 32-bit division (the output holds fewer than 2^31 voxels)
+      const unsigned int u = (unsigned int)o0, onx = (unsigned int)a.onx;
+      const unsigned int row = u / onx;
+      i = (int)(u - row * onx);
+      j = (int)(row % (unsigned int)a.ony);
+      k = (int)(row / (unsigned int)a.ony);
+    } else {
+      split3(o0, a.onx, a.ony, i, j, k);
+    }
     double cj[3], ck[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
@@ -170,21 +193,27 @@ __device__ __forceinline__ void resample_runs(const ResampleArgs &a, long long g
     TO v[4];
     uint8_t m[4] = {0, 0, 0, 0};
     const int cnt = n - o0 < 4 ? (int)(n - o0) : 4;
+    if (row_runs) {
+      // the run lies in one row: four independent voxels
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      st_copy(v[u], 0.0f);
-      if (u < cnt) {
-        resample_voxel<IMG, MSK, TI, TO>(a, i, cj, ck, &v[u], &m[u]);
-        if (++i == a.onx) {
-          i = 0;
-          if (++j == a.ony) {
-            j = 0;
-            ++k;
+      for (int u = 0; u < 4; ++u) resample_voxel<IMG, MSK, TI, TO>(a, i + u, cj, ck, &v[u], &m[u]);
+    } else {
 #pragma unroll
-            for (int r = 0; r < 3; ++r) ck[r] = __dmul_rn(a.C[3 * r + 2], (double)k);
+      for (int u = 0; u < 4; ++u) {
+        st_copy(v[u], 0.0f);
+        if (u < cnt) {
+          resample_voxel<IMG, MSK, TI, TO>(a, i, cj, ck, &v[u], &m[u]);
+          if (++i == a.onx) {
+            i = 0;
+            if (++j == a.ony) {
+              j = 0;
+              ++k;
+#pragma unroll
+              for (int r = 0; r < 3; ++r) ck[r] = __dmul_rn(a.C[3 * r + 2], (double)k);
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r) cj[r] = __dmul_rn(a.C[3 * r + 1], (double)j);
           }
-#pragma unroll
-          for (int r = 0; r < 3; ++r) cj[r] = __dmul_rn(a.C[3 * r + 1], (double)j);
         }
       }
     }
@@ -215,15 +244,20 @@ __device__ __forceinline__ void resample_runs(const ResampleArgs &a, long long g
   }
 }
 
+// resident CTAs of 256 threads per SM the resampling kernels are compiled for
+#ifndef MB2_RS_MINB
+#define MB2_RS_MINB 3
+#endif
+
 template <bool IMG, bool MSK, typename TI, typename TO>
-__global__ void __launch_bounds__(256, 3) resample_kernel(ResampleArgs a) {
+__global__ void __launch_bounds__(256, MB2_RS_MINB) resample_kernel(ResampleArgs a) {
   resample_runs<IMG, MSK, TI, TO>(a, blockIdx.x * (long long)blockDim.x + threadIdx.x,
                                   (long long)gridDim.x * blockDim.x);
 }
 
 // Many resampling passes in one launch (grid.y = job).  A job's image is
 // float32 in and `out_dtype` out (or absent: mask only).
-__global__ void __launch_bounds__(256, 3) resample_batch_kernel(const ResampleJob *jobs) {
+__global__ void __launch_bounds__(256, MB2_RS_MINB) resample_batch_kernel(const ResampleJob *jobs) {
   const ResampleJob &j = jobs[blockIdx.y];
   if (!j.active) return;
   ResampleArgs a;
@@ -289,6 +323,10 @@ mirorr_status launch_resample(const int in_size[3], const void *in, const uint8_
   if (n <= 0 || (!a.out && !a.outm)) return MIRORR_OK;
   if (((uintptr_t)a.out & 15u) || ((uintptr_t)a.outm & 3u)) {
     set_error("resampler output buffers must be 16-byte (image) and 4-byte (mask) aligned");
+    return MIRORR_EINVAL;
+  }
+  if ((long long)in_size[0] * in_size[1] >= (1LL << 31)) {
+    set_error("resampler input slice of %d x %d voxels: at most 2^31 - 1", in_size[0], in_size[1]);
     return MIRORR_EINVAL;
   }
   long long blocks = ((n + 3) / 4 + 255) / 256;

@@ -581,9 +581,19 @@ MB2_HD void half_step(const double *K, const double *trans, double *m12) {
   matrix_sqrt4(m, m12);
 }
 
-// One inner iteration of the symmetric fit (itkSymMirorrRegistrationMethod.txx:865-1432).
-MB2_HD void lts_symmetric_step(LtsState &s, const LtsMoments &mo) {
+// One inner iteration of the symmetric fit (itkSymMirorrRegistrationMethod.txx:865-1432)
+// in three parts: lts_symmetric_pre (the two least-squares fits and the
+// averaged half-way matrices Kf, Kb with translations tf, tb), the two
+// independent square roots half_step(Kf, tf) and half_step(Kb, tb), which the
+// device runs on two lanes at once, and lts_symmetric_post.
+struct SymHalf {
   double np[12];
+  double K[2][9];
+  double t[2][3];
+};
+
+MB2_HD void lts_symmetric_pre(LtsState &s, const LtsMoments &mo, SymHalf &h) {
+  double *np = h.np;
   for (int i = 0; i < 12; ++i) np[i] = s.last_params[i];
   const double *im = mo.mean_i, *mm = mo.mean_m;
   double translation[3], ntrans[3];
@@ -644,9 +654,15 @@ MB2_HD void lts_symmetric_step(LtsState &s, const LtsMoments &mo) {
     for (int i = 0; i < 9; ++i) { Kf[i] = a[i]; Kb[i] = b[i]; }
   }
   for (int i = 0; i < 3; ++i) { tf[i] = (ff.t[i] + iB.t[i]) / 2.0; tb[i] = (iF.t[i] + fb.t[i]) / 2.0; }
-  double m12[16], im12[16];
-  half_step(Kf, tf, m12);
-  half_step(Kb, tb, im12);
+  for (int i = 0; i < 9; ++i) { h.K[0][i] = Kf[i]; h.K[1][i] = Kb[i]; }
+  for (int i = 0; i < 3; ++i) { h.t[0][i] = tf[i]; h.t[1][i] = tb[i]; }
+}
+
+MB2_HD void lts_symmetric_post(LtsState &s, const SymHalf &h, const double *m12,
+                               const double *im12) {
+  const double *np = h.np;
+  Tfm &ff = s.fin;
+  Tfm &fb = s.finb;
   double k3[9], l3[9];
   for (int r = 0; r < 3; ++r)
     for (int c = 0; c < 3; ++c) { k3[3 * r + c] = m12[4 * r + c]; l3[3 * r + c] = im12[4 * r + c]; }
@@ -669,6 +685,15 @@ MB2_HD void lts_symmetric_step(LtsState &s, const LtsMoments &mo) {
   for (int i = 0; i < npar; ++i) { double e = s.last_params[i] - np[i]; d += e * e; }
   s.delta = d;
   for (int i = 0; i < 12; ++i) s.last_params[i] = np[i];
+}
+
+MB2_HD void lts_symmetric_step(LtsState &s, const LtsMoments &mo) {
+  SymHalf h;
+  lts_symmetric_pre(s, mo, h);
+  double m12[16], im12[16];
+  half_step(h.K[0], h.t[0], m12);
+  half_step(h.K[1], h.t[1], im12);
+  lts_symmetric_post(s, h, m12, im12);
 }
 
 // After the inner loop: m_Transform->Compose(final, true) (classic) or the

@@ -83,15 +83,17 @@ def test_registration_matches_oracle_at_classic_rigid_128x128x64(ctx):
     assert err < err_0
 
 
-@pytest.mark.parametrize("mode,kind", [("symmetric", "affine"), ("classic", "rigid")])
-def test_iteration_graphs_equal_direct_launches(ctx, mode, kind):
+@pytest.mark.parametrize("mode,kind,keep", [("symmetric", "affine", 1.0), ("classic", "rigid", 1.0),
+                                            ("symmetric", "affine", 0.5)])
+def test_iteration_graphs_equal_direct_launches(ctx, mode, kind, keep):
     """Iterations replayed from a per-level CUDA graph (the default for float32
     storage) run the same kernels on the same data as direct launches: the
-    registration is bit-identical either way."""
+    registration is bit-identical either way (block keep 0.5: the variance
+    selection's cooperative launch inside the graph)."""
     ph = make_phantom((72, 64, 48), n_gauss=20, kind=kind, seed=71, max_angle_deg=4.0,
                       max_shift_vox=4.0)
     p = mb.reg_params(symmetric=mode == "symmetric", kind=kind, levels=2, iterations=5,
-                      nhood_gap=3, nhood_width=7)
+                      nhood_gap=3, nhood_width=7, block_keep=keep)
     try:
         ctx.set_graphs(False)
         direct, st0 = mb.register(ctx, ph.fixed, ph.moving, p)
