@@ -484,32 +484,42 @@ __global__ void __launch_bounds__(C::NT, 4) ncc_masked_kernel(NccArgs a) {
     }
     if (tid < BPC) s_nstr[tid] = 0;
     __syncthreads();
-    // stage the windows one plane per pass, a 16-lane group per window row
-    // (consecutive x): (y - c) ms, zero outside the image and in the padding,
-    // and the row's mask bits (warp ballot); the base blocks as x - mu
+    // stage the windows, a 16-lane group per window row (consecutive x): the
+    // E EY rows of a window (plane-major) are dealt round-robin to the CTA's
+    // groups, and a group issues the loads of up to CH rows before it stores:
+    // (y - c) ms, zero outside the image and in the padding, and the row's
+    // mask bits (warp ballot); the base blocks as x - mu
     {
-      constexpr int LPR = 16;
-      const int xl = tid & (LPR - 1), yl = tid / LPR;
-      const long long plane = (long long)nx * ny;
+      constexpr int LPR = 16, NGRP = C::NT / LPR, RPG = (NROW + NGRP - 1) / NGRP;
+      constexpr int CH = RPG < 6 ? RPG : 6;  // rows in flight per thread (registers)
+      const int xl = tid & (LPR - 1), grp = tid / LPR;
       for (int s = 0; s < BPC; ++s) {
         if (!s_state[s]) continue;
-        const int gx = s_o[s][0] + xl, gy = s_o[s][1] + yl, gz0 = s_o[s][2];
-        const bool xyin = xl < E && yl < E && gx >= 0 && gy >= 0 && gx < nx && gy < ny;
+        const int gx = s_o[s][0] + xl;
+        const bool xin = xl < E && gx >= 0 && gx < nx;
         const float c = s_c[s];
-        const long long q0 = ((long long)gz0 * ny + gy) * nx + gx;
-        float *wd = win + s * WIN + yl * EXP + xl;
-        unsigned int *bd = bits + s * NROW + yl;
+#pragma unroll 1
+        for (int i0 = 0; i0 < RPG; i0 += CH) {
+          float yv[CH];
+          bool msv[CH];
 #pragma unroll
-        for (int z = 0; z < E; ++z) {
-          const int gz = gz0 + z;
-          const bool in = xyin && gz >= 0 && gz < nz;
-          const long long q = q0 + z * plane;
-          const float yv = in ? __ldg(&a.search[q]) : 0.f;
-          const bool ms = in && __ldg(&a.smask[q]) != 0;
-          const unsigned int bal = __ballot_sync(0xffffffffu, ms);
-          if (yl < EY) {
-            if (xl < EXP) wd[z * PS] = ms ? yv - c : 0.f;
-            if (xl == 0) bd[z * EY] = (bal >> (tid & LPR)) & 0xFFFFu;
+          for (int i = 0; i < CH; ++i) {
+            const int rr = grp + (i0 + i) * NGRP, z = rr / EY, yl = rr - z * EY;
+            const int gy = s_o[s][1] + yl, gz = s_o[s][2] + z;
+            const bool in =
+                rr < NROW && xin && yl < E && gy >= 0 && gy < ny && gz >= 0 && gz < nz;
+            const long long q = ((long long)gz * ny + gy) * nx + gx;
+            yv[i] = in ? __ldg(&a.search[q]) : 0.f;
+            msv[i] = in && __ldg(&a.smask[q]) != 0;
+          }
+#pragma unroll
+          for (int i = 0; i < CH; ++i) {
+            const int rr = grp + (i0 + i) * NGRP, z = rr / EY, yl = rr - z * EY;
+            const unsigned int bal = __ballot_sync(0xffffffffu, msv[i]);
+            if (rr < NROW) {
+              if (xl < EXP) win[s * WIN + z * PS + yl * EXP + xl] = msv[i] ? yv[i] - c : 0.f;
+              if (xl == 0) bits[s * NROW + rr] = (bal >> (tid & LPR)) & 0xFFFFu;
+            }
           }
         }
       }
