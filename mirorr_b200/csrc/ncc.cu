@@ -48,7 +48,8 @@ constexpr float kDelta = 1e-4f;    // bound on |FP32 score - FP64 score|
 struct NccRec {
   float f1, f2;
   int cnt;        // listed candidates; -1: final result already written; > kK: overflow
-  int pad;
+  int full;       // 1: the base block and every candidate footprint lie wholly
+                  // inside both masks (the refinement reads no mask)
   int32_t p[kK + 2];  // candidate origins (linear voxel index)
 };
 
@@ -417,6 +418,7 @@ __device__ void finish_tile(const NccArgs &a, TileTail<C::BPC, C::TPB> &tt, cons
       }
     }
     rc.cnt = cnt;
+    rc.full = 0;
     if (count_fast) atomicAdd(&a.ctl[3], 1u);
   }
 }
@@ -1103,6 +1105,7 @@ __global__ void __launch_bounds__(C::WPC * 32, C::MINB) ncc_warp_kernel(NccArgs 
         }
       }
       rc.cnt = cnt;
+      rc.full = 1;
       atomicAdd(&a.ctl[3], 1u);
     }
     __syncwarp();
@@ -1431,6 +1434,7 @@ __global__ void __launch_bounds__(32 * NW, kXWarpsPerSM / NW)
         }
       }
       rc.cnt = cnt;
+      rc.full = 1;
       atomicAdd(&a.ctl[3], 1u);
       if (a.xl_count) {
         // candidates of the clipped window: valid offsets per axis
@@ -1599,6 +1603,7 @@ __global__ void __launch_bounds__(128) ncc_general_kernel(NccArgs a) {
         }
       }
       rc.cnt = cnt;
+      rc.full = 0;
     }
   }
 }
@@ -1681,7 +1686,11 @@ __global__ void __launch_bounds__(128) ncc_refine_kernel(NccArgs a) {
       // the thread's base block in a transposed shared slice (conflict-free)
       __shared__ float xs[B][128];
       const long long plane = (long long)a.ny * a.nx;
-      unsigned long long mbm = 0;
+      // with both masks full over the block's footprints every mask bit is
+      // set: no mask is read
+      const bool full = rc.full == 1;
+      constexpr unsigned long long kAll = B == 64 ? ~0ULL : (1ULL << B) - 1ULL;
+      unsigned long long mbm = full ? kAll : 0ULL;
       {
         float x[B];
 #pragma unroll
@@ -1689,7 +1698,7 @@ __global__ void __launch_bounds__(128) ncc_refine_kernel(NccArgs a) {
           const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
           const long long q = o + vz * plane + (long long)vy * a.nx + vx;
           x[v] = __ldg(&a.base[q]);
-          if (__ldg(&a.bmask[q])) mbm |= 1ULL << v;
+          if (!full && __ldg(&a.bmask[q])) mbm |= 1ULL << v;
         }
 #pragma unroll
         for (int v = 0; v < B; ++v) xs[v][threadIdx.x] = x[v];
@@ -1701,13 +1710,13 @@ __global__ void __launch_bounds__(128) ncc_refine_kernel(NccArgs a) {
       for (int i = 0; i < n; ++i) {
         const long long p = rc.p[i];
         float y[B];
-        unsigned long long msm = 0;
+        unsigned long long msm = full ? kAll : 0ULL;
 #pragma unroll
         for (int v = 0; v < B; ++v) {
           const int vx = v % BW, vy = (v / BW) % BW, vz = v / (BW * BW);
           const long long q = p + vz * plane + (long long)vy * a.nx + vx;
           y[v] = __ldg(&a.search[q]);
-          if (__ldg(&a.smask[q])) msm |= 1ULL << v;
+          if (!full && __ldg(&a.smask[q])) msm |= 1ULL << v;
         }
         double ms = 0.0;
 #pragma unroll
