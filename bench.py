@@ -652,6 +652,31 @@ def c4_leg(mb, ctx, n_batch=8, seed0=4000):
                                          C4_SHAPE, phs[0].spacing), 3),
                      "h2d_bytes": int(st.h2d_bytes), "matcher_calls": int(st.matcher_calls),
                      "block_ncc_evaluated": int(st.block_ncc_evaluated)}
+    # roofline of the search stage: the same registration again with the
+    # per-stage CUDA events on (outside the timed region); the block-width-5
+    # search is the direct FP32 kernel (2 * 5^3 flops per block-candidate,
+    # the cross term) plus its preparation kernels, against the nominal FP32
+    # FMA peak
+    peaks, peak_src = load_peaks()
+    ctx.set_profiling(True)
+    ctx.stage_times()
+    _, st_p = mb.register(ctx, host[0][0], host[0][1], params())
+    stage_ms, _ = ctx.stage_times()
+    ctx.set_profiling(False)
+    fp32_peak = 148 * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    flops = 2.0 * 125 * float(st_p.block_ncc_evaluated)
+    tflops = flops / (float(stage_ms[2]) * 1e-3) / 1e12 if stage_ms[2] > 0 else 0.0
+    out["roofline_search_stage"] = {
+        "kernels": "search stage of every matcher call (box statistics, window-AND, block "
+                   "preparation and the direct FP32 search ncc_fb16_kernel<__half, 5>)",
+        "bound": "fma", "achieved": round(tflops, 3), "peak": round(fp32_peak, 2),
+        "unit": "TFLOP/s", "frac": round(tflops / fp32_peak, 4),
+        "flops_per_block_ncc": 250, "block_ncc": int(st_p.block_ncc_evaluated),
+        "search_stage_ms": round(float(stage_ms[2]), 3),
+        "stage_ms": {k: round(float(v), 3) for k, v in
+                     zip(["box_stats", "selection", "ncc", "postfilter"], stage_ms)},
+        "peak_source": "nominal FP32 FMA: 148 SMs x 128 lanes x 2 x sm_max_mhz from "
+                       f"MEASURED_PEAKS.json ({peak_src})"}
     b = mb.Batch(ctx, max_slots=n_batch, hbm_budget=150e9)
     passes = []
     for _ in range(2):

@@ -1145,18 +1145,28 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 
 // ---------------------------------------------------------------------------
 // Direct FP32 search for the blocks the tensor form does not take (each
-// call's fb_list): one CTA per block, candidates over the threads, the masked
-// sums of the reference formula per candidate.  A candidate whose footprint
-// lies inside the search mask with the base block inside its mask uses the
-// box statistics for Syy and one product per voxel.  grid.y = call.
+// call's fb_list; block width 5 takes every block here): one CTA per block.
+// The window (at most 16^3 values, rows padded to 17 floats so the rows the
+// threads of a warp read fall in distinct banks) and the base block are
+// staged in shared memory.  Thread t owns the x strip of candidates at
+// (py, pz) = (t % ncy, t / ncy): per base row (vy, vz) it reads the window row
+// once and updates all its candidates' cross terms from registers, in the
+// raster order of the base block, so each candidate's sum is the one a
+// per-candidate loop forms (windows of more than 128 strips deal them
+// round-robin).  A candidate whose footprint lies inside the
+// search mask with the base block inside its mask is scored from that cross
+// term and the box statistics (Syy); any other candidate is re-summed with
+// the masked sums of the reference formula.  grid.y = call.
 // ---------------------------------------------------------------------------
 template <typename T, int BW>
 __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
   constexpr int NT = 128;
   constexpr int NB = BW * BW * BW;
+  constexpr int RS = 17;             // padded window row stride (floats)
+  constexpr int NCX = 16 - BW + 1;   // longest x strip (window extent <= 16)
   __shared__ float s_xt[NB], s_mb[NB];
-  __shared__ float s_y[16 * 16 * 16];
-  __shared__ uint8_t s_m[16 * 16 * 16];
+  __shared__ float s_y[16 * 16 * RS];
+  __shared__ uint8_t s_m[16 * 16 * RS];
   __shared__ Top2 s_red[NT / 32];
   const Args16 &a = calls[blockIdx.y];
   if (!a.active) return;
@@ -1184,11 +1194,17 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
       s_xt[t] = S16<T>::f(base[qq]) - pp.mu;
       s_mb[t] = mv;
     }
-    for (int i = tid; i < ex * ey * ez; i += NT) {
-      const int wx = i % ex, wy = (i / ex) % ey, wz = i / (ex * ey);
-      const long long qq = ((long long)(zlo + wz) * a.ny + (ylo + wy)) * a.nx + (xlo + wx);
-      s_y[(wz * 16 + wy) * 16 + wx] = S16<T>::f(search[qq]);
-      s_m[(wz * 16 + wy) * 16 + wx] = a.smask[qq] != 0 ? 1 : 0;
+    {
+      // a 16-lane group per window row (ex <= 16)
+      const int wx = tid & 15;
+      for (int r = tid >> 4; r < ey * ez; r += NT / 16) {
+        const int wy = r % ey, wz = r / ey;
+        if (wx < ex) {
+          const long long qq = ((long long)(zlo + wz) * a.ny + (ylo + wy)) * a.nx + (xlo + wx);
+          s_y[(wz * 16 + wy) * RS + wx] = S16<T>::f(search[qq]);
+          s_m[(wz * 16 + wy) * RS + wx] = a.smask[qq] != 0 ? 1 : 0;
+        }
+      }
     }
     __syncthreads();
     Top2 tp;
@@ -1196,38 +1212,59 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
     tp.b2 = -3.f;
     tp.i1 = 0x7fffffffffffffffLL;
     const int nc = ncx * ncy * ncz;
-    for (int c = tid; c < nc; c += NT) {
-      const int px = c % ncx, py = (c / ncx) % ncy, pz = c / (ncx * ncy);
-      const int cx = xlo + px, cy = ylo + py, cz = zlo + pz;
-      const long long idx = ((long long)cz * a.ny + cy) * a.nx + cx;
-      const float2 st = __ldg(a.stats + ((long long)cz * a.ny + cy) * a.sp + cx);
-      const float muy = st.x;
-      float sxy = 0.f, sxx = 0.f, syy = 0.f;
-      if (pp.mmode == 1 && !signbit(st.y)) {
-        // footprint and base block wholly inside their masks
-#pragma unroll 5
-        for (int i = 0; i < NB; ++i) {
-          const int vx = i % BW, vy = (i / BW) % BW, vz = i / (BW * BW);
-          sxy = fmaf(s_xt[i], s_y[((pz + vz) * 16 + py + vy) * 16 + px + vx], sxy);
-        }
-        sxy -= muy * pp.sxt;
-        sxx = pp.sxx;
-        syy = st.y;
-      } else {
-#pragma unroll 5
-        for (int i = 0; i < NB; ++i) {
-          const int vx = i % BW, vy = (i / BW) % BW, vz = i / (BW * BW);
-          const int w = ((pz + vz) * 16 + py + vy) * 16 + px + vx;
-          const float mk = s_mb[i] * (float)s_m[w];
-          const float dy = s_y[w] - muy;
-          const float xm = mk * s_xt[i];
-          sxy = fmaf(xm, dy, sxy);
-          sxx = fmaf(xm, s_xt[i], sxx);
-          syy = fmaf(mk * dy, dy, syy);
-        }
+    for (int strip = tid; strip < ncy * ncz; strip += NT) {
+      const int py = strip % ncy, pz = strip / ncy;
+      const int cy = ylo + py, cz = zlo + pz;
+      // the strip's cross terms (base block inside its mask only)
+      float acc[NCX];
+#pragma unroll
+      for (int px = 0; px < NCX; ++px) acc[px] = 0.f;
+      if (pp.mmode == 1) {
+        for (int vz = 0; vz < BW; ++vz)
+#pragma unroll
+          for (int vy = 0; vy < BW; ++vy) {
+            const float *row = s_y + ((pz + vz) * 16 + py + vy) * RS;
+            float r[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) r[k] = k < ex ? row[k] : 0.f;
+            float t[BW];
+#pragma unroll
+            for (int vx = 0; vx < BW; ++vx) t[vx] = s_xt[(vz * BW + vy) * BW + vx];
+#pragma unroll
+            for (int px = 0; px < NCX; ++px)
+#pragma unroll
+              for (int vx = 0; vx < BW; ++vx) acc[px] = fmaf(t[vx], r[px + vx], acc[px]);
+          }
       }
-      const float sc = (sxx <= 0.f || syy <= 0.f) ? -2.f : __fdividef(sxy * sxy, sxx * syy);
-      top2_add(tp, sc, idx);
+#pragma unroll
+      for (int px = 0; px < NCX; ++px) {
+        if (px >= ncx) break;
+        const int cx = xlo + px;
+        const long long idx = ((long long)cz * a.ny + cy) * a.nx + cx;
+        const float2 st = __ldg(a.stats + ((long long)cz * a.ny + cy) * a.sp + cx);
+        const float muy = st.x;
+        float sxy = 0.f, sxx = 0.f, syy = 0.f;
+        if (pp.mmode == 1 && !signbit(st.y)) {
+          // footprint and base block wholly inside their masks
+          sxy = acc[px] - muy * pp.sxt;
+          sxx = pp.sxx;
+          syy = st.y;
+        } else {
+#pragma unroll 5
+          for (int i = 0; i < NB; ++i) {
+            const int vx = i % BW, vy = (i / BW) % BW, vz = i / (BW * BW);
+            const int w = ((pz + vz) * 16 + py + vy) * RS + px + vx;
+            const float mk = s_mb[i] * (float)s_m[w];
+            const float dy = s_y[w] - muy;
+            const float xm = mk * s_xt[i];
+            sxy = fmaf(xm, dy, sxy);
+            sxx = fmaf(xm, s_xt[i], sxx);
+            syy = fmaf(mk * dy, dy, syy);
+          }
+        }
+        const float sc = (sxx <= 0.f || syy <= 0.f) ? -2.f : __fdividef(sxy * sxy, sxx * syy);
+        top2_add(tp, sc, idx);
+      }
     }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) top2_merge(tp, top2_shfl_xor(tp, o));
@@ -1453,8 +1490,8 @@ mirorr_status run16(int ncalls, Match16Call *host_calls, DevBuf &calls_dev, cuda
       MB2_LAUNCH_CHECK();
     }
   }
-  if (BWc == 5) ncc_fb16_kernel<T, 5><<<dim3((unsigned)SM * 4, (unsigned)ncalls), 128, 0, s>>>(dc);
-  else ncc_fb16_kernel<T, 4><<<dim3((unsigned)SM * 4, (unsigned)ncalls), 128, 0, s>>>(dc);
+  if (BWc == 5) ncc_fb16_kernel<T, 5><<<dim3((unsigned)SM * 8, (unsigned)ncalls), 128, 0, s>>>(dc);
+  else ncc_fb16_kernel<T, 4><<<dim3((unsigned)SM * 8, (unsigned)ncalls), 128, 0, s>>>(dc);
   MB2_LAUNCH_CHECK();
   return MIRORR_OK;
 }

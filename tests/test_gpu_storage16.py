@@ -131,3 +131,37 @@ def test_register16_matches_oracle(ctx, store, mode, kind, bw, nw, keep, shape, 
     print(f"{mode} {kind} {store}: max |dM| {dM:.2e}, TRE gpu {err:.4f} oracle {err_o:.4f}")
     np.testing.assert_allclose(tg.M, to.M, atol=1e-4, rtol=0)
     np.testing.assert_allclose(tg.off, to.off, atol=1e-3, rtol=0)
+
+
+def test_register16_large_config_slab_matches_oracle(ctx):
+    """The large stress configuration's settings (FP16 storage, block 5,
+    radius 5, 30 % of blocks kept, symmetric affine, LTS keep 0.5) on a
+    112x104x64 slab cropped from the centre of its 512x512x256 phantom pair
+    (GPU-generated from seed 4000 with the quadratic +-20 % bias field, the
+    first pair the large-configuration benchmark times).  Both slabs keep the
+    crop's physical origin, so they stay related by the phantom's transform.
+    The registration (one level, 4 iterations) must equal the FP64 oracle's on
+    the same stored values: matrices within 1e-4, offsets within 1e-3 mm."""
+    from mirorr_b200.phantom import make_phantom_gpu
+    full = (512, 512, 256)
+    ph = make_phantom_gpu(full, n_gauss=200, kind="affine", seed=4000, bias=0.2,
+                          max_angle_deg=8.0, max_shift_vox=12.0)
+    sx, sy, sz = 112, 104, 64
+    x0, y0, z0 = (full[0] - sx) // 2, (full[1] - sy) // 2, (full[2] - sz) // 2
+    fixed = np.ascontiguousarray(ph.fixed[z0:z0 + sz, y0:y0 + sy, x0:x0 + sx])
+    moving = np.ascontiguousarray(ph.moving[z0:z0 + sz, y0:y0 + sy, x0:x0 + sx])
+    origin = np.array([x0, y0, z0], np.float64)
+    spacing = np.ones(3)
+    rp = O.RegParams("symmetric", "affine", 4, O.BMParams(5, 1, 3, 11, 0.3), 0.5, "f16")
+    to = O.register(O.Image(fixed, spacing, origin), O.Image(moving, spacing, origin), rp, 1)
+    p = mb.reg_params(symmetric=True, kind="affine", levels=1, iterations=4, block_width=5,
+                      nhood_gap=3, nhood_width=11, block_keep=0.3, lts_keep=0.5, storage="f16")
+    fs, ms = mb.to_storage(fixed, "f16"), mb.to_storage(moving, "f16")
+    tg, st = mb.register(ctx, fs, ms, p, fixed_geom=mb.Geometry.of(fs, spacing, origin),
+                         moving_geom=mb.Geometry.of(ms, spacing, origin))
+    assert st.levels_run == 1 and st.block_ncc_evaluated > 0
+    dM = np.max(np.abs(tg.M - to.M))
+    print(f"large-configuration slab: max |dM| {dM:.2e}, max |d offset| "
+          f"{np.max(np.abs(tg.off - to.off)):.2e}")
+    np.testing.assert_allclose(tg.M, to.M, atol=1e-4, rtol=0)
+    np.testing.assert_allclose(tg.off, to.off, atol=1e-3, rtol=0)
