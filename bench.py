@@ -839,13 +839,14 @@ def run_leg(args):
         print(json.dumps(res))
         m.close()
     elif args.leg == "matcher16":
-        # one matcher call with 16-bit storage (tensor-core search) beside the
-        # same call with float32 storage: block 4, radius --radius, spacing 3
+        # one matcher call with 16-bit storage (tensor-core search at block 4,
+        # the direct search at block 5) beside the same call with float32
+        # storage: block --bw, radius --radius, spacing 3
         res = {}
         for store in ["f32", args.store]:
             m = mb.BlockMatcher(ctx)
             m.SetStorage(store)
-            m.SetBlockWidth(BW)
+            m.SetBlockWidth(args.bw)
             m.SetNhoodWidth(2 * args.radius + 1)
             m.SetNhoodGap(G)
             m.SetBaseImage(ph.moving)
@@ -927,6 +928,7 @@ def main():
                     default=None)
     ap.add_argument("--store", default="bf16")
     ap.add_argument("--radius", type=int, default=3)
+    ap.add_argument("--bw", type=int, default=BW, help="block width of the matcher16 leg")
     ap.add_argument("--calls", type=int, default=3)
     ap.add_argument("--shape", default="256,256,128")
     ap.add_argument("--masked", action="store_true")

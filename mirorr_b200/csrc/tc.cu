@@ -1146,9 +1146,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 // ---------------------------------------------------------------------------
 // Direct FP32 search for the blocks the tensor form does not take (each
 // call's fb_list; block width 5 takes every block here): one CTA per block.
-// The window (at most 16^3 values, rows padded to 17 floats so the rows the
-// threads of a warp read fall in distinct banks) and the base block are
-// staged in shared memory.  Thread t owns the x strip of candidates at
+// The window (at most 16^3 values) and the base block are staged in shared
+// memory; window rows are 18 floats apart and planes 16 x 18 + 6, so the
+// rows the threads of a warp read (11 strips per plane at window 11) start on
+// distinct bank pairs and a row is read with 8-byte loads.  Thread t owns the x strip of candidates at
 // (py, pz) = (t % ncy, t / ncy): per base row (vy, vz) it reads the window row
 // once and updates all its candidates' cross terms from registers, in the
 // raster order of the base block, so each candidate's sum is the one a
@@ -1162,11 +1163,12 @@ template <typename T, int BW>
 __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
   constexpr int NT = 128;
   constexpr int NB = BW * BW * BW;
-  constexpr int RS = 17;             // padded window row stride (floats)
+  constexpr int RS = 18;             // window row stride (floats)
+  constexpr int PS = 16 * RS + 6;    // window plane stride (floats)
   constexpr int NCX = 16 - BW + 1;   // longest x strip (window extent <= 16)
   __shared__ float s_xt[NB], s_mb[NB];
-  __shared__ float s_y[16 * 16 * RS];
-  __shared__ uint8_t s_m[16 * 16 * RS];
+  __shared__ __align__(16) float s_y[16 * PS];
+  __shared__ uint8_t s_m[16 * PS];
   __shared__ Top2 s_red[NT / 32];
   const Args16 &a = calls[blockIdx.y];
   if (!a.active) return;
@@ -1195,14 +1197,24 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
       s_mb[t] = mv;
     }
     {
-      // a 16-lane group per window row (ex <= 16)
+      // a 16-lane group per window row (ex <= 16); the group's row (wy, wz)
+      // advances by NT / 16 rows without a division
       const int wx = tid & 15;
-      for (int r = tid >> 4; r < ey * ez; r += NT / 16) {
-        const int wy = r % ey, wz = r / ey;
+      int wy = tid >> 4, wz = ncx > 0 && ncy > 0 && ncz > 0 ? 0 : ez;  // empty window: none
+      while (wz < ez && wy >= ey) {
+        wy -= ey;
+        ++wz;
+      }
+      for (; wz < ez;) {
         if (wx < ex) {
           const long long qq = ((long long)(zlo + wz) * a.ny + (ylo + wy)) * a.nx + (xlo + wx);
-          s_y[(wz * 16 + wy) * RS + wx] = S16<T>::f(search[qq]);
-          s_m[(wz * 16 + wy) * RS + wx] = a.smask[qq] != 0 ? 1 : 0;
+          s_y[wz * PS + wy * RS + wx] = S16<T>::f(search[qq]);
+          s_m[wz * PS + wy * RS + wx] = a.smask[qq] != 0 ? 1 : 0;
+        }
+        wy += NT / 16;
+        while (wy >= ey) {
+          wy -= ey;
+          ++wz;
         }
       }
     }
@@ -1223,10 +1235,16 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
         for (int vz = 0; vz < BW; ++vz)
 #pragma unroll
           for (int vy = 0; vy < BW; ++vy) {
-            const float *row = s_y + ((pz + vz) * 16 + py + vy) * RS;
+            // values past the window's extent only feed strip positions
+            // px >= ncx, which are not scored
+            const float2 *row = reinterpret_cast<const float2 *>(s_y + (pz + vz) * PS + (py + vy) * RS);
             float r[16];
 #pragma unroll
-            for (int k = 0; k < 16; ++k) r[k] = k < ex ? row[k] : 0.f;
+            for (int k = 0; k < 8; ++k) {
+              const float2 q = row[k];
+              r[2 * k] = q.x;
+              r[2 * k + 1] = q.y;
+            }
             float t[BW];
 #pragma unroll
             for (int vx = 0; vx < BW; ++vx) t[vx] = s_xt[(vz * BW + vy) * BW + vx];
@@ -1253,7 +1271,7 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
 #pragma unroll 5
           for (int i = 0; i < NB; ++i) {
             const int vx = i % BW, vy = (i / BW) % BW, vz = i / (BW * BW);
-            const int w = ((pz + vz) * 16 + py + vy) * RS + px + vx;
+            const int w = (pz + vz) * PS + (py + vy) * RS + px + vx;
             const float mk = s_mb[i] * (float)s_m[w];
             const float dy = s_y[w] - muy;
             const float xm = mk * s_xt[i];
