@@ -28,6 +28,7 @@ Profiling legs (`--leg ...`), for ncu captures on one GPU:
   matcher        one finest-level matcher call (--masked, --base-masked add
                  field-of-view masks);
   matcher16      the same call with 16-bit storage beside float32;
+  registration   whole registrations of the benchmark workload;
   selector       the variance selection stage (block keep 0.5);
   resample-pass  one finest-level image + mask resampling pass;
   resample       the final-resampling interpolators through host buffers;
@@ -865,6 +866,18 @@ def run_leg(args):
                           "ms_postfilter": ts[-1][3], "diag": [int(v) for v in d]}
             m.close()
         print(json.dumps(res))
+    elif args.leg == "registration":
+        # --calls registrations of the benchmark workload (its pair, seed
+        # 1000, at --shape), host buffers in and out, for a launch list of the
+        # whole path
+        wp = ph
+        p = reg_params(mb)
+        out = []
+        for _ in range(args.calls):
+            r, st = mb.register(ctx, wp.fixed, wp.moving, p)
+            out.append({"iterations": list(st.iterations_run)[:LEVELS],
+                        "matcher_calls": int(st.matcher_calls)})
+        print(json.dumps({"registrations": out, "kernel_launches": ctx.kernel_launches()}))
     elif args.leg in ("selector", "resample-pass"):
         # the variance selection stage (keep 0.5) or one finest-level image +
         # mask resampling pass, with their HBM rooflines
@@ -924,7 +937,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched (64 uneven pairs) and served (Poisson) legs")
     ap.add_argument("--leg", choices=["matcher", "matcher16", "resample", "resample-pass",
-                                      "selector", "batched", "large"],
+                                      "selector", "registration", "batched", "large"],
                     default=None)
     ap.add_argument("--store", default="bf16")
     ap.add_argument("--radius", type=int, default=3)
