@@ -1160,7 +1160,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 // the masked sums of the reference formula.  grid.y = call.
 // ---------------------------------------------------------------------------
 template <typename T, int BW>
-__global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
+__global__ void __launch_bounds__(128, 8) ncc_fb16_kernel(const Args16 *calls) {
   constexpr int NT = 128;
   constexpr int NB = BW * BW * BW;
   constexpr int RS = 18;             // window row stride (floats)
@@ -1205,17 +1205,32 @@ __global__ void __launch_bounds__(128) ncc_fb16_kernel(const Args16 *calls) {
         wy -= ey;
         ++wz;
       }
-      for (; wz < ez;) {
-        if (wx < ex) {
-          const long long qq = ((long long)(zlo + wz) * a.ny + (ylo + wy)) * a.nx + (xlo + wx);
-          s_y[wz * PS + wy * RS + wx] = S16<T>::f(search[qq]);
-          s_m[wz * PS + wy * RS + wx] = a.smask[qq] != 0 ? 1 : 0;
+      // four rows per pass, all of their loads issued before the stores
+      while (wz < ez) {
+        T yv[4];
+        uint8_t mv[4];
+        int so[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          so[j] = -1;
+          if (wz < ez && wx < ex) {
+            const long long qq = ((long long)(zlo + wz) * a.ny + (ylo + wy)) * a.nx + (xlo + wx);
+            yv[j] = search[qq];
+            mv[j] = a.smask[qq];
+            so[j] = wz * PS + wy * RS + wx;
+          }
+          wy += NT / 16;
+          while (wz < ez && wy >= ey) {
+            wy -= ey;
+            ++wz;
+          }
         }
-        wy += NT / 16;
-        while (wy >= ey) {
-          wy -= ey;
-          ++wz;
-        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (so[j] >= 0) {
+            s_y[so[j]] = S16<T>::f(yv[j]);
+            s_m[so[j]] = mv[j] != 0 ? 1 : 0;
+          }
       }
     }
     __syncthreads();
