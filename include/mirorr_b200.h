@@ -145,7 +145,9 @@ MIRORR_API mirorr_status mirorr_bm_grid(mirorr_matcher m, int32_t nblocks[3], in
  * itkAbstractBlockMatcher.h:271-287) with the blocks that pass the post-filter,
  * in block-grid raster order.  *n_out receives the count.  If capacity is
  * too small returns ERANGE with *n_out = required count.  Zero kept blocks
- * -> ENOBLOCKS (the GPU matcher's BlockMatcherGPUExceptionAlgo). */
+ * -> ENOBLOCKS (the GPU matcher's BlockMatcherGPUExceptionAlgo).  ETIMEOUT:
+ * a bounded device wait of the search (a tensor copy, or the variance
+ * selection's grid barrier) gave up; the whole call's results are invalid. */
 MIRORR_API mirorr_status mirorr_bm_get_offsets(mirorr_matcher m, size_t capacity, double *block_positions,
                                     double *match_positions, size_t *n_out);
 /* Per-block results of the last GetOffsets, grid raster order, for every
