@@ -472,10 +472,12 @@ mirorr_status launch_variance_selection(const BmGeom &g, const void *base, doubl
 // ---------------------------------------------------------------------------
 constexpr int kTile = 2048;  // blocks per compaction tile (256 threads x 8)
 
+// The three reads are unconditional (every block has a status and scores),
+// so a thread's blocks are all read before the tests.
 __device__ inline bool keep_block(const BmOut &o, long long b) {
-  if (!(o.status[b] & 1)) return false;
-  double cb = (double)o.best[b], c2 = (double)o.second[b];
-  return cb > 1e-7 && fabs(cb - c2) > 1e-4;
+  const uint8_t st = o.status[b];
+  const double cb = (double)o.best[b], c2 = (double)o.second[b];
+  return (st & 1) && cb > 1e-7 && fabs(cb - c2) > 1e-4;
 }
 
 __device__ void pf_count_tile(const BmOut &o, long long n, unsigned int *tile_count, long long tile) {
@@ -485,8 +487,9 @@ __device__ void pf_count_tile(const BmOut &o, long long n, unsigned int *tile_co
   __syncthreads();
   long long t0 = tile * kTile;
   unsigned int c = 0;
-  for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
-    long long b = t0 + i;
+#pragma unroll
+  for (int k = 0; k < kTile / 256; ++k) {  // 256 threads per CTA
+    long long b = t0 + threadIdx.x + 256 * k;
     if (b < n && keep_block(o, b)) ++c;
   }
   c = __reduce_add_sync(0xffffffffu, c);
@@ -559,6 +562,7 @@ __device__ void pf_write_tile(const BmOut &o, long long n, const unsigned int *t
   const int per = kTile / 256;  // 8 consecutive blocks per thread
   long long t0 = tile * kTile + (long long)threadIdx.x * per;
   unsigned int flags = 0, c = 0;
+#pragma unroll
   for (int k = 0; k < per; ++k) {
     long long b = t0 + k;
     if (b < n && keep_block(o, b)) {

@@ -242,16 +242,22 @@ __device__ inline void finish_unmasked_block(const NccArgs &a, long long b) {
 // ---------------------------------------------------------------------------
 // base-block statistics (one thread per block)
 // ---------------------------------------------------------------------------
+// BW > 0: the block width known at compile time (the block's loads are all
+// issued before the sums); BW = 0: a.bw at run time.  Same arithmetic order.
+template <int BW>
 __global__ void block_stat_kernel(NccArgs a) {
   for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < a.nblocks;
        b += (long long)gridDim.x * blockDim.x) {
     int bx = (int)(b % a.nbx), by = (int)((b / a.nbx) % a.nby), bz = (int)(b / ((long long)a.nbx * a.nby));
     long long o = lin(a, a.stx + bx * a.G, a.sty + by * a.G, a.stz + bz * a.G);
-    const int bw = a.bw;
+    const int bw = BW > 0 ? BW : a.bw;
     double sum = 0.0;
     int nin = 0;
+#pragma unroll
     for (int z = 0; z < bw; ++z)
+#pragma unroll
       for (int y = 0; y < bw; ++y)
+#pragma unroll
         for (int x = 0; x < bw; ++x) {
           long long q = o + ((long long)z * a.ny + y) * a.nx + x;
           sum = __dadd_rn(sum, (double)__ldg(&a.base[q]));
@@ -259,8 +265,11 @@ __global__ void block_stat_kernel(NccArgs a) {
         }
     double mean = __ddiv_rn(sum, (double)(bw * bw * bw));
     double sxx = 0.0, sxt = 0.0;
+#pragma unroll
     for (int z = 0; z < bw; ++z)
+#pragma unroll
       for (int y = 0; y < bw; ++y)
+#pragma unroll
         for (int x = 0; x < bw; ++x) {
           long long q = o + ((long long)z * a.ny + y) * a.nx + x;
           if (__ldg(&a.bmask[q])) {
@@ -2051,7 +2060,9 @@ mirorr_status launch_ncc(const BmGeom &g, const float *base, const uint8_t *bmas
   {
     long long grid = (g.nblocks + 127) / 128;
     if (grid > (long long)sm_count() * 16) grid = (long long)sm_count() * 16;
-    block_stat_kernel<<<(unsigned)grid, 128, 0, s>>>(a);
+    if (a.bw == 4) block_stat_kernel<4><<<(unsigned)grid, 128, 0, s>>>(a);
+    else if (a.bw == 5) block_stat_kernel<5><<<(unsigned)grid, 128, 0, s>>>(a);
+    else block_stat_kernel<0><<<(unsigned)grid, 128, 0, s>>>(a);
     MB2_LAUNCH_CHECK();
   }
   mirorr_status st = MIRORR_OK;
