@@ -434,35 +434,104 @@ MB2_HD void quat_from_axis_angle(const double *axis, double angle, double *q) {
 // sum Q^T Q = sum_i C_i^T Z C_i over its coefficient vectors.  Returns the
 // eigenvector of the smallest eigenvalue as (x, y, z, r).
 MB2_HD void horn_quaternion(const double *Z, double *q) {
-  // coef[(i*4+j)*6 + k]: coefficient of z_k in Q[i][j]
-  double coef[16 * 6];
-  for (int i = 0; i < 16 * 6; ++i) coef[i] = 0.0;
-#define QC(i, j, k, v) coef[((i)*4 + (j)) * 6 + (k)] = (v)
-  QC(0, 1, 0, 1.0); QC(0, 1, 3, -1.0);
-  QC(0, 2, 1, 1.0); QC(0, 2, 4, -1.0);
-  QC(0, 3, 2, 1.0); QC(0, 3, 5, -1.0);
-  QC(1, 2, 2, -1.0); QC(1, 2, 5, -1.0);
-  QC(1, 3, 1, 1.0); QC(1, 3, 4, 1.0);
-  QC(2, 3, 0, -1.0); QC(2, 3, 3, -1.0);
-#undef QC
-  for (int i = 0; i < 4; ++i)
-    for (int j = i + 1; j < 4; ++j)
-      for (int k = 0; k < 6; ++k) coef[(j * 4 + i) * 6 + k] = -coef[(i * 4 + j) * 6 + k];
+  // tot = sum over the subset of Q^T Q, Q the 4x4 matrix of one pair whose
+  // entries are +-1 times the six centred coordinates z_k: entry (j, l) is
+  // sum_i sum_{a,b} c(i,j,a) c(i,l,b) Z[a][b] over the non-zero coefficients
+  // c (all +-1), written out term by term in that order (i, then a, then b),
+  // so every entry is the same sequence of additions as the coefficient form
   double tot[16];
-  for (int j = 0; j < 4; ++j)
-    for (int l = 0; l < 4; ++l) {
-      double s = 0.0;
-      for (int i = 0; i < 4; ++i) {
-        const double *u = &coef[(i * 4 + j) * 6];
-        const double *w = &coef[(i * 4 + l) * 6];
-        for (int a = 0; a < 6; ++a) {
-          if (u[a] == 0.0) continue;
-          for (int b = 0; b < 6; ++b)
-            if (w[b] != 0.0) s += u[a] * w[b] * Z[6 * a + b];
-        }
-      }
-      tot[4 * j + l] = s;
-    }
+  {  // entry (0, 0)
+    double s = 0.0;
+    s += Z[0]; s -= Z[3]; s -= Z[18]; s += Z[21]; s += Z[7]; s -= Z[10]; s -= Z[25]; s += Z[28];
+    s += Z[14]; s -= Z[17]; s -= Z[32]; s += Z[35];
+    tot[0] = s;
+  }
+  {  // entry (0, 1)
+    double s = 0.0;
+    s -= Z[8]; s -= Z[11]; s += Z[26]; s += Z[29]; s += Z[13]; s += Z[16]; s -= Z[31];
+    s -= Z[34];
+    tot[1] = s;
+  }
+  {  // entry (0, 2)
+    double s = 0.0;
+    s += Z[2]; s += Z[5]; s -= Z[20]; s -= Z[23]; s -= Z[12]; s -= Z[15]; s += Z[30];
+    s += Z[33];
+    tot[2] = s;
+  }
+  {  // entry (0, 3)
+    double s = 0.0;
+    s -= Z[1]; s -= Z[4]; s += Z[19]; s += Z[22]; s += Z[6]; s += Z[9]; s -= Z[24]; s -= Z[27];
+    tot[3] = s;
+  }
+  {  // entry (1, 0)
+    double s = 0.0;
+    s -= Z[13]; s += Z[16]; s -= Z[31]; s += Z[34]; s += Z[8]; s -= Z[11]; s += Z[26];
+    s -= Z[29];
+    tot[4] = s;
+  }
+  {  // entry (1, 1)
+    double s = 0.0;
+    s += Z[0]; s -= Z[3]; s -= Z[18]; s += Z[21]; s += Z[14]; s += Z[17]; s += Z[32];
+    s += Z[35]; s += Z[7]; s += Z[10]; s += Z[25]; s += Z[28];
+    tot[5] = s;
+  }
+  {  // entry (1, 2)
+    double s = 0.0;
+    s += Z[1]; s -= Z[4]; s -= Z[19]; s += Z[22]; s -= Z[6]; s -= Z[9]; s -= Z[24]; s -= Z[27];
+    tot[6] = s;
+  }
+  {  // entry (1, 3)
+    double s = 0.0;
+    s += Z[2]; s -= Z[5]; s -= Z[20]; s += Z[23]; s -= Z[12]; s -= Z[15]; s -= Z[30];
+    s -= Z[33];
+    tot[7] = s;
+  }
+  {  // entry (2, 0)
+    double s = 0.0;
+    s += Z[12]; s -= Z[15]; s += Z[30]; s -= Z[33]; s -= Z[2]; s += Z[5]; s -= Z[20];
+    s += Z[23];
+    tot[8] = s;
+  }
+  {  // entry (2, 1)
+    double s = 0.0;
+    s += Z[6]; s -= Z[9]; s -= Z[24]; s += Z[27]; s -= Z[1]; s -= Z[4]; s -= Z[19]; s -= Z[22];
+    tot[9] = s;
+  }
+  {  // entry (2, 2)
+    double s = 0.0;
+    s += Z[7]; s -= Z[10]; s -= Z[25]; s += Z[28]; s += Z[14]; s += Z[17]; s += Z[32];
+    s += Z[35]; s += Z[0]; s += Z[3]; s += Z[18]; s += Z[21];
+    tot[10] = s;
+  }
+  {  // entry (2, 3)
+    double s = 0.0;
+    s += Z[8]; s -= Z[11]; s -= Z[26]; s += Z[29]; s -= Z[13]; s -= Z[16]; s -= Z[31];
+    s -= Z[34];
+    tot[11] = s;
+  }
+  {  // entry (3, 0)
+    double s = 0.0;
+    s -= Z[6]; s += Z[9]; s -= Z[24]; s += Z[27]; s += Z[1]; s -= Z[4]; s += Z[19]; s -= Z[22];
+    tot[12] = s;
+  }
+  {  // entry (3, 1)
+    double s = 0.0;
+    s += Z[12]; s -= Z[15]; s -= Z[30]; s += Z[33]; s -= Z[2]; s -= Z[5]; s -= Z[20];
+    s -= Z[23];
+    tot[13] = s;
+  }
+  {  // entry (3, 2)
+    double s = 0.0;
+    s += Z[13]; s -= Z[16]; s -= Z[31]; s += Z[34]; s -= Z[8]; s -= Z[11]; s -= Z[26];
+    s -= Z[29];
+    tot[14] = s;
+  }
+  {  // entry (3, 3)
+    double s = 0.0;
+    s += Z[14]; s -= Z[17]; s -= Z[32]; s += Z[35]; s += Z[7]; s += Z[10]; s += Z[25];
+    s += Z[28]; s += Z[0]; s += Z[3]; s += Z[18]; s += Z[21];
+    tot[15] = s;
+  }
   double ev[4], vec[16];
   jacobi_eigen<4>(tot, ev, vec);
   q[0] = vec[4 * 1 + 0];
