@@ -365,7 +365,7 @@ int run(int argc, char **argv) {
   }
   for (const char *k : {"reorient-fixed", "reorient-moving", "save-fixed", "save-moving",
                         "save-reoriented-fixed", "save-reoriented-moving", "switch-images"})
-    if (a.has(k)) throw std::runtime_error(std::string("--") + k + " is outside this build's path");
+    if (a.has(k)) throw std::runtime_error(std::string("--") + k + " is not available in this command line (not part of the registration path it implements)");
   if (a.get("blockmetric", "nc") != "nc")
     throw std::runtime_error("only the normalised correlation block metric (nc) is available");
   if (a.get("resampling-mode", "middle") != "middle")

@@ -85,7 +85,7 @@ def test_help_and_errors(cli, tmp_path):
     write_nifti(str(img), np.zeros((4, 5, 6), np.float32))
     r = subprocess.run([cli, "-m", str(img), "-f", str(img), "--reorient-fixed"],
                        capture_output=True, text=True)
-    assert r.returncode == 1 and "outside" in r.stderr
+    assert r.returncode == 1 and "not available" in r.stderr
     r = subprocess.run([cli, "-m", str(img), "-f", str(img), "--crop", "4"],
                        capture_output=True, text=True)
     assert r.returncode == 1 and "movingX,movingY,fixedX,fixedY" in r.stderr
