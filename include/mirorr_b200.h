@@ -439,8 +439,8 @@ MIRORR_API mirorr_status mirorr_ctx_search_kernel_times(mirorr_ctx ctx, double *
 MIRORR_API mirorr_status mirorr_ctx_resample_times(mirorr_ctx ctx, double *ms, int64_t *passes,
                                         int64_t *voxels);
 /* A test aid with no counterpart in the reference: the number of polls a
- * grid-barrier wait of the LTS kernel makes before it gives up (0 restores the
- * default of 2^23 polls, about 0.84 s).  When a wait gives up, every CTA of the
+ * grid-barrier wait of the LTS kernel and of the variance selection makes
+ * before it gives up (0 restores the default of 2^23 polls, about 0.84 s).  When a wait gives up, every CTA of the
  * launch returns, the call returns MIRORR_ETIMEOUT, the caller's transforms
  * are left as they were, and the context stays usable.  A tiny limit makes the
  * waits give up on CTAs that are merely late, which is how the tests reach

@@ -429,7 +429,8 @@ size_t selection_state_bytes() { return sizeof(SelectCtl) + sizeof(unsigned int)
 
 mirorr_status launch_variance_selection(const BmGeom &g, const void *base, double keep,
                                         BmWork &w, const uint8_t **selected_out,
-                                        cudaStream_t s, int dtype, unsigned int *give_up) {
+                                        cudaStream_t s, int dtype, unsigned int *give_up,
+                                        long long spin_limit) {
   *selected_out = nullptr;
   if (!(keep < 1.0)) return MIRORR_OK;
   long long n = g.nblocks;
@@ -455,7 +456,7 @@ mirorr_status launch_variance_selection(const BmGeom &g, const void *base, doubl
   a.hist = reinterpret_cast<unsigned int *>(a.ctl + 1);
   a.selected = w.selected.as<uint8_t>();
   a.give_up = give_up;
-  a.spin_limit = 1LL << 23;  // about 0.84 s of polling
+  a.spin_limit = spin_limit > 0 ? spin_limit : 1LL << 23;  // default: about 0.84 s of polling
   // a memset, not a host copy, so the sequence can be captured into a graph
   MB2_CUDA_TRY(cudaMemsetAsync(w.select_state.ptr, 0, ctl_bytes, s));
   // the reference's FP64 variance (exact k-th value, so the selected blocks

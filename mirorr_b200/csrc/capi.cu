@@ -347,7 +347,7 @@ mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall
     unsigned int *give_up = nullptr;
     if (p.block_keep < 1.0) MB2_TRY(ncc_give_up_flag(c->bmw, s, &give_up));
     MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s, mc.dtype,
-                                      give_up));
+                                      give_up, c->ltsw.spin_limit));
     if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
     MB2_TRY(launch_match16(mc.dtype, g, mc.base, mc.bmask, mc.search, mc.smask, sel, out, c->bm16,
                            c->ncc_count.as<unsigned long long>(), s));
@@ -362,7 +362,7 @@ mirorr_status run_match(mirorr_ctx c, const mirorr_bm_params &p, const MatchCall
     unsigned int *give_up = nullptr;
     if (p.block_keep < 1.0) MB2_TRY(ncc_give_up_flag(c->bmw, s, &give_up));
     MB2_TRY(launch_variance_selection(g, mc.base, p.block_keep, c->bmw, &sel, s,
-                                      MIRORR_DTYPE_F32, give_up));
+                                      MIRORR_DTYPE_F32, give_up, c->ltsw.spin_limit));
     if (ev) MB2_CUDA_TRY(cudaEventRecord(ev[2], s));
     MB2_TRY(launch_ncc(g, static_cast<const float *>(mc.base), mc.bmask,
                        static_cast<const float *>(mc.search), mc.smask, c->bmw.stats.as<float2>(),
@@ -2322,7 +2322,7 @@ mirorr_status batch_issue(mirorr_batch b, int njobs, long long max_vox, int ncal
       if (!(s.p.bm.block_keep < 1.0)) continue;
       const uint8_t *sel = nullptr;
       MB2_TRY(launch_variance_selection(s.g, calls[ci].base, s.p.bm.block_keep, s.call[k].sel, &sel, st,
-                                        b->storage, calls[ci].ctl + 2));
+                                        b->storage, calls[ci].ctl + 2, c->ltsw.spin_limit));
     }
   }
   MB2_TRY(launch_match16_batch(b->storage, ncalls, b->h_calls.as<Match16Call>(), b->d_calls, st,

@@ -58,11 +58,13 @@ mirorr_status launch_box_stats(const BmGeom &g, const float *search, const uint8
 size_t selection_var_bytes(long long nblocks);
 size_t selection_state_bytes();
 // give_up: a device flag the selection sets when one of its grid-barrier waits
-// gives up (the call's result is then invalid), or null.
+// gives up (the call's result is then invalid), or null.  spin_limit: polls of
+// such a wait before it gives up (0: the default, about 0.84 s).
 mirorr_status launch_variance_selection(const BmGeom &g, const void *base, double keep,
                                         BmWork &w, const uint8_t **selected_out,
                                         cudaStream_t s, int dtype = MIRORR_DTYPE_F32,
-                                        unsigned int *give_up = nullptr);
+                                        unsigned int *give_up = nullptr,
+                                        long long spin_limit = 0);
 // ncc_count (optional): device counter incremented by the number of candidate
 // scores evaluated.  Profiling (optional): kev[0], kev[1] are recorded around
 // the per-x-lane search kernel's launch and xl_count adds up the candidates it

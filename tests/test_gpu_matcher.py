@@ -147,3 +147,34 @@ def test_parameter_errors(ctx):
     with pytest.raises(mb.MirorrError) as e:
         m.GetOffsets()
     assert e.value.name == "ESTATE"
+
+
+def test_selection_barrier_wait_gives_up_and_context_recovers(ctx):
+    """The variance selection's grid-barrier waits are bounded like the LTS
+    fit's (the context's wait limit).  With a limit of one poll the CTAs that
+    reach a barrier before the others give up and every CTA returns; GetOffsets
+    reports ETIMEOUT, its results being invalid.  With the default limit the
+    same call then returns exactly what it returned before: the context and
+    the GPU stay usable.  Nothing faults: the waits just end early."""
+    ph = make_phantom((256, 256, 96), n_gauss=20, kind="affine", seed=77)
+    m = mb.BlockMatcher(ctx)
+    m.SetNhoodGap(3)
+    m.SetNhoodWidth(7)
+    m.SetBlockKeep(0.5)  # ~220k blocks: the selection runs on many CTAs
+    m.SetBaseImage(ph.moving)
+    m.SetSearchImage(ph.fixed)
+    bp0, mp0 = m.GetOffsets()
+    res0 = m.BlockResults()
+    ctx.set_wait_limit(1)
+    try:
+        with pytest.raises(mb.MirorrError) as e:
+            m.GetOffsets()
+        assert e.value.name == "ETIMEOUT"
+    finally:
+        ctx.set_wait_limit(0)
+    bp1, mp1 = m.GetOffsets()
+    np.testing.assert_array_equal(bp1, bp0)
+    np.testing.assert_array_equal(mp1, mp0)
+    for a, b in zip(m.BlockResults(), res0):
+        np.testing.assert_array_equal(a, b)
+    m.close()
