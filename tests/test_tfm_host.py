@@ -95,3 +95,58 @@ def test_horn_terms_equal_coefficient_table(tmp_path):
                            str(src), "-o", str(exe)])
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
     assert int(out.strip()) == 0
+
+
+SRC_SQRT = r'''
+#include <cstdio>
+#include <cmath>
+#include <random>
+#include <initializer_list>
+#include "tfm.cuh"
+
+// Denman-Beavers half transform: sqrt(M)^2 = M for homogeneous affine M near
+// the identity, and the affine inverse undoes M.
+int main() {
+  std::mt19937_64 g(5);
+  std::uniform_real_distribution<double> U(-1.0, 1.0);
+  double worst_sq = 0.0, worst_inv = 0.0;
+  for (int t = 0; t < 2000; ++t) {
+    double m[16] = {0};
+    for (int r = 0; r < 3; ++r) {
+      for (int c = 0; c < 3; ++c) m[4 * r + c] = (r == c ? 1.0 : 0.0) + 0.08 * U(g);
+      m[4 * r + 3] = 12.0 * U(g);
+    }
+    m[15] = 1.0;
+    double h[16], hh[16], mi[16], id[16];
+    mb2::matrix_sqrt4(m, h);
+    mb2::mn_mul<4>(h, h, hh);
+    for (int i = 0; i < 16; ++i) worst_sq = std::fmax(worst_sq, std::fabs(hh[i] - m[i]));
+    if (!mb2::affine4_inverse(m, mi)) return 2;
+    mb2::mn_mul<4>(m, mi, id);
+    for (int i = 0; i < 16; ++i)
+      worst_inv = std::fmax(worst_inv, std::fabs(id[i] - (i % 5 == 0 ? 1.0 : 0.0)));
+  }
+  std::printf("%.3e %.3e\n", worst_sq, worst_inv);
+  return 0;
+}
+'''
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_half_transform_and_affine_inverse(tmp_path):
+    """matrix_sqrt4 (Denman-Beavers, vnl_utils.h:46-95) squares back to its
+    input and affine4_inverse inverts, to FP64 rounding, on 2,000 random
+    homogeneous affine matrices near the identity (rotation/scale entries
+    within 0.08 of it, translations up to 12 mm)."""
+    src = tmp_path / "sqrt.cpp"
+    src.write_text(SRC_SQRT)
+    exe = tmp_path / "sqrt"
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-x", "c++",
+                           "-I", os.path.join(ROOT, "mirorr_b200", "csrc"),
+                           "-I", os.path.join(ROOT, "include"),
+                           "-D__host__=", "-D__device__=", "-D__forceinline__=inline",
+                           str(src), "-o", str(exe)])
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    sq, inv = (float(v) for v in r.stdout.split())
+    assert sq < 1e-12 and inv < 1e-12, (sq, inv)
